@@ -1,0 +1,334 @@
+"""Benchmark of the ADMM solve loop on the 32x32x128 twisted-and-bent bar.
+
+Workload: 786,432 tets / 140,481 vertices (configs[1] of the benchmark
+definition), E = 1e5 Pa, nu = 0.45, global L-BFGS history 5, reweighting (and
+GPU refactorization) every 10 iterations, FP64.  One step = one ADMM iteration
+(local step, global L-BFGS step with its triangular solves, reweight check).
+
+Metric: ADMM element-iterations per second (elements x iterations / seconds),
+the throughput behind the time-to-energy-gap metric; `local_elems_per_s` adds
+the local step alone.  Inputs are far larger than L2 (the element state is
+~0.7 GB), so no L2 flush is needed between steps.
+
+Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+        [--precision fp64|mixed]
+For N > 1 launch with torchrun: every rank solves its own replica of the bar
+(the path does not shard; replicas only, weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time to rel. energy gap 1e-6: learned/FP32 vs plain FP64 GPU; local elems/s"
+UNIT = "elem-iter/s"
+E_YOUNG, NU = 1e5, 0.45
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ---- clocks ----------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and
+                          s[3 + i].lower() in ("active", "1", "yes")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---- distributed plumbing ----------------------------------------------------------
+def dist_setup(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], device="cuda", dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---- bytes / flops model (algorithmic, per launch) -----------------------------------
+def local_step_bytes(ne: int, fp: int) -> int:
+    """k_local per element: reads symF, U, Z (9 each, fp bytes), w2, vol (8), slast (3 fp);
+    writes Z, U (9 each), slast (3), w2c (8)."""
+    return ne * (fp * (9 + 9 + 9 + 3) + 16 + fp * (9 + 9 + 3) + 8)
+
+
+def grad_step_bytes(ne: int, nf: int, fp: int) -> int:
+    """k_grad per element: idx (16), Di (96), x of 4 vertices (96, mostly L2 hits; counted once per
+    vertex: 24 nf), Z, U (9 fp each), w2, vol (16); writes symF (9 fp), sig (3 fp), gel (12 fp)."""
+    return ne * (16 + 96 + fp * 18 + 16 + fp * 24) + 24 * nf
+
+
+# ---- reference arm -------------------------------------------------------------------
+def run_reference(args, rank):
+    """The reference's own CPU solver (oracle/_ref/quasi_ref, compiled from its sources)."""
+    if rank != 0:
+        return
+    from oracle import pyoracle as po
+    from wrapd_b200 import bars
+    cores = os.cpu_count() or 1
+    if not os.path.exists(po.QUASI_REF):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/quasi_ref not built (no reference sources)"}))
+        return
+    bar = bars.config1()
+    K, W = args.steps, args.warmup
+    with tempfile.TemporaryDirectory() as d:
+        files = bars.write_bar(bar, d, "c1")
+        t0 = time.perf_counter()
+        r = po.run_quasi_ref(files, E_YOUNG, NU, W + K, threads=cores, extra=["-rw", "0"], outdir=d + "/out",
+                             timeout=3000)
+        wall = time.perf_counter() - t0
+    acc = r["accumulated_time_s"]
+    timed = float(acc[W + K] - acc[W])
+    value = bar.n_tets * K / timed
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": 1, "steps": K,
+        "warmup": W, "ms_per_step": 1000.0 * timed / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bar generator)",
+        "config": {"workload": "bar 32x32x128 cubes x6 tets (786,432 tets), 360 deg twist + 90 deg bend",
+                   "solver": "reference quasi (Eigen SimplicialLDLT), -rw 0, L-BFGS history 6",
+                   "timed": f"ADMM iterations {W}..{W + K - 1} from the reference's accumulated_time_s"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"config-1 bar, {W + K} ADMM iterations, last {K} timed; setup "
+                                   f"{r['runtime']['setup_ms'] / 1000:.1f} s untimed; wall {wall:.1f} s"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---- CPU baseline inside our arm -------------------------------------------------------
+def cpu_baseline():
+    """The reference on a bounded sample of the workload: a 32x32x16 slice of the bar
+    (98,304 tets, same cross-section), 6 ADMM iterations, all host threads."""
+    from oracle import pyoracle as po
+    from wrapd_b200 import bars
+    cores = os.cpu_count() or 1
+    bar = bars.make_bar(32, 32, 16, twist_deg=45.0, noise=0.01, seed=0)
+    W, K = 1, 5
+    with tempfile.TemporaryDirectory() as d:
+        files = bars.write_bar(bar, d, "s")
+        if os.path.exists(po.QUASI_REF):
+            r = po.run_quasi_ref(files, E_YOUNG, NU, W + K, threads=cores, extra=["-rw", "0"],
+                                 outdir=d + "/out", timeout=600)
+            acc = r["accumulated_time_s"]
+            v = bar.n_tets * K / float(acc[W + K] - acc[W])
+            return {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                    "sample": "32x32x16 slice of the bar (98,304 tets), iterations 1-5 of 6, -rw 0"}
+    o = po.Oracle(bar.rest, bar.init, bar.tets, bar.pins, youngs=E_YOUNG, poisson=NU, max_iters=W + K)
+    o.setup()
+    o.iterate()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        o.iterate()
+    v = bar.n_tets * K / (time.perf_counter() - t0)
+    return {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "32x32x16 slice of the bar (98,304 tets), 5 iterations of the C oracle"}
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_local_config1.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---- our arm ------------------------------------------------------------------------------
+def run_ours(args, rank, world, local, pg):
+    from wrapd_b200 import bars, capi
+    from wrapd_b200.solver import Solver
+    import torch
+
+    torch.cuda.set_device(local)
+    bar = bars.config1(seed=rank)
+    settings = dict(youngs=E_YOUNG, poisson=NU, lbfgs_m=5, rw_every=10, max_iters=100000,
+                    precision=args.precision, device=local)
+    s = Solver(**settings)
+    s.add_tetmesh(bar.rest, bar.init, bar.tets)
+    s.set_pins(bar.pins)
+    s.initialize()
+    s.begin_solve()
+    for _ in range(args.warmup):
+        s.iterate(1)
+    rt0, c0 = s.runtime(), s.counters()
+    K = args.steps
+    barrier(pg)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record()
+        done, _ = s.iterate(K)
+        torch.cuda.synchronize()
+        ev1.record()
+        ev1.synchronize()
+    barrier(pg)
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(pg, ms)
+    rt1, c1 = s.runtime(), s.counters()
+    if done != K:
+        raise RuntimeError(f"only {done} of {K} iterations ran")
+    ne, nf = bar.n_tets, bar.n_verts - len(bar.pins)
+    value = world * ne * K / (ms / 1000.0)
+    local_ms = rt1["local_ms"] - rt0["local_ms"]
+    glob_ms = rt1["global_ms"] - rt0["global_ms"]
+    ref_ms = rt1["refactor_ms"] - rt0["refactor_ms"]
+    inner = rt1["inner_iters"] - rt0["inner_iters"]
+    fp = 4 if args.precision == "mixed" else 8
+    peak, peak_kind = peaks()
+    # dominant element kernel: the local step (one launch per iteration, timed by
+    # CUDA events on the library's stream around exactly that launch)
+    lbytes = local_step_bytes(ne, fp)
+    achieved = lbytes / (local_ms / K / 1000.0) / 1e9
+    traffic = profile_traffic()
+    # e2e: a fresh solve through the C ABI from host buffers, setup included
+    e2e = None
+    if rank == 0:
+        t0 = time.perf_counter()
+        s2 = Solver(**settings)
+        s2.add_tetmesh(bar.rest, bar.init, bar.tets)
+        s2.set_pins(bar.pins)
+        s2.initialize()
+        s2.begin_solve()
+        s2.iterate(K)
+        X = s2.positions()
+        e2e_s = time.perf_counter() - t0
+        assert np.isfinite(X).all()
+        h2d = bar.rest.nbytes + bar.init.nbytes + bar.tets.nbytes + bar.pins.nbytes
+        e2e = {"value": ne * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d // K),
+               "d2h_bytes_per_step": int(X.nbytes // K), "wall_s": e2e_s,
+               "includes": "create + add_tetmesh + initialize (symbolic + factor) + begin_solve + K iterations + positions"}
+        s2.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32-local/f64-global",
+            "data": "synthetic (seeded bar generator, seed = rank)",
+            "config": {"workload": "bar 32x32x128 cubes x6 tets (786,432 tets, 140,481 verts), 360 deg twist "
+                                   "+ 90 deg bend, E=1e5 nu=0.45",
+                       "solver": f"ADMM, L-BFGS history 5, reweight+refactor every 10 iterations, {args.precision}",
+                       "parallelism": f"replicas x{world}", "l2": "inputs > L2 (element state ~0.7 GB)"},
+            "local_elems_per_s": world * ne * K / (local_ms / 1000.0),
+            "phase_ms_per_step": {"local": local_ms / K, "global": glob_ms / K, "refactor": ref_ms / K},
+            "inner_iters_per_step": inner / K,
+            "roofline": {"kernel": "k_local (fused local step)", "bound": "hbm", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind, "bytes_per_launch": lbytes},
+            "gpu_launches": int(c1["kernel_launches"] - c0["kernel_launches"]),
+            "factorizations": int(c1["factorizations"] - c0["factorizations"]),
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    s.close()
+
+
+def main():
+    args = parse()
+    rank, world, local, pg = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank)
+        else:
+            run_ours(args, rank, world, local, pg)
+    finally:
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

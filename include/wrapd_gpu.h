@@ -1,0 +1,201 @@
+/* wrapd_gpu.h -- C ABI of the B200 implementation of WRAPD's ADMM solve loop.
+ *
+ * The reference (georgbrown/wrapd) exposes the path as C++ classes, not a C
+ * ABI: wrapd::Solver (src/Solver.hpp:37-72), wrapd::System (src/System.hpp:
+ * 41-174) and wrapd::TetElements (src/TetElements.hpp:165-247), driven by the
+ * `quasi` front end (samples/tests/quasi.cpp:44-144) and
+ * binding::add_tetmesh (samples/utils/AddMeshes.hpp:61-132).  Each entry point
+ * below names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Every function returns 0 on success or a negative WRAPD_E_* code; no C++
+ *     exception crosses this boundary.  wrapd_last_error() gives the message.
+ *   - The caller owns every host buffer; the library owns device memory.
+ *   - Positions are n x 3 row-major doubles; tets are n_tets x 4 0-based ids.
+ *   - One handle per host thread.  Each handle has its own CUDA stream.
+ *   - There is no CPU fallback: without a usable CUDA device wrapd_create
+ *     fails with WRAPD_E_CUDA.
+ */
+#ifndef WRAPD_GPU_H
+#define WRAPD_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WRAPD_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define WRAPD_API __attribute__((visibility("default")))
+#else
+#define WRAPD_API
+#endif
+
+enum {
+    WRAPD_OK = 0,
+    WRAPD_E_INPUT = -1,          /* bad argument (std::runtime_error in Settings.cpp:164, MeshIO.hpp:309-311) */
+    WRAPD_E_INVERTED_REST = -2,  /* inverted rest tet (src/TetElements.cpp:99-101) */
+    WRAPD_E_NOT_SPD = -3,        /* non-positive pivot while factoring D^T W D */
+    WRAPD_E_NAN = -4,            /* NaN L-BFGS decrement (deps/mcloptlib/include/MCL/SplitLBFGS.hpp:181-184) */
+    WRAPD_E_PROX_NEG = -5,       /* negative prox stretch (src/TetElements.cpp:320-323) */
+    WRAPD_E_TIMEOUT = -6,        /* a bounded device wait gave up */
+    WRAPD_E_OOM = -7,            /* device allocation failed */
+    WRAPD_E_CUDA = -8,           /* any other CUDA error, or no device */
+    WRAPD_E_STATE = -9,          /* call out of order (e.g. solve before initialize) */
+    WRAPD_E_UNSUPPORTED = -10    /* an option this build does not implement */
+};
+
+/* Solver options.  Field meanings and defaults follow wrapd::Settings
+ * (src/Settings.hpp:103-162), ModelSettings (src/ModelSettings.hpp:33-41),
+ * Settings::GStep (src/Settings.hpp:121-149) and the flags parsed in
+ * src/Settings.cpp:31-176; the fields after `prox_iters` are extensions. */
+typedef struct wrapd_settings {
+    int max_iters;        /* -it         5000  */
+    double tol;           /* -tol        1e-11 */
+    int rot_aware;        /* -ra         1 (0 is not implemented: WRAPD_E_UNSUPPORTED) */
+    int reweighting;      /* -rw         1     */
+    int rw_delay;         /* -rw_delay   50    */
+    double gamma;         /* -gamma      1.5   */
+    int global_iters;     /* -global_it  100   */
+    int global_ls;        /* -global_ls  0 (1 is not implemented: WRAPD_E_UNSUPPORTED) */
+    double kappa;         /* -kappa      1     */
+    int model;            /* -model      0 = nh (1 = arap: WRAPD_E_UNSUPPORTED) */
+    double poisson;       /* -poisson    0.45  */
+    double beta_static;   /* -beta_static 1    */
+    double beta_min;      /* -beta_min   0.1   */
+    double beta_max;      /* -beta_max   10    */
+    int prox_iters;       /* prox L-BFGS iterations, 20 (src/ModelSettings.hpp:40) */
+    /* extensions */
+    double youngs;        /* Young's modulus, 1e7 Pa (hard-coded in src/Lame.hpp:38) */
+    int lbfgs_m;          /* global L-BFGS history, 6 (SplitLBFGS.hpp:41) */
+    int rw_every;         /* 0: gamma rule; N > 0: reweight (and refactor) every N iterations */
+    int precision;        /* 0: FP64 throughout; 1: FP32 element math, FP64 global step */
+    int prox_mode;        /* 0: L-BFGS prox as the reference (parity mode) */
+    int leaf_size;        /* nested-dissection leaf size for the factorization, 64 */
+    int verbose;          /* -p          0 here (1 prints the reference's table) */
+    int device;           /* CUDA device ordinal, 0 */
+} wrapd_settings;
+
+typedef struct wrapd_handle wrapd_handle;
+
+/* Log channels of wrapd_get_log (AlgorithmData, src/AlgorithmData.hpp:43-73). */
+enum {
+    WRAPD_LOG_OBJECTIVES = 0,       /* iters + 1 entries: potential energy per iterate */
+    WRAPD_LOG_REWEIGHTED = 1,       /* iters + 1 entries (entry 0 is 1, as the reference logs) */
+    WRAPD_LOG_FLIPS = 2,            /* iters + 1 entries: inverted elements */
+    WRAPD_LOG_INNER_ITERS = 3,      /* iters entries: global L-BFGS iterations */
+    WRAPD_LOG_LS_DELTA_AL = 4,      /* iters entries: |delta AL| of the local step */
+    WRAPD_LOG_GS_DELTA_AL = 5,      /* iters entries: |delta AL| of the global step */
+    WRAPD_LOG_ACCUMULATED_TIME_S = 6, /* iters + 1 entries: local + global + refactor seconds */
+    WRAPD_LOG_X_ERRORS = 7          /* iters + 1 entries: |x - x_soln| / |x_init - x_soln| */
+};
+
+/* Defaults of wrapd::Settings() + ModelSettings() (src/Settings.hpp:154-162,
+ * src/ModelSettings.hpp:33-41). */
+WRAPD_API int wrapd_settings_default(wrapd_settings* s);
+
+/* wrapd::Solver::Solver(const Settings&) (src/Solver.cpp:32-35). */
+WRAPD_API int wrapd_create(const wrapd_settings* s, wrapd_handle** out);
+
+/* binding::add_tetmesh + System::add_nodes + create_tets_from_mesh +
+ * Solver::set_pins (samples/utils/AddMeshes.hpp:61-132, src/System.hpp:75-92,
+ * src/TetElements.hpp:250-288, src/System.cpp:33-44).  Pins are vertex ids
+ * held in place at init_xyz.  soln_xyz may be NULL.  One mesh per handle. */
+WRAPD_API int wrapd_add_tetmesh(wrapd_handle* h, const double* rest_xyz, const double* init_xyz,
+                      const double* soln_xyz, int n_verts, const int32_t* tets, int n_tets,
+                      const int32_t* pins, int n_pins);
+
+/* wrapd::Solver::initialize (src/Solver.cpp:48-60) -> ADMM::initialize
+ * (src/ADMM.cpp:34-56): element precompute, initial weights, symbolic
+ * analysis and the first numeric factorization, all on the device. */
+WRAPD_API int wrapd_initialize(wrapd_handle* h);
+
+/* wrapd::Solver::solve (src/Solver.cpp:38-46) -> ADMM::solve
+ * (src/ADMM.cpp:59-84): iterate to convergence or max_iters and write the
+ * final positions (n_verts x 3) to x_out (may be NULL). */
+WRAPD_API int wrapd_solve(wrapd_handle* h, double* x_out);
+
+/* The two halves of ADMM::solve, for stepping: wrapd_begin_solve runs
+ * setup_solve + initialize_weights (src/ADMM.cpp:60-72, 89-107);
+ * wrapd_iterate runs up to n iterations of ADMM::iterate + converged
+ * (src/ADMM.cpp:109-169) and reports *converged; wrapd_get_positions is
+ * ADMM::finish_solve (src/ADMM.cpp:171-182). */
+WRAPD_API int wrapd_begin_solve(wrapd_handle* h);
+WRAPD_API int wrapd_iterate(wrapd_handle* h, int n, int* iters_done, int* converged);
+WRAPD_API int wrapd_get_positions(wrapd_handle* h, double* x_out);
+
+/* AlgorithmData per-iteration logs (src/AlgorithmData.hpp:43-73).  Copies up
+ * to cap entries into out; *len receives the channel's length. */
+WRAPD_API int wrapd_get_log(wrapd_handle* h, int which, double* out, int cap, int* len);
+
+/* RuntimeData (src/RuntimeData.hpp:30-44): ms[0..5] = setup, local, global,
+ * refactor, finish, inner iterations (as a double).  Device times from CUDA
+ * events on the handle's stream. */
+WRAPD_API int wrapd_get_runtime(wrapd_handle* h, double ms[6]);
+
+/* Problem sizes: out[0..7] = n_verts, n_tets, n_free, n_pins, fronts, levels,
+ * nnz(L), factorization flops. */
+WRAPD_API int wrapd_get_info(wrapd_handle* h, double out[8]);
+
+/* Work counters since wrapd_create: out[0..3] = kernel launches issued by the
+ * handle, numeric factorizations, triangular solves (3 RHS each), host
+ * synchronisations.  (No reference counterpart: instrumentation.) */
+WRAPD_API int wrapd_get_counters(wrapd_handle* h, int64_t out[4]);
+
+WRAPD_API const char* wrapd_last_error(const wrapd_handle* h);
+WRAPD_API void wrapd_destroy(wrapd_handle* h);
+
+/* ---- TetElements-level entry points (public methods of wrapd::TetElements,
+ * src/TetElements.hpp:165-207), used by the parity tests. ---------------- */
+
+/* Read or overwrite a state array by name.  Per element, in input order:
+ * "Z","U","symF" (9, the reference's column-major Mat3x3), "slast" (3),
+ * "w2","w2c","vol" (1).  Per free vertex in ascending vertex id order:
+ * "xfree","grad" (3).  Returns the element count written via *len. */
+WRAPD_API int wrapd_get_state(wrapd_handle* h, const char* name, double* out, int64_t cap, int64_t* len);
+WRAPD_API int wrapd_set_state(wrapd_handle* h, const char* name, const double* in, int64_t n);
+
+/* TetElements::update_defo_cache(x_free) (src/TetElements.cpp:564-596). */
+WRAPD_API int wrapd_update_defo_cache(wrapd_handle* h);
+
+/* TetElements::polar_update (src/TetElements.cpp:256-356): returns delta-AL. */
+WRAPD_API int wrapd_polar_update(wrapd_handle* h, int update_candidates, double* delta_al);
+
+/* TetElements::global_obj_grad(x_free, g) (src/TetElements.cpp:691-738):
+ * refreshes the cache at x_free (n_free x 3, NULL = current), writes the
+ * gradient (n_free x 3) and the AL value. */
+WRAPD_API int wrapd_global_grad(wrapd_handle* h, const double* x_free, double* grad, double* value);
+
+/* TetElements::potential_energy_x + inversion_count on the cache
+ * (src/TetElements.cpp:444-468, 598-635). */
+WRAPD_API int wrapd_potential_energy(wrapd_handle* h, double* pe, int* flips);
+
+/* LinearSolver::solve applied to the 3 columns (SplitLBFGS.hpp:165-167):
+ * x = A^-1 b for an n_free x 3 block (free vertices in ascending id order). */
+WRAPD_API int wrapd_solve_A(wrapd_handle* h, const double* b, double* x);
+
+/* ---- per-element math over a batch, on the current device (handle-free) --
+ * The same device functions the ADMM kernels inline.  fp32 = 1 runs them in
+ * single precision (the element math of mixed mode). */
+
+/* math::svd with the rotation sign fix (src/Math.hpp:140-193): F is n x 9
+ * column-major 3x3 matrices; sigma n x 3; U, V n x 9. */
+WRAPD_API int wrapd_svd3_batch(int n, int fp32, const double* F, double* sigma, double* U, double* V);
+
+/* The per-element prox of polar_update (src/TetElements.cpp:312-317): NHProx
+ * with x0 = sigma0 and w^2/vol = wov, minimised by LBFGS<3> with cubic
+ * backtracking (deps/mcloptlib/include/MCL/LBFGS.hpp:52-152) from `start`;
+ * out n x 3, iters n (LBFGS::minimize's return value). */
+WRAPD_API int wrapd_prox_batch(int n, int fp32, double mu, double lambda, int max_iters, const double* sigma0,
+                               const double* wov, const double* start, double* out, int* iters);
+
+/* Candidate stiffness before the volume factor: max eigenvalue of
+ * makePD(hessian_density(sigma)) (src/TetElements.cpp:414-416). */
+WRAPD_API int wrapd_hess_lmax_batch(int n, double mu, double lambda, const double* sigma, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WRAPD_GPU_H */

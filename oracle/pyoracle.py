@@ -72,6 +72,7 @@ def load_oracle():
     lib.orc_set.restype = ctypes.c_int
     lib.orc_set.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _dp]
     lib.orc_update_defo_cache.argtypes = [ctypes.c_void_p]
+    lib.orc_init_state.argtypes = [ctypes.c_void_p]
     lib.orc_polar_update.restype = ctypes.c_double
     lib.orc_polar_update.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.orc_global_grad_cached.restype = ctypes.c_double
@@ -161,6 +162,9 @@ class Oracle:
         if self.lib.orc_set(self.h, name.encode(), _d(a)) != 0:
             raise KeyError(name)
 
+    def init_state(self):
+        self.lib.orc_init_state(self.h)
+
     def update_defo_cache(self):
         self.lib.orc_update_defo_cache(self.h)
 
@@ -210,7 +214,8 @@ def load_ref_elem():
     lib.ref_prox_value_grad.argtypes = [ctypes.c_int, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp]
     lib.ref_hess_lmax.argtypes = [ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double, _dp]
     lib.ref_local_and_grad.argtypes = [ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _ip, ctypes.c_int, _ip,
-                                       ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _dp, _ip, _dp]
+                                       ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _dp, _ip, _dp,
+                                       _dp, _dp, _dp]
     _ref = lib
     return lib
 

@@ -6,7 +6,11 @@
 #include <memory>
 #include <vector>
 
+// Expose TetElements' protected state to this test harness only (same class
+// layout; the reference's own translation units are compiled unchanged).
+#define protected public
 #include "TetElements.hpp"
+#undef protected
 
 using wrapd::math::Mat3x3;
 using wrapd::math::Vec3;
@@ -91,7 +95,7 @@ void ref_local_and_grad(int nv, const double* rest, const double* X, const doubl
                         int ntet, const int* tets, int npins, const int* pins,
                         double youngs, double poisson,
                         double* dal, double* grad, double* value, double* pe, int* flips,
-                        double* grad2) {
+                        double* grad2, double* Zout, double* Uout, double* symFout) {
     static wrapd::Settings settings;
     const_cast<wrapd::Lame&>(settings.m_model_settings.elastic_lame()) = wrapd::Lame(youngs, poisson);
     std::vector<int> free_index(nv), fix_index(nv, -1);
@@ -119,6 +123,11 @@ void ref_local_and_grad(int nv, const double* rest, const double* X, const doubl
     te->initialize_dual_vars(Xm);
     *dal = te->polar_update(false);
     te->update_defo_cache(xfree);
+    for (int e = 0; e < ntet; ++e) {
+        if (Zout) std::memcpy(Zout + 9 * e, te->m_Zi[e].data(), 9 * sizeof(double));
+        if (Uout) std::memcpy(Uout + 9 * e, te->m_Ui[e].data(), 9 * sizeof(double));
+        if (symFout) std::memcpy(symFout + 9 * e, te->m_cached_symF[e].data(), 9 * sizeof(double));
+    }
     MatX3 g = te->global_obj_grad();
     for (int i = 0; i < nfree; ++i)
         for (int c = 0; c < 3; ++c) grad[3 * i + c] = g(i, c);

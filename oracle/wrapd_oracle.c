@@ -976,11 +976,53 @@ static int lbfgs_minimize(orc_state* s, int* err) {
 }
 
 /* ---- ADMM driver --------------------------------------------------------- */
+static void load_positions(orc_state* s) {
+    const orc_problem* p = &s->p;
+    for (int i = 0; i < s->nv; ++i) {
+        if (s->fix_of_vert[i] >= 0) for (int c = 0; c < 3; ++c) s->xfix[3 * s->fix_of_vert[i] + c] = p->init[3 * i + c];
+        else for (int c = 0; c < 3; ++c) s->xfree[3 * s->free_of_vert[i] + c] = p->init[3 * i + c];
+    }
+    update_fix_cache(s);
+}
+
+/* initialize_dual_vars, src/TetElements.cpp:145-166, then m_curr_pe =
+ * polar_potential_energy (src/TetElements.cpp:638-675). */
+static void init_dual(orc_state* s) {
+    double pe = 0.0;
+    for (int e = 0; e < s->ne; ++e) {
+        double F[9], sg[3], Uu[9], Vv[9];
+        F_from_X(s, e, s->p.init, F);
+        orc_svd3(F, sg, Uu, Vv);
+        double* Z = s->Z + 9 * e;
+        for (int r = 0; r < 3; ++r)   /* Z = S^T with S = V diag(s) V^T */
+            for (int c = 0; c < 3; ++c) {
+                double v = 0.0;
+                for (int k = 0; k < 3; ++k) v += A3(Vv, c, k) * sg[k] * A3(Vv, r, k);
+                A3(Z, r, c) = v;
+            }
+        memset(s->U + 9 * e, 0, 9 * sizeof(double));
+    }
+    for (int e = 0; e < s->ne; ++e) {
+        double Zt[9], sg[3], Uu[9], Vv[9];
+        for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c) A3(Zt, r, c) = A3(s->Z + 9 * e, c, r);
+        orc_svd3(Zt, sg, Uu, Vv);
+        pe += s->vol[e] * orc_nh_psi_plain(s->mu, s->lambda, sg);
+    }
+    s->curr_pe = pe;
+}
+
+/* The TetElements-only sequence of a fresh mesh: positions at init, fix and
+ * defo caches, dual variables (no weights update, no factorization). */
+void orc_init_state(orc_state* s) {
+    load_positions(s);
+    defo_cache_at(s, s->xfree);
+    init_dual(s);
+}
+
 int orc_setup(orc_state* s) {
     const orc_problem* p = &s->p;
     int rc;
-    for (int j = 0, i = 0; i < s->nv; ++i) if (s->fix_of_vert[i] >= 0) { j = s->fix_of_vert[i]; for (int c = 0; c < 3; ++c) s->xfix[3 * j + c] = p->init[3 * i + c]; }
-    update_fix_cache(s);
+    load_positions(s);
     /* GlobalStepBehavior ctor: midupdate_weights(X_init), src/TetElements.cpp:360-381 */
     if (p->reweighting) {
         double* sg = NEWD(3 * s->ne);
@@ -997,31 +1039,9 @@ int orc_setup(orc_state* s) {
     if ((rc = factor_A(s)) != E_OK) return rc;
     s->m_k = 0;
     /* ADMM::setup_solve, src/ADMM.cpp:89-107 */
-    for (int i = 0; i < s->nv; ++i) if (s->free_of_vert[i] >= 0) for (int c = 0; c < 3; ++c) s->xfree[3 * s->free_of_vert[i] + c] = p->init[3 * i + c];
-    update_fix_cache(s);
+    load_positions(s);
     defo_cache_at(s, s->xfree);
-    /* initialize_dual_vars, src/TetElements.cpp:145-166 */
-    double pe = 0.0;
-    for (int e = 0; e < s->ne; ++e) {
-        double F[9], sg[3], Uu[9], Vv[9];
-        F_from_X(s, e, p->init, F);
-        orc_svd3(F, sg, Uu, Vv);
-        double* Z = s->Z + 9 * e;
-        for (int r = 0; r < 3; ++r)   /* Z = S^T with S = V diag(s) V^T */
-            for (int c = 0; c < 3; ++c) {
-                double v = 0.0;
-                for (int k = 0; k < 3; ++k) v += A3(Vv, c, k) * sg[k] * A3(Vv, r, k);
-                A3(Z, r, c) = v;
-            }
-        memset(s->U + 9 * e, 0, 9 * sizeof(double));
-    }
-    for (int e = 0; e < s->ne; ++e) {  /* polar_potential_energy, src/TetElements.cpp:638-675 */
-        double Zt[9], sg[3], Uu[9], Vv[9];
-        for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c) A3(Zt, r, c) = A3(s->Z + 9 * e, c, r);
-        orc_svd3(Zt, sg, Uu, Vv);
-        pe += s->vol[e] * orc_nh_psi_plain(s->mu, s->lambda, sg);
-    }
-    s->curr_pe = pe;
+    init_dual(s);
     s->iter = 0;
     s->objectives[0] = orc_potential_energy(s);
     s->flips[0] = orc_inversion_count(s);

@@ -73,6 +73,7 @@ long orc_get(const orc_state* s, const char* name, double* buf);
 int orc_set(orc_state* s, const char* name, const double* buf);
 
 /* Components, for per-stage parity checks. */
+void orc_init_state(orc_state* s);                           /* positions, caches, dual variables */
 void orc_update_defo_cache(orc_state* s);                   /* F, SVD, symF at xfree */
 double orc_polar_update(orc_state* s, int update_candidates); /* local step, returns delta-AL */
 double orc_global_grad_cached(orc_state* s, double* grad);   /* uses the cache */

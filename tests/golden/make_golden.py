@@ -1,0 +1,146 @@
+"""Generate the golden vectors in tests/golden/ from the reference itself.
+
+Needs the reference build (``make -C oracle ref``, which compiles the
+reference sources into oracle/_ref/).  Run from the repository root:
+
+    python tests/golden/make_golden.py
+
+Outputs (all seeded, reproducible):
+  elem_cases.npz    per-element functions: math::svd, the NH prox
+                    (LBFGS<3> + cubic backtracking), the prox value/gradient and
+                    the candidate-stiffness eigenvalue, on random and edge inputs
+  tiny_step.npz     one setup + local step + gradient of TetElements on a small bar
+  solve_small.npz   full reference solves of small bars (default and rw_delay 5)
+  solve_config0.npz the reference solve of the 8x8x32 bar (E = 1e5, nu = 0.45)
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import pyoracle as po  # noqa: E402
+from wrapd_b200 import bars  # noqa: E402
+
+E_YOUNG, NU = 1e5, 0.45
+
+
+def svd_inputs(rng):
+    n = 64
+    F = [rng.normal(size=(n, 3, 3))]
+    F.append(np.eye(3)[None] + 1e-7 * rng.normal(size=(n, 3, 3)))           # near identity
+    F.append(np.tile(np.eye(3), (8, 1, 1)))                                   # exact identity
+    refl = np.diag([1.0, 1.0, -1.0])
+    F.append(rng.normal(size=(n, 3, 3)) @ refl)                               # random, often inverted
+    A = rng.normal(size=(n, 3, 3)); A[:, :, 2] = A[:, :, 1]                   # rank 2
+    F.append(A)
+    B = rng.normal(size=(n, 3, 3)); B[:, :, 1] = 2 * B[:, :, 0]; B[:, :, 2] = -B[:, :, 0]  # rank 1
+    F.append(B)
+    F.append(np.zeros((2, 3, 3)))                                             # zero matrix
+    D = np.zeros((n, 3, 3))
+    for i in range(n):
+        D[i] = np.diag(rng.choice([-2.0, -0.5, 0.0, 0.5, 1.0, 3.0], size=3))  # diagonal, signs, ties
+    F.append(D)
+    R = []
+    for i in range(n):                                                        # rotations times stretch
+        q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        R.append(q @ np.diag(rng.uniform(0.05, 3.0, size=3)) @ np.linalg.qr(rng.normal(size=(3, 3)))[0])
+    F.append(np.array(R))
+    F.append(1e-5 * rng.normal(size=(16, 3, 3)))                              # tiny scale
+    F.append(1e5 * rng.normal(size=(16, 3, 3)))                               # large scale
+    sym = rng.normal(size=(n, 3, 3)); sym = sym + np.transpose(sym, (0, 2, 1))  # symmetric, like S_in
+    F.append(sym)
+    F = np.concatenate(F)
+    return np.ascontiguousarray(np.transpose(F, (0, 2, 1)).reshape(-1, 9))    # column-major per matrix
+
+
+def elem_cases(ref, rng):
+    Fc = svd_inputs(rng)
+    n = Fc.shape[0]
+    sig, U, V = np.zeros((n, 3)), np.zeros((n, 9)), np.zeros((n, 9))
+    ref.ref_svd3(n, po._d(Fc), po._d(sig), po._d(U), po._d(V))
+    mu, lam = po.lame(E_YOUNG, NU)
+    k = 2.0066 * mu + 1.0122 * lam
+    m = 512
+    s0 = np.abs(rng.normal(1.0, 0.3, size=(m, 3)))
+    s0[:32, 2] *= -1.0                                  # inverted inputs
+    s0[32:48] = rng.uniform(0.05, 0.3, size=(16, 3))    # strongly compressed: J < J0 branch
+    s0[48:64] = 1.0                                     # rest
+    wov = rng.uniform(0.1, 10.0, size=m) * k
+    start = np.abs(rng.normal(1.0, 0.1, size=(m, 3)))
+    start[64:96] = 1.0
+    out, its = np.zeros((m, 3)), np.zeros(m, dtype=np.int32)
+    ref.ref_prox(m, po._d(s0), po._d(wov), po._d(start), mu, lam, po._d(out), its.ctypes.data_as(po._ip))
+    xv = np.abs(rng.normal(1.0, 0.4, size=(m, 3)))
+    xv[:16] = rng.uniform(0.05, 0.4, size=(16, 3))
+    val, grad = np.zeros(m), np.zeros((m, 3))
+    ref.ref_prox_value_grad(m, po._d(xv), po._d(s0), po._d(wov), mu, lam, po._d(val), po._d(grad))
+    hs = np.concatenate([out, rng.uniform(0.05, 0.5, size=(32, 3)), rng.uniform(0.5, 3.0, size=(32, 3))])
+    hl = np.zeros(hs.shape[0])
+    ref.ref_hess_lmax(hs.shape[0], po._d(np.ascontiguousarray(hs)), mu, lam, po._d(hl))
+    np.savez_compressed(os.path.join(HERE, "elem_cases.npz"), F=Fc, sigma=sig, U=U, V=V, mu=mu, lam=lam,
+                        prox_s0=s0, prox_wov=wov, prox_start=start, prox_out=out, prox_iters=its,
+                        vg_x=xv, vg_value=val, vg_grad=grad, hess_sigma=hs, hess_lmax=hl)
+
+
+def tiny_step(ref):
+    b = bars.make_bar(2, 2, 6, twist_deg=90.0, noise=0.05, seed=3)
+    rng = np.random.default_rng(11)
+    X2 = b.init + 0.01 * b.h * rng.normal(size=b.init.shape)
+    X2[b.pins] = b.init[b.pins]
+    nf = b.n_verts - len(b.pins)
+    dal, val, pe = np.zeros(1), np.zeros(1), np.zeros(1)
+    flips = np.zeros(1, dtype=np.int32)
+    g, g2 = np.zeros((nf, 3)), np.zeros((nf, 3))
+    rest, init, X2c = (np.ascontiguousarray(a) for a in (b.rest, b.init, X2))
+    tets = np.ascontiguousarray(b.tets, dtype=np.int32)
+    pins = np.ascontiguousarray(b.pins, dtype=np.int32)
+    ref.ref_local_and_grad(b.n_verts, po._d(rest), po._d(init), po._d(X2c), b.n_tets, tets.ctypes.data_as(po._ip),
+                           len(pins), pins.ctypes.data_as(po._ip), E_YOUNG, NU, po._d(dal), po._d(g), po._d(val),
+                           po._d(pe), flips.ctypes.data_as(po._ip), po._d(g2))
+    np.savez_compressed(os.path.join(HERE, "tiny_step.npz"), rest=b.rest, init=b.init, X2=X2, tets=b.tets,
+                        pins=b.pins, dal=dal[0], grad=g, value=val[0], pe=pe[0], flips=flips[0], grad2=g2)
+
+
+def ref_solve(bar, max_iters, extra=()):
+    with tempfile.TemporaryDirectory() as d:
+        files = bars.write_bar(bar, d, "m")
+        return po.run_quasi_ref(files, E_YOUNG, NU, max_iters, threads=1, extra=list(extra), outdir=d + "/out")
+
+
+def solves():
+    out = {}
+    small = bars.make_bar(3, 3, 10, twist_deg=120.0, noise=0.03, seed=5)
+    for tag, bar, extra, it in [("a", small, (), 300), ("b", small, ("-rw_delay", "5"), 300)]:
+        r = ref_solve(bar, it, extra)
+        out.update({f"{tag}_objectives": r["objectives"], f"{tag}_inner": r["inner_iters"],
+                    f"{tag}_reweighted": r["reweighted"], f"{tag}_x": r["x"],
+                    f"{tag}_ls_dal": r["ls_delta_al"], f"{tag}_gs_dal": r["gs_delta_al"]})
+    np.savez_compressed(os.path.join(HERE, "solve_small.npz"), rest=small.rest, init=small.init,
+                        tets=small.tets, pins=small.pins, **out)
+    c0 = bars.config0()
+    r = ref_solve(c0, 500)
+    np.savez_compressed(os.path.join(HERE, "solve_config0.npz"), objectives=r["objectives"],
+                        inner=r["inner_iters"], reweighted=r["reweighted"], x=r["x"],
+                        ls_dal=r["ls_delta_al"], gs_dal=r["gs_delta_al"])
+
+
+def main():
+    if not po.ref_available():
+        raise SystemExit("oracle/_ref is not built: run `make -C oracle ref` (needs the reference sources)")
+    ref = po.load_ref_elem()
+    rng = np.random.default_rng(20240611)
+    elem_cases(ref, rng)
+    tiny_step(ref)
+    solves()
+    print("golden vectors written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

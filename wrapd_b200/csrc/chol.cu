@@ -1,0 +1,606 @@
+// GPU multifrontal Cholesky and 3-RHS solve; see chol.cuh.
+//
+// Factorization, per level of the assembly tree (leaves first):
+//   extend-add   children's update matrices into the fronts (one launch per
+//                child slot, so two children never write one entry at once);
+//   then per panel of NB = 32 columns (right-looking partial Cholesky):
+//   diag         one CTA per front: Cholesky of the NB x NB diagonal block,
+//                its inverse Li (stored as a diagonal block of Y), and
+//                Y[p, 0:p0] <- Li * Y[p, 0:p0];
+//   trsm         the panel rows below the block: P <- P * Li^T (FP64 DMMA);
+//   update       trailing lower triangle  F -= P P^T  and the inverse rows
+//                Y[p+1:, 0:p0+nb] -= P_k Y[p, 0:p0+nb]  (FP64 DMMA tiles).
+// A is assembled once per factorization straight into the zeroed F pool.
+//
+// Every tile product is mma.sync.m8n8k4 f64 (the FP64 tensor-core path of
+// sm_100a; tcgen05 has no f64 kind).
+#include "chol.cuh"
+
+#include <algorithm>
+#include <numeric>
+
+namespace wrapd {
+
+namespace {
+
+constexpr int NB = 32;        // panel width
+constexpr int TL = 64;        // output tile of the DMMA kernels
+constexpr int SLD = NB + 4;   // smem row pitch (doubles) for [row][k] operand tiles
+constexpr int GEMM_THREADS = 128;
+constexpr int ROWS_PER_CTA = 128;  // solve row tiles
+constexpr int COLS_PER_CTA = 8;    // solve / extend-add column groups (one warp each)
+
+__device__ __forceinline__ int find_item(const int* prefix, int n, int b) {
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (prefix[mid] <= b) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// S[i][t] = base[i*rs + t*cs] for i < rows, t < K; zero elsewhere (TL x K4).
+__device__ __forceinline__ void load_tile(double* S, const double* __restrict__ base, int64_t rs, int64_t cs,
+                                          int rows, int K, int K4) {
+    const int total = TL * K4;
+    if (rs == 1) {
+        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+            const int i = idx % TL, t = idx / TL;
+            S[i * SLD + t] = (i < rows && t < K) ? base[i + t * cs] : 0.0;
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+            const int t = idx % K4, i = idx / K4;
+            S[i * SLD + t] = (i < rows && t < K) ? base[i * rs + t * cs] : 0.0;
+        }
+    }
+}
+
+// acc += As * Bs^T over K4 (multiple of 4); 4 warps in a 2x2 grid of 32x32.
+__device__ __forceinline__ void tile_mma(const double* As, const double* Bs, int K4, double (&acc)[4][4][2]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int r = lane >> 2, c = lane & 3;
+    for (int kk = 0; kk < K4; kk += 4) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[(wm * 32 + i * 8 + r) * SLD + kk + c];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Bs[(wn * 32 + j * 8 + r) * SLD + kk + c];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+}
+
+enum { EPI_SUB = 0, EPI_SUB_LOWER = 1, EPI_SET = 2 };
+
+// C[row*crs + col*ccs] (op)= acc for row < M, col < N.
+__device__ __forceinline__ void tile_store(double* C, int64_t crs, int64_t ccs, int M, int N, int mode,
+                                           const double (&acc)[4][4][2]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wm = warp & 1, wn = warp >> 1;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int row = wm * 32 + i * 8 + (lane >> 2);
+                const int col = wn * 32 + j * 8 + 2 * (lane & 3) + h;
+                if (row >= M || col >= N) continue;
+                if (mode == EPI_SUB_LOWER && row < col) continue;
+                double* p = C + row * crs + col * ccs;
+                if (mode == EPI_SET) *p = acc[i][j][h];
+                else *p -= acc[i][j][h];
+            }
+}
+
+// ---- assembly ----------------------------------------------------------------
+__global__ void k_assemble_A(double* __restrict__ F, const int64_t* __restrict__ pos, const int* __restrict__ ptr,
+                             const int* __restrict__ con, int nA, const double* __restrict__ w2,
+                             const double* __restrict__ Di, int ne) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nA) return;
+    double v = 0.0;
+    for (int q = ptr[t]; q < ptr[t + 1]; ++q) {
+        const int c = con[q];
+        const int e = c >> 4, a = (c >> 2) & 3, b = c & 3;
+        double d = 0.0;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) d += Di[(int64_t)(r + 3 * a) * ne + e] * Di[(int64_t)(r + 3 * b) * ne + e];
+        v += w2[e] * d;
+    }
+    F[pos[t]] = v;
+}
+
+__global__ void k_y_identity(double* __restrict__ Y, const FrontDesc* __restrict__ desc, int nfronts) {
+    const int f = blockIdx.x;
+    if (f >= nfronts) return;
+    const FrontDesc d = desc[f];
+    for (int i = threadIdx.x; i < d.k; i += blockDim.x) Y[d.y_off + i + (int64_t)i * d.k] = 1.0;
+}
+
+// children slot `slot` of each front in the list: F_s[rel[i], rel[j]] += U_c[i, j], i >= j
+__global__ void k_extend_add(double* __restrict__ F, const FrontDesc* __restrict__ desc, const int* __restrict__ rel,
+                             WorkList wl, int slot) {
+    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
+    const int s = wl.d_fronts[item];
+    const FrontDesc ds = desc[s];
+    const int c = slot == 0 ? ds.child0 : ds.child1;
+    const FrontDesc dc = desc[c];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int j = (blockIdx.x - wl.d_prefix[item]) * COLS_PER_CTA + warp;
+    if (j >= dc.r) return;
+    const int* rc = rel + dc.rel_off;
+    const double* Uc = F + dc.f_off + dc.k + (int64_t)(dc.k + j) * dc.ld;
+    double* Fs = F + ds.f_off + (int64_t)rc[j] * ds.ld;
+    for (int i = j + lane; i < dc.r; i += 32) Fs[rc[i]] += Uc[i];
+}
+
+// ---- panel factorization -------------------------------------------------------
+__global__ void __launch_bounds__(256) k_diag(double* __restrict__ F, double* __restrict__ Y,
+                                              const FrontDesc* __restrict__ desc, WorkList wl, int p,
+                                              int* __restrict__ status) {
+    __shared__ double L[NB][NB + 1];
+    __shared__ double Li[NB][NB + 1];
+    __shared__ double C[NB][NB + 1];
+    const FrontDesc d = desc[wl.d_fronts[blockIdx.x]];
+    const int p0 = p * NB;
+    const int nb = min(NB, d.k - p0);
+    if (nb <= 0) return;
+    const int tid = threadIdx.x;
+    double* Fd = F + d.f_off + p0 + (int64_t)p0 * d.ld;
+    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+        const int i = idx % NB, j = idx / NB;
+        L[i][j] = (i < nb && j < nb && i >= j) ? Fd[i + (int64_t)j * d.ld] : 0.0;
+        Li[i][j] = 0.0;
+    }
+    __syncthreads();
+    for (int j = 0; j < nb; ++j) {
+        if (tid == 0) {
+            double v = L[j][j];
+            if (!(v > 0.0)) {   // non-SPD or NaN pivot: flag it and continue with a unit pivot
+                atomicExch(status, WRAPD_E_NOT_SPD);
+                v = 1.0;
+            }
+            L[j][j] = sqrt(v);
+        }
+        __syncthreads();
+        for (int i = j + 1 + tid; i < nb; i += blockDim.x) L[i][j] /= L[j][j];
+        __syncthreads();
+        const int m = nb - j - 1;
+        for (int idx = tid; idx < m * m; idx += blockDim.x) {
+            const int i = j + 1 + idx % m, c = j + 1 + idx / m;
+            if (c <= i) L[i][c] -= L[i][j] * L[c][j];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        const int i = idx % nb, j = idx / nb;
+        if (i >= j) Fd[i + (int64_t)j * d.ld] = L[i][j];
+    }
+    if (tid < nb) {   // column tid of inv(L) by forward substitution
+        const int c = tid;
+        for (int i = c; i < nb; ++i) {
+            double v = (i == c) ? 1.0 : 0.0;
+            for (int t = c; t < i; ++t) v -= L[i][t] * Li[t][c];
+            Li[i][c] = v / L[i][i];
+        }
+    }
+    __syncthreads();
+    double* Yp = Y + d.y_off + p0;   // row block p of Y (column-major, ld = k)
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        const int i = idx % nb, j = idx / nb;
+        Yp[i + (int64_t)(p0 + j) * d.k] = Li[i][j];
+    }
+    // Y[p, 0:p0] <- Li * Y[p, 0:p0], 32 columns at a time
+    for (int c0 = 0; c0 < p0; c0 += NB) {
+        for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+            const int t = idx % NB, jj = idx / NB;
+            C[t][jj] = (t < nb) ? Yp[t + (int64_t)(c0 + jj) * d.k] : 0.0;
+        }
+        __syncthreads();
+        for (int idx = tid; idx < nb * NB; idx += blockDim.x) {
+            const int i = idx % nb, jj = idx / nb;
+            double v = 0.0;
+            for (int t = 0; t <= i; ++t) v += Li[i][t] * C[t][jj];
+            Yp[i + (int64_t)(c0 + jj) * d.k] = v;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(GEMM_THREADS) k_trsm(double* __restrict__ F, const double* __restrict__ Y,
+                                                       const FrontDesc* __restrict__ desc, WorkList wl, int p) {
+    __shared__ double As[TL * SLD];
+    __shared__ double Bs[TL * SLD];
+    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
+    const FrontDesc d = desc[wl.d_fronts[item]];
+    const int tile = blockIdx.x - wl.d_prefix[item];
+    const int p0 = p * NB, nb = min(NB, d.k - p0), j0 = p0 + nb;
+    const int m = d.ld - j0 - tile * TL;
+    if (nb <= 0 || m <= 0) return;
+    const int K4 = (nb + 3) & ~3;
+    double* A = F + d.f_off + j0 + tile * TL + (int64_t)p0 * d.ld;
+    load_tile(As, A, 1, d.ld, min(m, TL), nb, K4);
+    load_tile(Bs, Y + d.y_off + p0 + (int64_t)p0 * d.k, 1, d.k, nb, nb, K4);
+    __syncthreads();
+    double acc[4][4][2] = {};
+    tile_mma(As, Bs, K4, acc);
+    tile_store(A, 1, d.ld, min(m, TL), nb, EPI_SET, acc);
+}
+
+// Items: for each front, nF trailing tiles (lower triangle) then nY inverse tiles.
+__global__ void __launch_bounds__(GEMM_THREADS) k_update(double* __restrict__ F, double* __restrict__ Y,
+                                                         const FrontDesc* __restrict__ desc, WorkList wl,
+                                                         const int* __restrict__ nF_of_item, int p) {
+    __shared__ double As[TL * SLD];
+    __shared__ double Bs[TL * SLD];
+    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
+    const FrontDesc d = desc[wl.d_fronts[item]];
+    int t = blockIdx.x - wl.d_prefix[item];
+    const int nF = nF_of_item[item];
+    const int p0 = p * NB, nb = min(NB, d.k - p0), j0 = p0 + nb;
+    if (nb <= 0) return;
+    const int K4 = (nb + 3) & ~3;
+    const double* P = F + d.f_off + j0 + (int64_t)p0 * d.ld;   // panel rows j0.. (column-major)
+    double acc[4][4][2] = {};
+    if (t < nF) {
+        // lower-triangular tile index -> (ti, tj), ti >= tj
+        int ti = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+        while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+        while (ti * (ti + 1) / 2 > t) --ti;
+        const int tj = t - ti * (ti + 1) / 2;
+        const int m = d.ld - j0;
+        const int r0 = ti * TL, c0 = tj * TL;
+        load_tile(As, P + r0, 1, d.ld, min(m - r0, TL), nb, K4);
+        load_tile(Bs, P + c0, 1, d.ld, min(m - c0, TL), nb, K4);
+        __syncthreads();
+        tile_mma(As, Bs, K4, acc);
+        double* C = F + d.f_off + (j0 + r0) + (int64_t)(j0 + c0) * d.ld;
+        tile_store(C, 1, d.ld, min(m - r0, TL), min(m - c0, TL), ti == tj ? EPI_SUB_LOWER : EPI_SUB, acc);
+    } else {
+        t -= nF;
+        const int mY = d.k - j0, nY = j0;
+        const int tc = (nY + TL - 1) / TL;
+        const int ti = t / tc, tj = t % tc;
+        const int r0 = ti * TL, c0 = tj * TL;
+        load_tile(As, P + r0, 1, d.ld, min(mY - r0, TL), nb, K4);
+        load_tile(Bs, Y + d.y_off + p0 + (int64_t)c0 * d.k, d.k, 1, min(nY - c0, TL), nb, K4);
+        __syncthreads();
+        tile_mma(As, Bs, K4, acc);
+        double* C = Y + d.y_off + (j0 + r0) + (int64_t)c0 * d.k;
+        tile_store(C, 1, d.k, min(mY - r0, TL), min(nY - c0, TL), EPI_SUB, acc);
+    }
+}
+
+// ---- solve -----------------------------------------------------------------------
+__global__ void k_fwd_gather(const double* __restrict__ x, double* __restrict__ T, double* __restrict__ U,
+                             const FrontDesc* __restrict__ desc, const int* __restrict__ rel, WorkList wl) {
+    const FrontDesc d = desc[wl.d_fronts[blockIdx.x]];
+    for (int i = threadIdx.x; i < 3 * d.k; i += blockDim.x) T[3 * (int64_t)d.first + i] = x[3 * (int64_t)d.first + i];
+    for (int i = threadIdx.x; i < 3 * d.r; i += blockDim.x) U[d.u_off + i] = 0.0;
+    __syncthreads();
+    for (int s = 0; s < d.nchild; ++s) {
+        const FrontDesc dc = desc[s == 0 ? d.child0 : d.child1];
+        const int* rc = rel + dc.rel_off;
+        for (int i = threadIdx.x; i < dc.r; i += blockDim.x) {
+            const int pos = rc[i];
+            double* dst = pos < d.k ? T + 3 * ((int64_t)d.first + pos) : U + d.u_off + 3 * (int64_t)(pos - d.k);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) dst[c] += U[dc.u_off + 3 * (int64_t)i + c];
+        }
+        __syncthreads();
+    }
+}
+
+// x_s = Y_s t_s (row tiles)
+__global__ void __launch_bounds__(ROWS_PER_CTA) k_fwd_diag(double* __restrict__ x, const double* __restrict__ T,
+                                                           const double* __restrict__ Y,
+                                                           const FrontDesc* __restrict__ desc, WorkList wl) {
+    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
+    const FrontDesc d = desc[wl.d_fronts[item]];
+    const int r0 = (blockIdx.x - wl.d_prefix[item]) * ROWS_PER_CTA;
+    const int i = r0 + threadIdx.x;
+    const int jmax = min(d.k, r0 + ROWS_PER_CTA);
+    const double* t = T + 3 * (int64_t)d.first;
+    const double* Yc = Y + d.y_off + (i < d.k ? i : 0);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int j = 0; j < jmax; ++j) {
+        const double y = Yc[(int64_t)j * d.k];
+        a0 += y * t[3 * j]; a1 += y * t[3 * j + 1]; a2 += y * t[3 * j + 2];
+    }
+    if (i < d.k) {
+        double* o = x + 3 * ((int64_t)d.first + i);
+        o[0] = a0; o[1] = a1; o[2] = a2;
+    }
+}
+
+// u_s = v_s - L_rs x_s (row tiles of r)
+__global__ void __launch_bounds__(ROWS_PER_CTA) k_fwd_off(const double* __restrict__ x, double* __restrict__ U,
+                                                          const double* __restrict__ F,
+                                                          const FrontDesc* __restrict__ desc, WorkList wl) {
+    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
+    const FrontDesc d = desc[wl.d_fronts[item]];
+    const int i = (blockIdx.x - wl.d_prefix[item]) * ROWS_PER_CTA + threadIdx.x;
+    if (i >= d.r) return;
+    const double* xs = x + 3 * (int64_t)d.first;
+    const double* Lr = F + d.f_off + d.k + i;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int j = 0; j < d.k; ++j) {
+        const double l = Lr[(int64_t)j * d.ld];
+        a0 += l * xs[3 * j]; a1 += l * xs[3 * j + 1]; a2 += l * xs[3 * j + 2];
+    }
+    double* u = U + d.u_off + 3 * (int64_t)i;
+    u[0] -= a0; u[1] -= a1; u[2] -= a2;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// h_s = z_s - L_rs^T y_rows (column groups)
+__global__ void __launch_bounds__(32 * COLS_PER_CTA) k_bwd_off(const double* __restrict__ x, double* __restrict__ T,
+                                                               const double* __restrict__ F,
+                                                               const int* __restrict__ rows,
+                                                               const FrontDesc* __restrict__ desc, WorkList wl) {
+    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
+    const FrontDesc d = desc[wl.d_fronts[item]];
+    const int j = (blockIdx.x - wl.d_prefix[item]) * COLS_PER_CTA + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (j >= d.k) return;
+    const double* Lc = F + d.f_off + d.k + (int64_t)j * d.ld;
+    const int* rw = rows + d.rows_off;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int i = lane; i < d.r; i += 32) {
+        const double l = Lc[i];
+        const double* y = x + 3 * (int64_t)rw[i];
+        a0 += l * y[0]; a1 += l * y[1]; a2 += l * y[2];
+    }
+    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
+    if (lane == 0) {
+        const double* z = x + 3 * ((int64_t)d.first + j);
+        double* h = T + 3 * ((int64_t)d.first + j);
+        h[0] = z[0] - a0; h[1] = z[1] - a1; h[2] = z[2] - a2;
+    }
+}
+
+// y_s = Y_s^T h_s (column groups)
+__global__ void __launch_bounds__(32 * COLS_PER_CTA) k_bwd_diag(double* __restrict__ x, const double* __restrict__ T,
+                                                                const double* __restrict__ Y,
+                                                                const FrontDesc* __restrict__ desc, WorkList wl) {
+    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
+    const FrontDesc d = desc[wl.d_fronts[item]];
+    const int j = (blockIdx.x - wl.d_prefix[item]) * COLS_PER_CTA + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (j >= d.k) return;
+    const double* Yc = Y + d.y_off + (int64_t)j * d.k;
+    const double* h = T + 3 * (int64_t)d.first;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int i = j + lane; i < d.k; i += 32) {
+        const double y = Yc[i];
+        a0 += y * h[3 * i]; a1 += y * h[3 * i + 1]; a2 += y * h[3 * i + 2];
+    }
+    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
+    if (lane == 0) {
+        double* o = x + 3 * ((int64_t)d.first + j);
+        o[0] = a0; o[1] = a1; o[2] = a2;
+    }
+}
+
+}  // namespace
+
+CholGPU::~CholGPU() {
+    for (void* p : allocs_) cudaFree(p);
+}
+
+template <typename X>
+X* CholGPU::upload(const std::vector<X>& v, cudaStream_t st) {
+    X* p = nullptr;
+    const size_t bytes = std::max<size_t>(1, v.size()) * sizeof(X);
+    if (cudaMalloc(&p, bytes) != cudaSuccess) throw CudaError(WRAPD_E_OOM, "cudaMalloc failed (factor structures)");
+    allocs_.push_back(p);
+    device_bytes += bytes;
+    if (!v.empty()) WRAPD_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice, st));
+    return p;
+}
+
+WorkList CholGPU::make_list(const std::vector<int>& fronts, const std::vector<int>& ctas, cudaStream_t st) {
+    WorkList w;
+    std::vector<int> f, pre(1, 0);
+    for (size_t i = 0; i < fronts.size(); ++i)
+        if (ctas[i] > 0) { f.push_back(fronts[i]); pre.push_back(pre.back() + ctas[i]); }
+    w.n = static_cast<int>(f.size());
+    w.total = pre.back();
+    if (w.n == 0) return w;
+    w.d_fronts = upload(f, st);
+    w.d_prefix = upload(pre, st);
+    return w;
+}
+
+void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const std::vector<int>& A_ptr,
+                    const std::vector<int>& A_contrib, cudaStream_t st) {
+    n = S.n;
+    nfronts = static_cast<int>(S.fronts.size());
+    nlevels = static_cast<int>(S.levels.size());
+    nnz_L = S.nnz_L;
+    flops = S.flops;
+    if (S.max_children > 2) throw CudaError(WRAPD_E_INPUT, "assembly tree with more than 2 children");
+    h_desc_.resize(nfronts);
+    std::vector<int> rows;
+    int64_t roff = 0;
+    for (int f = 0; f < nfronts; ++f) {
+        const Front& F = S.fronts[f];
+        FrontDesc& d = h_desc_[f];
+        d.first = F.first; d.k = F.ncols; d.r = F.nrows(); d.ld = F.ld();
+        d.f_off = F.f_off; d.y_off = F.y_off; d.u_off = F.u_off; d.rel_off = F.rel_off;
+        d.rows_off = roff;
+        rows.insert(rows.end(), F.rows.begin(), F.rows.end());
+        roff += F.nrows();
+        d.nchild = static_cast<int>(F.children.size());
+        d.child0 = d.nchild > 0 ? F.children[0] : -1;
+        d.child1 = d.nchild > 1 ? F.children[1] : -1;
+        d.pad = 0;
+    }
+    d_desc_ = upload(h_desc_, st);
+    d_rows_ = upload(rows, st);
+    d_rel_ = upload(S.relmap, st);
+    nA_ = static_cast<int>(A_pos.size());
+    d_Apos_ = upload(A_pos, st);
+    d_Aptr_ = upload(A_ptr, st);
+    d_Acon_ = upload(A_contrib, st);
+    f_pool_ = S.f_pool; y_pool_ = S.y_pool; u_pool_ = S.u_pool;
+    auto dalloc = [&](size_t count) {
+        double* p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(double)) != cudaSuccess)
+            throw CudaError(WRAPD_E_OOM, "cudaMalloc failed (factor pools)");
+        allocs_.push_back(p);
+        device_bytes += std::max<size_t>(1, count) * sizeof(double);
+        return p;
+    };
+    d_F_ = dalloc(f_pool_);
+    d_Y_ = dalloc(y_pool_);
+    d_U_ = dalloc(u_pool_);
+    d_T_ = dalloc(3 * (size_t)n);
+    int* st_ptr = nullptr;
+    WRAPD_CUDA(cudaMalloc(&st_ptr, sizeof(int)));
+    allocs_.push_back(st_ptr);
+    d_status = st_ptr;
+    WRAPD_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+
+    levels_.assign(nlevels, Level());
+    launches_factor = 3;  // memsets + assembly + identity
+    launches_solve = 0;
+    for (int l = 0; l < nlevels; ++l) {
+        Level& L = levels_[l];
+        L.fronts_sorted = S.levels[l];
+        std::stable_sort(L.fronts_sorted.begin(), L.fronts_sorted.end(),
+                         [&](int a, int b) { return h_desc_[a].k > h_desc_[b].k; });
+        const auto& fs = L.fronts_sorted;
+        L.kmax = fs.empty() ? 0 : h_desc_[fs[0]].k;
+        std::vector<int> one(fs.size(), 1), cnt(fs.size());
+        L.all = make_list(fs, one, st);
+        for (int slot = 0; slot < 2; ++slot) {
+            for (size_t i = 0; i < fs.size(); ++i) {
+                const FrontDesc& d = h_desc_[fs[i]];
+                const int c = slot == 0 ? d.child0 : d.child1;
+                cnt[i] = c < 0 ? 0 : ceil_div(h_desc_[c].r, COLS_PER_CTA);
+            }
+            L.extend.push_back(make_list(fs, cnt, st));
+            if (L.extend.back().total) launches_factor++;
+        }
+        const int steps = ceil_div(L.kmax, NB);
+        for (int p = 0; p < steps; ++p) {
+            std::vector<int> act, cd, ct, cu, nF;
+            for (int f : fs) {
+                const FrontDesc& d = h_desc_[f];
+                const int p0 = p * NB;
+                if (d.k <= p0) continue;
+                const int nb = std::min(NB, d.k - p0), j0 = p0 + nb;
+                const int m = d.ld - j0;
+                const int T = ceil_div(m, TL);
+                const int mY = d.k - j0, nY = j0;
+                const int tY = (mY > 0) ? ceil_div(mY, TL) * ceil_div(nY, TL) : 0;
+                act.push_back(f);
+                cd.push_back(1);
+                ct.push_back(ceil_div(m, TL));
+                cu.push_back(T * (T + 1) / 2 + tY);
+                nF.push_back(T * (T + 1) / 2);
+            }
+            L.diag.push_back(make_list(act, cd, st));
+            L.trsm.push_back(make_list(act, ct, st));
+            // keep only fronts with update work, with nF aligned to the compacted list
+            std::vector<int> act2, cu2, nF2;
+            for (size_t i = 0; i < act.size(); ++i)
+                if (cu[i] > 0) { act2.push_back(act[i]); cu2.push_back(cu[i]); nF2.push_back(nF[i]); }
+            L.update.push_back(make_list(act2, cu2, st));
+            L.update_split.push_back(nF2);
+            launches_factor += 1 + (L.trsm.back().total ? 1 : 0) + (L.update.back().total ? 1 : 0);
+        }
+        std::vector<int> fr(fs.size()), ur(fs.size()), bc(fs.size());
+        for (size_t i = 0; i < fs.size(); ++i) {
+            const FrontDesc& d = h_desc_[fs[i]];
+            fr[i] = ceil_div(d.k, ROWS_PER_CTA);
+            ur[i] = ceil_div(d.r, ROWS_PER_CTA);
+            bc[i] = ceil_div(d.k, COLS_PER_CTA);
+        }
+        L.fwd_rows = make_list(fs, fr, st);
+        L.fwd_urows = make_list(fs, ur, st);
+        L.bwd_cols = make_list(fs, bc, st);
+        launches_solve += 2 + (L.fwd_urows.total ? 1 : 0) + 2;
+    }
+    // per-step nF arrays on the device (aligned with the update lists)
+    upd_nF_.clear();
+    for (auto& L : levels_) {
+        std::vector<int*> v;
+        for (auto& nF : L.update_split) v.push_back(nF.empty() ? nullptr : upload(nF, st));
+        upd_nF_.push_back(v);
+    }
+    WRAPD_CUDA(cudaStreamSynchronize(st));
+}
+
+void CholGPU::factor(const double* d_w2, const double* d_Di, int ne, cudaStream_t st) {
+    WRAPD_CUDA(cudaMemsetAsync(d_F_, 0, f_pool_ * sizeof(double), st));
+    WRAPD_CUDA(cudaMemsetAsync(d_Y_, 0, y_pool_ * sizeof(double), st));
+    if (nA_ > 0) {
+        k_assemble_A<<<ceil_div(nA_, 256), 256, 0, st>>>(d_F_, d_Apos_, d_Aptr_, d_Acon_, nA_, d_w2, d_Di, ne);
+        WRAPD_LAUNCH_CHECK();
+    }
+    k_y_identity<<<nfronts, 128, 0, st>>>(d_Y_, d_desc_, nfronts);
+    WRAPD_LAUNCH_CHECK();
+    for (int l = 0; l < nlevels; ++l) {
+        Level& L = levels_[l];
+        for (int slot = 0; slot < 2; ++slot)
+            if (L.extend[slot].total) {
+                k_extend_add<<<L.extend[slot].total, 32 * COLS_PER_CTA, 0, st>>>(d_F_, d_desc_, d_rel_, L.extend[slot], slot);
+                WRAPD_LAUNCH_CHECK();
+            }
+        for (size_t p = 0; p < L.diag.size(); ++p) {
+            if (L.diag[p].total) {
+                k_diag<<<L.diag[p].total, 256, 0, st>>>(d_F_, d_Y_, d_desc_, L.diag[p], (int)p, d_status);
+                WRAPD_LAUNCH_CHECK();
+            }
+            if (L.trsm[p].total) {
+                k_trsm<<<L.trsm[p].total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_desc_, L.trsm[p], (int)p);
+                WRAPD_LAUNCH_CHECK();
+            }
+            if (L.update[p].total) {
+                k_update<<<L.update[p].total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_desc_, L.update[p],
+                                                                     upd_nF_[l][p], (int)p);
+                WRAPD_LAUNCH_CHECK();
+            }
+        }
+    }
+}
+
+void CholGPU::solve(double* d_x, cudaStream_t st) {
+    for (int l = 0; l < nlevels; ++l) {
+        Level& L = levels_[l];
+        k_fwd_gather<<<L.all.total, 256, 0, st>>>(d_x, d_T_, d_U_, d_desc_, d_rel_, L.all);
+        WRAPD_LAUNCH_CHECK();
+        k_fwd_diag<<<L.fwd_rows.total, ROWS_PER_CTA, 0, st>>>(d_x, d_T_, d_Y_, d_desc_, L.fwd_rows);
+        WRAPD_LAUNCH_CHECK();
+        if (L.fwd_urows.total) {
+            k_fwd_off<<<L.fwd_urows.total, ROWS_PER_CTA, 0, st>>>(d_x, d_U_, d_F_, d_desc_, L.fwd_urows);
+            WRAPD_LAUNCH_CHECK();
+        }
+    }
+    for (int l = nlevels - 1; l >= 0; --l) {
+        Level& L = levels_[l];
+        k_bwd_off<<<L.bwd_cols.total, 32 * COLS_PER_CTA, 0, st>>>(d_x, d_T_, d_F_, d_rows_, d_desc_, L.bwd_cols);
+        WRAPD_LAUNCH_CHECK();
+        k_bwd_diag<<<L.bwd_cols.total, 32 * COLS_PER_CTA, 0, st>>>(d_x, d_T_, d_Y_, d_desc_, L.bwd_cols);
+        WRAPD_LAUNCH_CHECK();
+    }
+}
+
+}  // namespace wrapd

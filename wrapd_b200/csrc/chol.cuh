@@ -1,0 +1,100 @@
+// GPU multifrontal Cholesky of the free-vertex weighted Laplacian
+// A = sum_e w_e^2 D_e^T D_e and its 3-right-hand-side solve.  Replaces the
+// reference's Eigen SimplicialLDLT (deps/mcloptlib/include/MCL/
+// LinearSolver.hpp:279-298): `factor` is LinearSolver::factorize,
+// `solve` is the three LinearSolver::solve calls of SplitLBFGS.hpp:165-167.
+//
+// Storage (all device, FP64):
+//   F pool  one (k+r) x (k+r) column-major frontal matrix per front.  After
+//           factoring, columns 0..k-1 hold the front's panel of L
+//           (L_ss on top, L_rs below) and the trailing r x r block holds the
+//           update matrix that the parent assembles.
+//   Y pool  one k x k lower-triangular block per front: inv(L_ss), built
+//           during the factorization so the solve is a sequence of
+//           bandwidth-bound matrix-vector products with no serial substitution.
+//   vectors n x 3 row-major in the nested-dissection order (3 RHS at once).
+#pragma once
+#include <vector>
+
+#include "common.cuh"
+#include "symbolic.hpp"
+
+namespace wrapd {
+
+struct FrontDesc {
+    int first, k, r, ld;
+    int64_t f_off, y_off, u_off, rows_off, rel_off;
+    int nchild, child0, child1, pad;
+};
+
+// One launch's work: `n` fronts (ids), each owning prefix[i+1]-prefix[i] CTAs.
+struct WorkList {
+    int n = 0;
+    int total = 0;       // total CTAs
+    int* d_fronts = nullptr;
+    int* d_prefix = nullptr;
+};
+
+class CholGPU {
+public:
+    CholGPU() = default;
+    ~CholGPU();
+    CholGPU(const CholGPU&) = delete;
+    CholGPU& operator=(const CholGPU&) = delete;
+
+    // Upload the symbolic structures.  A_pos/A_ptr/A_contrib describe the
+    // lower-triangle entries of A: entry t goes to F-pool offset A_pos[t] and
+    // sums w2[e] * (D_e^T D_e)(a, b) over contributions c = e*16 + a*4 + b in
+    // A_contrib[A_ptr[t] .. A_ptr[t+1]).
+    void build(const Symbolic& S, const std::vector<int64_t>& A_pos, const std::vector<int>& A_ptr,
+               const std::vector<int>& A_contrib, cudaStream_t st);
+    // Numeric factorization from the element weights w2 (ne) and the element
+    // matrices Di (12 x ne, SoA, Di[(r + 3a) * ne + e]).  Sets *d_status to
+    // WRAPD_E_NOT_SPD on a non-positive pivot (checked by the caller later).
+    void factor(const double* d_w2, const double* d_Di, int ne, cudaStream_t st);
+    // In place: x <- A^-1 x for an n x 3 block in the dissection order.
+    void solve(double* d_x, cudaStream_t st);
+
+    int n = 0;
+    int* d_status = nullptr;
+    int64_t nnz_L = 0;
+    double flops = 0.0;
+    int nfronts = 0, nlevels = 0;
+    size_t device_bytes = 0;
+    int launches_factor = 0, launches_solve = 0;
+
+private:
+    struct Level {
+        std::vector<int> fronts_sorted;   // by k descending
+        int kmax = 0;
+        WorkList all;                    // one CTA per front (gather, diag...)
+        std::vector<WorkList> extend;    // per child slot: CTAs over child columns
+        std::vector<WorkList> diag;      // per panel step
+        std::vector<WorkList> trsm;      // per panel step
+        std::vector<WorkList> update;    // per panel step (F trailing tiles + Y tiles)
+        std::vector<std::vector<int>> update_split;  // per step: per front number of F tiles
+        WorkList fwd_rows, fwd_urows;    // solve forward: row tiles of Y and of L_rs
+        WorkList bwd_cols;               // solve backward: column groups
+    };
+    std::vector<Level> levels_;
+    FrontDesc* d_desc_ = nullptr;
+    int* d_rows_ = nullptr;
+    int* d_rel_ = nullptr;
+    int64_t* d_Apos_ = nullptr;
+    int* d_Aptr_ = nullptr;
+    int* d_Acon_ = nullptr;
+    int nA_ = 0;
+    double* d_F_ = nullptr;
+    double* d_Y_ = nullptr;
+    double* d_U_ = nullptr;      // solve update vectors
+    double* d_T_ = nullptr;      // solve temporaries (n x 3)
+    int64_t f_pool_ = 0, y_pool_ = 0, u_pool_ = 0;
+    std::vector<void*> allocs_;
+    std::vector<FrontDesc> h_desc_;
+    std::vector<std::vector<int*>> upd_nF_;   // per level, per panel step: F-tile counts per item
+
+    template <typename X> X* upload(const std::vector<X>& v, cudaStream_t st);
+    WorkList make_list(const std::vector<int>& fronts, const std::vector<int>& ctas, cudaStream_t st);
+};
+
+}  // namespace wrapd

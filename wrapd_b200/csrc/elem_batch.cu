@@ -1,0 +1,122 @@
+// Batched entry points over the per-element device math (the same svd3,
+// prox_lbfgs and hess_lmax the ADMM kernels inline), for parity checks of
+// each function on its own.  Handle-free; they run on the current device.
+#include <vector>
+
+#include "elem_math.cuh"
+
+namespace wrapd {
+namespace {
+
+template <typename T>
+__global__ void k_svd_batch(int n, const double* __restrict__ F, double* __restrict__ sig, double* __restrict__ U,
+                            double* __restrict__ V) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    T f[9], s[3], u[9], v[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f[i] = T(F[9 * (size_t)e + i]);
+    svd3(f, s, u, v);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) sig[3 * (size_t)e + i] = s[i];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) { U[9 * (size_t)e + i] = u[i]; V[9 * (size_t)e + i] = v[i]; }
+}
+
+template <typename T>
+__global__ void k_prox_batch(int n, double mu, double lambda, int max_iters, const double* __restrict__ s0,
+                             const double* __restrict__ wov, const double* __restrict__ start, double* __restrict__ out,
+                             int* __restrict__ iters) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    Prox<T> P;
+    P.nh.mu = T(mu);
+    P.nh.lambda = T(lambda);
+    T x[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { P.x0[i] = T(s0[3 * (size_t)e + i]); x[i] = T(start[3 * (size_t)e + i]); }
+    P.wov = T(wov[e]);
+    iters[e] = prox_lbfgs(P, x, max_iters);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) out[3 * (size_t)e + i] = x[i];
+}
+
+__global__ void k_hess_batch(int n, double mu, double lambda, const double* __restrict__ s, double* __restrict__ out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const double x[3] = {s[3 * (size_t)e], s[3 * (size_t)e + 1], s[3 * (size_t)e + 2]};
+    out[e] = NH<double>{mu, lambda}.hess_lmax(x);
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    explicit DevBuf(size_t bytes) {
+        if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) { cudaGetLastError(); p = nullptr; }
+    }
+    ~DevBuf() { if (p) cudaFree(p); }
+    template <typename X> X* as() const { return static_cast<X*>(p); }
+};
+
+int finish(cudaError_t e) {
+    if (e == cudaErrorMemoryAllocation) return WRAPD_E_OOM;
+    return e == cudaSuccess ? WRAPD_OK : WRAPD_E_CUDA;
+}
+
+}  // namespace
+}  // namespace wrapd
+
+using namespace wrapd;
+
+extern "C" {
+
+WRAPD_API int wrapd_svd3_batch(int n, int fp32, const double* F, double* sigma, double* U, double* V) {
+    if (n < 0 || (n > 0 && (!F || !sigma || !U || !V))) return WRAPD_E_INPUT;
+    if (n == 0) return WRAPD_OK;
+    DevBuf dF(9 * (size_t)n * 8), dS(3 * (size_t)n * 8), dU(9 * (size_t)n * 8), dV(9 * (size_t)n * 8);
+    if (!dF.p || !dS.p || !dU.p || !dV.p) return WRAPD_E_OOM;
+    cudaError_t e = cudaMemcpy(dF.p, F, 9 * (size_t)n * 8, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return finish(e);
+    const int b = (n + 127) / 128;
+    if (fp32) k_svd_batch<float><<<b, 128>>>(n, dF.as<double>(), dS.as<double>(), dU.as<double>(), dV.as<double>());
+    else k_svd_batch<double><<<b, 128>>>(n, dF.as<double>(), dS.as<double>(), dU.as<double>(), dV.as<double>());
+    if ((e = cudaGetLastError()) != cudaSuccess) return finish(e);
+    if ((e = cudaMemcpy(sigma, dS.p, 3 * (size_t)n * 8, cudaMemcpyDeviceToHost)) != cudaSuccess) return finish(e);
+    if ((e = cudaMemcpy(U, dU.p, 9 * (size_t)n * 8, cudaMemcpyDeviceToHost)) != cudaSuccess) return finish(e);
+    return finish(cudaMemcpy(V, dV.p, 9 * (size_t)n * 8, cudaMemcpyDeviceToHost));
+}
+
+WRAPD_API int wrapd_prox_batch(int n, int fp32, double mu, double lambda, int max_iters, const double* sigma0,
+                               const double* wov, const double* start, double* out, int* iters) {
+    if (n < 0 || max_iters < 1 || (n > 0 && (!sigma0 || !wov || !start || !out || !iters))) return WRAPD_E_INPUT;
+    if (n == 0) return WRAPD_OK;
+    DevBuf d0(3 * (size_t)n * 8), dw((size_t)n * 8), ds(3 * (size_t)n * 8), dout(3 * (size_t)n * 8), dit((size_t)n * 4);
+    if (!d0.p || !dw.p || !ds.p || !dout.p || !dit.p) return WRAPD_E_OOM;
+    cudaError_t e;
+    if ((e = cudaMemcpy(d0.p, sigma0, 3 * (size_t)n * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return finish(e);
+    if ((e = cudaMemcpy(dw.p, wov, (size_t)n * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return finish(e);
+    if ((e = cudaMemcpy(ds.p, start, 3 * (size_t)n * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return finish(e);
+    const int b = (n + 127) / 128;
+    if (fp32)
+        k_prox_batch<float><<<b, 128>>>(n, mu, lambda, max_iters, d0.as<double>(), dw.as<double>(), ds.as<double>(),
+                                        dout.as<double>(), dit.as<int>());
+    else
+        k_prox_batch<double><<<b, 128>>>(n, mu, lambda, max_iters, d0.as<double>(), dw.as<double>(), ds.as<double>(),
+                                         dout.as<double>(), dit.as<int>());
+    if ((e = cudaGetLastError()) != cudaSuccess) return finish(e);
+    if ((e = cudaMemcpy(out, dout.p, 3 * (size_t)n * 8, cudaMemcpyDeviceToHost)) != cudaSuccess) return finish(e);
+    return finish(cudaMemcpy(iters, dit.p, (size_t)n * 4, cudaMemcpyDeviceToHost));
+}
+
+WRAPD_API int wrapd_hess_lmax_batch(int n, double mu, double lambda, const double* sigma, double* out) {
+    if (n < 0 || (n > 0 && (!sigma || !out))) return WRAPD_E_INPUT;
+    if (n == 0) return WRAPD_OK;
+    DevBuf ds(3 * (size_t)n * 8), dout((size_t)n * 8);
+    if (!ds.p || !dout.p) return WRAPD_E_OOM;
+    cudaError_t e;
+    if ((e = cudaMemcpy(ds.p, sigma, 3 * (size_t)n * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return finish(e);
+    k_hess_batch<<<(n + 127) / 128, 128>>>(n, mu, lambda, ds.as<double>(), dout.as<double>());
+    if ((e = cudaGetLastError()) != cudaSuccess) return finish(e);
+    return finish(cudaMemcpy(out, dout.p, (size_t)n * 8, cudaMemcpyDeviceToHost));
+}
+
+}  // extern "C"

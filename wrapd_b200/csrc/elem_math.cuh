@@ -1,0 +1,396 @@
+// Per-element device math, in registers, templated on the arithmetic type
+// (double for the FP64 path, float for the FP32 local step of mixed mode).
+// 3x3 matrices are 9 scalars column-major: a[r + 3*c].
+#pragma once
+#include "common.cuh"
+
+namespace wrapd {
+
+#define M3(a, r, c) (a)[(r) + 3 * (c)]
+
+template <typename T>
+__device__ __forceinline__ T det3(const T* m) {
+    return M3(m, 0, 0) * (M3(m, 1, 1) * M3(m, 2, 2) - M3(m, 1, 2) * M3(m, 2, 1)) -
+           M3(m, 0, 1) * (M3(m, 1, 0) * M3(m, 2, 2) - M3(m, 1, 2) * M3(m, 2, 0)) +
+           M3(m, 0, 2) * (M3(m, 1, 0) * M3(m, 2, 1) - M3(m, 1, 1) * M3(m, 2, 0));
+}
+
+// Two-sided Jacobi SVD of a 3x3 matrix with the rotation sign fix.  Restates
+// Eigen 3.3.7 JacobiSVD::compute for square inputs (scale by the max |entry|,
+// sweep the (1,0),(2,0),(2,1) pairs with real_2x2_jacobi_svd until every
+// off-diagonal entry is below max(min_normal, 2 eps max|diag|), make the
+// diagonal non-negative, sort descending), then wrapd's math::svd sign fix
+// (src/Math.hpp:147-160): a reflection in U or V negates column 2 and sigma_2.
+// The sweep loop is capped at 64 (Jacobi needs < 10 sweeps on finite 3x3
+// input; the cap only bounds non-finite input).
+template <typename T>
+__device__ __forceinline__ void svd3(const T* A, T* sig, T* U, T* V) {
+    T W[9];
+    T scale = T(0);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) scale = fmax(scale, fabs(A[i]));
+    if (scale == T(0)) scale = T(1);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        W[i] = A[i] / scale;
+        U[i] = V[i] = (i % 4 == 0) ? T(1) : T(0);
+    }
+    const T prec = T(2) * Lim<T>::eps(), tiny = Lim<T>::min();
+    T maxd = fmax(fabs(W[0]), fmax(fabs(W[4]), fabs(W[8])));
+    bool finished = false;
+    for (int sweep = 0; sweep < 64 && !finished; ++sweep) {
+        finished = true;
+#pragma unroll
+        for (int p = 1; p < 3; ++p) {
+#pragma unroll
+            for (int q = 0; q < p; ++q) {
+                const T thr = fmax(tiny, prec * maxd);
+                if (fabs(M3(W, p, q)) > thr || fabs(M3(W, q, p)) > thr) {
+                    finished = false;
+                    const T m00 = M3(W, p, p), m01 = M3(W, p, q), m10 = M3(W, q, p), m11 = M3(W, q, q);
+                    const T t = m00 + m11, d = m10 - m01;
+                    T c1, s1;
+                    if (fabs(d) < tiny) { s1 = T(0); c1 = T(1); }
+                    else { const T u = t / d, tmp = sqrt(T(1) + u * u); s1 = T(1) / tmp; c1 = u / tmp; }
+                    const T a00 = c1 * m00 + s1 * m10, a01 = c1 * m01 + s1 * m11;
+                    const T a11 = -s1 * m01 + c1 * m11;
+                    T cr, sr;
+                    const T deno = T(2) * fabs(a01);
+                    if (deno < tiny) { cr = T(1); sr = T(0); }
+                    else {
+                        const T tau = (a00 - a11) / deno, w = sqrt(tau * tau + T(1));
+                        const T tt = tau > T(0) ? T(1) / (tau + w) : T(1) / (tau - w);
+                        const T sgn = tt > T(0) ? T(1) : T(-1);
+                        const T n = T(1) / sqrt(tt * tt + T(1));
+                        sr = -sgn * (a01 / fabs(a01)) * fabs(tt) * n;
+                        cr = n;
+                    }
+                    const T cl = c1 * cr + s1 * sr;
+                    const T sl = -c1 * sr + s1 * cr;
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const T x = M3(W, p, i), y = M3(W, q, i);
+                        M3(W, p, i) = cl * x + sl * y;
+                        M3(W, q, i) = -sl * x + cl * y;
+                    }
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const T x = M3(U, i, p), y = M3(U, i, q);
+                        M3(U, i, p) = cl * x + sl * y;
+                        M3(U, i, q) = -sl * x + cl * y;
+                    }
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const T x = M3(W, i, p), y = M3(W, i, q);
+                        M3(W, i, p) = cr * x - sr * y;
+                        M3(W, i, q) = sr * x + cr * y;
+                    }
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const T x = M3(V, i, p), y = M3(V, i, q);
+                        M3(V, i, p) = cr * x - sr * y;
+                        M3(V, i, q) = sr * x + cr * y;
+                    }
+                    maxd = fmax(maxd, fmax(fabs(M3(W, p, p)), fabs(M3(W, q, q))));
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const T a = M3(W, i, i);
+        sig[i] = fabs(a);
+        if (a < T(0)) {
+#pragma unroll
+            for (int r = 0; r < 3; ++r) M3(U, r, i) = -M3(U, r, i);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) sig[i] *= scale;
+    // selection sort, descending, first maximum wins (Eigen's maxCoeff)
+    auto swapcol = [&](int i, int j) {
+        T t = sig[i]; sig[i] = sig[j]; sig[j] = t;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            t = M3(U, r, i); M3(U, r, i) = M3(U, r, j); M3(U, r, j) = t;
+            t = M3(V, r, i); M3(V, r, i) = M3(V, r, j); M3(V, r, j) = t;
+        }
+    };
+    {
+        int pos = 0;
+        T mx = sig[0];
+        if (sig[1] > mx) { mx = sig[1]; pos = 1; }
+        if (sig[2] > mx) { mx = sig[2]; pos = 2; }
+        if (mx != T(0)) {
+            if (pos == 1) swapcol(0, 1);
+            else if (pos == 2) swapcol(0, 2);
+            if (sig[2] > sig[1] && sig[2] != T(0)) swapcol(1, 2);
+        }
+    }
+    if (det3(U) < T(0)) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) M3(U, r, 2) = -M3(U, r, 2);
+        sig[2] = -sig[2];
+    }
+    if (det3(V) < T(0)) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) M3(V, r, 2) = -M3(V, r, 2);
+        sig[2] = -sig[2];
+    }
+}
+
+// ---- compressible Neo-Hookean with the extended log (J0 = 0.1) -------------
+// src/TetElements.hpp:61-144; energies of src/TetElements.cpp:619-628.
+template <typename T>
+struct NH {
+    T mu, lambda;
+    static constexpr double J0 = 0.1;
+
+    __device__ __forceinline__ T fJ_ext(T J) const {
+        const T r = J / T(J0) - T(1);
+        return log(T(J0)) + ((J - T(J0)) / T(J0)) - T(0.5) * r * r;
+    }
+    // energy density without the negative-stretch guard (energies)
+    __device__ __forceinline__ T psi_plain(T x0, T x1, T x2) const {
+        const T I1 = x0 * x0 + x1 * x1 + x2 * x2;
+        const T J = x0 * x1 * x2;
+        T e = T(0.5) * mu * (I1 - T(3));
+        if (J > T(J0)) {
+            const T lj = log(J);
+            e += -mu * lj + T(0.5) * lambda * lj * lj;
+        } else {
+            const T fJ = fJ_ext(J);
+            e += -mu * fJ + T(0.5) * lambda * fJ * fJ;
+        }
+        return e;
+    }
+    // NHProx::energy_density: 1e15 for a negative stretch
+    __device__ __forceinline__ T psi(T x0, T x1, T x2) const {
+        if (x0 < T(0) || x1 < T(0) || x2 < T(0)) return T(1.e15);
+        return psi_plain(x0, x1, x2);
+    }
+    // gradient of the density (without the prox penalty)
+    __device__ __forceinline__ void dpsi(const T* x, T* g) const {
+        const T J = x[0] * x[1] * x[2];
+        T f;
+        if (J > T(J0)) {
+            f = lambda * log(J) - mu;
+        } else {
+            const T fJ = fJ_ext(J);
+            const T dfJdJ = T(1) / T(J0) - (J - T(J0)) / (T(J0) * T(J0));
+            f = (lambda * fJ - mu) * dfJdJ * J;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) g[i] = mu * x[i] + f * (T(1) / x[i]);
+    }
+    // lambda_max of makePD(hessian_density(x)) = max(lambda_max(H), 0); the
+    // PSD projection of src/Math.hpp:243-261 only zeroes negative eigenvalues.
+    __device__ __forceinline__ T hess_lmax(const T* x) const;
+};
+
+// Largest eigenvalue of a symmetric 3x3 (cyclic Jacobi, at most 12 sweeps).
+template <typename T>
+__device__ __forceinline__ T sym3_lmax(T a00, T a11, T a22, T a01, T a02, T a12) {
+    T a[9] = {a00, a01, a02, a01, a11, a12, a02, a12, a22};
+    for (int sweep = 0; sweep < 12; ++sweep) {
+        const T off = M3(a, 0, 1) * M3(a, 0, 1) + M3(a, 0, 2) * M3(a, 0, 2) + M3(a, 1, 2) * M3(a, 1, 2);
+        const T dn = M3(a, 0, 0) * M3(a, 0, 0) + M3(a, 1, 1) * M3(a, 1, 1) + M3(a, 2, 2) * M3(a, 2, 2);
+        if (off <= T(1e-40) * dn || off == T(0)) break;
+#pragma unroll
+        for (int p = 0; p < 2; ++p)
+#pragma unroll
+            for (int q = p + 1; q < 3; ++q) {
+                const T apq = M3(a, p, q);
+                if (apq != T(0)) {
+                    const T theta = (M3(a, q, q) - M3(a, p, p)) / (T(2) * apq);
+                    const T t = (theta >= T(0) ? T(1) : T(-1)) / (fabs(theta) + sqrt(theta * theta + T(1)));
+                    const T c = T(1) / sqrt(t * t + T(1)), s = t * c;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const T akp = M3(a, k, p), akq = M3(a, k, q);
+                        M3(a, k, p) = c * akp - s * akq;
+                        M3(a, k, q) = s * akp + c * akq;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const T apk = M3(a, p, k), aqk = M3(a, q, k);
+                        M3(a, p, k) = c * apk - s * aqk;
+                        M3(a, q, k) = s * apk + c * aqk;
+                    }
+                }
+            }
+    }
+    return fmax(M3(a, 0, 0), fmax(M3(a, 1, 1), M3(a, 2, 2)));
+}
+
+template <typename T>
+__device__ __forceinline__ T NH<T>::hess_lmax(const T* x) const {
+    const T J = x[0] * x[1] * x[2];
+    T h00, h11, h22, h01, h02, h12;
+    if (J > T(J0)) {
+        const T lj = log(J);
+        const T ct = mu - lambda * (lj - T(1));
+        h00 = mu + ct / (x[0] * x[0]);
+        h11 = mu + ct / (x[1] * x[1]);
+        h22 = mu + ct / (x[2] * x[2]);
+        h01 = lambda / (x[0] * x[1]);
+        h02 = lambda / (x[0] * x[2]);
+        h12 = lambda / (x[1] * x[2]);
+    } else {
+        const T fJ = fJ_ext(J);
+        const T dfJdJ = T(1) / T(J0) - (J - T(J0)) / (T(J0) * T(J0));
+        const T lfm = lambda * fJ - mu;
+        const T a = x[1] * x[2], b = x[0] * x[2], c = x[0] * x[1];
+        h00 = mu - lfm * (a / T(J0)) * (a / T(J0)) + lambda * (dfJdJ * a) * (dfJdJ * a);
+        h11 = mu - lfm * (b / T(J0)) * (b / T(J0)) + lambda * (dfJdJ * b) * (dfJdJ * b);
+        h22 = mu - lfm * (c / T(J0)) * (c / T(J0)) + lambda * (dfJdJ * c) * (dfJdJ * c);
+        const T ct = lfm * (dfJdJ - J / (T(J0) * T(J0))) + lambda * J * dfJdJ * dfJdJ;
+        h01 = x[2] * ct;
+        h02 = x[1] * ct;
+        h12 = x[0] * ct;
+    }
+    const T m = sym3_lmax(h00, h11, h22, h01, h02, h12);
+    return m > T(0) ? m : T(0);
+}
+
+// ---- the proximal stretch solve --------------------------------------------
+// min_x psi(x) + (wov/2)|x - x0|^2 by LBFGS<3, M=8> with cubic-interpolating
+// Armijo backtracking, restating deps/mcloptlib/include/MCL/LBFGS.hpp:52-152,
+// Backtracking.hpp:268-332 and Prox::converged (src/TetElements.hpp:40-42).
+// The history is kept in registers (fully unrolled, predicated loops); the
+// line search is capped at 4096 trials instead of 100000 (the step shrinks by
+// at least 2x per trial, so it underflows to zero long before).
+template <typename T>
+struct Prox {
+    NH<T> nh;
+    T x0[3];
+    T wov;
+
+    __device__ __forceinline__ T value(const T* x) const {
+        const T d0 = x[0] - x0[0], d1 = x[1] - x0[1], d2 = x[2] - x0[2];
+        return nh.psi(x[0], x[1], x[2]) + (wov * T(0.5)) * (d0 * d0 + d1 * d1 + d2 * d2);
+    }
+    __device__ __forceinline__ T value_grad(const T* x, T* g) const {
+        nh.dpsi(x, g);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) g[i] = g[i] + wov * (x[i] - x0[i]);
+        return value(x);
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ T dot3(const T* a, const T* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+template <typename T>
+__device__ __forceinline__ T cubic_step(T fx0, T gtp, T fxa, T alpha, T fxp, T alphap) {
+    const T mult = T(1) / (alpha * alpha * alphap * alphap * (alpha - alphap));
+    const T a00 = mult * (alphap * alphap), a01 = mult * (-alpha * alpha);
+    const T a10 = mult * (-alphap * alphap * alphap), a11 = mult * (alpha * alpha * alpha);
+    const T b0 = fxa - fx0 - alpha * gtp, b1 = fxp - fx0 - alphap * gtp;
+    const T r0 = a00 * b0 + a01 * b1, r1 = a10 * b0 + a11 * b1;
+    if (fabs(r0) <= T(0)) return -gtp / (T(2) * r1);
+    const T d = sqrt(r1 * r1 - T(3) * r0 * gtp);
+    return (-r1 + d) / (T(3) * r0);
+}
+
+template <typename T>
+__device__ __forceinline__ T linesearch_cubic(const Prox<T>& P, const T* x, const T* p, T alpha0) {
+    if (sqrt(dot3(p, p)) <= Lim<T>::eps()) return T(1e-4);
+    T alpha = alpha0, g[3];
+    const T fx0 = P.value_grad(x, g);
+    const T gtp = dot3(g, p);
+    T fxp = fx0, alphap = alpha;
+    for (int it = 0; it < 4096; ++it) {
+        const T xa[3] = {x[0] + alpha * p[0], x[1] + alpha * p[1], x[2] + alpha * p[2]};
+        const T fxa = P.value(xa);
+        if (fxa <= fx0 + alpha * T(1e-4) * gtp) return alpha;
+        const T at = it == 0 ? (gtp / (T(2) * (fx0 + gtp - fxa))) : cubic_step(fx0, gtp, fxa, alpha, fxp, alphap);
+        fxp = fxa;
+        alphap = alpha;
+        const T lo = T(0.1) * alpha, hi = T(0.5) * alpha;
+        alpha = at < lo ? lo : (at > hi ? hi : at);
+    }
+    return T(-1);
+}
+
+// Returns the iteration count (or -1 when the line search fails; x keeps the
+// last iterate, as in the reference).
+template <typename T>
+__device__ __forceinline__ int prox_lbfgs(const Prox<T>& P, T* x, int max_iters) {
+    constexpr int M = 8;
+    T s[M][3], y[M][3], alpha[M], rho[M];
+    T grad[3], q[3], gold[3], xold[3];
+    P.value_grad(x, grad);
+    T gamma_k = T(1), alpha_init = T(1);
+    int global_iter = 0;
+    for (int k = 0; k < max_iters; ++k) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { xold[c] = x[c]; gold[c] = grad[c]; q[c] = grad[c]; }
+        global_iter++;
+        const int iter = k < M ? k : M;
+#pragma unroll
+        for (int i = M - 1; i >= 0; --i) {
+            if (i < iter) {
+                rho[i] = T(1) / dot3(s[i], y[i]);
+                alpha[i] = rho[i] * dot3(s[i], q);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) q[c] = q[c] - alpha[i] * y[i][c];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) q[c] = gamma_k * q[c];
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            if (i < iter) {
+                const T beta = rho[i] * dot3(q, y[i]);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) q[c] = q[c] + (alpha[i] - beta) * s[i][c];
+            }
+        }
+        const T dir = dot3(q, grad);
+        if (dir <= T(0)) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) q[c] = grad[c];
+            max_iters -= k;
+            k = 0;
+            const T ninf = fmax(fabs(grad[0]), fmax(fabs(grad[1]), fabs(grad[2])));
+            alpha_init = fmin(T(1), T(1) / ninf);
+        }
+        const T mq[3] = {-q[0], -q[1], -q[2]};
+        const T rate = linesearch_cubic(P, x, mq, alpha_init);
+        if (rate <= T(0)) return -1;
+        T xl[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { xl[c] = x[c]; x[c] -= rate * q[c]; }
+        {
+            const T dx[3] = {xl[0] - x[0], xl[1] - x[1], xl[2] - x[2]};
+            if (sqrt(dot3(grad, grad)) < T(1e-8) || sqrt(dot3(dx, dx)) < T(1e-8)) break;
+        }
+        P.value_grad(x, grad);
+        T st[3], yt[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { st[c] = x[c] - xold[c]; yt[c] = grad[c] - gold[c]; }
+        if (k < M) {
+#pragma unroll
+            for (int i = 0; i < M; ++i)
+                if (i == k) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) { s[i][c] = st[c]; y[i][c] = yt[c]; }
+                }
+        } else {
+#pragma unroll
+            for (int i = 0; i < M - 1; ++i)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) { s[i][c] = s[i + 1][c]; y[i][c] = y[i + 1][c]; }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) { s[M - 1][c] = st[c]; y[M - 1][c] = yt[c]; }
+        }
+        const T denom = dot3(yt, yt);
+        if (fabs(denom) <= T(0)) break;
+        gamma_k = dot3(st, yt) / denom;
+        alpha_init = T(1);
+    }
+    return global_iter;
+}
+
+}  // namespace wrapd

@@ -1,0 +1,443 @@
+// Per-element kernels of the ADMM loop (one thread per tet) and the free-vertex
+// vectors kernels.  Element arrays are SoA: component k of element e is at
+// [k * ne + e], so every load and store of a warp is coalesced.  Element
+// state is typed T (double in FP64 mode, float for the FP32 element math of
+// mixed mode); vertex positions, weights, volumes and every reduction are FP64.
+#pragma once
+#include "elem_math.cuh"
+
+namespace wrapd {
+
+template <typename T>
+struct ElemView {
+    int ne;
+    const int4* idx;     // per vertex slot: free vertex (dissection order) or -(pin + 1)
+    const double* Di;    // 12 x ne: Di(r, a) at [(r + 3a) * ne + e], Di = (S Dm^-1)^T
+    const double* vol;
+    double* w2;
+    double* w2c;
+    T* Z;                // 9 x ne, the reference's Mat3x3 m_Zi (column-major)
+    T* U;                // 9 x ne, m_Ui
+    T* symF;             // 9 x ne, cached V diag(sigma) V^T at the last gradient point
+    T* sig;              // 3 x ne, cached singular values at the last gradient point
+    T* slast;            // 3 x ne, prox warm start (m_last_sigma)
+    T* gel;              // 12 x ne, per-element gradient rows g(a, r) at [(r + 3a) * ne + e]
+};
+
+struct Material {
+    double mu, lambda;
+    double wr, wmin, wmax;   // rest stiffness k and its beta_min / beta_max multiples
+};
+
+// Candidate-weight modes of update_all_candidate_weights (src/TetElements.cpp:391-432).
+enum { CAND_NONE = 0, CAND_REST = 1, CAND_HESSIAN = 2 };
+
+// ---- deterministic grid reduction: per-block partials, summed in block order
+// by whichever block finishes last. -------------------------------------------
+// out[k] = total_k, or for k = 0 with an affine epilogue: (base ? *base : 0) + scale * total_0.
+template <int NV, bool MAX = false>
+__device__ __forceinline__ void grid_reduce(const double (&v)[NV], double* partials, unsigned* counter, double* out,
+                                            const double* base = nullptr, double scale = 1.0) {
+    __shared__ double sm[32];
+    __shared__ bool last;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        const double r = MAX ? block_max(v[k], sm) : block_sum(v[k], sm);
+        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * NV + k] = r;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double acc = MAX ? -1.0e308 : 0.0;
+        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+            const double p = __ldcg(partials + (size_t)b * NV + k);
+            acc = MAX ? fmax(acc, p) : acc + p;
+        }
+        const double r = MAX ? block_max(acc, sm) : block_sum(acc, sm);
+        if (threadIdx.x == 0) out[k] = (k == 0 && (base || scale != 1.0)) ? (base ? *base : 0.0) + scale * r : r;
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+}
+
+template <typename T>
+__device__ __forceinline__ void load9(const T* a, int ne, int e, T* m) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) m[k] = a[(size_t)k * ne + e];
+}
+template <typename T>
+__device__ __forceinline__ void store9(T* a, int ne, int e, const T* m) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a[(size_t)k * ne + e] = m[k];
+}
+
+// F = (D_free x_free + D_fix x_fix)^T, src/TetElements.cpp:568-586, computed
+// in FP64.  `split` sums free then pinned slots as the reference does for
+// partially pinned tets; otherwise the four slots in order (Di * x_local).
+template <typename T>
+__device__ __forceinline__ void deformation(const ElemView<T>& E, int e, const double* __restrict__ x,
+                                            const double* __restrict__ xfix, bool split, double* F) {
+    const int4 id = E.idx[e];
+    const int ids[4] = {id.x, id.y, id.z, id.w};
+    double xa[4][3];
+    bool fixed[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        fixed[a] = ids[a] < 0;
+        const double* p = fixed[a] ? xfix + 3 * (size_t)(-ids[a] - 1) : x + 3 * (size_t)ids[a];
+        xa[a][0] = p[0]; xa[a][1] = p[1]; xa[a][2] = p[2];
+    }
+    const bool any_fixed = fixed[0] || fixed[1] || fixed[2] || fixed[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double d[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) d[a] = E.Di[(size_t)(c + 3 * a) * E.ne + e];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            if (split && any_fixed) {
+                double vf = 0.0, vx = 0.0;
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    if (fixed[a]) vx += d[a] * xa[a][r];
+                    else vf += d[a] * xa[a][r];
+                }
+                F[r + 3 * c] = vf + vx;
+            } else {
+                double v = 0.0;
+#pragma unroll
+                for (int a = 0; a < 4; ++a) v += d[a] * xa[a][r];
+                F[r + 3 * c] = v;
+            }
+        }
+    }
+}
+
+// ---- the defo cache + gradient of the global AL objective -------------------
+// update_defo_cache (src/TetElements.cpp:564-596) fused with
+// global_obj_grad (src/TetElements.cpp:691-738): F, SVD, symF, Q = V^T P V,
+// K + K^T, M = F - U diag(s) (K+K^T) V^T and g_e = w^2 Di^T M^T, plus the AL
+// value 0.5 w^2 |symF - P|^2, the potential energy and the inversion count at
+// x (src/TetElements.cpp:444-468, 598-635).  Outputs out[0..2] = value, pe, flips.
+template <typename T>
+__global__ void __launch_bounds__(128) k_grad(ElemView<T> E, const double* __restrict__ x,
+                                              const double* __restrict__ xfix, Material mat, int write_gel,
+                                              double* partials, unsigned* counter, double* out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[3] = {0.0, 0.0, 0.0};
+    if (e < E.ne) {
+        double Fd[9];
+        deformation(E, e, x, xfix, true, Fd);
+        T F[9], s[3], Us[9], Vs[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) F[i] = T(Fd[i]);
+        svd3(F, s, Us, Vs);
+        T S[9];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                M3(S, r, c) = M3(Vs, r, 0) * s[0] * M3(Vs, c, 0) + M3(Vs, r, 1) * s[1] * M3(Vs, c, 1) +
+                              M3(Vs, r, 2) * s[2] * M3(Vs, c, 2);
+        store9(E.symF, E.ne, e, S);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) E.sig[(size_t)i * E.ne + e] = s[i];
+        T Zm[9], Um[9], P[9];
+        load9(E.Z, E.ne, e, Zm);
+        load9(E.U, E.ne, e, Um);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) M3(P, r, c) = M3(Zm, c, r) - M3(Um, c, r);
+        const double w2 = E.w2[e];
+        {
+            double v = 0.0;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) { const double d = double(S[i]) - double(P[i]); v += d * d; }
+            red[0] = (0.5 * w2) * v;
+        }
+        red[1] = E.vol[e] * NH<double>{mat.mu, mat.lambda}.psi_plain(double(s[0]), double(s[1]), double(s[2]));
+        red[2] = (s[0] < T(0) || s[1] < T(0) || s[2] < T(0)) ? 1.0 : 0.0;
+        if (write_gel) {
+            T Tm[9], Q[9], K[9], Mm[9];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    M3(Tm, r, c) = M3(Vs, 0, r) * M3(P, 0, c) + M3(Vs, 1, r) * M3(P, 1, c) + M3(Vs, 2, r) * M3(P, 2, c);
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    M3(Q, r, c) = M3(Tm, r, 0) * M3(Vs, 0, c) + M3(Tm, r, 1) * M3(Vs, 1, c) + M3(Tm, r, 2) * M3(Vs, 2, c);
+            M3(K, 0, 0) = M3(Q, 0, 0) / s[0];
+            M3(K, 1, 1) = M3(Q, 1, 1) / s[1];
+            M3(K, 2, 2) = M3(Q, 2, 2) / s[2];
+            M3(K, 0, 1) = M3(K, 1, 0) = (M3(Q, 0, 1) + M3(Q, 1, 0)) / (s[0] + s[1]);
+            M3(K, 0, 2) = M3(K, 2, 0) = (M3(Q, 0, 2) + M3(Q, 2, 0)) / (s[0] + s[2]);
+            M3(K, 1, 2) = M3(K, 2, 1) = (M3(Q, 1, 2) + M3(Q, 2, 1)) / (s[1] + s[2]);
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    T v = T(0);
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const T t = M3(K, a, 0) * M3(Vs, c, 0) + M3(K, a, 1) * M3(Vs, c, 1) + M3(K, a, 2) * M3(Vs, c, 2);
+                        v += M3(Us, r, a) * s[a] * t;
+                    }
+                    M3(Mm, r, c) = F[r + 3 * c] - v;
+                }
+            const T w2t = T(w2);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    T v = T(0);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) v += T(E.Di[(size_t)(c + 3 * a) * E.ne + e]) * (w2t * M3(Mm, r, c));
+                    E.gel[(size_t)(r + 3 * a) * E.ne + e] = v;
+                }
+        }
+    }
+    grid_reduce<3>(red, partials, counter, out);
+}
+
+// Free-vertex gather of the element gradients (atomic-free; incidences are in
+// element order, the reference's single-thread accumulation order):
+//   grad[i] = sum over (e, a) incident to i of gel(a, :)[e].
+// With gold: d = grad - gold; ystage <- d (if given); out[0] = |d|^2 and
+// out[1] = <sstage, d> (if sstage given).
+template <typename T>
+__global__ void __launch_bounds__(256) k_gather(int nf, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
+                                                const T* __restrict__ gel, int ne, double* __restrict__ grad,
+                                                const double* __restrict__ gold, double* __restrict__ ystage,
+                                                const double* __restrict__ sstage, double* partials,
+                                                unsigned* counter, double* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[2] = {0.0, 0.0};
+    if (i < nf) {
+        double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+        for (int t = inc_ptr[i]; t < inc_ptr[i + 1]; ++t) {
+            const int c = inc[t];
+            const int e = c >> 2, a = c & 3;
+            g0 += double(gel[(size_t)(0 + 3 * a) * ne + e]);
+            g1 += double(gel[(size_t)(1 + 3 * a) * ne + e]);
+            g2 += double(gel[(size_t)(2 + 3 * a) * ne + e]);
+        }
+        grad[3 * (size_t)i] = g0; grad[3 * (size_t)i + 1] = g1; grad[3 * (size_t)i + 2] = g2;
+        if (gold) {
+            const double d0 = g0 - gold[3 * (size_t)i], d1 = g1 - gold[3 * (size_t)i + 1], d2 = g2 - gold[3 * (size_t)i + 2];
+            if (ystage) { ystage[3 * (size_t)i] = d0; ystage[3 * (size_t)i + 1] = d1; ystage[3 * (size_t)i + 2] = d2; }
+            red[0] = d0 * d0 + d1 * d1 + d2 * d2;
+            if (sstage) red[1] = sstage[3 * (size_t)i] * d0 + sstage[3 * (size_t)i + 1] * d1 + sstage[3 * (size_t)i + 2] * d2;
+        }
+    }
+    grid_reduce<2>(red, partials, counter, out);
+}
+
+// ---- local step ---------------------------------------------------------------
+// TetElements::polar_update, NH branch (src/TetElements.cpp:284-346), fused
+// per element: S_in = (symF + U)^T, SVD, prox from the last stretches, Z and
+// U update, and the candidate weight (src/TetElements.cpp:391-432).
+// out[0..3] = bef_penalty, aft_penalty, curr_pe, negative-stretch count.
+template <typename T>
+__global__ void __launch_bounds__(128) k_local(ElemView<T> E, Material mat, int prox_iters, int cand_mode,
+                                               double* partials, unsigned* counter, double* out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[4] = {0.0, 0.0, 0.0, 0.0};
+    if (e < E.ne) {
+        T S[9], Um[9], Zm[9];
+        load9(E.symF, E.ne, e, S);
+        load9(E.U, E.ne, e, Um);
+        load9(E.Z, E.ne, e, Zm);
+        const double w2 = E.w2[e], vol = E.vol[e];
+        T Sin[9];
+        double bef = 0.0;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                M3(Sin, r, c) = M3(S, c, r) + M3(Um, c, r);
+                const double d = double(M3(S, r, c)) - (double(M3(Zm, r, c)) - double(M3(Um, r, c)));
+                bef += d * d;
+            }
+        red[0] = 0.5 * w2 * bef;
+        T sg[3], Ue[9], Ve[9];
+        svd3(Sin, sg, Ue, Ve);
+        Prox<T> P;
+        P.nh.mu = T(mat.mu);
+        P.nh.lambda = T(mat.lambda);
+        P.x0[0] = sg[0]; P.x0[1] = sg[1]; P.x0[2] = sg[2];
+        P.wov = T(w2 / vol);
+        T xs[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) xs[i] = E.slast[(size_t)i * E.ne + e];
+        prox_lbfgs(P, xs, prox_iters);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) E.slast[(size_t)i * E.ne + e] = xs[i];
+        red[3] = (xs[0] < T(0) || xs[1] < T(0) || xs[2] < T(0)) ? 1.0 : 0.0;
+        T So[9];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                M3(So, r, c) = M3(Ve, r, 0) * xs[0] * M3(Ue, c, 0) + M3(Ve, r, 1) * xs[1] * M3(Ue, c, 1) +
+                               M3(Ve, r, 2) * xs[2] * M3(Ue, c, 2);
+        red[2] = vol * NH<double>{mat.mu, mat.lambda}.psi_plain(double(xs[0]), double(xs[1]), double(xs[2]));
+        double aft = 0.0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const double d = double(S[i]) - (double(So[i]) - double(Um[i]));
+            aft += d * d;
+            Zm[i] = So[i];
+            Um[i] = Um[i] + (S[i] - So[i]);
+        }
+        red[1] = 0.5 * w2 * aft;
+        store9(E.Z, E.ne, e, Zm);
+        store9(E.U, E.ne, e, Um);
+        if (cand_mode == CAND_REST) {
+            E.w2c[e] = vol * mat.wr;
+        } else if (cand_mode == CAND_HESSIAN) {
+            const double xd[3] = {double(xs[0]), double(xs[1]), double(xs[2])};
+            const double lm = NH<double>{mat.mu, mat.lambda}.hess_lmax(xd);
+            double c = lm;
+            if (lm < mat.wmin) c = mat.wmin;
+            if (lm > mat.wmax) c = mat.wmax;
+            E.w2c[e] = vol * c;
+        }
+    }
+    grid_reduce<4>(red, partials, counter, out);
+}
+
+// initialize_dual_vars (src/TetElements.cpp:145-166): Z = (V diag(s) V^T)^T of
+// F(X) with all four slots read from X, U = 0; then polar_potential_energy
+// (src/TetElements.cpp:638-675) of the new Z.  out[0] = that energy.
+template <typename T>
+__global__ void __launch_bounds__(128) k_init_dual(ElemView<T> E, const double* __restrict__ x,
+                                                   const double* __restrict__ xfix, Material mat,
+                                                   double* partials, unsigned* counter, double* out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[1] = {0.0};
+    if (e < E.ne) {
+        double Fd[9];
+        deformation(E, e, x, xfix, false, Fd);
+        T F[9], s[3], Us[9], Vs[9], Zm[9], Zt[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) F[i] = T(Fd[i]);
+        svd3(F, s, Us, Vs);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                M3(Zm, r, c) = M3(Vs, c, 0) * s[0] * M3(Vs, r, 0) + M3(Vs, c, 1) * s[1] * M3(Vs, r, 1) +
+                               M3(Vs, c, 2) * s[2] * M3(Vs, r, 2);
+        store9(E.Z, E.ne, e, Zm);
+        T zero[9] = {};
+        store9(E.U, E.ne, e, zero);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) M3(Zt, r, c) = M3(Zm, c, r);
+        svd3(Zt, s, Us, Vs);
+        red[0] = E.vol[e] * NH<double>{mat.mu, mat.lambda}.psi_plain(double(s[0]), double(s[1]), double(s[2]));
+    }
+    grid_reduce<1>(red, partials, counter, out);
+}
+
+// Candidate weights of midupdate_weights (src/TetElements.cpp:360-388): from
+// F(X) (from_x = 1) or from the cached singular values.
+template <typename T>
+__global__ void __launch_bounds__(128) k_mid_candidates(ElemView<T> E, const double* __restrict__ x,
+                                                        const double* __restrict__ xfix, Material mat,
+                                                        int from_x, int cand_mode) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E.ne) return;
+    double s[3];
+    if (from_x) {
+        double Fd[9];
+        deformation(E, e, x, xfix, false, Fd);
+        T F[9], st[3], Us[9], Vs[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) F[i] = T(Fd[i]);
+        svd3(F, st, Us, Vs);
+        s[0] = st[0]; s[1] = st[1]; s[2] = st[2];
+    } else {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) s[i] = double(E.sig[(size_t)i * E.ne + e]);
+    }
+    const double vol = E.vol[e];
+    if (cand_mode == CAND_HESSIAN) {
+        const double lm = NH<double>{mat.mu, mat.lambda}.hess_lmax(s);
+        double c = lm;
+        if (lm < mat.wmin) c = mat.wmin;
+        if (lm > mat.wmax) c = mat.wmax;
+        E.w2c[e] = vol * c;
+    } else {
+        E.w2c[e] = vol * mat.wr;
+    }
+}
+
+// max_wsq_ratio (src/Elements.hpp:56-69): out[0] = max_e max(w2/w2c, w2c/w2).
+template <typename T>
+__global__ void __launch_bounds__(256) k_ratio(ElemView<T> E, double* partials, unsigned* counter, double* out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[1] = {0.0};
+    if (e < E.ne) {
+        const double a = E.w2[e] / E.w2c[e], b = 1.0 / a;
+        red[0] = fmax(a, b);
+    }
+    grid_reduce<1, true>(red, partials, counter, out);
+}
+
+// update_actual_weights (src/TetElements.cpp:435-442).
+template <typename T>
+__global__ void __launch_bounds__(256) k_apply_weights(ElemView<T> E) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E.ne) return;
+    const double r = E.w2[e] / E.w2c[e];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) E.U[(size_t)k * E.ne + e] = T(r * double(E.U[(size_t)k * E.ne + e]));
+    E.w2[e] = E.w2c[e];
+}
+
+// ---- global-step vector kernels (n x 3 FP64, dissection order) ----------------
+// q = src + sign * coef * v; out = base + scale * <w, q>  (w, v optional).
+// The two-loop recursion of SplitLBFGS::minimize (SplitLBFGS.hpp:152-177) is a
+// chain of these: alpha_i = rho_i <s_i, q>, q -= alpha_i y_i, then
+// c_i = alpha_i - rho_i <y_i, q>, q += c_i s_i, and finally <grad, q>.
+static __global__ void __launch_bounds__(256) k_axpy_dot(int n, double* __restrict__ q, const double* __restrict__ src,
+                                                  const double* __restrict__ v, const double* __restrict__ coef,
+                                                  double sign, const double* __restrict__ w,
+                                                  const double* __restrict__ base, double scale, double* partials,
+                                                  unsigned* counter, double* out) {
+    double red[1] = {0.0};
+    const double cf = v ? sign * (*coef) : 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double qi = src ? src[i] : q[i];
+        if (v) qi = qi + cf * v[i];
+        q[i] = qi;
+        if (w) red[0] += w[i] * qi;
+    }
+    grid_reduce<1>(red, partials, counter, out, base, scale);
+}
+
+// x <- x - step with step = q, or grad when the decrement dir <= 0 (the
+// steepest-descent restart of SplitLBFGS.hpp:189-194); s = x_new - x_old.
+static __global__ void __launch_bounds__(256) k_xupdate(int n, double* __restrict__ x, const double* __restrict__ q,
+                                                 const double* __restrict__ grad, const double* __restrict__ dir,
+                                                 double* __restrict__ s) {
+    const bool restart = !(*dir > 0.0);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double xo = x[i];
+        const double xn = xo - (restart ? grad[i] : q[i]);
+        s[i] = xn - xo;
+        x[i] = xn;
+    }
+}
+
+}  // namespace wrapd

@@ -1,0 +1,762 @@
+// Host orchestration of the ADMM solve loop; see solver.cuh.
+#include "solver.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace wrapd {
+
+namespace {
+
+// Slots of the device scalar block (one pinned download per sync point).
+enum : int {
+    S_GRAD = 0,      // value, pe, flips
+    S_GATHER = 4,    // |grad - gold|^2, <s, y>
+    S_LOCAL = 8,     // bef, aft, pe, negative stretches
+    S_INIT = 12,     // polar potential energy after initialize_dual_vars
+    S_RATIO = 14,    // max weight ratio
+    S_DIR = 16,      // L-BFGS decrement
+    S_XERR = 18,     // |x - x_soln|^2
+    S_DUMMY = 19,
+    S_ALPHA = 20,    // alpha_i, up to 32 entries
+    S_C = 52,        // alpha_i - beta_i, up to 32 entries
+    S_COUNT = 84
+};
+constexpr int kMaxHistory = 32;
+
+int blocks_for(int64_t n, int threads) { return std::max(1, ceil_div(n, threads)); }
+
+// Vector kernels use a fixed grid of 2 CTAs per SM (grid-stride loops).
+int vec_blocks(int64_t n) { return std::max(1, std::min(2 * kNumSMs, ceil_div(n, 256))); }
+
+// (S * Dm^-1)^T and the rest volume of one tet, src/TetElements.cpp:93-118.
+void element_geometry(const double* p0, const double* p1, const double* p2, const double* p3, double* Di,
+                      double* vol) {
+    double ed[9];
+    for (int r = 0; r < 3; ++r) {
+        ed[r + 0] = p1[r] - p0[r];
+        ed[r + 3] = p2[r] - p0[r];
+        ed[r + 6] = p3[r] - p0[r];
+    }
+    auto m = [&](int r, int c) { return ed[r + 3 * c]; };
+    const double c00 = m(1, 1) * m(2, 2) - m(1, 2) * m(2, 1);
+    const double c01 = m(1, 2) * m(2, 0) - m(1, 0) * m(2, 2);
+    const double c02 = m(1, 0) * m(2, 1) - m(1, 1) * m(2, 0);
+    const double det = m(0, 0) * c00 + m(0, 1) * c01 + m(0, 2) * c02;
+    const double id = 1.0 / det;
+    double inv[9];
+    inv[0 + 3 * 0] = c00 * id;
+    inv[1 + 3 * 0] = c01 * id;
+    inv[2 + 3 * 0] = c02 * id;
+    inv[0 + 3 * 1] = (m(0, 2) * m(2, 1) - m(0, 1) * m(2, 2)) * id;
+    inv[1 + 3 * 1] = (m(0, 0) * m(2, 2) - m(0, 2) * m(2, 0)) * id;
+    inv[2 + 3 * 1] = (m(0, 1) * m(2, 0) - m(0, 0) * m(2, 1)) * id;
+    inv[0 + 3 * 2] = (m(0, 1) * m(1, 2) - m(0, 2) * m(1, 1)) * id;
+    inv[1 + 3 * 2] = (m(0, 2) * m(1, 0) - m(0, 0) * m(1, 2)) * id;
+    inv[2 + 3 * 2] = (m(0, 0) * m(1, 1) - m(0, 1) * m(1, 0)) * id;
+    // Di(r, a): a = 0 -> minus the column sums of Dm^-1 rows; a >= 1 -> row a-1 of Dm^-1
+    for (int r = 0; r < 3; ++r) {
+        Di[r + 0] = -inv[0 + 3 * r] - inv[1 + 3 * r] - inv[2 + 3 * r];
+        for (int a = 1; a < 4; ++a) Di[r + 3 * a] = inv[(a - 1) + 3 * r];
+    }
+    *vol = det / 6.0;
+}
+
+}  // namespace
+
+SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
+    if (cfg.rot_aware != 1) throw CudaError(WRAPD_E_UNSUPPORTED, "rotation-unaware global step (-ra 0) is not implemented");
+    if (cfg.global_ls != 0) throw CudaError(WRAPD_E_UNSUPPORTED, "global-step line search (-global_ls 1) is not implemented");
+    if (cfg.model != 0) throw CudaError(WRAPD_E_UNSUPPORTED, "only the Neo-Hookean model is implemented");
+    if (cfg.prox_mode != 0) throw CudaError(WRAPD_E_UNSUPPORTED, "prox_mode other than 0 is not implemented");
+    if (cfg.lbfgs_m < 1 || cfg.lbfgs_m > kMaxHistory) throw CudaError(WRAPD_E_INPUT, "lbfgs_m must be in [1, 32]");
+    if (cfg.max_iters < 0 || cfg.global_iters < 1 || cfg.prox_iters < 1) throw CudaError(WRAPD_E_INPUT, "bad iteration limits");
+    if (!(cfg.poisson > -1.0 && cfg.poisson < 0.5) || !(cfg.youngs > 0.0)) throw CudaError(WRAPD_E_INPUT, "bad material");
+    if (cfg.precision != 0 && cfg.precision != 1) throw CudaError(WRAPD_E_INPUT, "precision must be 0 or 1");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) throw CudaError(WRAPD_E_CUDA, "no CUDA device");
+    if (cfg.device < 0 || cfg.device >= ndev) throw CudaError(WRAPD_E_INPUT, "bad device ordinal");
+    WRAPD_CUDA(cudaSetDevice(cfg.device));
+    WRAPD_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    for (auto& e : ev_) WRAPD_CUDA(cudaEventCreate(&e));
+    WRAPD_CUDA(cudaMallocHost(&h_scal_, S_COUNT * sizeof(double)));
+    // Lame(E, nu), src/Lame.hpp:50-53; k = 2.0066 mu + 1.0122 lambda, src/TetElements.cpp:84
+    mat_.mu = cfg.youngs / (2.0 * (1.0 + cfg.poisson));
+    mat_.lambda = cfg.youngs * cfg.poisson / ((1.0 + cfg.poisson) * (1.0 - 2.0 * cfg.poisson));
+    mat_.wr = 2.0066 * mat_.mu + 1.0122 * mat_.lambda;
+    mat_.wmin = mat_.wr * cfg.beta_min;
+    mat_.wmax = mat_.wr * cfg.beta_max;
+}
+
+SolverGPU::~SolverGPU() {
+    if (st_) cudaStreamSynchronize(st_);
+    for (void* p : allocs_) cudaFree(p);
+    for (auto& e : ev_) if (e) cudaEventDestroy(e);
+    if (h_scal_) cudaFreeHost(h_scal_);
+    if (st_) cudaStreamDestroy(st_);
+}
+
+void* SolverGPU::dalloc(size_t bytes) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) {
+        cudaGetLastError();
+        throw CudaError(WRAPD_E_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+    }
+    allocs_.push_back(p);
+    return p;
+}
+
+template <typename X>
+X* SolverGPU::dupload(const std::vector<X>& v) {
+    X* p = static_cast<X*>(dalloc(v.size() * sizeof(X)));
+    if (!v.empty()) WRAPD_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice, st_));
+    return p;
+}
+
+template <typename T>
+ElemView<T> SolverGPU::view() {
+    ElemView<T> v;
+    v.ne = ne;
+    v.idx = d_idx_;
+    v.Di = d_Di_;
+    v.vol = d_vol_;
+    v.w2 = d_w2_;
+    v.w2c = d_w2c_;
+    v.Z = static_cast<T*>(d_Z_);
+    v.U = static_cast<T*>(d_U_);
+    v.symF = static_cast<T*>(d_symF_);
+    v.sig = static_cast<T*>(d_sig_);
+    v.slast = static_cast<T*>(d_slast_);
+    v.gel = static_cast<T*>(d_gel_);
+    return v;
+}
+
+void SolverGPU::add_mesh(const double* rest, const double* init, const double* soln, int nv_, const int32_t* tets,
+                         int ne_, const int32_t* pins, int np_) {
+    if (initialized_ || nv > 0) throw CudaError(WRAPD_E_STATE, "one mesh per handle");
+    if (!rest || !init || !tets || nv_ <= 0 || ne_ <= 0 || np_ < 0 || np_ >= nv_ || (np_ > 0 && !pins))
+        throw CudaError(WRAPD_E_INPUT, "bad mesh arguments");
+    nv = nv_; ne = ne_; np = np_; nf = nv - np;
+    rest_.assign(rest, rest + 3 * (size_t)nv);
+    init_.assign(init, init + 3 * (size_t)nv);
+    have_soln_ = soln != nullptr;
+    soln_ = have_soln_ ? std::vector<double>(soln, soln + 3 * (size_t)nv) : rest_;
+    tets_.assign(tets, tets + 4 * (size_t)ne);
+    for (int v : tets_) if (v < 0 || v >= nv) throw CudaError(WRAPD_E_INPUT, "tet vertex id out of range");
+    pins_.assign(pins, pins + np);
+    std::sort(pins_.begin(), pins_.end());
+    for (int j = 0; j < np; ++j)
+        if (pins_[j] < 0 || pins_[j] >= nv || (j > 0 && pins_[j] == pins_[j - 1]))
+            throw CudaError(WRAPD_E_INPUT, "pin ids must be distinct vertex ids");
+    // free/fixed maps, samples/utils/AddMeshes.hpp:268-289
+    free_of_vert_.assign(nv, -1);
+    fix_of_vert_.assign(nv, -1);
+    for (int i = 0, j = 0, k = 0; i < nv; ++i) {
+        if (j < np && i == pins_[j]) fix_of_vert_[i] = j++;
+        else free_of_vert_[i] = k++;
+    }
+}
+
+void SolverGPU::initialize() {
+    if (nv == 0) throw CudaError(WRAPD_E_STATE, "initialize before add_tetmesh");
+    if (initialized_) throw CudaError(WRAPD_E_STATE, "already initialized");
+    auto t0 = std::chrono::steady_clock::now();
+    // ---- element geometry (TetElements ctor, src/TetElements.cpp:90-142) ----
+    std::vector<double> Di(12 * (size_t)ne), vol(ne), w2(ne);
+    for (int e = 0; e < ne; ++e) {
+        const int* t = &tets_[4 * (size_t)e];
+        double d[12], v;
+        element_geometry(&rest_[3 * (size_t)t[0]], &rest_[3 * (size_t)t[1]], &rest_[3 * (size_t)t[2]],
+                         &rest_[3 * (size_t)t[3]], d, &v);
+        if (v < 0.0) throw CudaError(WRAPD_E_INVERTED_REST, "inverted tet " + std::to_string(e) + " in the rest mesh");
+        for (int k = 0; k < 12; ++k) Di[(size_t)k * ne + e] = d[k];
+        vol[e] = v;
+        w2[e] = cfg.beta_static * mat_.wr * v;
+    }
+    // ---- free-vertex graph, nested dissection, symbolic factorization ----
+    std::vector<std::vector<int>> nb(nf);
+    for (int e = 0; e < ne; ++e)
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) {
+                const int i = free_of_vert_[tets_[4 * (size_t)e + a]], j = free_of_vert_[tets_[4 * (size_t)e + b]];
+                if (i >= 0 && j >= 0 && i != j) nb[i].push_back(j);
+            }
+    std::vector<int> ptr(nf + 1, 0), adj;
+    for (int i = 0; i < nf; ++i) {
+        auto& v = nb[i];
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        ptr[i + 1] = ptr[i] + (int)v.size();
+    }
+    adj.reserve(ptr[nf]);
+    for (auto& v : nb) { adj.insert(adj.end(), v.begin(), v.end()); std::vector<int>().swap(v); }
+    std::vector<double> coords(3 * (size_t)nf);
+    for (int i = 0; i < nv; ++i)
+        if (free_of_vert_[i] >= 0)
+            for (int c = 0; c < 3; ++c) coords[3 * (size_t)free_of_vert_[i] + c] = rest_[3 * (size_t)i + c];
+    Symbolic S = analyse(nf, ptr, adj, coords, cfg.leaf_size > 0 ? cfg.leaf_size : 64);
+    perm_ = S.perm;
+    iperm_ = S.iperm;
+    // element slots: free -> dissection index, pinned -> -(pin + 1)
+    std::vector<int4> idx(ne);
+    for (int e = 0; e < ne; ++e) {
+        int s[4];
+        for (int a = 0; a < 4; ++a) {
+            const int v = tets_[4 * (size_t)e + a];
+            s[a] = free_of_vert_[v] >= 0 ? iperm_[free_of_vert_[v]] : -(fix_of_vert_[v] + 1);
+        }
+        idx[e] = make_int4(s[0], s[1], s[2], s[3]);
+    }
+    // lower-triangle entries of A in front storage, with their element contributions
+    std::vector<int> col2front(nf, -1);
+    for (size_t f = 0; f < S.fronts.size(); ++f)
+        for (int j = 0; j < S.fronts[f].ncols; ++j) col2front[S.fronts[f].first + j] = (int)f;
+    std::vector<std::pair<int64_t, int>> contrib;
+    contrib.reserve(10 * (size_t)ne);
+    for (int e = 0; e < ne; ++e) {
+        const int s[4] = {idx[e].x, idx[e].y, idx[e].z, idx[e].w};
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) {
+                if (s[a] < 0 || s[b] < 0) continue;
+                // one contribution per unordered pair: the reference's (i <= j) triplet
+                const int fa = free_of_vert_[tets_[4 * (size_t)e + a]], fb = free_of_vert_[tets_[4 * (size_t)e + b]];
+                if (fa > fb || (fa == fb && a != b)) continue;
+                const int r = std::max(s[a], s[b]), c = std::min(s[a], s[b]);
+                const Front& F = S.fronts[col2front[c]];
+                int lr;
+                if (r < F.first + F.ncols) lr = r - F.first;
+                else lr = F.ncols + (int)(std::lower_bound(F.rows.begin(), F.rows.end(), r) - F.rows.begin());
+                const int64_t pos = F.f_off + lr + (int64_t)(c - F.first) * F.ld();
+                contrib.emplace_back(pos, e * 16 + a * 4 + b);
+            }
+    }
+    std::sort(contrib.begin(), contrib.end());
+    std::vector<int64_t> A_pos;
+    std::vector<int> A_ptr(1, 0), A_con;
+    A_con.reserve(contrib.size());
+    for (size_t i = 0; i < contrib.size(); ++i) {
+        if (i == 0 || contrib[i].first != contrib[i - 1].first) {
+            if (i > 0) A_ptr.push_back((int)A_con.size());
+            A_pos.push_back(contrib[i].first);
+        }
+        A_con.push_back(contrib[i].second);
+    }
+    A_ptr.push_back((int)A_con.size());
+    std::vector<std::pair<int64_t, int>>().swap(contrib);
+    // gather incidences, element order per free vertex
+    std::vector<int> inc_ptr(nf + 1, 0), inc;
+    for (int e = 0; e < ne; ++e) {
+        const int s[4] = {idx[e].x, idx[e].y, idx[e].z, idx[e].w};
+        for (int a = 0; a < 4; ++a) if (s[a] >= 0) inc_ptr[s[a] + 1]++;
+    }
+    for (int i = 0; i < nf; ++i) inc_ptr[i + 1] += inc_ptr[i];
+    inc.resize(inc_ptr[nf]);
+    {
+        std::vector<int> fill(inc_ptr.begin(), inc_ptr.end() - 1);
+        for (int e = 0; e < ne; ++e) {
+            const int s[4] = {idx[e].x, idx[e].y, idx[e].z, idx[e].w};
+            for (int a = 0; a < 4; ++a) if (s[a] >= 0) inc[fill[s[a]]++] = e * 4 + a;
+        }
+    }
+    // ---- device state ----
+    const size_t TS = fp32() ? sizeof(float) : sizeof(double);
+    d_idx_ = dupload(idx);
+    d_Di_ = dupload(Di);
+    d_vol_ = dupload(vol);
+    d_w2_ = dupload(w2);
+    d_w2c_ = static_cast<double*>(dalloc(ne * sizeof(double)));
+    d_Z_ = dalloc(9 * (size_t)ne * TS);
+    d_U_ = dalloc(9 * (size_t)ne * TS);
+    d_symF_ = dalloc(9 * (size_t)ne * TS);
+    d_sig_ = dalloc(3 * (size_t)ne * TS);
+    d_slast_ = dalloc(3 * (size_t)ne * TS);
+    d_gel_ = dalloc(12 * (size_t)ne * TS);
+    WRAPD_CUDA(cudaMemsetAsync(d_U_, 0, 9 * (size_t)ne * TS, st_));
+    WRAPD_CUDA(cudaMemsetAsync(d_Z_, 0, 9 * (size_t)ne * TS, st_));
+    {
+        // m_last_sigma = (1, 1, 1)
+        if (fp32()) { std::vector<float> ones(3 * (size_t)ne, 1.0f); WRAPD_CUDA(cudaMemcpyAsync(d_slast_, ones.data(), ones.size() * 4, cudaMemcpyHostToDevice, st_)); WRAPD_CUDA(cudaStreamSynchronize(st_)); }
+        else { std::vector<double> ones(3 * (size_t)ne, 1.0); WRAPD_CUDA(cudaMemcpyAsync(d_slast_, ones.data(), ones.size() * 8, cudaMemcpyHostToDevice, st_)); WRAPD_CUDA(cudaStreamSynchronize(st_)); }
+    }
+    d_inc_ptr_ = dupload(inc_ptr);
+    d_inc_ = dupload(inc);
+    std::vector<double> xp(3 * (size_t)nf), xs(3 * (size_t)nf), xfix(3 * (size_t)std::max(np, 1));
+    for (int i = 0; i < nv; ++i) {
+        if (free_of_vert_[i] >= 0) {
+            const int p = iperm_[free_of_vert_[i]];
+            for (int c = 0; c < 3; ++c) { xp[3 * (size_t)p + c] = init_[3 * (size_t)i + c]; xs[3 * (size_t)p + c] = soln_[3 * (size_t)i + c]; }
+        } else {
+            for (int c = 0; c < 3; ++c) xfix[3 * (size_t)fix_of_vert_[i] + c] = init_[3 * (size_t)i + c];
+        }
+    }
+    d_x_ = dupload(xp);
+    d_xinit_ = dupload(xp);
+    d_xsoln_ = dupload(xs);
+    d_xfix_ = dupload(xfix);
+    const size_t vb = 3 * (size_t)nf * sizeof(double);
+    d_q_ = static_cast<double*>(dalloc(vb));
+    d_gcur_ = static_cast<double*>(dalloc(vb));
+    d_gold_ = static_cast<double*>(dalloc(vb));
+    d_gnew_ = static_cast<double*>(dalloc(vb));
+    d_sstage_ = static_cast<double*>(dalloc(vb));
+    d_ystage_ = static_cast<double*>(dalloc(vb));
+    WRAPD_CUDA(cudaMemsetAsync(d_gold_, 0, vb, st_));
+    WRAPD_CUDA(cudaMemsetAsync(d_gcur_, 0, vb, st_));
+    s_.assign(cfg.lbfgs_m, nullptr);
+    y_.assign(cfg.lbfgs_m, nullptr);
+    for (int i = 0; i < cfg.lbfgs_m; ++i) {
+        s_[i] = static_cast<double*>(dalloc(vb));
+        y_[i] = static_cast<double*>(dalloc(vb));
+    }
+    rho_.assign(cfg.lbfgs_m, 0.0);
+    const size_t nblk = (size_t)blocks_for(std::max(ne, nf), 128) + 2 * kNumSMs + 8;
+    d_partials_ = static_cast<double*>(dalloc(nblk * 4 * sizeof(double)));
+    d_counter_ = static_cast<unsigned*>(dalloc(sizeof(unsigned)));
+    d_scal_ = static_cast<double*>(dalloc(S_COUNT * sizeof(double)));
+    WRAPD_CUDA(cudaMemsetAsync(d_counter_, 0, sizeof(unsigned), st_));
+    WRAPD_CUDA(cudaMemsetAsync(d_scal_, 0, S_COUNT * sizeof(double), st_));
+    chol.build(S, A_pos, A_ptr, A_con, st_);
+    // ---- GlobalStepBehavior ctor: midupdate_weights(X_init) and the first factorization ----
+    if (cfg.reweighting) {
+        mid_candidates(true, cand_mode_now());
+        count_++;
+        apply_weights();
+    }
+    factor();
+    m_k_ = 0;
+    check_status();
+    initialized_ = true;
+    runtime_ms[0] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+int SolverGPU::cand_mode_now() const {
+    if (!cfg.reweighting) return CAND_NONE;
+    return count_ > cfg.rw_delay ? CAND_HESSIAN : CAND_REST;
+}
+
+#define WRAPD_ELEM_LAUNCH(kernel, grid, block, ...)                                        \
+    do {                                                                                   \
+        if (fp32()) kernel<float><<<grid, block, 0, st_>>>(view<float>(), __VA_ARGS__);    \
+        else kernel<double><<<grid, block, 0, st_>>>(view<double>(), __VA_ARGS__);         \
+        WRAPD_LAUNCH_CHECK();                                                              \
+        kernel_launches++;                                                                 \
+    } while (0)
+
+void SolverGPU::grad_at_x(bool write_gel) {
+    WRAPD_ELEM_LAUNCH(k_grad, blocks_for(ne, 128), 128, d_x_, d_xfix_, mat_, write_gel ? 1 : 0, d_partials_,
+                      d_counter_, d_scal_ + S_GRAD);
+}
+
+void SolverGPU::gather(double* grad, const double* gold, double* ystage, const double* sstage) {
+    if (fp32())
+        k_gather<float><<<blocks_for(nf, 256), 256, 0, st_>>>(nf, d_inc_ptr_, d_inc_, static_cast<float*>(d_gel_), ne,
+                                                              grad, gold, ystage, sstage, d_partials_, d_counter_,
+                                                              d_scal_ + S_GATHER);
+    else
+        k_gather<double><<<blocks_for(nf, 256), 256, 0, st_>>>(nf, d_inc_ptr_, d_inc_, static_cast<double*>(d_gel_),
+                                                               ne, grad, gold, ystage, sstage, d_partials_, d_counter_,
+                                                               d_scal_ + S_GATHER);
+    WRAPD_LAUNCH_CHECK();
+    kernel_launches++;
+}
+
+void SolverGPU::local_step(int cand_mode) {
+    WRAPD_ELEM_LAUNCH(k_local, blocks_for(ne, 128), 128, mat_, cfg.prox_iters, cand_mode, d_partials_, d_counter_,
+                      d_scal_ + S_LOCAL);
+}
+
+void SolverGPU::mid_candidates(bool from_x, int cand_mode) {
+    WRAPD_ELEM_LAUNCH(k_mid_candidates, blocks_for(ne, 128), 128, d_x_, d_xfix_, mat_, from_x ? 1 : 0, cand_mode);
+}
+
+void SolverGPU::apply_weights() {
+    if (fp32()) k_apply_weights<float><<<blocks_for(ne, 256), 256, 0, st_>>>(view<float>());
+    else k_apply_weights<double><<<blocks_for(ne, 256), 256, 0, st_>>>(view<double>());
+    WRAPD_LAUNCH_CHECK();
+    kernel_launches++;
+}
+
+void SolverGPU::factor() {
+    chol.factor(d_w2_, d_Di_, ne, st_);
+    kernel_launches += chol.launches_factor;
+    n_factor++;
+}
+
+void SolverGPU::sync_read() {
+    WRAPD_CUDA(cudaMemcpyAsync(h_scal_, d_scal_, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st_));
+    WRAPD_CUDA(cudaStreamSynchronize(st_));
+    n_sync++;
+}
+
+void SolverGPU::check_status() {
+    int status = 0;
+    WRAPD_CUDA(cudaMemcpyAsync(&status, chol.d_status, sizeof(int), cudaMemcpyDeviceToHost, st_));
+    WRAPD_CUDA(cudaStreamSynchronize(st_));
+    if (status != 0) {
+        WRAPD_CUDA(cudaMemsetAsync(chol.d_status, 0, sizeof(int), st_));
+        throw CudaError(status, "factorization of D^T W D hit a non-positive pivot");
+    }
+}
+
+double SolverGPU::x_error() {
+    if (!have_soln_) return 1.0;
+    // |x - x_soln| on the device with the vector kernel: q = x - x_soln, <q, q>
+    const int n = 3 * nf;
+    double one = 1.0;
+    WRAPD_CUDA(cudaMemcpyAsync(d_scal_ + S_DUMMY, &one, sizeof(double), cudaMemcpyHostToDevice, st_));
+    k_axpy_dot<<<vec_blocks(n), 256, 0, st_>>>(n, d_q_, d_x_, d_xsoln_, d_scal_ + S_DUMMY, -1.0, nullptr, nullptr,
+                                               1.0, d_partials_, d_counter_, d_scal_ + S_XERR);
+    k_axpy_dot<<<vec_blocks(n), 256, 0, st_>>>(n, d_q_, nullptr, nullptr, nullptr, 0.0, d_q_, nullptr, 1.0,
+                                               d_partials_, d_counter_, d_scal_ + S_XERR);
+    WRAPD_LAUNCH_CHECK();
+    kernel_launches += 2;
+    sync_read();
+    return std::sqrt(h_scal_[S_XERR]);
+}
+
+void SolverGPU::begin_solve() {
+    if (!initialized_) throw CudaError(WRAPD_E_STATE, "begin_solve before initialize");
+    auto t0 = std::chrono::steady_clock::now();
+    logs_ = Logs();
+    iter = 0;
+    converged_ = false;
+    for (double& r : runtime_ms) r = 0.0;
+    // setup_solve (src/ADMM.cpp:89-107): X = X_init, defo cache, dual variables
+    WRAPD_CUDA(cudaMemcpyAsync(d_x_, d_xinit_, 3 * (size_t)nf * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    grad_at_x(false);
+    WRAPD_ELEM_LAUNCH(k_init_dual, blocks_for(ne, 128), 128, d_x_, d_xfix_, mat_, d_partials_, d_counter_,
+                      d_scal_ + S_INIT);
+    sync_read();
+    curr_pe_ = h_scal_[S_INIT];
+    // log_initial_data (src/AlgorithmData.cpp:50-64)
+    logs_.objectives.push_back(h_scal_[S_GRAD + 1]);
+    logs_.flips.push_back((int)h_scal_[S_GRAD + 2]);
+    logs_.reweighted.push_back(1);
+    logs_.acc_time_s.push_back(0.0);
+    logs_.x_errors.push_back(1.0);
+    init_xerr_ = have_soln_ ? x_error() : 1.0;
+    // initialize_weights (src/GlobalStepBehavior.hpp:223-230)
+    if (cfg.reweighting) {
+        mid_candidates(false, cand_mode_now());
+        count_++;
+        apply_weights();
+        factor();
+        m_k_ = 0;
+        check_status();
+    }
+    solving_ = true;
+    runtime_ms[0] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// SplitLBFGS::minimize (deps/mcloptlib/include/MCL/SplitLBFGS.hpp:114-256) with
+// LSMethod::None (rate 1).  On entry the gradient at x is in d_gcur_ and the
+// |grad - grad_old|^2 early-return test has passed.
+int SolverGPU::lbfgs_minimize() {
+    const int M = cfg.lbfgs_m, n = 3 * nf, vb = vec_blocks(n);
+    int max_iters = cfg.global_iters, global_iter = 1;
+    bool breaking = false;
+    double* A = d_scal_ + S_ALPHA;
+    double* C = d_scal_ + S_C;
+    for (; global_iter <= max_iters; ++global_iter) {
+        const int it = std::min(M, m_k_);
+        // first loop (newest to oldest): alpha_i = rho_i <s_i, q>, q -= alpha_i y_i
+        if (it == 0) {
+            k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, d_gcur_, nullptr, nullptr, 0.0, nullptr, nullptr, 1.0,
+                                            d_partials_, d_counter_, d_scal_ + S_DUMMY);
+            kernel_launches++;
+        } else {
+            k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, d_gcur_, nullptr, nullptr, 0.0, s_[it - 1], nullptr,
+                                            rho_[it - 1], d_partials_, d_counter_, A + (it - 1));
+            for (int i = it - 2; i >= 0; --i)
+                k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, y_[i + 1], A + (i + 1), -1.0, s_[i], nullptr,
+                                                rho_[i], d_partials_, d_counter_, A + i);
+            k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, y_[0], A, -1.0, nullptr, nullptr, 1.0, d_partials_,
+                                            d_counter_, d_scal_ + S_DUMMY);
+            kernel_launches += it + 1;
+        }
+        WRAPD_LAUNCH_CHECK();
+        // q = A^-1 q, three right-hand sides at once
+        chol.solve(d_q_, st_);
+        kernel_launches += chol.launches_solve;
+        n_solve++;
+        // second loop (oldest to newest): c_i = alpha_i - rho_i <y_i, q>, q += c_i s_i; then dir = <grad, q>
+        if (it == 0) {
+            k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, nullptr, nullptr, 0.0, d_gcur_, nullptr, 1.0,
+                                            d_partials_, d_counter_, d_scal_ + S_DIR);
+            kernel_launches++;
+        } else {
+            k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, nullptr, nullptr, 0.0, y_[0], A, -rho_[0], d_partials_,
+                                            d_counter_, C);
+            for (int i = 1; i < it; ++i)
+                k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, s_[i - 1], C + (i - 1), 1.0, y_[i], A + i, -rho_[i],
+                                                d_partials_, d_counter_, C + i);
+            k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, s_[it - 1], C + (it - 1), 1.0, d_gcur_, nullptr, 1.0,
+                                            d_partials_, d_counter_, d_scal_ + S_DIR);
+            kernel_launches += it + 1;
+        }
+        // x -= q (or grad on a non-descent direction); s = x_new - x_old
+        k_xupdate<<<vb, 256, 0, st_>>>(n, d_x_, d_q_, d_gcur_, d_scal_ + S_DIR, d_sstage_);
+        WRAPD_LAUNCH_CHECK();
+        kernel_launches++;
+        // gradient at the new x; y = grad_new - grad
+        grad_at_x(true);
+        gather(d_gnew_, d_gcur_, d_ystage_, d_sstage_);
+        sync_read();
+        const double dir = h_scal_[S_DIR];
+        const double yy = h_scal_[S_GATHER], sy = h_scal_[S_GATHER + 1];
+        if (std::isnan(dir)) throw CudaError(WRAPD_E_NAN, "L-BFGS decrement is NaN");
+        if (dir <= 0.0) {
+            max_iters -= m_k_;
+            m_k_ = 0;
+        }
+        // history push: s[m_k] / y[m_k], or erase(begin) + push_back
+        if (m_k_ < M) {
+            std::swap(s_[m_k_], d_sstage_);
+            std::swap(y_[m_k_], d_ystage_);
+            rho_[m_k_] = 1.0 / sy;
+        } else {
+            double* so = s_[0];
+            double* yo = y_[0];
+            for (int i = 0; i + 1 < M; ++i) { s_[i] = s_[i + 1]; y_[i] = y_[i + 1]; rho_[i] = rho_[i + 1]; }
+            s_[M - 1] = d_sstage_; y_[M - 1] = d_ystage_; rho_[M - 1] = 1.0 / sy;
+            d_sstage_ = so; d_ystage_ = yo;
+        }
+        // grad_old <- grad, grad <- grad_new
+        double* t = d_gold_;
+        d_gold_ = d_gcur_;
+        d_gcur_ = d_gnew_;
+        d_gnew_ = t;
+        if (dir > 0.0 && (dir < cfg.kappa * m_tol_ || dir < cfg.kappa * 1.e-12)) {
+            m_k_ += 1;
+            breaking = true;
+            break;
+        }
+        if (std::fabs(yy) <= 0.0) { breaking = true; break; }
+        m_k_++;
+    }
+    m_k_ = std::min(M, m_k_);
+    return breaking ? global_iter : global_iter - 1;
+}
+
+int SolverGPU::iterate(int n, bool* conv) {
+    if (!solving_) throw CudaError(WRAPD_E_STATE, "iterate before begin_solve");
+    int done = 0;
+    *conv = converged_;
+    while (done < n && iter < cfg.max_iters && !converged_) {
+        // ---- local step: polar_update (src/TetElements.cpp:256-356) ----
+        WRAPD_CUDA(cudaEventRecord(ev_[0], st_));
+        local_step(cand_mode_now());
+        if (cfg.reweighting) count_++;
+        WRAPD_CUDA(cudaEventRecord(ev_[1], st_));
+        // ---- global step: RotAwareGS::global_step (src/GlobalStepBehavior.hpp:246-258) ----
+        if (m_k_ == 0) WRAPD_CUDA(cudaMemsetAsync(d_gold_, 0, 3 * (size_t)nf * sizeof(double), st_));
+        grad_at_x(true);
+        gather(d_gcur_, d_gold_, nullptr, nullptr);
+        sync_read();
+        const double bef = h_scal_[S_LOCAL], aft = h_scal_[S_LOCAL + 1], pe = h_scal_[S_LOCAL + 2];
+        if (h_scal_[S_LOCAL + 3] > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
+        const double dal = aft - bef + pe - curr_pe_;
+        curr_pe_ = pe;
+        const double obj_bef = h_scal_[S_GRAD];
+        m_tol_ = std::fabs(dal);
+        int its = 0;
+        if (!(h_scal_[S_GATHER] < 1.e-13)) its = lbfgs_minimize();
+        const double obj_aft = h_scal_[S_GRAD];
+        const double pe_x = h_scal_[S_GRAD + 1];
+        const int flips = (int)h_scal_[S_GRAD + 2];
+        WRAPD_CUDA(cudaEventRecord(ev_[2], st_));
+        // ---- reweighting: possibly_update_weights (src/System.cpp:50-63) ----
+        bool rw = false;
+        if (cfg.reweighting) {
+            if (cfg.rw_every > 0) {
+                rw = ((iter + 1) % cfg.rw_every) == 0;
+            } else {
+                if (fp32()) k_ratio<float><<<blocks_for(ne, 256), 256, 0, st_>>>(view<float>(), d_partials_, d_counter_, d_scal_ + S_RATIO);
+                else k_ratio<double><<<blocks_for(ne, 256), 256, 0, st_>>>(view<double>(), d_partials_, d_counter_, d_scal_ + S_RATIO);
+                WRAPD_LAUNCH_CHECK();
+                kernel_launches++;
+                sync_read();
+                rw = h_scal_[S_RATIO] > cfg.gamma;
+            }
+            if (rw) {
+                apply_weights();
+                factor();
+                m_k_ = 0;
+            }
+        }
+        WRAPD_CUDA(cudaEventRecord(ev_[3], st_));
+        WRAPD_CUDA(cudaEventSynchronize(ev_[3]));
+        if (rw) check_status();
+        float ml = 0.f, mg = 0.f, mr = 0.f;
+        WRAPD_CUDA(cudaEventElapsedTime(&ml, ev_[0], ev_[1]));
+        WRAPD_CUDA(cudaEventElapsedTime(&mg, ev_[1], ev_[2]));
+        WRAPD_CUDA(cudaEventElapsedTime(&mr, ev_[2], ev_[3]));
+        runtime_ms[1] += ml; runtime_ms[2] += mg; runtime_ms[3] += mr; runtime_ms[5] += its;
+        // ---- AlgorithmData::update_per_iter_* (src/AlgorithmData.cpp:66-83) ----
+        const int k = iter;
+        logs_.reweighted.push_back(rw ? 1 : 0);
+        logs_.ls_dal.push_back(std::fabs(dal));
+        logs_.gs_dal.push_back(std::fabs(obj_aft - obj_bef));
+        logs_.inner.push_back(its);
+        logs_.objectives.push_back(pe_x);
+        logs_.flips.push_back(flips);
+        logs_.acc_time_s.push_back((runtime_ms[1] + runtime_ms[2] + runtime_ms[3]) / 1000.0);
+        const double xe = have_soln_ ? x_error() / init_xerr_ : 1.0;
+        logs_.x_errors.push_back(xe);
+        iter = k + 1;
+        done++;
+        // ---- ADMM::converged (src/ADMM.cpp:158-169) ----
+        const double res = std::fabs(logs_.objectives[k + 1] - logs_.objectives[k]) / (std::fabs(logs_.objectives[k + 1]) + 1.0);
+        if ((logs_.flips[k + 1] == 0 && logs_.flips[k] == 0 && res < cfg.tol) || (have_soln_ && xe < 1.e-4))
+            converged_ = true;
+    }
+    *conv = converged_;
+    return done;
+}
+
+void SolverGPU::positions(double* out) {
+    std::vector<double> xp(3 * (size_t)nf);
+    WRAPD_CUDA(cudaMemcpyAsync(xp.data(), d_x_, xp.size() * sizeof(double), cudaMemcpyDeviceToHost, st_));
+    WRAPD_CUDA(cudaStreamSynchronize(st_));
+    // finish_solve (src/ADMM.cpp:171-182): X = S_free x_free + S_fix x_fix
+    for (int i = 0; i < nv; ++i)
+        for (int c = 0; c < 3; ++c)
+            out[3 * (size_t)i + c] = free_of_vert_[i] >= 0 ? xp[3 * (size_t)iperm_[free_of_vert_[i]] + c]
+                                                            : init_[3 * (size_t)i + c];
+}
+
+void SolverGPU::solve(double* out) {
+    if (!initialized_) throw CudaError(WRAPD_E_STATE, "solve before initialize");
+    begin_solve();
+    bool conv = false;
+    while (iter < cfg.max_iters && !conv) iterate(cfg.max_iters, &conv);
+    if (out) positions(out);
+}
+
+// ---- components ------------------------------------------------------------------
+void SolverGPU::download_elem(const void* d, int comps, std::vector<double>& out) {
+    const size_t n = (size_t)comps * ne;
+    std::vector<double> soa(n);
+    if (fp32() && d != d_w2_ && d != d_w2c_ && d != d_vol_) {
+        std::vector<float> f(n);
+        WRAPD_CUDA(cudaMemcpyAsync(f.data(), d, n * 4, cudaMemcpyDeviceToHost, st_));
+        WRAPD_CUDA(cudaStreamSynchronize(st_));
+        for (size_t i = 0; i < n; ++i) soa[i] = f[i];
+    } else {
+        WRAPD_CUDA(cudaMemcpyAsync(soa.data(), d, n * 8, cudaMemcpyDeviceToHost, st_));
+        WRAPD_CUDA(cudaStreamSynchronize(st_));
+    }
+    out.resize(n);
+    for (int e = 0; e < ne; ++e)
+        for (int k = 0; k < comps; ++k) out[(size_t)e * comps + k] = soa[(size_t)k * ne + e];
+}
+
+void SolverGPU::upload_elem(void* d, int comps, const double* in) {
+    const size_t n = (size_t)comps * ne;
+    std::vector<double> soa(n);
+    for (int e = 0; e < ne; ++e)
+        for (int k = 0; k < comps; ++k) soa[(size_t)k * ne + e] = in[(size_t)e * comps + k];
+    if (fp32() && d != d_w2_ && d != d_w2c_ && d != d_vol_) {
+        std::vector<float> f(soa.begin(), soa.end());
+        WRAPD_CUDA(cudaMemcpyAsync(d, f.data(), n * 4, cudaMemcpyHostToDevice, st_));
+        WRAPD_CUDA(cudaStreamSynchronize(st_));
+    } else {
+        WRAPD_CUDA(cudaMemcpyAsync(d, soa.data(), n * 8, cudaMemcpyHostToDevice, st_));
+        WRAPD_CUDA(cudaStreamSynchronize(st_));
+    }
+}
+
+void SolverGPU::get_state(const std::string& name, std::vector<double>& out) {
+    if (!initialized_) throw CudaError(WRAPD_E_STATE, "state before initialize");
+    if (name == "Z") download_elem(d_Z_, 9, out);
+    else if (name == "U") download_elem(d_U_, 9, out);
+    else if (name == "symF") download_elem(d_symF_, 9, out);
+    else if (name == "sigma") download_elem(d_sig_, 3, out);
+    else if (name == "slast") download_elem(d_slast_, 3, out);
+    else if (name == "w2") download_elem(d_w2_, 1, out);
+    else if (name == "w2c") download_elem(d_w2c_, 1, out);
+    else if (name == "vol") download_elem(d_vol_, 1, out);
+    else if (name == "xfree" || name == "grad") {
+        std::vector<double> xp(3 * (size_t)nf);
+        WRAPD_CUDA(cudaMemcpyAsync(xp.data(), name == "xfree" ? d_x_ : d_gcur_, xp.size() * 8, cudaMemcpyDeviceToHost, st_));
+        WRAPD_CUDA(cudaStreamSynchronize(st_));
+        out.resize(xp.size());
+        for (int i = 0; i < nf; ++i)
+            for (int c = 0; c < 3; ++c) out[3 * (size_t)i + c] = xp[3 * (size_t)iperm_[i] + c];
+    } else {
+        throw CudaError(WRAPD_E_INPUT, "unknown state name " + name);
+    }
+}
+
+void SolverGPU::set_state(const std::string& name, const double* in, int64_t n) {
+    if (!initialized_) throw CudaError(WRAPD_E_STATE, "state before initialize");
+    auto need = [&](int64_t m) { if (n != m) throw CudaError(WRAPD_E_INPUT, "wrong length for " + name); };
+    if (name == "Z") { need(9LL * ne); upload_elem(d_Z_, 9, in); }
+    else if (name == "U") { need(9LL * ne); upload_elem(d_U_, 9, in); }
+    else if (name == "slast") { need(3LL * ne); upload_elem(d_slast_, 3, in); }
+    else if (name == "w2") { need(ne); upload_elem(d_w2_, 1, in); }
+    else if (name == "xfree") {
+        need(3LL * nf);
+        std::vector<double> xp(3 * (size_t)nf);
+        for (int i = 0; i < nf; ++i)
+            for (int c = 0; c < 3; ++c) xp[3 * (size_t)iperm_[i] + c] = in[3 * (size_t)i + c];
+        WRAPD_CUDA(cudaMemcpyAsync(d_x_, xp.data(), xp.size() * 8, cudaMemcpyHostToDevice, st_));
+        WRAPD_CUDA(cudaStreamSynchronize(st_));
+    } else {
+        throw CudaError(WRAPD_E_INPUT, "state " + name + " is read-only");
+    }
+}
+
+void SolverGPU::update_defo_cache() {
+    grad_at_x(false);
+    sync_read();
+}
+
+double SolverGPU::polar_update(bool update_candidates) {
+    local_step(update_candidates ? cand_mode_now() : CAND_NONE);
+    if (update_candidates && cfg.reweighting) count_++;
+    sync_read();
+    if (h_scal_[S_LOCAL + 3] > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
+    const double dal = h_scal_[S_LOCAL + 1] - h_scal_[S_LOCAL] + h_scal_[S_LOCAL + 2] - curr_pe_;
+    curr_pe_ = h_scal_[S_LOCAL + 2];
+    return dal;
+}
+
+double SolverGPU::global_grad(const double* xfree, double* grad) {
+    if (xfree) set_state("xfree", xfree, 3LL * nf);
+    grad_at_x(true);
+    gather(d_gcur_, nullptr, nullptr, nullptr);
+    sync_read();
+    if (grad) {
+        std::vector<double> g;
+        get_state("grad", g);
+        std::memcpy(grad, g.data(), g.size() * sizeof(double));
+    }
+    return h_scal_[S_GRAD];
+}
+
+void SolverGPU::potential_energy(double* pe, int* flips) {
+    grad_at_x(false);
+    sync_read();
+    if (pe) *pe = h_scal_[S_GRAD + 1];
+    if (flips) *flips = (int)h_scal_[S_GRAD + 2];
+}
+
+void SolverGPU::solve_A(const double* b, double* x) {
+    if (!initialized_) throw CudaError(WRAPD_E_STATE, "solve_A before initialize");
+    std::vector<double> xp(3 * (size_t)nf);
+    for (int i = 0; i < nf; ++i)
+        for (int c = 0; c < 3; ++c) xp[3 * (size_t)iperm_[i] + c] = b[3 * (size_t)i + c];
+    WRAPD_CUDA(cudaMemcpyAsync(d_q_, xp.data(), xp.size() * 8, cudaMemcpyHostToDevice, st_));
+    chol.solve(d_q_, st_);
+    kernel_launches += chol.launches_solve;
+    WRAPD_CUDA(cudaMemcpyAsync(xp.data(), d_q_, xp.size() * 8, cudaMemcpyDeviceToHost, st_));
+    WRAPD_CUDA(cudaStreamSynchronize(st_));
+    for (int i = 0; i < nf; ++i)
+        for (int c = 0; c < 3; ++c) x[3 * (size_t)i + c] = xp[3 * (size_t)iperm_[i] + c];
+}
+
+}  // namespace wrapd

@@ -1,0 +1,109 @@
+// Host orchestration of the ADMM solve loop on one GPU (the role of the
+// reference's ADMM, RotAwareGS, SplitLBFGS, System and AlgorithmData classes:
+// src/ADMM.cpp, src/GlobalStepBehavior.hpp:196-268,
+// deps/mcloptlib/include/MCL/SplitLBFGS.hpp, src/System.cpp,
+// src/AlgorithmData.cpp).  All numeric work runs in the CUDA kernels of
+// elements.cuh and chol.cu; the host keeps only the integer bookkeeping and
+// the scalar decisions (L-BFGS history ring, early exits, reweight trigger).
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "chol.cuh"
+#include "elements.cuh"
+#include "symbolic.hpp"
+
+namespace wrapd {
+
+struct Logs {
+    std::vector<double> objectives, ls_dal, gs_dal, acc_time_s, x_errors;
+    std::vector<int> flips, reweighted, inner;
+};
+
+class SolverGPU {
+public:
+    explicit SolverGPU(const wrapd_settings& s);
+    ~SolverGPU();
+
+    void add_mesh(const double* rest, const double* init, const double* soln, int nv, const int32_t* tets, int ne,
+                  const int32_t* pins, int np);
+    void initialize();
+    void begin_solve();
+    // runs up to n iterations; returns iterations done; *converged set when the test passes
+    int iterate(int n, bool* converged);
+    void positions(double* out);
+    void solve(double* out);
+
+    // components
+    void get_state(const std::string& name, std::vector<double>& out);
+    void set_state(const std::string& name, const double* in, int64_t n);
+    void update_defo_cache();
+    double polar_update(bool update_candidates);
+    double global_grad(const double* xfree, double* grad);
+    void potential_energy(double* pe, int* flips);
+    void solve_A(const double* b, double* x);
+
+    const Logs& logs() const { return logs_; }
+    double runtime_ms[6] = {0, 0, 0, 0, 0, 0};
+    wrapd_settings cfg;
+    int nv = 0, ne = 0, np = 0, nf = 0;
+    int iter = 0;
+    CholGPU chol;
+    int64_t kernel_launches = 0;   // launches issued by this handle (element, vector and factor kernels)
+    int64_t n_factor = 0, n_solve = 0, n_sync = 0;
+
+private:
+    bool fp32() const { return cfg.precision == 1; }
+    template <typename T> ElemView<T> view();
+    void* dalloc(size_t bytes);
+    template <typename X> X* dupload(const std::vector<X>& v);
+    void sync_read();
+    void check_status();
+    void grad_at_x(bool write_gel);
+    void gather(double* grad, const double* gold, double* ystage, const double* sstage);
+    void local_step(int cand_mode);
+    void mid_candidates(bool from_x, int cand_mode);
+    void apply_weights();
+    void factor();
+    int lbfgs_minimize();
+    int cand_mode_now() const;
+    void download_elem(const void* d, int comps, std::vector<double>& out);
+    void upload_elem(void* d, int comps, const double* in);
+    double x_error();
+
+    // host mesh
+    std::vector<double> rest_, init_, soln_;
+    std::vector<int> tets_, pins_;         // pins sorted
+    std::vector<int> free_of_vert_, fix_of_vert_;
+    std::vector<int> perm_, iperm_;        // dissection order over free vertices
+    bool have_soln_ = false;
+    Material mat_{};
+    // device
+    cudaStream_t st_ = nullptr;
+    cudaEvent_t ev_[4] = {};
+    std::vector<void*> allocs_;
+    int4* d_idx_ = nullptr;
+    double *d_Di_ = nullptr, *d_vol_ = nullptr, *d_w2_ = nullptr, *d_w2c_ = nullptr;
+    void *d_Z_ = nullptr, *d_U_ = nullptr, *d_symF_ = nullptr, *d_sig_ = nullptr, *d_slast_ = nullptr, *d_gel_ = nullptr;
+    int *d_inc_ptr_ = nullptr, *d_inc_ = nullptr;
+    double *d_x_ = nullptr, *d_xfix_ = nullptr, *d_xsoln_ = nullptr, *d_xinit_ = nullptr;
+    double *d_q_ = nullptr, *d_gcur_ = nullptr, *d_gold_ = nullptr, *d_gnew_ = nullptr;
+    double *d_sstage_ = nullptr, *d_ystage_ = nullptr;
+    std::vector<double*> s_, y_;
+    std::vector<double> rho_;
+    double* d_partials_ = nullptr;
+    unsigned* d_counter_ = nullptr;
+    double* d_scal_ = nullptr;
+    double* h_scal_ = nullptr;
+    // algorithm state
+    int count_ = 0;          // reweight-delay counter (src/TetElements.cpp:404)
+    int m_k_ = 0;
+    double m_tol_ = 1e-15;
+    double curr_pe_ = 0.0;
+    double init_xerr_ = 1.0;
+    bool initialized_ = false, solving_ = false, converged_ = false;
+    Logs logs_;
+};
+
+}  // namespace wrapd

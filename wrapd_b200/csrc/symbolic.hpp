@@ -1,0 +1,54 @@
+// Host-side symbolic analysis for the GPU multifrontal Cholesky of the
+// free-vertex weighted Laplacian A = sum_e w_e^2 D_e^T D_e (the matrix the
+// reference factors with Eigen's SimplicialLDLT in
+// deps/mcloptlib/include/MCL/LinearSolver.hpp:279-298, built by
+// src/TetElements.cpp:483-510).  Integer work only, done once per mesh:
+//   * a fill-reducing order by geometric nested dissection on the rest
+//     positions (recursive median cuts along the longest box axis, one-sided
+//     vertex separators);
+//   * the separator tree as the assembly tree: every separator or leaf block
+//     is one dense front whose columns are contiguous in the new order;
+//   * each front's row structure, the relative-index maps for extend-add,
+//     the device pool offsets, and the level schedule (a front's level is one
+//     more than its highest child's, so each level can run as one launch).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace wrapd {
+
+struct Front {
+    int first = 0;             // first column (new numbering)
+    int ncols = 0;             // k
+    std::vector<int> rows;     // r struct rows (new numbering, sorted, > last column)
+    int parent = -1;
+    std::vector<int> children;
+    int level = 0;
+    int64_t f_off = 0;         // F pool: (k + r) x (k + r) column-major, ld = k + r
+    int64_t y_off = 0;         // Y pool: k x k column-major (inverse of the diagonal factor)
+    int64_t u_off = 0;         // solve update pool: r x 3
+    int64_t rel_off = 0;       // this front's map of `rows` into the parent's front rows
+    int ld() const { return ncols + static_cast<int>(rows.size()); }
+    int nrows() const { return static_cast<int>(rows.size()); }
+};
+
+struct Symbolic {
+    int n = 0;
+    std::vector<int> perm;    // new -> old
+    std::vector<int> iperm;   // old -> new
+    std::vector<Front> fronts;
+    std::vector<std::vector<int>> levels;  // front ids per level (level 0 = leaves)
+    std::vector<int> relmap;  // concatenated child -> parent relative row maps
+    int64_t f_pool = 0, y_pool = 0, u_pool = 0;
+    int max_children = 0;
+    // statistics
+    int64_t nnz_L = 0;        // stored entries of the factor panels (dense fronts)
+    double flops = 0.0;       // factorization flops (dense front model)
+};
+
+// adj_ptr/adj: symmetric adjacency of the n free vertices (no self loops).
+// coords: n x 3 positions used for the geometric cuts.  leaf: max leaf size.
+Symbolic analyse(int n, const std::vector<int>& adj_ptr, const std::vector<int>& adj,
+                 const std::vector<double>& coords, int leaf);
+
+}  // namespace wrapd
