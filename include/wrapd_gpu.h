@@ -71,8 +71,8 @@ typedef struct wrapd_settings {
     double youngs;        /* Young's modulus, 1e7 Pa (hard-coded in src/Lame.hpp:38) */
     int lbfgs_m;          /* global L-BFGS history, 6 (SplitLBFGS.hpp:41) */
     int rw_every;         /* 0: gamma rule; N > 0: reweight (and refactor) every N iterations */
-    int precision;        /* 0: FP64 throughout; 1: FP32 element math, FP64 global step */
-    int prox_mode;        /* 0: L-BFGS prox as the reference (parity mode) */
+    int precision;        /* 0: FP64 throughout; 1: FP32 local step (SVD + Newton prox), FP64 elsewhere */
+    int prox_mode;        /* 0: L-BFGS prox as the reference (parity mode); 1: Newton prox */
     int leaf_size;        /* nested-dissection leaf size for the factorization, 64 */
     int verbose;          /* -p          0 here (1 prints the reference's table) */
     int device;           /* CUDA device ordinal, 0 */

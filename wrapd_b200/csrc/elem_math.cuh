@@ -186,6 +186,9 @@ struct NH {
     // lambda_max of makePD(hessian_density(x)) = max(lambda_max(H), 0); the
     // PSD projection of src/Math.hpp:243-261 only zeroes negative eigenvalues.
     __device__ __forceinline__ T hess_lmax(const T* x) const;
+    // hessian_density before the PSD projection (src/TetElements.hpp:109-142):
+    // h = {h00, h11, h22, h01, h02, h12}
+    __device__ __forceinline__ void hess(const T* x, T* h) const;
 };
 
 // Largest eigenvalue of a symmetric 3x3 (cyclic Jacobi, at most 12 sweeps).
@@ -224,32 +227,37 @@ __device__ __forceinline__ T sym3_lmax(T a00, T a11, T a22, T a01, T a02, T a12)
 }
 
 template <typename T>
-__device__ __forceinline__ T NH<T>::hess_lmax(const T* x) const {
+__device__ __forceinline__ void NH<T>::hess(const T* x, T* h) const {
     const T J = x[0] * x[1] * x[2];
-    T h00, h11, h22, h01, h02, h12;
     if (J > T(J0)) {
         const T lj = log(J);
         const T ct = mu - lambda * (lj - T(1));
-        h00 = mu + ct / (x[0] * x[0]);
-        h11 = mu + ct / (x[1] * x[1]);
-        h22 = mu + ct / (x[2] * x[2]);
-        h01 = lambda / (x[0] * x[1]);
-        h02 = lambda / (x[0] * x[2]);
-        h12 = lambda / (x[1] * x[2]);
+        h[0] = mu + ct / (x[0] * x[0]);
+        h[1] = mu + ct / (x[1] * x[1]);
+        h[2] = mu + ct / (x[2] * x[2]);
+        h[3] = lambda / (x[0] * x[1]);
+        h[4] = lambda / (x[0] * x[2]);
+        h[5] = lambda / (x[1] * x[2]);
     } else {
         const T fJ = fJ_ext(J);
         const T dfJdJ = T(1) / T(J0) - (J - T(J0)) / (T(J0) * T(J0));
         const T lfm = lambda * fJ - mu;
         const T a = x[1] * x[2], b = x[0] * x[2], c = x[0] * x[1];
-        h00 = mu - lfm * (a / T(J0)) * (a / T(J0)) + lambda * (dfJdJ * a) * (dfJdJ * a);
-        h11 = mu - lfm * (b / T(J0)) * (b / T(J0)) + lambda * (dfJdJ * b) * (dfJdJ * b);
-        h22 = mu - lfm * (c / T(J0)) * (c / T(J0)) + lambda * (dfJdJ * c) * (dfJdJ * c);
+        h[0] = mu - lfm * (a / T(J0)) * (a / T(J0)) + lambda * (dfJdJ * a) * (dfJdJ * a);
+        h[1] = mu - lfm * (b / T(J0)) * (b / T(J0)) + lambda * (dfJdJ * b) * (dfJdJ * b);
+        h[2] = mu - lfm * (c / T(J0)) * (c / T(J0)) + lambda * (dfJdJ * c) * (dfJdJ * c);
         const T ct = lfm * (dfJdJ - J / (T(J0) * T(J0))) + lambda * J * dfJdJ * dfJdJ;
-        h01 = x[2] * ct;
-        h02 = x[1] * ct;
-        h12 = x[0] * ct;
+        h[3] = x[2] * ct;
+        h[4] = x[1] * ct;
+        h[5] = x[0] * ct;
     }
-    const T m = sym3_lmax(h00, h11, h22, h01, h02, h12);
+}
+
+template <typename T>
+__device__ __forceinline__ T NH<T>::hess_lmax(const T* x) const {
+    T h[6];
+    hess(x, h);
+    const T m = sym3_lmax(h[0], h[1], h[2], h[3], h[4], h[5]);
     return m > T(0) ? m : T(0);
 }
 
@@ -294,13 +302,14 @@ __device__ __forceinline__ T cubic_step(T fx0, T gtp, T fxa, T alpha, T fxp, T a
 }
 
 template <typename T>
-__device__ __forceinline__ T linesearch_cubic(const Prox<T>& P, const T* x, const T* p, T alpha0) {
+__device__ __forceinline__ T linesearch_cubic(const Prox<T>& P, const T* x, const T* p, T alpha0,
+                                              int max_trials = 4096) {
     if (sqrt(dot3(p, p)) <= Lim<T>::eps()) return T(1e-4);
     T alpha = alpha0, g[3];
     const T fx0 = P.value_grad(x, g);
     const T gtp = dot3(g, p);
     T fxp = fx0, alphap = alpha;
-    for (int it = 0; it < 4096; ++it) {
+    for (int it = 0; it < max_trials; ++it) {
         const T xa[3] = {x[0] + alpha * p[0], x[1] + alpha * p[1], x[2] + alpha * p[2]};
         const T fxa = P.value(xa);
         if (fxa <= fx0 + alpha * T(1e-4) * gtp) return alpha;
@@ -391,6 +400,67 @@ __device__ __forceinline__ int prox_lbfgs(const Prox<T>& P, T* x, int max_iters)
         alpha_init = T(1);
     }
     return global_iter;
+}
+
+// Newton's method on the same prox objective -- the reference's commented-out
+// alternative prox solver (src/TetElements.cpp:215, 304;
+// deps/mcloptlib/include/MCL/Newton.hpp:30-74) -- with the same cubic
+// backtracking.  The step solves (hess_density + wov I) d = -g by a 3x3
+// Cholesky; where that matrix is not positive definite the step falls back to
+// -g / (wov + |H|_max).  Stops when |g| or the step is below tol * max(1, |x|).
+// Quadratic convergence reaches the arithmetic's resolution in a few steps,
+// which is what lets the prox run in FP32 (where the L-BFGS prox's absolute
+// 1e-8 stop is below the type's resolution).
+template <typename T>
+__device__ __forceinline__ int prox_newton(const Prox<T>& P, T* x, int max_iters, T tol) {
+    int it = 0;
+    for (; it < max_iters; ++it) {
+        T g[3], h[6];
+        P.value_grad(x, g);
+        const T xs = fmax(T(1), fmax(fabs(x[0]), fmax(fabs(x[1]), fabs(x[2]))));
+        if (sqrt(dot3(g, g)) <= tol * P.wov * xs) break;
+        P.nh.hess(x, h);
+        h[0] += P.wov; h[1] += P.wov; h[2] += P.wov;
+        T d[3];
+        // 3x3 Cholesky of [h0 h3 h4; h3 h1 h5; h4 h5 h2]
+        const T l00 = h[0];
+        bool pd = l00 > T(0);
+        T L00 = 0, L10 = 0, L20 = 0, L11 = 0, L21 = 0, L22 = 0;
+        if (pd) {
+            L00 = sqrt(l00); L10 = h[3] / L00; L20 = h[4] / L00;
+            const T a11 = h[1] - L10 * L10;
+            pd = a11 > T(0);
+            if (pd) {
+                L11 = sqrt(a11); L21 = (h[5] - L20 * L10) / L11;
+                const T a22 = h[2] - L20 * L20 - L21 * L21;
+                pd = a22 > T(0);
+                if (pd) L22 = sqrt(a22);
+            }
+        }
+        if (pd) {
+            const T y0 = -g[0] / L00;
+            const T y1 = (-g[1] - L10 * y0) / L11;
+            const T y2 = (-g[2] - L20 * y0 - L21 * y1) / L22;
+            d[2] = y2 / L22;
+            d[1] = (y1 - L21 * d[2]) / L11;
+            d[0] = (y0 - L10 * d[1] - L20 * d[2]) / L00;
+        } else {
+            const T sc = P.wov + fmax(fabs(h[0]), fmax(fabs(h[1]), fabs(h[2])));
+            d[0] = -g[0] / sc; d[1] = -g[1] / sc; d[2] = -g[2] / sc;
+        }
+        if (dot3(d, g) >= T(0)) { d[0] = -g[0] / P.wov; d[1] = -g[1] / P.wov; d[2] = -g[2] / P.wov; }
+        if (sqrt(dot3(d, d)) <= tol * xs) {   // converged: take the last (tiny) step without a search
+            x[0] += d[0]; x[1] += d[1]; x[2] += d[2];
+            ++it;
+            break;
+        }
+        const T rate = linesearch_cubic(P, x, d, T(1), 40);
+        if (rate <= T(0)) break;
+        const T st[3] = {rate * d[0], rate * d[1], rate * d[2]};
+        x[0] += st[0]; x[1] += st[1]; x[2] += st[2];
+        if (sqrt(dot3(st, st)) <= tol * xs) { ++it; break; }
+    }
+    return it;
 }
 
 }  // namespace wrapd

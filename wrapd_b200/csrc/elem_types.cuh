@@ -1,0 +1,28 @@
+// Device views of the per-element state shared by the kernels and the host
+// orchestration.
+#pragma once
+#include "common.cuh"
+
+namespace wrapd {
+
+struct ElemView {
+    int ne;
+    const int4* idx;     // per vertex slot: free vertex (dissection order) or -(pin + 1)
+    const double* Di;    // 12 x ne: Di(r, a) at [(r + 3a) * ne + e], Di = (S Dm^-1)^T
+    const double* vol;
+    double* w2;
+    double* w2c;
+    double* Z;           // 9 x ne, the reference's Mat3x3 m_Zi (column-major)
+    double* U;           // 9 x ne, m_Ui
+    double* symF;        // 9 x ne, cached V diag(sigma) V^T at the last gradient point
+    double* sig;         // 3 x ne, cached singular values at the last gradient point
+    double* slast;       // 3 x ne, prox warm start (m_last_sigma)
+    double* gel;         // 12 x ne, per-element gradient rows g(a, r) at [(r + 3a) * ne + e]
+};
+
+struct Material {
+    double mu, lambda;
+    double wr, wmin, wmax;   // rest stiffness k and its beta_min / beta_max multiples
+};
+
+}  // namespace wrapd

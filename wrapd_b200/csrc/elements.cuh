@@ -1,33 +1,13 @@
 // Per-element kernels of the ADMM loop (one thread per tet) and the free-vertex
-// vectors kernels.  Element arrays are SoA: component k of element e is at
-// [k * ne + e], so every load and store of a warp is coalesced.  Element
-// state is typed T (double in FP64 mode, float for the FP32 element math of
-// mixed mode); vertex positions, weights, volumes and every reduction are FP64.
+// vector kernels.  Element arrays are SoA: component k of element e is at
+// [k * ne + e], so every load and store of a warp is coalesced.  All state is
+// stored in FP64; the local step's SVD and prox can run in FP32 (mixed mode),
+// everything else (gradient assembly, reductions, the global step) is FP64.
 #pragma once
 #include "elem_math.cuh"
+#include "elem_types.cuh"
 
 namespace wrapd {
-
-template <typename T>
-struct ElemView {
-    int ne;
-    const int4* idx;     // per vertex slot: free vertex (dissection order) or -(pin + 1)
-    const double* Di;    // 12 x ne: Di(r, a) at [(r + 3a) * ne + e], Di = (S Dm^-1)^T
-    const double* vol;
-    double* w2;
-    double* w2c;
-    T* Z;                // 9 x ne, the reference's Mat3x3 m_Zi (column-major)
-    T* U;                // 9 x ne, m_Ui
-    T* symF;             // 9 x ne, cached V diag(sigma) V^T at the last gradient point
-    T* sig;              // 3 x ne, cached singular values at the last gradient point
-    T* slast;            // 3 x ne, prox warm start (m_last_sigma)
-    T* gel;              // 12 x ne, per-element gradient rows g(a, r) at [(r + 3a) * ne + e]
-};
-
-struct Material {
-    double mu, lambda;
-    double wr, wmin, wmax;   // rest stiffness k and its beta_min / beta_max multiples
-};
 
 // Candidate-weight modes of update_all_candidate_weights (src/TetElements.cpp:391-432).
 enum { CAND_NONE = 0, CAND_REST = 1, CAND_HESSIAN = 2 };
@@ -65,21 +45,20 @@ __device__ __forceinline__ void grid_reduce(const double (&v)[NV], double* parti
 }
 
 template <typename T>
-__device__ __forceinline__ void load9(const T* a, int ne, int e, T* m) {
+__device__ __forceinline__ void load9(const double* a, int ne, int e, T* m) {
 #pragma unroll
-    for (int k = 0; k < 9; ++k) m[k] = a[(size_t)k * ne + e];
+    for (int k = 0; k < 9; ++k) m[k] = T(a[(size_t)k * ne + e]);
 }
 template <typename T>
-__device__ __forceinline__ void store9(T* a, int ne, int e, const T* m) {
+__device__ __forceinline__ void store9(double* a, int ne, int e, const T* m) {
 #pragma unroll
-    for (int k = 0; k < 9; ++k) a[(size_t)k * ne + e] = m[k];
+    for (int k = 0; k < 9; ++k) a[(size_t)k * ne + e] = double(m[k]);
 }
 
 // F = (D_free x_free + D_fix x_fix)^T, src/TetElements.cpp:568-586, computed
 // in FP64.  `split` sums free then pinned slots as the reference does for
 // partially pinned tets; otherwise the four slots in order (Di * x_local).
-template <typename T>
-__device__ __forceinline__ void deformation(const ElemView<T>& E, int e, const double* __restrict__ x,
+__device__ __forceinline__ void deformation(const ElemView& E, int e, const double* __restrict__ x,
                                             const double* __restrict__ xfix, bool split, double* F) {
     const int4 id = E.idx[e];
     const int ids[4] = {id.x, id.y, id.z, id.w};
@@ -123,8 +102,7 @@ __device__ __forceinline__ void deformation(const ElemView<T>& E, int e, const d
 // K + K^T, M = F - U diag(s) (K+K^T) V^T and g_e = w^2 Di^T M^T, plus the AL
 // value 0.5 w^2 |symF - P|^2, the potential energy and the inversion count at
 // x (src/TetElements.cpp:444-468, 598-635).  Outputs out[0..2] = value, pe, flips.
-template <typename T>
-__global__ void __launch_bounds__(128) k_grad(ElemView<T> E, const double* __restrict__ x,
+static __global__ void __launch_bounds__(128) k_grad(ElemView E, const double* __restrict__ x,
                                               const double* __restrict__ xfix, Material mat, int write_gel,
                                               double* partials, unsigned* counter, double* out) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -132,11 +110,11 @@ __global__ void __launch_bounds__(128) k_grad(ElemView<T> E, const double* __res
     if (e < E.ne) {
         double Fd[9];
         deformation(E, e, x, xfix, true, Fd);
-        T F[9], s[3], Us[9], Vs[9];
+        double F[9], s[3], Us[9], Vs[9];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) F[i] = T(Fd[i]);
+        for (int i = 0; i < 9; ++i) F[i] = double(Fd[i]);
         svd3(F, s, Us, Vs);
-        T S[9];
+        double S[9];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -146,7 +124,7 @@ __global__ void __launch_bounds__(128) k_grad(ElemView<T> E, const double* __res
         store9(E.symF, E.ne, e, S);
 #pragma unroll
         for (int i = 0; i < 3; ++i) E.sig[(size_t)i * E.ne + e] = s[i];
-        T Zm[9], Um[9], P[9];
+        double Zm[9], Um[9], P[9];
         load9(E.Z, E.ne, e, Zm);
         load9(E.U, E.ne, e, Um);
 #pragma unroll
@@ -161,9 +139,9 @@ __global__ void __launch_bounds__(128) k_grad(ElemView<T> E, const double* __res
             red[0] = (0.5 * w2) * v;
         }
         red[1] = E.vol[e] * NH<double>{mat.mu, mat.lambda}.psi_plain(double(s[0]), double(s[1]), double(s[2]));
-        red[2] = (s[0] < T(0) || s[1] < T(0) || s[2] < T(0)) ? 1.0 : 0.0;
+        red[2] = (s[0] < double(0) || s[1] < double(0) || s[2] < double(0)) ? 1.0 : 0.0;
         if (write_gel) {
-            T Tm[9], Q[9], K[9], Mm[9];
+            double Tm[9], Q[9], K[9], Mm[9];
 #pragma unroll
             for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -184,22 +162,22 @@ __global__ void __launch_bounds__(128) k_grad(ElemView<T> E, const double* __res
             for (int r = 0; r < 3; ++r)
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    T v = T(0);
+                    double v = double(0);
 #pragma unroll
                     for (int a = 0; a < 3; ++a) {
-                        const T t = M3(K, a, 0) * M3(Vs, c, 0) + M3(K, a, 1) * M3(Vs, c, 1) + M3(K, a, 2) * M3(Vs, c, 2);
+                        const double t = M3(K, a, 0) * M3(Vs, c, 0) + M3(K, a, 1) * M3(Vs, c, 1) + M3(K, a, 2) * M3(Vs, c, 2);
                         v += M3(Us, r, a) * s[a] * t;
                     }
                     M3(Mm, r, c) = F[r + 3 * c] - v;
                 }
-            const T w2t = T(w2);
+            const double w2t = double(w2);
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
                 for (int r = 0; r < 3; ++r) {
-                    T v = T(0);
+                    double v = double(0);
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) v += T(E.Di[(size_t)(c + 3 * a) * E.ne + e]) * (w2t * M3(Mm, r, c));
+                    for (int c = 0; c < 3; ++c) v += double(E.Di[(size_t)(c + 3 * a) * E.ne + e]) * (w2t * M3(Mm, r, c));
                     E.gel[(size_t)(r + 3 * a) * E.ne + e] = v;
                 }
         }
@@ -212,9 +190,8 @@ __global__ void __launch_bounds__(128) k_grad(ElemView<T> E, const double* __res
 //   grad[i] = sum over (e, a) incident to i of gel(a, :)[e].
 // With gold: d = grad - gold; ystage <- d (if given); out[0] = |d|^2 and
 // out[1] = <sstage, d> (if sstage given).
-template <typename T>
-__global__ void __launch_bounds__(256) k_gather(int nf, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
-                                                const T* __restrict__ gel, int ne, double* __restrict__ grad,
+static __global__ void __launch_bounds__(256) k_gather(int nf, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
+                                                const double* __restrict__ gel, int ne, double* __restrict__ grad,
                                                 const double* __restrict__ gold, double* __restrict__ ystage,
                                                 const double* __restrict__ sstage, double* partials,
                                                 unsigned* counter, double* out) {
@@ -225,9 +202,9 @@ __global__ void __launch_bounds__(256) k_gather(int nf, const int* __restrict__ 
         for (int t = inc_ptr[i]; t < inc_ptr[i + 1]; ++t) {
             const int c = inc[t];
             const int e = c >> 2, a = c & 3;
-            g0 += double(gel[(size_t)(0 + 3 * a) * ne + e]);
-            g1 += double(gel[(size_t)(1 + 3 * a) * ne + e]);
-            g2 += double(gel[(size_t)(2 + 3 * a) * ne + e]);
+            g0 += gel[(size_t)(0 + 3 * a) * ne + e];
+            g1 += gel[(size_t)(1 + 3 * a) * ne + e];
+            g2 += gel[(size_t)(2 + 3 * a) * ne + e];
         }
         grad[3 * (size_t)i] = g0; grad[3 * (size_t)i + 1] = g1; grad[3 * (size_t)i + 2] = g2;
         if (gold) {
@@ -243,59 +220,84 @@ __global__ void __launch_bounds__(256) k_gather(int nf, const int* __restrict__ 
 // ---- local step ---------------------------------------------------------------
 // TetElements::polar_update, NH branch (src/TetElements.cpp:284-346), fused
 // per element: S_in = (symF + U)^T, SVD, prox from the last stretches, Z and
-// U update, and the candidate weight (src/TetElements.cpp:391-432).
+// U update, and the candidate weight (src/TetElements.cpp:391-432).  C is the
+// arithmetic of the SVD and the prox (double, or float in mixed mode); loads,
+// stores, the dual update and every sum are FP64.
 // out[0..3] = bef_penalty, aft_penalty, curr_pe, negative-stretch count.
-template <typename T>
-__global__ void __launch_bounds__(128) k_local(ElemView<T> E, Material mat, int prox_iters, int cand_mode,
-                                               double* partials, unsigned* counter, double* out) {
+// prox_mode 0: the reference's L-BFGS prox; 1: Newton (prox_newton).  The FP32
+// instantiation always uses Newton (see prox_newton).
+template <typename C>
+__global__ void __launch_bounds__(128) k_local(ElemView E, Material mat, int prox_iters, int cand_mode,
+                                               int prox_mode, double* partials, unsigned* counter, double* out) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     double red[4] = {0.0, 0.0, 0.0, 0.0};
     if (e < E.ne) {
-        T S[9], Um[9], Zm[9];
+        double S[9], Um[9], Zm[9];
         load9(E.symF, E.ne, e, S);
         load9(E.U, E.ne, e, Um);
         load9(E.Z, E.ne, e, Zm);
         const double w2 = E.w2[e], vol = E.vol[e];
-        T Sin[9];
+        C Sin[9];
         double bef = 0.0;
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                M3(Sin, r, c) = M3(S, c, r) + M3(Um, c, r);
-                const double d = double(M3(S, r, c)) - (double(M3(Zm, r, c)) - double(M3(Um, r, c)));
+                M3(Sin, r, c) = C(M3(S, c, r) + M3(Um, c, r));
+                const double d = M3(S, r, c) - (M3(Zm, r, c) - M3(Um, r, c));
                 bef += d * d;
             }
         red[0] = 0.5 * w2 * bef;
-        T sg[3], Ue[9], Ve[9];
+        C sg[3], Ue[9], Ve[9];
         svd3(Sin, sg, Ue, Ve);
-        Prox<T> P;
-        P.nh.mu = T(mat.mu);
-        P.nh.lambda = T(mat.lambda);
+        Prox<C> P;
+        P.nh.mu = C(mat.mu);
+        P.nh.lambda = C(mat.lambda);
         P.x0[0] = sg[0]; P.x0[1] = sg[1]; P.x0[2] = sg[2];
-        P.wov = T(w2 / vol);
-        T xs[3];
+        P.wov = C(w2 / vol);
+        C xs[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) xs[i] = E.slast[(size_t)i * E.ne + e];
-        prox_lbfgs(P, xs, prox_iters);
+        for (int i = 0; i < 3; ++i) xs[i] = C(E.slast[(size_t)i * E.ne + e]);
+        if (sizeof(C) < sizeof(double) || prox_mode == 1)
+            prox_newton(P, xs, prox_iters, sizeof(C) < sizeof(double) ? C(8) * Lim<C>::eps() : C(1e-12));
+        else
+            prox_lbfgs(P, xs, prox_iters);
+        if (sizeof(C) < sizeof(double) &&
+            !(isfinite(xs[0]) && isfinite(xs[1]) && isfinite(xs[2]) && xs[0] >= C(0) && xs[1] >= C(0) && xs[2] >= C(0))) {
+            // FP32 range guard: near a vanishing stretch 1/x overflows in single
+            // precision; redo this element's prox in FP64 from the same inputs.
+            Prox<double> Pd;
+            Pd.nh.mu = mat.mu;
+            Pd.nh.lambda = mat.lambda;
+            Pd.x0[0] = double(sg[0]); Pd.x0[1] = double(sg[1]); Pd.x0[2] = double(sg[2]);
+            Pd.wov = w2 / vol;
+            double xd[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) E.slast[(size_t)i * E.ne + e] = xs[i];
-        red[3] = (xs[0] < T(0) || xs[1] < T(0) || xs[2] < T(0)) ? 1.0 : 0.0;
-        T So[9];
+            for (int i = 0; i < 3; ++i) xd[i] = E.slast[(size_t)i * E.ne + e];
+            prox_newton(Pd, xd, prox_iters, 1e-12);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) xs[i] = C(xd[i]);
+        }
+        double xo[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) { xo[i] = double(xs[i]); E.slast[(size_t)i * E.ne + e] = xo[i]; }
+        red[3] = (xo[0] < 0.0 || xo[1] < 0.0 || xo[2] < 0.0) ? 1.0 : 0.0;
+        C Soc[9];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
             for (int c = 0; c < 3; ++c)
-                M3(So, r, c) = M3(Ve, r, 0) * xs[0] * M3(Ue, c, 0) + M3(Ve, r, 1) * xs[1] * M3(Ue, c, 1) +
-                               M3(Ve, r, 2) * xs[2] * M3(Ue, c, 2);
-        red[2] = vol * NH<double>{mat.mu, mat.lambda}.psi_plain(double(xs[0]), double(xs[1]), double(xs[2]));
+                M3(Soc, r, c) = M3(Ve, r, 0) * xs[0] * M3(Ue, c, 0) + M3(Ve, r, 1) * xs[1] * M3(Ue, c, 1) +
+                                M3(Ve, r, 2) * xs[2] * M3(Ue, c, 2);
+        red[2] = vol * NH<double>{mat.mu, mat.lambda}.psi_plain(xo[0], xo[1], xo[2]);
         double aft = 0.0;
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
-            const double d = double(S[i]) - (double(So[i]) - double(Um[i]));
+            const double So = double(Soc[i]);
+            const double d = S[i] - (So - Um[i]);
             aft += d * d;
-            Zm[i] = So[i];
-            Um[i] = Um[i] + (S[i] - So[i]);
+            Zm[i] = So;
+            Um[i] = Um[i] + (S[i] - So);
         }
         red[1] = 0.5 * w2 * aft;
         store9(E.Z, E.ne, e, Zm);
@@ -303,8 +305,7 @@ __global__ void __launch_bounds__(128) k_local(ElemView<T> E, Material mat, int 
         if (cand_mode == CAND_REST) {
             E.w2c[e] = vol * mat.wr;
         } else if (cand_mode == CAND_HESSIAN) {
-            const double xd[3] = {double(xs[0]), double(xs[1]), double(xs[2])};
-            const double lm = NH<double>{mat.mu, mat.lambda}.hess_lmax(xd);
+            const double lm = NH<double>{mat.mu, mat.lambda}.hess_lmax(xo);
             double c = lm;
             if (lm < mat.wmin) c = mat.wmin;
             if (lm > mat.wmax) c = mat.wmax;
@@ -317,8 +318,7 @@ __global__ void __launch_bounds__(128) k_local(ElemView<T> E, Material mat, int 
 // initialize_dual_vars (src/TetElements.cpp:145-166): Z = (V diag(s) V^T)^T of
 // F(X) with all four slots read from X, U = 0; then polar_potential_energy
 // (src/TetElements.cpp:638-675) of the new Z.  out[0] = that energy.
-template <typename T>
-__global__ void __launch_bounds__(128) k_init_dual(ElemView<T> E, const double* __restrict__ x,
+static __global__ void __launch_bounds__(128) k_init_dual(ElemView E, const double* __restrict__ x,
                                                    const double* __restrict__ xfix, Material mat,
                                                    double* partials, unsigned* counter, double* out) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -326,9 +326,9 @@ __global__ void __launch_bounds__(128) k_init_dual(ElemView<T> E, const double* 
     if (e < E.ne) {
         double Fd[9];
         deformation(E, e, x, xfix, false, Fd);
-        T F[9], s[3], Us[9], Vs[9], Zm[9], Zt[9];
+        double F[9], s[3], Us[9], Vs[9], Zm[9], Zt[9];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) F[i] = T(Fd[i]);
+        for (int i = 0; i < 9; ++i) F[i] = double(Fd[i]);
         svd3(F, s, Us, Vs);
 #pragma unroll
         for (int r = 0; r < 3; ++r)
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(128) k_init_dual(ElemView<T> E, const double* 
                 M3(Zm, r, c) = M3(Vs, c, 0) * s[0] * M3(Vs, r, 0) + M3(Vs, c, 1) * s[1] * M3(Vs, r, 1) +
                                M3(Vs, c, 2) * s[2] * M3(Vs, r, 2);
         store9(E.Z, E.ne, e, Zm);
-        T zero[9] = {};
+        double zero[9] = {};
         store9(E.U, E.ne, e, zero);
 #pragma unroll
         for (int r = 0; r < 3; ++r)
@@ -351,8 +351,7 @@ __global__ void __launch_bounds__(128) k_init_dual(ElemView<T> E, const double* 
 
 // Candidate weights of midupdate_weights (src/TetElements.cpp:360-388): from
 // F(X) (from_x = 1) or from the cached singular values.
-template <typename T>
-__global__ void __launch_bounds__(128) k_mid_candidates(ElemView<T> E, const double* __restrict__ x,
+static __global__ void __launch_bounds__(128) k_mid_candidates(ElemView E, const double* __restrict__ x,
                                                         const double* __restrict__ xfix, Material mat,
                                                         int from_x, int cand_mode) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -361,9 +360,9 @@ __global__ void __launch_bounds__(128) k_mid_candidates(ElemView<T> E, const dou
     if (from_x) {
         double Fd[9];
         deformation(E, e, x, xfix, false, Fd);
-        T F[9], st[3], Us[9], Vs[9];
+        double F[9], st[3], Us[9], Vs[9];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) F[i] = T(Fd[i]);
+        for (int i = 0; i < 9; ++i) F[i] = double(Fd[i]);
         svd3(F, st, Us, Vs);
         s[0] = st[0]; s[1] = st[1]; s[2] = st[2];
     } else {
@@ -383,8 +382,7 @@ __global__ void __launch_bounds__(128) k_mid_candidates(ElemView<T> E, const dou
 }
 
 // max_wsq_ratio (src/Elements.hpp:56-69): out[0] = max_e max(w2/w2c, w2c/w2).
-template <typename T>
-__global__ void __launch_bounds__(256) k_ratio(ElemView<T> E, double* partials, unsigned* counter, double* out) {
+static __global__ void __launch_bounds__(256) k_ratio(ElemView E, double* partials, unsigned* counter, double* out) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     double red[1] = {0.0};
     if (e < E.ne) {
@@ -395,13 +393,12 @@ __global__ void __launch_bounds__(256) k_ratio(ElemView<T> E, double* partials, 
 }
 
 // update_actual_weights (src/TetElements.cpp:435-442).
-template <typename T>
-__global__ void __launch_bounds__(256) k_apply_weights(ElemView<T> E) {
+static __global__ void __launch_bounds__(256) k_apply_weights(ElemView E) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= E.ne) return;
     const double r = E.w2[e] / E.w2c[e];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) E.U[(size_t)k * E.ne + e] = T(r * double(E.U[(size_t)k * E.ne + e]));
+    for (int k = 0; k < 9; ++k) E.U[(size_t)k * E.ne + e] = r * E.U[(size_t)k * E.ne + e];
     E.w2[e] = E.w2c[e];
 }
 

@@ -1,6 +1,8 @@
 // Host orchestration of the ADMM solve loop; see solver.cuh.
 #include "solver.cuh"
 
+#include "elements.cuh"
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -26,6 +28,9 @@ enum : int {
     S_COUNT = 84
 };
 constexpr int kMaxHistory = 32;
+// Mixed mode switches its local step to FP64 when the normalized energy
+// residual drops below this (the FP32 local step's noise floor is ~1e-7).
+constexpr double kMixedSwitch = 1e-7;
 
 int blocks_for(int64_t n, int threads) { return std::max(1, ceil_div(n, threads)); }
 
@@ -71,7 +76,8 @@ SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
     if (cfg.rot_aware != 1) throw CudaError(WRAPD_E_UNSUPPORTED, "rotation-unaware global step (-ra 0) is not implemented");
     if (cfg.global_ls != 0) throw CudaError(WRAPD_E_UNSUPPORTED, "global-step line search (-global_ls 1) is not implemented");
     if (cfg.model != 0) throw CudaError(WRAPD_E_UNSUPPORTED, "only the Neo-Hookean model is implemented");
-    if (cfg.prox_mode != 0) throw CudaError(WRAPD_E_UNSUPPORTED, "prox_mode other than 0 is not implemented");
+    if (cfg.prox_mode != 0 && cfg.prox_mode != 1)
+        throw CudaError(WRAPD_E_UNSUPPORTED, "prox_mode must be 0 (L-BFGS) or 1 (Newton)");
     if (cfg.lbfgs_m < 1 || cfg.lbfgs_m > kMaxHistory) throw CudaError(WRAPD_E_INPUT, "lbfgs_m must be in [1, 32]");
     if (cfg.max_iters < 0 || cfg.global_iters < 1 || cfg.prox_iters < 1) throw CudaError(WRAPD_E_INPUT, "bad iteration limits");
     if (!(cfg.poisson > -1.0 && cfg.poisson < 0.5) || !(cfg.youngs > 0.0)) throw CudaError(WRAPD_E_INPUT, "bad material");
@@ -116,21 +122,20 @@ X* SolverGPU::dupload(const std::vector<X>& v) {
     return p;
 }
 
-template <typename T>
-ElemView<T> SolverGPU::view() {
-    ElemView<T> v;
+ElemView SolverGPU::view() {
+    ElemView v;
     v.ne = ne;
     v.idx = d_idx_;
     v.Di = d_Di_;
     v.vol = d_vol_;
     v.w2 = d_w2_;
     v.w2c = d_w2c_;
-    v.Z = static_cast<T*>(d_Z_);
-    v.U = static_cast<T*>(d_U_);
-    v.symF = static_cast<T*>(d_symF_);
-    v.sig = static_cast<T*>(d_sig_);
-    v.slast = static_cast<T*>(d_slast_);
-    v.gel = static_cast<T*>(d_gel_);
+    v.Z = d_Z_;
+    v.U = d_U_;
+    v.symF = d_symF_;
+    v.sig = d_sig_;
+    v.slast = d_slast_;
+    v.gel = d_gel_;
     return v;
 }
 
@@ -262,24 +267,25 @@ void SolverGPU::initialize() {
         }
     }
     // ---- device state ----
-    const size_t TS = fp32() ? sizeof(float) : sizeof(double);
+    const size_t TS = sizeof(double);
     d_idx_ = dupload(idx);
     d_Di_ = dupload(Di);
     d_vol_ = dupload(vol);
     d_w2_ = dupload(w2);
     d_w2c_ = static_cast<double*>(dalloc(ne * sizeof(double)));
-    d_Z_ = dalloc(9 * (size_t)ne * TS);
-    d_U_ = dalloc(9 * (size_t)ne * TS);
-    d_symF_ = dalloc(9 * (size_t)ne * TS);
-    d_sig_ = dalloc(3 * (size_t)ne * TS);
-    d_slast_ = dalloc(3 * (size_t)ne * TS);
-    d_gel_ = dalloc(12 * (size_t)ne * TS);
+    d_Z_ = static_cast<double*>(dalloc(9 * (size_t)ne * TS));
+    d_U_ = static_cast<double*>(dalloc(9 * (size_t)ne * TS));
+    d_symF_ = static_cast<double*>(dalloc(9 * (size_t)ne * TS));
+    d_sig_ = static_cast<double*>(dalloc(3 * (size_t)ne * TS));
+    d_slast_ = static_cast<double*>(dalloc(3 * (size_t)ne * TS));
+    d_gel_ = static_cast<double*>(dalloc(12 * (size_t)ne * TS));
     WRAPD_CUDA(cudaMemsetAsync(d_U_, 0, 9 * (size_t)ne * TS, st_));
     WRAPD_CUDA(cudaMemsetAsync(d_Z_, 0, 9 * (size_t)ne * TS, st_));
     {
         // m_last_sigma = (1, 1, 1)
-        if (fp32()) { std::vector<float> ones(3 * (size_t)ne, 1.0f); WRAPD_CUDA(cudaMemcpyAsync(d_slast_, ones.data(), ones.size() * 4, cudaMemcpyHostToDevice, st_)); WRAPD_CUDA(cudaStreamSynchronize(st_)); }
-        else { std::vector<double> ones(3 * (size_t)ne, 1.0); WRAPD_CUDA(cudaMemcpyAsync(d_slast_, ones.data(), ones.size() * 8, cudaMemcpyHostToDevice, st_)); WRAPD_CUDA(cudaStreamSynchronize(st_)); }
+        std::vector<double> ones(3 * (size_t)ne, 1.0);
+        WRAPD_CUDA(cudaMemcpyAsync(d_slast_, ones.data(), ones.size() * 8, cudaMemcpyHostToDevice, st_));
+        WRAPD_CUDA(cudaStreamSynchronize(st_));
     }
     d_inc_ptr_ = dupload(inc_ptr);
     d_inc_ = dupload(inc);
@@ -337,12 +343,11 @@ int SolverGPU::cand_mode_now() const {
     return count_ > cfg.rw_delay ? CAND_HESSIAN : CAND_REST;
 }
 
-#define WRAPD_ELEM_LAUNCH(kernel, grid, block, ...)                                        \
-    do {                                                                                   \
-        if (fp32()) kernel<float><<<grid, block, 0, st_>>>(view<float>(), __VA_ARGS__);    \
-        else kernel<double><<<grid, block, 0, st_>>>(view<double>(), __VA_ARGS__);         \
-        WRAPD_LAUNCH_CHECK();                                                              \
-        kernel_launches++;                                                                 \
+#define WRAPD_ELEM_LAUNCH(kernel, grid, block, ...)                    \
+    do {                                                               \
+        kernel<<<grid, block, 0, st_>>>(view(), __VA_ARGS__);          \
+        WRAPD_LAUNCH_CHECK();                                          \
+        kernel_launches++;                                             \
     } while (0)
 
 void SolverGPU::grad_at_x(bool write_gel) {
@@ -351,21 +356,22 @@ void SolverGPU::grad_at_x(bool write_gel) {
 }
 
 void SolverGPU::gather(double* grad, const double* gold, double* ystage, const double* sstage) {
-    if (fp32())
-        k_gather<float><<<blocks_for(nf, 256), 256, 0, st_>>>(nf, d_inc_ptr_, d_inc_, static_cast<float*>(d_gel_), ne,
-                                                              grad, gold, ystage, sstage, d_partials_, d_counter_,
-                                                              d_scal_ + S_GATHER);
-    else
-        k_gather<double><<<blocks_for(nf, 256), 256, 0, st_>>>(nf, d_inc_ptr_, d_inc_, static_cast<double*>(d_gel_),
-                                                               ne, grad, gold, ystage, sstage, d_partials_, d_counter_,
-                                                               d_scal_ + S_GATHER);
+    k_gather<<<blocks_for(nf, 256), 256, 0, st_>>>(nf, d_inc_ptr_, d_inc_, d_gel_, ne, grad, gold, ystage, sstage,
+                                                   d_partials_, d_counter_, d_scal_ + S_GATHER);
     WRAPD_LAUNCH_CHECK();
     kernel_launches++;
 }
 
-void SolverGPU::local_step(int cand_mode) {
-    WRAPD_ELEM_LAUNCH(k_local, blocks_for(ne, 128), 128, mat_, cfg.prox_iters, cand_mode, d_partials_, d_counter_,
-                      d_scal_ + S_LOCAL);
+void SolverGPU::local_step(int cand_mode, bool fp32_compute) {
+    if (fp32_compute)
+        k_local<float><<<blocks_for(ne, 128), 128, 0, st_>>>(view(), mat_, cfg.prox_iters, cand_mode, 1,
+                                                             d_partials_, d_counter_, d_scal_ + S_LOCAL);
+    else
+        k_local<double><<<blocks_for(ne, 128), 128, 0, st_>>>(view(), mat_, cfg.prox_iters, cand_mode,
+                                                              fp32() ? 1 : cfg.prox_mode, d_partials_, d_counter_,
+                                                              d_scal_ + S_LOCAL);
+    WRAPD_LAUNCH_CHECK();
+    kernel_launches++;
 }
 
 void SolverGPU::mid_candidates(bool from_x, int cand_mode) {
@@ -373,8 +379,7 @@ void SolverGPU::mid_candidates(bool from_x, int cand_mode) {
 }
 
 void SolverGPU::apply_weights() {
-    if (fp32()) k_apply_weights<float><<<blocks_for(ne, 256), 256, 0, st_>>>(view<float>());
-    else k_apply_weights<double><<<blocks_for(ne, 256), 256, 0, st_>>>(view<double>());
+    k_apply_weights<<<blocks_for(ne, 256), 256, 0, st_>>>(view());
     WRAPD_LAUNCH_CHECK();
     kernel_launches++;
 }
@@ -423,6 +428,7 @@ void SolverGPU::begin_solve() {
     logs_ = Logs();
     iter = 0;
     converged_ = false;
+    fp64_phase_ = false;
     for (double& r : runtime_ms) r = 0.0;
     // setup_solve (src/ADMM.cpp:89-107): X = X_init, defo cache, dual variables
     WRAPD_CUDA(cudaMemcpyAsync(d_x_, d_xinit_, 3 * (size_t)nf * sizeof(double), cudaMemcpyDeviceToDevice, st_));
@@ -548,7 +554,7 @@ int SolverGPU::iterate(int n, bool* conv) {
     while (done < n && iter < cfg.max_iters && !converged_) {
         // ---- local step: polar_update (src/TetElements.cpp:256-356) ----
         WRAPD_CUDA(cudaEventRecord(ev_[0], st_));
-        local_step(cand_mode_now());
+        local_step(cand_mode_now(), fp32() && !fp64_phase_);
         if (cfg.reweighting) count_++;
         WRAPD_CUDA(cudaEventRecord(ev_[1], st_));
         // ---- global step: RotAwareGS::global_step (src/GlobalStepBehavior.hpp:246-258) ----
@@ -574,8 +580,7 @@ int SolverGPU::iterate(int n, bool* conv) {
             if (cfg.rw_every > 0) {
                 rw = ((iter + 1) % cfg.rw_every) == 0;
             } else {
-                if (fp32()) k_ratio<float><<<blocks_for(ne, 256), 256, 0, st_>>>(view<float>(), d_partials_, d_counter_, d_scal_ + S_RATIO);
-                else k_ratio<double><<<blocks_for(ne, 256), 256, 0, st_>>>(view<double>(), d_partials_, d_counter_, d_scal_ + S_RATIO);
+                k_ratio<<<blocks_for(ne, 256), 256, 0, st_>>>(view(), d_partials_, d_counter_, d_scal_ + S_RATIO);
                 WRAPD_LAUNCH_CHECK();
                 kernel_launches++;
                 sync_read();
@@ -610,6 +615,9 @@ int SolverGPU::iterate(int n, bool* conv) {
         done++;
         // ---- ADMM::converged (src/ADMM.cpp:158-169) ----
         const double res = std::fabs(logs_.objectives[k + 1] - logs_.objectives[k]) / (std::fabs(logs_.objectives[k + 1]) + 1.0);
+        // Mixed mode refinement: once the energy moves less than FP32 can
+        // resolve, finish with FP64 local steps.
+        if (fp32() && !fp64_phase_ && res < kMixedSwitch) fp64_phase_ = true;
         if ((logs_.flips[k + 1] == 0 && logs_.flips[k] == 0 && res < cfg.tol) || (have_soln_ && xe < 1.e-4))
             converged_ = true;
     }
@@ -637,36 +645,23 @@ void SolverGPU::solve(double* out) {
 }
 
 // ---- components ------------------------------------------------------------------
-void SolverGPU::download_elem(const void* d, int comps, std::vector<double>& out) {
+void SolverGPU::download_elem(const double* d, int comps, std::vector<double>& out) {
     const size_t n = (size_t)comps * ne;
     std::vector<double> soa(n);
-    if (fp32() && d != d_w2_ && d != d_w2c_ && d != d_vol_) {
-        std::vector<float> f(n);
-        WRAPD_CUDA(cudaMemcpyAsync(f.data(), d, n * 4, cudaMemcpyDeviceToHost, st_));
-        WRAPD_CUDA(cudaStreamSynchronize(st_));
-        for (size_t i = 0; i < n; ++i) soa[i] = f[i];
-    } else {
-        WRAPD_CUDA(cudaMemcpyAsync(soa.data(), d, n * 8, cudaMemcpyDeviceToHost, st_));
-        WRAPD_CUDA(cudaStreamSynchronize(st_));
-    }
+    WRAPD_CUDA(cudaMemcpyAsync(soa.data(), d, n * 8, cudaMemcpyDeviceToHost, st_));
+    WRAPD_CUDA(cudaStreamSynchronize(st_));
     out.resize(n);
     for (int e = 0; e < ne; ++e)
         for (int k = 0; k < comps; ++k) out[(size_t)e * comps + k] = soa[(size_t)k * ne + e];
 }
 
-void SolverGPU::upload_elem(void* d, int comps, const double* in) {
+void SolverGPU::upload_elem(double* d, int comps, const double* in) {
     const size_t n = (size_t)comps * ne;
     std::vector<double> soa(n);
     for (int e = 0; e < ne; ++e)
         for (int k = 0; k < comps; ++k) soa[(size_t)k * ne + e] = in[(size_t)e * comps + k];
-    if (fp32() && d != d_w2_ && d != d_w2c_ && d != d_vol_) {
-        std::vector<float> f(soa.begin(), soa.end());
-        WRAPD_CUDA(cudaMemcpyAsync(d, f.data(), n * 4, cudaMemcpyHostToDevice, st_));
-        WRAPD_CUDA(cudaStreamSynchronize(st_));
-    } else {
-        WRAPD_CUDA(cudaMemcpyAsync(d, soa.data(), n * 8, cudaMemcpyHostToDevice, st_));
-        WRAPD_CUDA(cudaStreamSynchronize(st_));
-    }
+    WRAPD_CUDA(cudaMemcpyAsync(d, soa.data(), n * 8, cudaMemcpyHostToDevice, st_));
+    WRAPD_CUDA(cudaStreamSynchronize(st_));
 }
 
 void SolverGPU::get_state(const std::string& name, std::vector<double>& out) {
@@ -716,7 +711,7 @@ void SolverGPU::update_defo_cache() {
 }
 
 double SolverGPU::polar_update(bool update_candidates) {
-    local_step(update_candidates ? cand_mode_now() : CAND_NONE);
+    local_step(update_candidates ? cand_mode_now() : CAND_NONE, fp32() && !fp64_phase_);
     if (update_candidates && cfg.reweighting) count_++;
     sync_read();
     if (h_scal_[S_LOCAL + 3] > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");

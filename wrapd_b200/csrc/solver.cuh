@@ -11,7 +11,7 @@
 #include <vector>
 
 #include "chol.cuh"
-#include "elements.cuh"
+#include "elem_types.cuh"
 #include "symbolic.hpp"
 
 namespace wrapd {
@@ -55,21 +55,21 @@ public:
 
 private:
     bool fp32() const { return cfg.precision == 1; }
-    template <typename T> ElemView<T> view();
+    ElemView view();
     void* dalloc(size_t bytes);
     template <typename X> X* dupload(const std::vector<X>& v);
     void sync_read();
     void check_status();
     void grad_at_x(bool write_gel);
     void gather(double* grad, const double* gold, double* ystage, const double* sstage);
-    void local_step(int cand_mode);
+    void local_step(int cand_mode, bool fp32_compute);
     void mid_candidates(bool from_x, int cand_mode);
     void apply_weights();
     void factor();
     int lbfgs_minimize();
     int cand_mode_now() const;
-    void download_elem(const void* d, int comps, std::vector<double>& out);
-    void upload_elem(void* d, int comps, const double* in);
+    void download_elem(const double* d, int comps, std::vector<double>& out);
+    void upload_elem(double* d, int comps, const double* in);
     double x_error();
 
     // host mesh
@@ -85,7 +85,7 @@ private:
     std::vector<void*> allocs_;
     int4* d_idx_ = nullptr;
     double *d_Di_ = nullptr, *d_vol_ = nullptr, *d_w2_ = nullptr, *d_w2c_ = nullptr;
-    void *d_Z_ = nullptr, *d_U_ = nullptr, *d_symF_ = nullptr, *d_sig_ = nullptr, *d_slast_ = nullptr, *d_gel_ = nullptr;
+    double *d_Z_ = nullptr, *d_U_ = nullptr, *d_symF_ = nullptr, *d_sig_ = nullptr, *d_slast_ = nullptr, *d_gel_ = nullptr;
     int *d_inc_ptr_ = nullptr, *d_inc_ = nullptr;
     double *d_x_ = nullptr, *d_xfix_ = nullptr, *d_xsoln_ = nullptr, *d_xinit_ = nullptr;
     double *d_q_ = nullptr, *d_gcur_ = nullptr, *d_gold_ = nullptr, *d_gnew_ = nullptr;
@@ -103,6 +103,7 @@ private:
     double curr_pe_ = 0.0;
     double init_xerr_ = 1.0;
     bool initialized_ = false, solving_ = false, converged_ = false;
+    bool fp64_phase_ = false;   // mixed mode: switched to FP64 local steps (refinement)
     Logs logs_;
 };
 
