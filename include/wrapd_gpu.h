@@ -195,6 +195,12 @@ WRAPD_API int wrapd_prox_batch(int n, int fp32, double mu, double lambda, int ma
  * makePD(hessian_density(sigma)) (src/TetElements.cpp:414-416). */
 WRAPD_API int wrapd_hess_lmax_batch(int n, double mu, double lambda, const double* sigma, double* out);
 
+/* TetElements::potential_energy_x + inversion_count (src/TetElements.cpp:
+ * 598-635, 444-468) over a batch of stretch triples: *pe = sum vol * psi(sigma),
+ * *flips = triples with a negative entry.  sigma n x 3, vol n (host). */
+WRAPD_API int wrapd_potential_energy_batch(int n, double mu, double lambda, const double* sigma, const double* vol,
+                                           double* pe, int* flips);
+
 #ifdef __cplusplus
 }
 #endif

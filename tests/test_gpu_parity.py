@@ -82,6 +82,21 @@ def test_hessian_eigenvalue_matches_reference(golden):
     np.testing.assert_allclose(lm, g["hess_lmax"], rtol=1e-12, atol=1e-6)
 
 
+def test_potential_energy_batch_matches_oracle():
+    rng = np.random.default_rng(21)
+    n = 100_003
+    sig = np.abs(rng.normal(1.0, 0.3, size=(n, 3)))
+    sig[::97, 2] *= -1.0
+    sig[5::53] = rng.uniform(0.05, 0.3, size=sig[5::53].shape)
+    vol = rng.uniform(1e-4, 1e-3, size=n)
+    mu, lam = po.lame(E_YOUNG, NU)
+    pe, flips = capi.potential_energy_batch(mu, lam, sig, vol)
+    lib = po.load_oracle()
+    psi = np.array([lib.orc_nh_psi_plain(mu, lam, po._d(np.ascontiguousarray(s))) for s in sig])
+    assert pe == pytest.approx(float(np.sum(vol * psi)), rel=1e-12)
+    assert flips == int(np.sum((sig < 0).any(axis=1)))
+
+
 # ---- TetElements-level steps ------------------------------------------------------
 def test_tiny_step_matches_reference(golden):
     g = golden("tiny_step.npz")

@@ -77,6 +77,8 @@ SIGNATURES = [
     ("wrapd_prox_batch", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                          _dp, _dp, _dp, _dp, _ip]),
     ("wrapd_hess_lmax_batch", ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp]),
+    ("wrapd_potential_energy_batch", ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp,
+                                                     ctypes.POINTER(ctypes.c_int)]),
 ]
 
 
@@ -104,6 +106,16 @@ def prox_batch(mu, lam, sigma0, wov, start, max_iters: int = 20, fp32: bool = Fa
     _check_free(load().wrapd_prox_batch(n, int(fp32), mu, lam, max_iters, dptr(s0), dptr(w), dptr(st), dptr(out),
                                         iptr(its)))
     return out, its
+
+
+def potential_energy_batch(mu, lam, sigma, vol):
+    """(sum vol * psi(sigma), inverted count) over a batch of stretch triples."""
+    s = np.ascontiguousarray(sigma, dtype=np.float64).reshape(-1, 3)
+    v = np.ascontiguousarray(vol, dtype=np.float64).ravel()
+    pe, fl = ctypes.c_double(0.0), ctypes.c_int(0)
+    _check_free(load().wrapd_potential_energy_batch(s.shape[0], mu, lam, dptr(s), dptr(v), ctypes.byref(pe),
+                                                    ctypes.byref(fl)))
+    return pe.value, fl.value
 
 
 def hess_lmax_batch(mu, lam, sigma):

@@ -41,6 +41,24 @@ __global__ void k_prox_batch(int n, double mu, double lambda, int max_iters, con
     for (int i = 0; i < 3; ++i) out[3 * (size_t)e + i] = x[i];
 }
 
+// potential_energy_x + inversion_count over a batch of stretch triples
+// (src/TetElements.cpp:598-635, 444-468): out[0] = sum vol * psi(sigma),
+// out[1] = number of triples with a negative entry.  Deterministic two-level
+// sum: per-block partials in `partials`, added in block order by the last block.
+__global__ void __launch_bounds__(256) k_energy_batch(int n, double mu, double lambda,
+                                                      const double* __restrict__ sigma,
+                                                      const double* __restrict__ vol, double* partials,
+                                                      unsigned* counter, double* out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[2] = {0.0, 0.0};
+    if (e < n) {
+        const double* s = sigma + 3 * (size_t)e;
+        red[0] = vol[e] * NH<double>{mu, lambda}.psi_plain(s[0], s[1], s[2]);
+        red[1] = (s[0] < 0.0 || s[1] < 0.0 || s[2] < 0.0) ? 1.0 : 0.0;
+    }
+    grid_reduce<2>(red, partials, counter, out);
+}
+
 __global__ void k_hess_batch(int n, double mu, double lambda, const double* __restrict__ s, double* __restrict__ out) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
@@ -105,6 +123,27 @@ WRAPD_API int wrapd_prox_batch(int n, int fp32, double mu, double lambda, int ma
     if ((e = cudaGetLastError()) != cudaSuccess) return finish(e);
     if ((e = cudaMemcpy(out, dout.p, 3 * (size_t)n * 8, cudaMemcpyDeviceToHost)) != cudaSuccess) return finish(e);
     return finish(cudaMemcpy(iters, dit.p, (size_t)n * 4, cudaMemcpyDeviceToHost));
+}
+
+WRAPD_API int wrapd_potential_energy_batch(int n, double mu, double lambda, const double* sigma, const double* vol,
+                                           double* pe, int* flips) {
+    if (n < 0 || !pe || !flips || (n > 0 && (!sigma || !vol))) return WRAPD_E_INPUT;
+    if (n == 0) { *pe = 0.0; *flips = 0; return WRAPD_OK; }
+    const int blocks = (n + 255) / 256;
+    DevBuf ds(3 * (size_t)n * 8), dv((size_t)n * 8), dp(2 * (size_t)blocks * 8), dc(sizeof(unsigned)), dout(16);
+    if (!ds.p || !dv.p || !dp.p || !dc.p || !dout.p) return WRAPD_E_OOM;
+    cudaError_t e;
+    if ((e = cudaMemcpy(ds.p, sigma, 3 * (size_t)n * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return finish(e);
+    if ((e = cudaMemcpy(dv.p, vol, (size_t)n * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return finish(e);
+    if ((e = cudaMemset(dc.p, 0, sizeof(unsigned))) != cudaSuccess) return finish(e);
+    k_energy_batch<<<blocks, 256>>>(n, mu, lambda, ds.as<double>(), dv.as<double>(), dp.as<double>(),
+                                    dc.as<unsigned>(), dout.as<double>());
+    if ((e = cudaGetLastError()) != cudaSuccess) return finish(e);
+    double out[2];
+    if ((e = cudaMemcpy(out, dout.p, 16, cudaMemcpyDeviceToHost)) != cudaSuccess) return finish(e);
+    *pe = out[0];
+    *flips = (int)out[1];
+    return WRAPD_OK;
 }
 
 WRAPD_API int wrapd_hess_lmax_batch(int n, double mu, double lambda, const double* sigma, double* out) {

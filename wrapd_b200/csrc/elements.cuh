@@ -12,38 +12,6 @@ namespace wrapd {
 // Candidate-weight modes of update_all_candidate_weights (src/TetElements.cpp:391-432).
 enum { CAND_NONE = 0, CAND_REST = 1, CAND_HESSIAN = 2 };
 
-// ---- deterministic grid reduction: per-block partials, summed in block order
-// by whichever block finishes last. -------------------------------------------
-// out[k] = total_k, or for k = 0 with an affine epilogue: (base ? *base : 0) + scale * total_0.
-template <int NV, bool MAX = false>
-__device__ __forceinline__ void grid_reduce(const double (&v)[NV], double* partials, unsigned* counter, double* out,
-                                            const double* base = nullptr, double scale = 1.0) {
-    __shared__ double sm[32];
-    __shared__ bool last;
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        const double r = MAX ? block_max(v[k], sm) : block_sum(v[k], sm);
-        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * NV + k] = r;
-    }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        double acc = MAX ? -1.0e308 : 0.0;
-        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-            const double p = __ldcg(partials + (size_t)b * NV + k);
-            acc = MAX ? fmax(acc, p) : acc + p;
-        }
-        const double r = MAX ? block_max(acc, sm) : block_sum(acc, sm);
-        if (threadIdx.x == 0) out[k] = (k == 0 && (base || scale != 1.0)) ? (base ? *base : 0.0) + scale * r : r;
-    }
-    if (threadIdx.x == 0) *counter = 0u;
-}
-
 template <typename T>
 __device__ __forceinline__ void load9(const double* a, int ne, int e, T* m) {
 #pragma unroll
