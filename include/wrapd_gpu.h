@@ -201,6 +201,26 @@ WRAPD_API int wrapd_hess_lmax_batch(int n, double mu, double lambda, const doubl
 WRAPD_API int wrapd_potential_energy_batch(int n, double mu, double lambda, const double* sigma, const double* vol,
                                            double* pe, int* flips);
 
+/* The batched potential energy and inversion count above, for callers that may
+ * not allocate device memory: host code that has handed the GPU's memory to its
+ * own allocator, or that runs under a rule of no device allocation after
+ * start-up (an application that reserves all GPU memory up front, a loop that
+ * cannot take the implicit synchronisation of cudaMalloc).  No counterpart in
+ * the reference.
+ *   d_sigma (n x 3), d_vol (n) and d_out (2 doubles: sum vol * psi, inverted
+ *   count) are device pointers owned by the caller; the work is queued on
+ *   `stream` (a cudaStream_t, NULL for the default stream) and d_out is ready
+ *   when that stream has reached it.
+ *   Nothing is allocated: the reduction's scratch is a fixed array of about
+ *   1 MiB inside the library, held by every GPU that loads it until exit.
+ *   n may be at most 16,777,216; larger n returns WRAPD_E_INPUT without work.
+ *   The first call on each device looks up that array's device address (with
+ *   the device current); make that first call before any stream capture.
+ *   All calls share the one array: calls that overlap on the GPU (other
+ *   streams or threads) race and give wrong sums, so serialise them. */
+WRAPD_API int wrapd_potential_energy_batch_noalloc(int n, double mu, double lambda, const double* d_sigma,
+                                                   const double* d_vol, double* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,6 +79,9 @@ SIGNATURES = [
     ("wrapd_hess_lmax_batch", ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp]),
     ("wrapd_potential_energy_batch", ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp,
                                                      ctypes.POINTER(ctypes.c_int)]),
+    ("wrapd_potential_energy_batch_noalloc", ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                             ctypes.c_void_p]),
 ]
 
 

@@ -1,6 +1,7 @@
 // Batched entry points over the per-element device math (the same svd3,
 // prox_lbfgs and hess_lmax the ADMM kernels inline), for parity checks of
 // each function on its own.  Handle-free; they run on the current device.
+#include <mutex>
 #include <vector>
 
 #include "elem_math.cuh"
@@ -80,6 +81,37 @@ int finish(cudaError_t e) {
     return e == cudaSuccess ? WRAPD_OK : WRAPD_E_CUDA;
 }
 
+// ---- fixed scratch for wrapd_potential_energy_batch_noalloc ------------------
+// The reduction needs one partial pair per 256-element block plus a block
+// counter.  This array is that scratch, sized for the largest batch the entry
+// point accepts; every device that loads the library holds it (about 1 MiB)
+// until the process exits.
+constexpr int kNoAllocThreads = 256;
+constexpr int kNoAllocMaxBlocks = 65536;                       // 16,777,216 elements per call
+constexpr int kNoAllocScratch = 2 * kNoAllocMaxBlocks + 32;    // partials, then the counter
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratch];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[kMaxDevices] = {};   // device address of the array, per device
+
+// Host code may not hand `g_noalloc_scratch` to a kernel: on the host that name
+// is only a stand-in for the device variable.  Look the device address up
+// once per device, with that device current.
+int noalloc_scratch(double** out) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) { cudaGetLastError(); return WRAPD_E_CUDA; }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) { cudaGetLastError(); return WRAPD_E_CUDA; }
+        g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return WRAPD_OK;
+}
+
 }  // namespace
 }  // namespace wrapd
 
@@ -144,6 +176,28 @@ WRAPD_API int wrapd_potential_energy_batch(int n, double mu, double lambda, cons
     *pe = out[0];
     *flips = (int)out[1];
     return WRAPD_OK;
+}
+
+// Same sums as wrapd_potential_energy_batch, for callers that cannot allocate
+// device memory: inputs and the output live in caller memory on the device and
+// the reduction's scratch is the fixed array above, so this call allocates
+// nothing.  See include/wrapd_gpu.h for the contract.
+WRAPD_API int wrapd_potential_energy_batch_noalloc(int n, double mu, double lambda, const double* d_sigma,
+                                                   const double* d_vol, double* d_out, void* stream) {
+    if (n < 0 || n > kNoAllocMaxBlocks * kNoAllocThreads || !d_out || (n > 0 && (!d_sigma || !d_vol)))
+        return WRAPD_E_INPUT;
+    double* scratch = nullptr;
+    const int rc = noalloc_scratch(&scratch);
+    if (rc != WRAPD_OK) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned* counter = reinterpret_cast<unsigned*>(scratch + 2 * kNoAllocMaxBlocks);
+    // the array keeps the previous call's contents: the block counter must start at zero
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return finish(e);
+    if (n == 0) return finish(cudaMemsetAsync(d_out, 0, 2 * sizeof(double), st));
+    const int blocks = (n + kNoAllocThreads - 1) / kNoAllocThreads;
+    k_energy_batch<<<blocks, kNoAllocThreads, 0, st>>>(n, mu, lambda, d_sigma, d_vol, scratch, counter, d_out);
+    return finish(cudaGetLastError());
 }
 
 WRAPD_API int wrapd_hess_lmax_batch(int n, double mu, double lambda, const double* sigma, double* out) {
