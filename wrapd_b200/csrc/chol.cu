@@ -147,59 +147,66 @@ __global__ void k_extend_add(double* __restrict__ F, const FrontDesc* __restrict
 }
 
 // ---- panel factorization -------------------------------------------------------
-__global__ void __launch_bounds__(256) k_diag(double* __restrict__ F, double* __restrict__ Y,
-                                              const FrontDesc* __restrict__ desc, WorkList wl, int p,
-                                              int* __restrict__ status) {
-    __shared__ double L[NB][NB + 1];
-    __shared__ double Li[NB][NB + 1];
+// One warp per front: lane i owns row i of the NB x NB diagonal block (lower
+// triangle in registers); column j's pivot and multipliers are broadcast by
+// shuffles, so the factorization and the inverse need no block barriers.
+__global__ void __launch_bounds__(32) k_diag(double* __restrict__ F, double* __restrict__ Y,
+                                             const FrontDesc* __restrict__ desc, WorkList wl, int p,
+                                             int* __restrict__ status) {
     const FrontDesc d = desc[wl.d_fronts[blockIdx.x]];
     const int p0 = p * NB;
     const int nb = min(NB, d.k - p0);
     if (nb <= 0) return;
-    const int tid = threadIdx.x;
+    const int lane = threadIdx.x;
     double* Fd = F + d.f_off + p0 + (int64_t)p0 * d.ld;
-    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-        const int i = idx % NB, j = idx / NB;
-        L[i][j] = (i < nb && j < nb && i >= j) ? Fd[i + (int64_t)j * d.ld] : 0.0;
-        Li[i][j] = 0.0;
-    }
-    __syncthreads();
-    for (int j = 0; j < nb; ++j) {
-        if (tid == 0) {
-            double v = L[j][j];
-            if (!(v > 0.0)) {   // non-SPD or NaN pivot: flag it and continue with a unit pivot
-                atomicExch(status, WRAPD_E_NOT_SPD);
-                v = 1.0;
+    double a[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) a[j] = (lane < nb && j < nb && j <= lane) ? Fd[lane + (int64_t)j * d.ld] : 0.0;
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        if (j < nb) {
+            double piv = __shfl_sync(0xffffffffu, a[j], j);
+            if (!(piv > 0.0)) { bad = true; piv = 1.0; }   // non-SPD or NaN pivot: flag, continue with a unit pivot
+            const double ljj = sqrt(piv);
+            if (lane == j) a[j] = ljj;
+            if (lane > j) a[j] /= ljj;
+            const double lij = a[j];   // L(lane, j) for lane > j
+#pragma unroll
+            for (int c = j + 1; c < NB; ++c) {
+                const double lcj = __shfl_sync(0xffffffffu, a[j], c);   // L(c, j)
+                if (c < nb && lane >= c) a[c] -= lij * lcj;
             }
-            L[j][j] = sqrt(v);
-        }
-        __syncthreads();
-        for (int i = j + 1 + tid; i < nb; i += blockDim.x) L[i][j] /= L[j][j];
-        __syncthreads();
-        const int m = nb - j - 1;
-        for (int idx = tid; idx < m * m; idx += blockDim.x) {
-            const int i = j + 1 + idx % m, c = j + 1 + idx / m;
-            if (c <= i) L[i][c] -= L[i][j] * L[c][j];
-        }
-        __syncthreads();
-    }
-    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
-        const int i = idx % nb, j = idx / nb;
-        if (i >= j) Fd[i + (int64_t)j * d.ld] = L[i][j];
-    }
-    if (tid < nb) {   // column tid of inv(L) by forward substitution
-        const int c = tid;
-        for (int i = c; i < nb; ++i) {
-            double v = (i == c) ? 1.0 : 0.0;
-            for (int t = c; t < i; ++t) v -= L[i][t] * Li[t][c];
-            Li[i][c] = v / L[i][i];
         }
     }
-    __syncthreads();
+    if (bad && lane == 0) atomicExch(status, WRAPD_E_NOT_SPD);
+    if (lane < nb) {
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+            if (j < nb && j <= lane) Fd[lane + (int64_t)j * d.ld] = a[j];
+    }
+    // inv(L): lane c holds column c, computed row by row from the top
+    double inv[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) inv[i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+        if (i < nb) {
+            // inv(i, c) = (delta_ic - sum_{t<i} L(i, t) inv(t, c)) / L(i, i), for c <= i
+            double s = (lane == i) ? 1.0 : 0.0;
+#pragma unroll
+            for (int t = 0; t < NB; ++t) {
+                if (t < i) s -= __shfl_sync(0xffffffffu, a[t], i) * inv[t];
+            }
+            const double lii = __shfl_sync(0xffffffffu, a[i], i);
+            inv[i] = (lane <= i) ? s / lii : 0.0;
+        }
+    }
     double* Yp = Y + d.y_off + p0;   // row block p of Y (column-major, ld = k)
-    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
-        const int i = idx % nb, j = idx / nb;
-        Yp[i + (int64_t)(p0 + j) * d.k] = Li[i][j];
+    if (lane < nb) {
+#pragma unroll
+        for (int i = 0; i < NB; ++i)
+            if (i < nb) Yp[i + (int64_t)(p0 + lane) * d.k] = inv[i];
     }
 }
 
@@ -412,13 +419,16 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// Backward tile: partial[rt][j] = sum_{i in row tile} M(i, j) in(i), in = [z_s; -y_rows];
-// 8 warps x 8 columns, lanes over the 64 rows.
+// Backward tile: partial[rt][j] = sum_{i in row tile} M(i, j) in(i), in = [z_s; -y_rows].
+// The 64 x 64 tile is staged through shared memory with coalesced column loads,
+// then each thread sums 16 rows of one column; 4 row groups are added in order.
 __global__ void __launch_bounds__(256) k_bwd_tiles(const double* __restrict__ x, const double* __restrict__ Y,
                                                    const double* __restrict__ W, const int* __restrict__ rows,
                                                    double* __restrict__ P, const FrontDesc* __restrict__ desc,
                                                    WorkList wl) {
     __shared__ double in[TL * 3];
+    __shared__ double Ms[TL][TL + 1];
+    __shared__ double part[4][TL][3];
     const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
     const FrontDesc d = desc[wl.d_fronts[item]];
     bool wp; int ti, tj;
@@ -438,25 +448,29 @@ __global__ void __launch_bounds__(256) k_bwd_tiles(const double* __restrict__ x,
         }
         in[3 * i] = v0; in[3 * i + 1] = v1; in[3 * i + 2] = v2;
     }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int T = (d.k + TL - 1) / TL;
-    const int rt = wp ? T + ti : ti;
     const int64_t ld = wp ? d.r : d.k;
-    const double* Mb = wp ? W + d.w_off + r0 : Y + d.y_off + r0;
-    for (int jj = warp; jj < nc; jj += 8) {
-        const int j = c0 + jj;
-        const double* M = Mb + (int64_t)j * ld;
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        for (int i = lane; i < nr; i += 32) {
-            const double m = M[i];
-            a0 += m * in[3 * i]; a1 += m * in[3 * i + 1]; a2 += m * in[3 * i + 2];
-        }
-        a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
-        if (lane == 0) {
-            double* o = P + d.bp_off + 3 * ((int64_t)rt * d.k + j);
-            o[0] = a0; o[1] = a1; o[2] = a2;
-        }
+    const double* Mb = (wp ? W + d.w_off : Y + d.y_off) + r0 + (int64_t)c0 * ld;
+    for (int idx = threadIdx.x; idx < TL * TL; idx += blockDim.x) {
+        const int i = idx & (TL - 1), j = idx >> 6;
+        Ms[j][i] = (i < nr && j < nc) ? Mb[i + (int64_t)j * ld] : 0.0;
+    }
+    __syncthreads();
+    const int j = threadIdx.x & (TL - 1), grp = threadIdx.x >> 6;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll 4
+    for (int i = grp * 16; i < grp * 16 + 16; ++i) {
+        const double m = Ms[j][i];
+        a0 += m * in[3 * i]; a1 += m * in[3 * i + 1]; a2 += m * in[3 * i + 2];
+    }
+    part[grp][j][0] = a0; part[grp][j][1] = a1; part[grp][j][2] = a2;
+    __syncthreads();
+    if (threadIdx.x < nc) {
+        const int jj = threadIdx.x;
+        const int T = (d.k + TL - 1) / TL;
+        const int rt = wp ? T + ti : ti;
+        double* o = P + d.bp_off + 3 * ((int64_t)rt * d.k + c0 + jj);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) o[c] = ((part[0][jj][c] + part[1][jj][c]) + part[2][jj][c]) + part[3][jj][c];
     }
 }
 
@@ -667,7 +681,7 @@ void CholGPU::factor_launches(const double* d_w2, const double* d_Di, int ne, cu
             }
         for (size_t p = 0; p < L.diag.size(); ++p) {
             if (L.diag[p].total) {
-                k_diag<<<L.diag[p].total, 256, 0, st>>>(d_F_, d_Y_, d_desc_, L.diag[p], (int)p, d_status);
+                k_diag<<<L.diag[p].total, 32, 0, st>>>(d_F_, d_Y_, d_desc_, L.diag[p], (int)p, d_status);
                 WRAPD_LAUNCH_CHECK();
             }
             if (L.trsm[p].total) {

@@ -37,7 +37,9 @@ __global__ void k_prox_batch(int n, double mu, double lambda, int max_iters, con
 #pragma unroll
     for (int i = 0; i < 3; ++i) { P.x0[i] = T(s0[3 * (size_t)e + i]); x[i] = T(start[3 * (size_t)e + i]); }
     P.wov = T(wov[e]);
-    iters[e] = prox_lbfgs(P, x, max_iters);
+    extern __shared__ unsigned char prox_hist_raw[];   // 48 x blockDim values of T
+    T* hist = reinterpret_cast<T*>(prox_hist_raw);
+    iters[e] = prox_lbfgs(P, x, max_iters, ProxHistory<T>{hist + threadIdx.x, (int)blockDim.x});
 #pragma unroll
     for (int i = 0; i < 3; ++i) out[3 * (size_t)e + i] = x[i];
 }
@@ -145,13 +147,15 @@ WRAPD_API int wrapd_prox_batch(int n, int fp32, double mu, double lambda, int ma
     if ((e = cudaMemcpy(d0.p, sigma0, 3 * (size_t)n * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return finish(e);
     if ((e = cudaMemcpy(dw.p, wov, (size_t)n * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return finish(e);
     if ((e = cudaMemcpy(ds.p, start, 3 * (size_t)n * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return finish(e);
-    const int b = (n + 127) / 128;
+    const int b = fp32 ? (n + 127) / 128 : (n + 63) / 64;
     if (fp32)
-        k_prox_batch<float><<<b, 128>>>(n, mu, lambda, max_iters, d0.as<double>(), dw.as<double>(), ds.as<double>(),
-                                        dout.as<double>(), dit.as<int>());
+        k_prox_batch<float><<<b, 128, 48 * 128 * sizeof(float)>>>(n, mu, lambda, max_iters, d0.as<double>(),
+                                                                  dw.as<double>(), ds.as<double>(), dout.as<double>(),
+                                                                  dit.as<int>());
     else
-        k_prox_batch<double><<<b, 128>>>(n, mu, lambda, max_iters, d0.as<double>(), dw.as<double>(), ds.as<double>(),
-                                         dout.as<double>(), dit.as<int>());
+        k_prox_batch<double><<<b, 64, 48 * 64 * sizeof(double)>>>(n, mu, lambda, max_iters, d0.as<double>(),
+                                                                  dw.as<double>(), ds.as<double>(), dout.as<double>(),
+                                                                  dit.as<int>());
     if ((e = cudaGetLastError()) != cudaSuccess) return finish(e);
     if ((e = cudaMemcpy(out, dout.p, 3 * (size_t)n * 8, cudaMemcpyDeviceToHost)) != cudaSuccess) return finish(e);
     return finish(cudaMemcpy(iters, dit.p, (size_t)n * 4, cudaMemcpyDeviceToHost));

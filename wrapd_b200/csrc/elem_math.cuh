@@ -322,39 +322,52 @@ __device__ __forceinline__ T linesearch_cubic(const Prox<T>& P, const T* x, cons
     return T(-1);
 }
 
+// History of the 3-D L-BFGS: M pairs (s_i, y_i) kept outside registers, in a
+// thread-private strided slice of shared memory (entry (i, c) of s at
+// base[(6 i + c) * stride], of y at base[(6 i + 3 + c) * stride]); with the
+// thread index as offset and the block size as stride, a warp's accesses fall
+// in distinct banks.
+template <typename T>
+struct ProxHistory {
+    T* base;
+    int stride;
+    __device__ __forceinline__ T& s(int i, int c) const { return base[(6 * i + c) * stride]; }
+    __device__ __forceinline__ T& y(int i, int c) const { return base[(6 * i + 3 + c) * stride]; }
+};
+
 // Returns the iteration count (or -1 when the line search fails; x keeps the
 // last iterate, as in the reference).
 template <typename T>
-__device__ __forceinline__ int prox_lbfgs(const Prox<T>& P, T* x, int max_iters) {
+__device__ __forceinline__ int prox_lbfgs(const Prox<T>& P, T* x, int max_iters, const ProxHistory<T>& H) {
     constexpr int M = 8;
-    T s[M][3], y[M][3], alpha[M], rho[M];
+    T alpha[M], rho[M];
     T grad[3], q[3], gold[3], xold[3];
     P.value_grad(x, grad);
     T gamma_k = T(1), alpha_init = T(1);
     int global_iter = 0;
+    int head = 0;   // ring position of the oldest pair once the history is full
     for (int k = 0; k < max_iters; ++k) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) { xold[c] = x[c]; gold[c] = grad[c]; q[c] = grad[c]; }
         global_iter++;
         const int iter = k < M ? k : M;
-#pragma unroll
-        for (int i = M - 1; i >= 0; --i) {
-            if (i < iter) {
-                rho[i] = T(1) / dot3(s[i], y[i]);
-                alpha[i] = rho[i] * dot3(s[i], q);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) q[c] = q[c] - alpha[i] * y[i][c];
-            }
+        for (int i = iter - 1; i >= 0; --i) {
+            const int slot = k < M ? i : (head + i) % M;
+            const T s0 = H.s(slot, 0), s1 = H.s(slot, 1), s2 = H.s(slot, 2);
+            const T y0 = H.y(slot, 0), y1 = H.y(slot, 1), y2 = H.y(slot, 2);
+            const T r = T(1) / (s0 * y0 + s1 * y1 + s2 * y2);
+            const T a = r * (s0 * q[0] + s1 * q[1] + s2 * q[2]);
+            rho[i] = r;
+            alpha[i] = a;
+            q[0] = q[0] - a * y0; q[1] = q[1] - a * y1; q[2] = q[2] - a * y2;
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) q[c] = gamma_k * q[c];
-#pragma unroll
-        for (int i = 0; i < M; ++i) {
-            if (i < iter) {
-                const T beta = rho[i] * dot3(q, y[i]);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) q[c] = q[c] + (alpha[i] - beta) * s[i][c];
-            }
+        for (int i = 0; i < iter; ++i) {
+            const int slot = k < M ? i : (head + i) % M;
+            const T beta = rho[i] * (q[0] * H.y(slot, 0) + q[1] * H.y(slot, 1) + q[2] * H.y(slot, 2));
+            const T cf = alpha[i] - beta;
+            q[0] = q[0] + cf * H.s(slot, 0); q[1] = q[1] + cf * H.s(slot, 1); q[2] = q[2] + cf * H.s(slot, 2);
         }
         const T dir = dot3(q, grad);
         if (dir <= T(0)) {
@@ -362,6 +375,7 @@ __device__ __forceinline__ int prox_lbfgs(const Prox<T>& P, T* x, int max_iters)
             for (int c = 0; c < 3; ++c) q[c] = grad[c];
             max_iters -= k;
             k = 0;
+            head = 0;
             const T ninf = fmax(fabs(grad[0]), fmax(fabs(grad[1]), fabs(grad[2])));
             alpha_init = fmin(T(1), T(1) / ninf);
         }
@@ -379,21 +393,11 @@ __device__ __forceinline__ int prox_lbfgs(const Prox<T>& P, T* x, int max_iters)
         T st[3], yt[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) { st[c] = x[c] - xold[c]; yt[c] = grad[c] - gold[c]; }
-        if (k < M) {
+        // history push: column k while k < M, else drop the oldest (ring head)
+        const int slot = k < M ? k : head;
 #pragma unroll
-            for (int i = 0; i < M; ++i)
-                if (i == k) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) { s[i][c] = st[c]; y[i][c] = yt[c]; }
-                }
-        } else {
-#pragma unroll
-            for (int i = 0; i < M - 1; ++i)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) { s[i][c] = s[i + 1][c]; y[i][c] = y[i + 1][c]; }
-#pragma unroll
-            for (int c = 0; c < 3; ++c) { s[M - 1][c] = st[c]; y[M - 1][c] = yt[c]; }
-        }
+        for (int c = 0; c < 3; ++c) { H.s(slot, c) = st[c]; H.y(slot, c) = yt[c]; }
+        if (k >= M) head = (head + 1) % M;
         const T denom = dot3(yt, yt);
         if (fabs(denom) <= T(0)) break;
         gamma_k = dot3(st, yt) / denom;

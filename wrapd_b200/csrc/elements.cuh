@@ -195,7 +195,7 @@ static __global__ void __launch_bounds__(256) k_gather(int nf, const int* __rest
 // prox_mode 0: the reference's L-BFGS prox; 1: Newton (prox_newton).  The FP32
 // instantiation always uses Newton (see prox_newton).
 template <typename C>
-__global__ void __launch_bounds__(128) k_local(ElemView E, Material mat, int prox_iters, int cand_mode,
+__global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat, int prox_iters, int cand_mode,
                                                int prox_mode, double* partials, unsigned* counter, double* out) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     double red[4] = {0.0, 0.0, 0.0, 0.0};
@@ -226,10 +226,16 @@ __global__ void __launch_bounds__(128) k_local(ElemView E, Material mat, int pro
         C xs[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i) xs[i] = C(E.slast[(size_t)i * E.ne + e]);
-        if (sizeof(C) < sizeof(double) || prox_mode == 1)
-            prox_newton(P, xs, prox_iters, sizeof(C) < sizeof(double) ? C(8) * Lim<C>::eps() : C(1e-12));
-        else
-            prox_lbfgs(P, xs, prox_iters);
+        if constexpr (sizeof(C) == sizeof(double)) {
+            if (prox_mode == 1) {
+                prox_newton(P, xs, prox_iters, C(1e-12));
+            } else {
+                extern __shared__ double prox_hist[];   // 48 x blockDim doubles
+                prox_lbfgs(P, xs, prox_iters, ProxHistory<double>{prox_hist + threadIdx.x, (int)blockDim.x});
+            }
+        } else {
+            prox_newton(P, xs, prox_iters, C(8) * Lim<C>::eps());
+        }
         if (sizeof(C) < sizeof(double) &&
             !(isfinite(xs[0]) && isfinite(xs[1]) && isfinite(xs[2]) && xs[0] >= C(0) && xs[1] >= C(0) && xs[2] >= C(0))) {
             // FP32 range guard: near a vanishing stretch 1/x overflows in single

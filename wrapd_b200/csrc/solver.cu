@@ -28,6 +28,9 @@ enum : int {
     S_COUNT = 84
 };
 constexpr int kMaxHistory = 32;
+// Dynamic shared memory of k_local<double>: the prox L-BFGS history, 48 doubles
+// per thread of a 128-thread block.
+constexpr int kLocalHistBytes = 48 * 128 * (int)sizeof(double);
 // Mixed mode switches its local step to FP64 when the normalized energy
 // residual drops below this (the FP32 local step's noise floor is ~1e-7).
 constexpr double kMixedSwitch = 1e-7;
@@ -89,6 +92,7 @@ SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
     WRAPD_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     for (auto& e : ev_) WRAPD_CUDA(cudaEventCreate(&e));
     WRAPD_CUDA(cudaMallocHost(&h_scal_, S_COUNT * sizeof(double)));
+    WRAPD_CUDA(cudaFuncSetAttribute(k_local<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLocalHistBytes));
     // Lame(E, nu), src/Lame.hpp:50-53; k = 2.0066 mu + 1.0122 lambda, src/TetElements.cpp:84
     mat_.mu = cfg.youngs / (2.0 * (1.0 + cfg.poisson));
     mat_.lambda = cfg.youngs * cfg.poisson / ((1.0 + cfg.poisson) * (1.0 - 2.0 * cfg.poisson));
@@ -367,7 +371,7 @@ void SolverGPU::local_step(int cand_mode, bool fp32_compute) {
         k_local<float><<<blocks_for(ne, 128), 128, 0, st_>>>(view(), mat_, cfg.prox_iters, cand_mode, 1,
                                                              d_partials_, d_counter_, d_scal_ + S_LOCAL);
     else
-        k_local<double><<<blocks_for(ne, 128), 128, 0, st_>>>(view(), mat_, cfg.prox_iters, cand_mode,
+        k_local<double><<<blocks_for(ne, 128), 128, kLocalHistBytes, st_>>>(view(), mat_, cfg.prox_iters, cand_mode,
                                                               fp32() ? 1 : cfg.prox_mode, d_partials_, d_counter_,
                                                               d_scal_ + S_LOCAL);
     WRAPD_LAUNCH_CHECK();
