@@ -8,8 +8,12 @@
 //                its inverse Li (stored as a diagonal block of Y);
 //   trsm         the panel rows below the block, P <- P Li^T, and the inverse
 //                row block Y[p, 0:p0] <- Li Y[p, 0:p0] (FP64 DMMA tiles);
-//   update       trailing lower triangle  F -= P P^T  and the inverse rows
-//                Y[p+1:, 0:p0+nb] -= P_k Y[p, 0:p0+nb]  (FP64 DMMA tiles);
+//   update       blocked right-looking: inside the current OB-column block,
+//                F[j0:, j0:be] -= P P^T and Y[j0:be, 0:j0] -= P Y[p, 0:j0];
+//                after a block's last panel, the deferred trailing update
+//                F[be:, be:] -= B B^T and Y[be:, 0:be] -= B Y[block, 0:be] with
+//                K = OB (FP64 DMMA tiles, K-looped), so the large trailing
+//                matrix is read and written once per OB columns, not per panel;
 //   then         W = L_rs Y for the level's fronts (FP64 DMMA, K-looped).
 // A is assembled once per factorization straight into the zeroed F pool.
 //
@@ -25,6 +29,7 @@ namespace wrapd {
 namespace {
 
 constexpr int NB = 32;        // panel width
+constexpr int OB = 128;       // outer block: trailing updates beyond it are deferred to one K = OB update
 constexpr int TL = 64;        // output tile of the DMMA kernels
 constexpr int SLD = NB + 4;   // smem row pitch (doubles) for [row][k] operand tiles
 constexpr int GEMM_THREADS = 128;
@@ -244,47 +249,58 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_trsm(double* __restrict__ F, d
     }
 }
 
-// Items: for each front, nF trailing tiles (lower triangle) then nY inverse tiles.
+// Tile t of a job: kind 0 enumerates lower tiles (ti >= tj) column by column,
+// kind 1 the full rectangle.
+__device__ __forceinline__ void job_tile(const GemmJob& jb, int t, int& ti, int& tj) {
+    const int Tr = (jb.r1 - jb.r0 + TL - 1) / TL, Tc = (jb.c1 - jb.c0 + TL - 1) / TL;
+    if (jb.kind == 1) { ti = t / Tc; tj = t % Tc; return; }
+    for (tj = 0; tj < Tc; ++tj) {
+        const int cnt = Tr - tj;
+        if (t < cnt) { ti = tj + t; return; }
+        t -= cnt;
+    }
+    ti = Tr;   // not reached for valid t
+}
+
 __global__ void __launch_bounds__(GEMM_THREADS) k_update(double* __restrict__ F, double* __restrict__ Y,
-                                                         const FrontDesc* __restrict__ desc, WorkList wl,
-                                                         const int* __restrict__ nF_of_item, int p) {
+                                                         const FrontDesc* __restrict__ desc, JobList jl) {
     __shared__ double As[TL * SLD];
     __shared__ double Bs[TL * SLD];
-    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
-    const FrontDesc d = desc[wl.d_fronts[item]];
-    int t = blockIdx.x - wl.d_prefix[item];
-    const int nF = nF_of_item[item];
-    const int p0 = p * NB, nb = min(NB, d.k - p0), j0 = p0 + nb;
-    if (nb <= 0) return;
-    const int K4 = (nb + 3) & ~3;
-    const double* P = F + d.f_off + j0 + (int64_t)p0 * d.ld;   // panel rows j0.. (column-major)
+    const int item = find_item(jl.d_prefix, jl.n, blockIdx.x);
+    const GemmJob jb = jl.d_jobs[item];
+    const FrontDesc d = desc[jb.front];
+    int ti, tj;
+    job_tile(jb, blockIdx.x - jl.d_prefix[item], ti, tj);
+    const int r0 = jb.r0 + ti * TL, c0 = jb.c0 + tj * TL;
+    const int M = min(TL, jb.r1 - r0), N = min(TL, jb.c1 - c0);
     double acc[4][4][2] = {};
-    if (t < nF) {
-        // lower-triangular tile index -> (ti, tj), ti >= tj
-        int ti = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-        while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
-        while (ti * (ti + 1) / 2 > t) --ti;
-        const int tj = t - ti * (ti + 1) / 2;
-        const int m = d.ld - j0;
-        const int r0 = ti * TL, c0 = tj * TL;
-        load_tile(As, P + r0, 1, d.ld, min(m - r0, TL), nb, K4);
-        load_tile(Bs, P + c0, 1, d.ld, min(m - c0, TL), nb, K4);
+    for (int k0 = jb.k0; k0 < jb.k1; k0 += NB) {
+        const int K = min(NB, jb.k1 - k0), K4 = (K + 3) & ~3;
+        load_tile(As, F + d.f_off + r0 + (int64_t)k0 * d.ld, 1, d.ld, M, K, K4);
+        if (jb.kind == 0) load_tile(Bs, F + d.f_off + c0 + (int64_t)k0 * d.ld, 1, d.ld, N, K, K4);
+        else load_tile(Bs, Y + d.y_off + k0 + (int64_t)c0 * d.k, d.k, 1, N, K, K4);
         __syncthreads();
         tile_mma(As, Bs, K4, acc);
-        double* C = F + d.f_off + (j0 + r0) + (int64_t)(j0 + c0) * d.ld;
-        tile_store(C, 1, d.ld, min(m - r0, TL), min(m - c0, TL), ti == tj ? EPI_SUB_LOWER : EPI_SUB, acc);
+        __syncthreads();
+    }
+    if (jb.kind == 0) {
+        // on tiles crossing the diagonal keep only row >= column (global indices)
+        double* C = F + d.f_off + r0 + (int64_t)c0 * d.ld;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const int wm = warp & 1, wn = warp >> 1;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int row = wm * 32 + i * 8 + (lane >> 2);
+                    const int col = wn * 32 + j * 8 + 2 * (lane & 3) + h;
+                    if (row >= M || col >= N || r0 + row < c0 + col) continue;
+                    C[row + (int64_t)col * d.ld] -= acc[i][j][h];
+                }
     } else {
-        t -= nF;
-        const int mY = d.k - j0, nY = j0;
-        const int tc = (nY + TL - 1) / TL;
-        const int ti = t / tc, tj = t % tc;
-        const int r0 = ti * TL, c0 = tj * TL;
-        load_tile(As, P + r0, 1, d.ld, min(mY - r0, TL), nb, K4);
-        load_tile(Bs, Y + d.y_off + p0 + (int64_t)c0 * d.k, d.k, 1, min(nY - c0, TL), nb, K4);
-        __syncthreads();
-        tile_mma(As, Bs, K4, acc);
-        double* C = Y + d.y_off + (j0 + r0) + (int64_t)c0 * d.k;
-        tile_store(C, 1, d.k, min(mY - r0, TL), min(nY - c0, TL), EPI_SUB, acc);
+        tile_store(Y + d.y_off + r0 + (int64_t)c0 * d.k, 1, d.k, M, N, EPI_SUB, acc);
     }
 }
 
@@ -510,6 +526,28 @@ X* CholGPU::upload(const std::vector<X>& v, cudaStream_t st) {
     return p;
 }
 
+JobList CholGPU::make_jobs(const std::vector<GemmJob>& jobs, cudaStream_t st) {
+    JobList l;
+    std::vector<GemmJob> keep;
+    std::vector<int> pre(1, 0);
+    for (const GemmJob& jb : jobs) {
+        const int Tr = ceil_div(jb.r1 - jb.r0, TL), Tc = ceil_div(jb.c1 - jb.c0, TL);
+        if (Tr <= 0 || Tc <= 0 || jb.k1 <= jb.k0) continue;
+        int tiles = 0;
+        if (jb.kind == 1) tiles = Tr * Tc;
+        else for (int tj = 0; tj < Tc; ++tj) tiles += std::max(0, Tr - tj);
+        if (tiles <= 0) continue;
+        keep.push_back(jb);
+        pre.push_back(pre.back() + tiles);
+    }
+    l.n = static_cast<int>(keep.size());
+    l.total = pre.back();
+    if (l.n == 0) return l;
+    l.d_jobs = upload(keep, st);
+    l.d_prefix = upload(pre, st);
+    return l;
+}
+
 WorkList CholGPU::make_list(const std::vector<int>& fronts, const std::vector<int>& ctas, cudaStream_t st) {
     WorkList w;
     std::vector<int> f, pre(1, 0);
@@ -604,22 +642,28 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         }
         const int steps = ceil_div(L.kmax, NB);
         for (int p = 0; p < steps; ++p) {
-            std::vector<int> act, cd, ct, nP, cu, nF;
+            std::vector<int> act, cd, ct, nP;
+            std::vector<GemmJob> jobs;
             for (int f : fs) {
                 const FrontDesc& d = h_desc_[f];
                 const int p0 = p * NB;
                 if (d.k <= p0) continue;
                 const int nb = std::min(NB, d.k - p0), j0 = p0 + nb;
                 const int m = d.ld - j0;
-                const int T = ceil_div(m, TL);
-                const int mY = d.k - j0, nY = j0;
-                const int tY = (mY > 0) ? ceil_div(mY, TL) * ceil_div(nY, TL) : 0;
+                const int bs = (p0 / OB) * OB, be = std::min(d.k, bs + OB);
                 act.push_back(f);
                 cd.push_back(1);
                 nP.push_back(ceil_div(m, TL));
                 ct.push_back(ceil_div(m, TL) + ceil_div(p0, TL));
-                cu.push_back(T * (T + 1) / 2 + tY);
-                nF.push_back(T * (T + 1) / 2);
+                if (j0 < be) {
+                    // inside the outer block: only the block's remaining columns, K = this panel
+                    jobs.push_back(GemmJob{f, 0, j0, d.ld, j0, be, p0, j0});
+                    jobs.push_back(GemmJob{f, 1, j0, be, 0, j0, p0, j0});
+                } else {
+                    // the block's last panel: the deferred trailing update, K = the whole block
+                    jobs.push_back(GemmJob{f, 0, be, d.ld, be, d.ld, bs, be});
+                    jobs.push_back(GemmJob{f, 1, be, d.k, 0, be, bs, be});
+                }
             }
             L.diag.push_back(make_list(act, cd, st));
             std::vector<int> actt, ct2, nP2;
@@ -627,11 +671,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
                 if (ct[i] > 0) { actt.push_back(act[i]); ct2.push_back(ct[i]); nP2.push_back(nP[i]); }
             L.trsm.push_back(make_list(actt, ct2, st));
             L.trsm_split.push_back(nP2);
-            std::vector<int> act2, cu2, nF2;
-            for (size_t i = 0; i < act.size(); ++i)
-                if (cu[i] > 0) { act2.push_back(act[i]); cu2.push_back(cu[i]); nF2.push_back(nF[i]); }
-            L.update.push_back(make_list(act2, cu2, st));
-            L.update_split.push_back(nF2);
+            L.update.push_back(make_jobs(jobs, st));
             launches_factor += 1 + (L.trsm.back().total ? 1 : 0) + (L.update.back().total ? 1 : 0);
         }
         std::vector<int> wg(fs.size()), ft(fs.size()), fr(fs.size()), bc(fs.size());
@@ -651,13 +691,10 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         L.bwd_cols = make_list(fs, bc, st);
         launches_solve += 5;
     }
-    upd_nF_.clear();
     trsm_nP_.clear();
     for (auto& L : levels_) {
-        std::vector<int*> v, w;
-        for (auto& nF : L.update_split) v.push_back(nF.empty() ? nullptr : upload(nF, st));
+        std::vector<int*> w;
         for (auto& nP : L.trsm_split) w.push_back(nP.empty() ? nullptr : upload(nP, st));
-        upd_nF_.push_back(v);
         trsm_nP_.push_back(w);
     }
     WRAPD_CUDA(cudaStreamSynchronize(st));
@@ -689,8 +726,7 @@ void CholGPU::factor_launches(const double* d_w2, const double* d_Di, int ne, cu
                 WRAPD_LAUNCH_CHECK();
             }
             if (L.update[p].total) {
-                k_update<<<L.update[p].total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_desc_, L.update[p],
-                                                                     upd_nF_[l][p], (int)p);
+                k_update<<<L.update[p].total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_desc_, L.update[p]);
                 WRAPD_LAUNCH_CHECK();
             }
         }

@@ -30,6 +30,21 @@ struct FrontDesc {
     int nchild, child0, child1, pad;
 };
 
+// A trailing-update job of the blocked factorization: C -= A B'^T over a K range
+// of panel columns.  kind 0: C is F[r0:r1, c0:c1] of the front (lower part
+// where rows and columns overlap), A = F[r0:r1, k0:k1], B' = F[c0:c1, k0:k1];
+// kind 1: C is Y[r0:r1, c0:c1], A = F[r0:r1, k0:k1], B'(j, t) = Y[k0 + t, c0 + j].
+struct GemmJob {
+    int front, kind, r0, r1, c0, c1, k0, k1;
+};
+
+struct JobList {
+    int n = 0;
+    int total = 0;       // total CTAs (64 x 64 output tiles)
+    GemmJob* d_jobs = nullptr;
+    int* d_prefix = nullptr;
+};
+
 // One launch's work: `n` fronts (ids), each owning prefix[i+1]-prefix[i] CTAs.
 struct WorkList {
     int n = 0;
@@ -78,8 +93,8 @@ private:
         std::vector<WorkList> extend;    // per child slot: CTAs over child columns
         std::vector<WorkList> diag;      // per panel step
         std::vector<WorkList> trsm;      // per panel step (panel row tiles + Y row-block tiles)
-        std::vector<WorkList> update;    // per panel step (F trailing tiles + Y tiles)
-        std::vector<std::vector<int>> trsm_split, update_split;  // per step: first-kind tiles per item
+        std::vector<JobList> update;     // per panel step: blocked trailing-update jobs (F and Y)
+        std::vector<std::vector<int>> trsm_split;  // per step: panel-row tiles per item
         WorkList wgemm;                  // W = L_rs Y tiles
         WorkList fwd_tiles, fwd_rows;    // solve forward: [Y; W] t tiles, row reduction
         WorkList bwd_tiles, bwd_cols;    // solve backward: [Y; W]^T in tiles, column reduction
@@ -106,7 +121,8 @@ private:
     void solve_launches(double* d_x, cudaStream_t st);
     std::vector<void*> allocs_;
     std::vector<FrontDesc> h_desc_;
-    std::vector<std::vector<int*>> upd_nF_, trsm_nP_;   // per level, per panel step: first-kind tile counts
+    std::vector<std::vector<int*>> trsm_nP_;   // per level, per panel step: panel-row tile counts
+    JobList make_jobs(const std::vector<GemmJob>& jobs, cudaStream_t st);
 
     template <typename X> X* upload(const std::vector<X>& v, cudaStream_t st);
     WorkList make_list(const std::vector<int>& fronts, const std::vector<int>& ctas, cudaStream_t st);
