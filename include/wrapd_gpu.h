@@ -144,6 +144,16 @@ WRAPD_API int wrapd_get_info(wrapd_handle* h, double out[8]);
  * synchronisations.  (No reference counterpart: instrumentation.) */
 WRAPD_API int wrapd_get_counters(wrapd_handle* h, int64_t out[4]);
 
+/* Per-phase device timeline (no reference counterpart; the reference's
+ * MicroTimer splits only local/global/refactor).  wrapd_set_profiling(h, 1)
+ * records CUDA events at phase boundaries of every later iteration;
+ * wrapd_get_profile returns accumulated ms and interval counts for the slots
+ * 0 local step, 1 gradient + gather, 2 two-loop and x-update vector kernels,
+ * 3 triangular solves, 4 (unused), 5 device idle around host synchronisations
+ * and the reweight/refactor phase. */
+WRAPD_API int wrapd_set_profiling(wrapd_handle* h, int on);
+WRAPD_API int wrapd_get_profile(wrapd_handle* h, double ms[6], int64_t counts[6]);
+
 WRAPD_API const char* wrapd_last_error(const wrapd_handle* h);
 WRAPD_API void wrapd_destroy(wrapd_handle* h);
 

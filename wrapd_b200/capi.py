@@ -63,6 +63,8 @@ SIGNATURES = [
     ("wrapd_get_runtime", ctypes.c_int, [ctypes.c_void_p, _dp]),
     ("wrapd_get_info", ctypes.c_int, [ctypes.c_void_p, _dp]),
     ("wrapd_get_counters", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    ("wrapd_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("wrapd_get_profile", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_int64)]),
     ("wrapd_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("wrapd_destroy", None, [ctypes.c_void_p]),
     ("wrapd_get_state", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, _dp, ctypes.c_int64,

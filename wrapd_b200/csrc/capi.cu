@@ -166,6 +166,17 @@ int wrapd_get_counters(wrapd_handle* h, int64_t out[4]) {
     });
 }
 
+int wrapd_set_profiling(wrapd_handle* h, int on) {
+    return guarded(h, [&](wrapd::SolverGPU& s) { s.profiling = on != 0; });
+}
+
+int wrapd_get_profile(wrapd_handle* h, double ms[6], int64_t counts[6]) {
+    if (!ms || !counts) return WRAPD_E_INPUT;
+    return guarded(h, [&](wrapd::SolverGPU& s) {
+        for (int i = 0; i < 6; ++i) { ms[i] = s.profile_ms[i]; counts[i] = s.profile_n[i]; }
+    });
+}
+
 const char* wrapd_last_error(const wrapd_handle* h) {
     if (!h) return g_create_error.c_str();
     return h->err.c_str();

@@ -152,66 +152,61 @@ __global__ void k_extend_add(double* __restrict__ F, const FrontDesc* __restrict
 }
 
 // ---- panel factorization -------------------------------------------------------
-// One warp per front: lane i owns row i of the NB x NB diagonal block (lower
-// triangle in registers); column j's pivot and multipliers are broadcast by
-// shuffles, so the factorization and the inverse need no block barriers.
-__global__ void __launch_bounds__(32) k_diag(double* __restrict__ F, double* __restrict__ Y,
-                                             const FrontDesc* __restrict__ desc, WorkList wl, int p,
-                                             int* __restrict__ status) {
+// One CTA per front: Cholesky of the NB x NB diagonal block in shared memory
+// and its inverse Li, written as the diagonal block of Y.
+__global__ void __launch_bounds__(256) k_diag(double* __restrict__ F, double* __restrict__ Y,
+                                              const FrontDesc* __restrict__ desc, WorkList wl, int p,
+                                              int* __restrict__ status) {
+    __shared__ double L[NB][NB + 1];
+    __shared__ double Li[NB][NB + 1];
     const FrontDesc d = desc[wl.d_fronts[blockIdx.x]];
     const int p0 = p * NB;
     const int nb = min(NB, d.k - p0);
     if (nb <= 0) return;
-    const int lane = threadIdx.x;
+    const int tid = threadIdx.x;
     double* Fd = F + d.f_off + p0 + (int64_t)p0 * d.ld;
-    double a[NB];
-#pragma unroll
-    for (int j = 0; j < NB; ++j) a[j] = (lane < nb && j < nb && j <= lane) ? Fd[lane + (int64_t)j * d.ld] : 0.0;
-    bool bad = false;
-#pragma unroll
-    for (int j = 0; j < NB; ++j) {
-        if (j < nb) {
-            double piv = __shfl_sync(0xffffffffu, a[j], j);
-            if (!(piv > 0.0)) { bad = true; piv = 1.0; }   // non-SPD or NaN pivot: flag, continue with a unit pivot
-            const double ljj = sqrt(piv);
-            if (lane == j) a[j] = ljj;
-            if (lane > j) a[j] /= ljj;
-            const double lij = a[j];   // L(lane, j) for lane > j
-#pragma unroll
-            for (int c = j + 1; c < NB; ++c) {
-                const double lcj = __shfl_sync(0xffffffffu, a[j], c);   // L(c, j)
-                if (c < nb && lane >= c) a[c] -= lij * lcj;
+    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+        const int i = idx % NB, j = idx / NB;
+        L[i][j] = (i < nb && j < nb && i >= j) ? Fd[i + (int64_t)j * d.ld] : 0.0;
+        Li[i][j] = 0.0;
+    }
+    __syncthreads();
+    for (int j = 0; j < nb; ++j) {
+        if (tid == 0) {
+            double v = L[j][j];
+            if (!(v > 0.0)) {   // non-SPD or NaN pivot: flag it and continue with a unit pivot
+                atomicExch(status, WRAPD_E_NOT_SPD);
+                v = 1.0;
             }
+            L[j][j] = sqrt(v);
+        }
+        __syncthreads();
+        for (int i = j + 1 + tid; i < nb; i += blockDim.x) L[i][j] /= L[j][j];
+        __syncthreads();
+        const int m = nb - j - 1;
+        for (int idx = tid; idx < m * m; idx += blockDim.x) {
+            const int i = j + 1 + idx % m, c = j + 1 + idx / m;
+            if (c <= i) L[i][c] -= L[i][j] * L[c][j];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        const int i = idx % nb, j = idx / nb;
+        if (i >= j) Fd[i + (int64_t)j * d.ld] = L[i][j];
+    }
+    if (tid < nb) {   // column tid of inv(L) by forward substitution
+        const int c = tid;
+        for (int i = c; i < nb; ++i) {
+            double v = (i == c) ? 1.0 : 0.0;
+            for (int t = c; t < i; ++t) v -= L[i][t] * Li[t][c];
+            Li[i][c] = v / L[i][i];
         }
     }
-    if (bad && lane == 0) atomicExch(status, WRAPD_E_NOT_SPD);
-    if (lane < nb) {
-#pragma unroll
-        for (int j = 0; j < NB; ++j)
-            if (j < nb && j <= lane) Fd[lane + (int64_t)j * d.ld] = a[j];
-    }
-    // inv(L): lane c holds column c, computed row by row from the top
-    double inv[NB];
-#pragma unroll
-    for (int i = 0; i < NB; ++i) inv[i] = 0.0;
-#pragma unroll
-    for (int i = 0; i < NB; ++i) {
-        if (i < nb) {
-            // inv(i, c) = (delta_ic - sum_{t<i} L(i, t) inv(t, c)) / L(i, i), for c <= i
-            double s = (lane == i) ? 1.0 : 0.0;
-#pragma unroll
-            for (int t = 0; t < NB; ++t) {
-                if (t < i) s -= __shfl_sync(0xffffffffu, a[t], i) * inv[t];
-            }
-            const double lii = __shfl_sync(0xffffffffu, a[i], i);
-            inv[i] = (lane <= i) ? s / lii : 0.0;
-        }
-    }
+    __syncthreads();
     double* Yp = Y + d.y_off + p0;   // row block p of Y (column-major, ld = k)
-    if (lane < nb) {
-#pragma unroll
-        for (int i = 0; i < NB; ++i)
-            if (i < nb) Yp[i + (int64_t)(p0 + lane) * d.k] = inv[i];
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        const int i = idx % nb, j = idx / nb;
+        Yp[i + (int64_t)(p0 + j) * d.k] = Li[i][j];
     }
 }
 
@@ -331,180 +326,188 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_wgemm(const double* __restrict
 }
 
 // ---- solve -----------------------------------------------------------------------
-// Per front: T = ceil(k/64) column tiles; Y part tiles (ti >= tj) then W part
-// tiles (ceil(r/64) x T).
-__device__ __forceinline__ void solve_tile(const FrontDesc& d, int t, bool& wpart, int& ti, int& tj) {
-    const int T = (d.k + TL - 1) / TL;
-    const int nY = T * (T + 1) / 2;
-    if (t < nY) {
-        int a = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-        while ((a + 1) * (a + 2) / 2 <= t) ++a;
-        while (a * (a + 1) / 2 > t) --a;
-        wpart = false; ti = a; tj = t - a * (a + 1) / 2;
+// Per level, one launch per direction.  Forward: a CTA owns a band of 64 rows of
+// M = [Y; W] ((k + r) x k) and streams all its columns (Y rows only up to the
+// diagonal): rows < k give z_s = Y t_s, rows >= k give u_s = v_s - W t_s.
+// Backward: a CTA owns a band of 64 columns and streams the rows below the
+// diagonal plus all W rows: y_s = Y^T z_s - W^T y_rows.  The right-hand side is
+// read from B (a copy of the input), z from Zb, and y written to x, so no CTA
+// reads what another CTA of the same launch writes.
+
+// t_s(i) for i < k, or v_s(i) for i >= k: own b entry plus the children's update
+// entries landing on front row i, in child order (inv: offsets in U, or -1).
+__device__ __forceinline__ void front_rhs(const double* __restrict__ B, const double* __restrict__ U,
+                                          const int64_t* __restrict__ inv, const FrontDesc& d, int i,
+                                          double& v0, double& v1, double& v2) {
+    if (i < d.k) {
+        const double* b = B + 3 * ((int64_t)d.first + i);
+        v0 = b[0]; v1 = b[1]; v2 = b[2];
     } else {
-        const int u = t - nY;
-        wpart = true; ti = u / T; tj = u % T;
+        v0 = v1 = v2 = 0.0;
     }
-}
-
-__global__ void k_fwd_gather(const double* __restrict__ x, double* __restrict__ Tv, double* __restrict__ U,
-                             const FrontDesc* __restrict__ desc, const int* __restrict__ rel, WorkList wl) {
-    const FrontDesc d = desc[wl.d_fronts[blockIdx.x]];
-    for (int i = threadIdx.x; i < 3 * d.k; i += blockDim.x) Tv[3 * (int64_t)d.first + i] = x[3 * (int64_t)d.first + i];
-    for (int i = threadIdx.x; i < 3 * d.r; i += blockDim.x) U[d.u_off + i] = 0.0;
-    __syncthreads();
-    for (int s = 0; s < d.nchild; ++s) {
-        const FrontDesc dc = desc[s == 0 ? d.child0 : d.child1];
-        const int* rc = rel + dc.rel_off;
-        for (int i = threadIdx.x; i < dc.r; i += blockDim.x) {
-            const int pos = rc[i];
-            double* dst = pos < d.k ? Tv + 3 * ((int64_t)d.first + pos) : U + d.u_off + 3 * (int64_t)(pos - d.k);
+    const int64_t* iv = inv + d.inv_off + 2 * (int64_t)i;
 #pragma unroll
-            for (int c = 0; c < 3; ++c) dst[c] += U[dc.u_off + 3 * (int64_t)i + c];
-        }
-        __syncthreads();
+    for (int q = 0; q < 2; ++q) {
+        const int64_t o = iv[q];
+        if (o >= 0) { v0 += U[o]; v1 += U[o + 1]; v2 += U[o + 2]; }
     }
 }
 
-// Forward tile: partial[tj][row] = sum_{j in tile tj} M(row, j) t_s(j), M = [Y; W];
-// 64 rows x 4 column groups of 16 per CTA.
-__global__ void __launch_bounds__(256) k_fwd_tiles(const double* __restrict__ Tv, const double* __restrict__ Y,
-                                                   const double* __restrict__ W, double* __restrict__ P,
-                                                   const FrontDesc* __restrict__ desc, WorkList wl) {
-    __shared__ double tv[TL * 3];
-    __shared__ double part[4][TL][3];
-    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
-    const FrontDesc d = desc[wl.d_fronts[item]];
-    bool wp; int ti, tj;
-    solve_tile(d, blockIdx.x - wl.d_prefix[item], wp, ti, tj);
-    const int c0 = tj * TL, nc = min(TL, d.k - c0);
-    const int r0 = ti * TL, nr = min(TL, (wp ? d.r : d.k) - r0);
-    for (int i = threadIdx.x; i < 3 * TL; i += blockDim.x)
-        tv[i] = i < 3 * nc ? Tv[3 * ((int64_t)d.first + c0) + i] : 0.0;
+// Each CTA takes one item: a 64-wide band (rows forward, columns backward) times
+// a chunk of the other dimension (at most SCH).  The CTAs of one band write
+// partial sums; the last one to arrive adds them in chunk order (deterministic)
+// and writes the band's result, then resets the band counter.
+constexpr int SCH = 256;
+
+__device__ __forceinline__ bool band_arrive(unsigned* counter, int nchunk) {
+    __shared__ bool last;
+    __threadfence();
     __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned old = atomicAdd(counter, 1u);
+        last = old == (unsigned)nchunk - 1;
+        if (last) *counter = 0u;
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+__global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B, double* __restrict__ Zb,
+                                                   double* __restrict__ U, const int64_t* __restrict__ inv,
+                                                   const double* __restrict__ Y, const double* __restrict__ W,
+                                                   const FrontDesc* __restrict__ desc, const SolveItem* __restrict__ items,
+                                                   double* __restrict__ P, unsigned* __restrict__ counters) {
+    __shared__ double tv[SCH * 3];
+    __shared__ double part[4][TL][3];
+    const SolveItem it = items[blockIdx.x];
+    const FrontDesc d = desc[it.front];
+    const int R = d.k + d.r;
     const int row = threadIdx.x & (TL - 1), grp = threadIdx.x >> 6;
+    const int i = it.b0 + row;
+    const int nc = it.hi - it.lo;
+    for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+        double v0, v1, v2;
+        front_rhs(B, U, inv, d, it.lo + j, v0, v1, v2);
+        tv[3 * j] = v0; tv[3 * j + 1] = v1; tv[3 * j + 2] = v2;
+    }
+    __syncthreads();
+    const bool wrow = i >= d.k;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    if (row < nr) {
-        const double* M = wp ? W + d.w_off + r0 + row + (int64_t)c0 * d.r : Y + d.y_off + r0 + row + (int64_t)c0 * d.k;
-        const int64_t ld = wp ? d.r : d.k;
-        const int jb = grp * 16, je = min(nc, jb + 16);
+    if (i < R) {
+        const int64_t ld = wrow ? d.r : d.k;
+        const double* M = (wrow ? W + d.w_off + (i - d.k) : Y + d.y_off + i) + (int64_t)it.lo * ld;
 #pragma unroll 4
-        for (int j = jb; j < je; ++j) {
+        for (int j = grp; j < nc; j += 4) {
             const double m = M[(int64_t)j * ld];
             a0 += m * tv[3 * j]; a1 += m * tv[3 * j + 1]; a2 += m * tv[3 * j + 2];
         }
     }
     part[grp][row][0] = a0; part[grp][row][1] = a1; part[grp][row][2] = a2;
     __syncthreads();
-    if (threadIdx.x < TL && threadIdx.x < nr) {
-        const int i = threadIdx.x;
-        const int64_t R = (int64_t)d.k + d.r;
-        double* o = P + d.fp_off + 3 * ((int64_t)tj * R + (wp ? d.k : 0) + r0 + i);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) o[c] = ((part[0][i][c] + part[1][i][c]) + part[2][i][c]) + part[3][i][c];
-    }
-}
-
-// Forward reduction: rows < k -> x_s; rows >= k -> u_s = v_s - sum.
-__global__ void __launch_bounds__(128) k_fwd_reduce(double* __restrict__ x, double* __restrict__ U,
-                                                    const double* __restrict__ P, const FrontDesc* __restrict__ desc,
-                                                    WorkList wl) {
-    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
-    const FrontDesc d = desc[wl.d_fronts[item]];
-    const int i = (blockIdx.x - wl.d_prefix[item]) * 128 + threadIdx.x;
-    const int64_t R = (int64_t)d.k + d.r;
-    if (i >= R) return;
-    const int T = (d.k + TL - 1) / TL;
-    const int tmax = i < d.k ? i / TL : T - 1;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    for (int tj = 0; tj <= tmax; ++tj) {
-        const double* p = P + d.fp_off + 3 * ((int64_t)tj * R + i);
-        s0 += p[0]; s1 += p[1]; s2 += p[2];
+    if (threadIdx.x < TL) {
+        s0 = ((part[0][row][0] + part[1][row][0]) + part[2][row][0]) + part[3][row][0];
+        s1 = ((part[0][row][1] + part[1][row][1]) + part[2][row][1]) + part[3][row][1];
+        s2 = ((part[0][row][2] + part[1][row][2]) + part[2][row][2]) + part[3][row][2];
     }
-    if (i < d.k) {
-        double* o = x + 3 * ((int64_t)d.first + i);
-        o[0] = s0; o[1] = s1; o[2] = s2;
-    } else {
-        double* u = U + d.u_off + 3 * (int64_t)(i - d.k);
-        u[0] -= s0; u[1] -= s1; u[2] -= s2;
-    }
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// Backward tile: partial[rt][j] = sum_{i in row tile} M(i, j) in(i), in = [z_s; -y_rows].
-// The 64 x 64 tile is staged through shared memory with coalesced column loads,
-// then each thread sums 16 rows of one column; 4 row groups are added in order.
-__global__ void __launch_bounds__(256) k_bwd_tiles(const double* __restrict__ x, const double* __restrict__ Y,
-                                                   const double* __restrict__ W, const int* __restrict__ rows,
-                                                   double* __restrict__ P, const FrontDesc* __restrict__ desc,
-                                                   WorkList wl) {
-    __shared__ double in[TL * 3];
-    __shared__ double Ms[TL][TL + 1];
-    __shared__ double part[4][TL][3];
-    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
-    const FrontDesc d = desc[wl.d_fronts[item]];
-    bool wp; int ti, tj;
-    solve_tile(d, blockIdx.x - wl.d_prefix[item], wp, ti, tj);
-    const int c0 = tj * TL, nc = min(TL, d.k - c0);
-    const int r0 = ti * TL, nr = min(TL, (wp ? d.r : d.k) - r0);
-    for (int i = threadIdx.x; i < TL; i += blockDim.x) {
-        double v0 = 0.0, v1 = 0.0, v2 = 0.0;
-        if (i < nr) {
-            if (wp) {
-                const double* y = x + 3 * (int64_t)rows[d.rows_off + r0 + i];
-                v0 = -y[0]; v1 = -y[1]; v2 = -y[2];
-            } else {
-                const double* z = x + 3 * ((int64_t)d.first + r0 + i);
-                v0 = z[0]; v1 = z[1]; v2 = z[2];
+    if (it.nchunk > 1) {
+        if (threadIdx.x < TL) {
+            double* p = P + 3 * ((int64_t)blockIdx.x * TL + row);
+            p[0] = s0; p[1] = s1; p[2] = s2;
+        }
+        if (!band_arrive(counters + it.band, it.nchunk)) return;
+        if (threadIdx.x < TL) {
+            s0 = s1 = s2 = 0.0;
+            for (int q = 0; q < it.nchunk; ++q) {
+                const double* p = P + 3 * ((int64_t)(it.first + q) * TL + row);
+                s0 += __ldcg(p); s1 += __ldcg(p + 1); s2 += __ldcg(p + 2);
             }
         }
-        in[3 * i] = v0; in[3 * i + 1] = v1; in[3 * i + 2] = v2;
     }
-    const int64_t ld = wp ? d.r : d.k;
-    const double* Mb = (wp ? W + d.w_off : Y + d.y_off) + r0 + (int64_t)c0 * ld;
-    for (int idx = threadIdx.x; idx < TL * TL; idx += blockDim.x) {
-        const int i = idx & (TL - 1), j = idx >> 6;
-        Ms[j][i] = (i < nr && j < nc) ? Mb[i + (int64_t)j * ld] : 0.0;
-    }
-    __syncthreads();
-    const int j = threadIdx.x & (TL - 1), grp = threadIdx.x >> 6;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-#pragma unroll 4
-    for (int i = grp * 16; i < grp * 16 + 16; ++i) {
-        const double m = Ms[j][i];
-        a0 += m * in[3 * i]; a1 += m * in[3 * i + 1]; a2 += m * in[3 * i + 2];
-    }
-    part[grp][j][0] = a0; part[grp][j][1] = a1; part[grp][j][2] = a2;
-    __syncthreads();
-    if (threadIdx.x < nc) {
-        const int jj = threadIdx.x;
-        const int T = (d.k + TL - 1) / TL;
-        const int rt = wp ? T + ti : ti;
-        double* o = P + d.bp_off + 3 * ((int64_t)rt * d.k + c0 + jj);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) o[c] = ((part[0][jj][c] + part[1][jj][c]) + part[2][jj][c]) + part[3][jj][c];
+    if (threadIdx.x < TL && i < R) {
+        if (!wrow) {
+            double* o = Zb + 3 * ((int64_t)d.first + i);
+            o[0] = s0; o[1] = s1; o[2] = s2;
+        } else {
+            double v0, v1, v2;
+            front_rhs(B, U, inv, d, i, v0, v1, v2);
+            double* u = U + d.u_off + 3 * (int64_t)(i - d.k);
+            u[0] = v0 - s0; u[1] = v1 - s1; u[2] = v2 - s2;
+        }
     }
 }
 
-// Backward reduction: y_s(j) = sum over the Y row tiles rt >= j/64 and all W row tiles.
-__global__ void __launch_bounds__(128) k_bwd_reduce(double* __restrict__ x, const double* __restrict__ P,
-                                                    const FrontDesc* __restrict__ desc, WorkList wl) {
-    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
-    const FrontDesc d = desc[wl.d_fronts[item]];
-    const int j = (blockIdx.x - wl.d_prefix[item]) * 128 + threadIdx.x;
-    if (j >= d.k) return;
-    const int T = (d.k + TL - 1) / TL, nW = (d.r + TL - 1) / TL;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    for (int rt = j / TL; rt < T + nW; ++rt) {
-        const double* p = P + d.bp_off + 3 * ((int64_t)rt * d.k + j);
-        s0 += p[0]; s1 += p[1]; s2 += p[2];
+// Backward: one warp per column of the band, lanes along the rows of the chunk.
+__global__ void __launch_bounds__(256) k_bwd_level(double* __restrict__ x, const double* __restrict__ Zb,
+                                                   const double* __restrict__ Y, const double* __restrict__ W,
+                                                   const int* __restrict__ rows, const FrontDesc* __restrict__ desc,
+                                                   const SolveItem* __restrict__ items, double* __restrict__ P,
+                                                   unsigned* __restrict__ counters) {
+    __shared__ double in[SCH * 3];
+    __shared__ double res[TL][3];
+    const SolveItem it = items[blockIdx.x];
+    const FrontDesc d = desc[it.front];
+    const int nr = it.hi - it.lo;
+    const int nc = min(TL, d.k - it.b0);
+    for (int t = threadIdx.x; t < nr; t += blockDim.x) {
+        const int i = it.lo + t;
+        double v0, v1, v2;
+        if (i < d.k) {
+            const double* z = Zb + 3 * ((int64_t)d.first + i);
+            v0 = z[0]; v1 = z[1]; v2 = z[2];
+        } else {
+            const double* y = x + 3 * (int64_t)rows[d.rows_off + i - d.k];
+            v0 = -y[0]; v1 = -y[1]; v2 = -y[2];
+        }
+        in[3 * t] = v0; in[3 * t + 1] = v1; in[3 * t + 2] = v2;
     }
-    double* o = x + 3 * ((int64_t)d.first + j);
-    o[0] = s0; o[1] = s1; o[2] = s2;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // the chunk lies entirely in Y rows or entirely in W rows
+    const bool wpart = it.lo >= d.k;
+    const int64_t ld = wpart ? d.r : d.k;
+    const double* base = wpart ? W + d.w_off + (it.lo - d.k) : Y + d.y_off + it.lo;
+    for (int jj = warp; jj < TL; jj += 8) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        if (jj < nc) {
+            const double* M = base + (int64_t)(it.b0 + jj) * ld;
+#pragma unroll 4
+            for (int t = lane; t < nr; t += 32) {
+                const double m = M[t];
+                a0 += m * in[3 * t]; a1 += m * in[3 * t + 1]; a2 += m * in[3 * t + 2];
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a0 += __shfl_down_sync(0xffffffffu, a0, o);
+            a1 += __shfl_down_sync(0xffffffffu, a1, o);
+            a2 += __shfl_down_sync(0xffffffffu, a2, o);
+        }
+        if (lane == 0) { res[jj][0] = a0; res[jj][1] = a1; res[jj][2] = a2; }
+    }
+    __syncthreads();
+    const int j = threadIdx.x;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    if (j < TL) { s0 = res[j][0]; s1 = res[j][1]; s2 = res[j][2]; }
+    if (it.nchunk > 1) {
+        if (j < TL) {
+            double* p = P + 3 * ((int64_t)blockIdx.x * TL + j);
+            p[0] = s0; p[1] = s1; p[2] = s2;
+        }
+        if (!band_arrive(counters + it.band, it.nchunk)) return;
+        if (j < TL) {
+            s0 = s1 = s2 = 0.0;
+            for (int q = 0; q < it.nchunk; ++q) {
+                const double* p = P + 3 * ((int64_t)(it.first + q) * TL + j);
+                s0 += __ldcg(p); s1 += __ldcg(p + 1); s2 += __ldcg(p + 2);
+            }
+        }
+    }
+    if (j < nc) {
+        double* o = x + 3 * ((int64_t)d.first + it.b0 + j);
+        o[0] = s0; o[1] = s1; o[2] = s2;
+    }
 }
 
 }  // namespace
@@ -571,7 +574,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
     if (S.max_children > 2) throw CudaError(WRAPD_E_INPUT, "assembly tree with more than 2 children");
     h_desc_.resize(nfronts);
     std::vector<int> rows;
-    int64_t roff = 0, woff = 0, fpoff = 0, bpoff = 0;
+    int64_t roff = 0, woff = 0, ioff = 0;
     for (int f = 0; f < nfronts; ++f) {
         const Front& F = S.fronts[f];
         FrontDesc& d = h_desc_[f];
@@ -580,15 +583,23 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         d.rows_off = roff;
         rows.insert(rows.end(), F.rows.begin(), F.rows.end());
         roff += F.nrows();
-        const int64_t T = ceil_div(d.k, TL), nW = ceil_div(d.r, TL);
         d.w_off = woff; woff += (int64_t)d.r * d.k;
-        d.fp_off = fpoff; fpoff += 3 * T * ((int64_t)d.k + d.r);
-        d.bp_off = bpoff; bpoff += 3 * (T + nW) * d.k;
+        d.inv_off = ioff; ioff += 2 * ((int64_t)d.k + d.r);
         d.nchild = static_cast<int>(F.children.size());
         d.child0 = d.nchild > 0 ? F.children[0] : -1;
         d.child1 = d.nchild > 1 ? F.children[1] : -1;
         d.pad = 0;
     }
+    std::vector<int64_t> inv(ioff, -1);
+    for (int f = 0; f < nfronts; ++f) {
+        const Front& F = S.fronts[f];
+        for (size_t q = 0; q < F.children.size(); ++q) {
+            const Front& C = S.fronts[F.children[q]];
+            for (int i = 0; i < C.nrows(); ++i)
+                inv[h_desc_[f].inv_off + 2 * (int64_t)S.relmap[C.rel_off + i] + (int64_t)q] = C.u_off + 3 * (int64_t)i;
+        }
+    }
+    d_inv_ = upload(inv, st);
     d_desc_ = upload(h_desc_, st);
     d_rows_ = upload(rows, st);
     d_rel_ = upload(S.relmap, st);
@@ -596,7 +607,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
     d_Apos_ = upload(A_pos, st);
     d_Aptr_ = upload(A_ptr, st);
     d_Acon_ = upload(A_contrib, st);
-    f_pool_ = S.f_pool; y_pool_ = S.y_pool; u_pool_ = S.u_pool; w_pool_ = woff; p_pool_ = std::max(fpoff, bpoff);
+    f_pool_ = S.f_pool; y_pool_ = S.y_pool; u_pool_ = S.u_pool; w_pool_ = woff;
     auto dalloc = [&](size_t count) {
         double* p = nullptr;
         if (cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(double)) != cudaSuccess) {
@@ -612,7 +623,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
     d_W_ = dalloc(w_pool_);
     d_U_ = dalloc(u_pool_);
     d_T_ = dalloc(3 * (size_t)n);
-    d_P_ = dalloc(p_pool_);
+    d_Z_ = dalloc(3 * (size_t)n);
     int* st_ptr = nullptr;
     WRAPD_CUDA(cudaMalloc(&st_ptr, sizeof(int)));
     allocs_.push_back(st_ptr);
@@ -674,28 +685,56 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
             L.update.push_back(make_jobs(jobs, st));
             launches_factor += 1 + (L.trsm.back().total ? 1 : 0) + (L.update.back().total ? 1 : 0);
         }
-        std::vector<int> wg(fs.size()), ft(fs.size()), fr(fs.size()), bc(fs.size());
-        for (size_t i = 0; i < fs.size(); ++i) {
-            const FrontDesc& d = h_desc_[fs[i]];
+        std::vector<int> wg(fs.size());
+        std::vector<SolveItem> fwd, bwd;
+        int fbands = 0, bbands = 0;
+        for (size_t q = 0; q < fs.size(); ++q) {
+            const FrontDesc& d = h_desc_[fs[q]];
             const int T = ceil_div(d.k, TL), nW = ceil_div(d.r, TL);
-            wg[i] = nW * T;
-            ft[i] = T * (T + 1) / 2 + nW * T;
-            fr[i] = ceil_div((int64_t)d.k + d.r, 128);
-            bc[i] = ceil_div(d.k, 128);
+            wg[q] = nW * T;
+            const int R = d.k + d.r;
+            // forward: row bands; Y bands use columns up to their last row
+            for (int b0 = 0; b0 < R; b0 += TL) {
+                const int cend = b0 < d.k ? std::min(d.k, b0 + TL) : d.k;
+                const int nch = ceil_div(cend, SCH), first = static_cast<int>(fwd.size());
+                for (int c = 0; c < nch; ++c)
+                    fwd.push_back({fs[q], b0, c * SCH, std::min(cend, (c + 1) * SCH), nch, first, fbands});
+                fbands++;
+            }
+            // backward: column bands over rows [b0, k) of Y, then the W rows; no chunk crosses k
+            for (int b0 = 0; b0 < d.k; b0 += TL) {
+                std::vector<std::pair<int, int>> ch;
+                for (int lo = b0; lo < d.k; lo += SCH) ch.push_back({lo, std::min(d.k, lo + SCH)});
+                for (int lo = d.k; lo < R; lo += SCH) ch.push_back({lo, std::min(R, lo + SCH)});
+                const int nch = static_cast<int>(ch.size()), first = static_cast<int>(bwd.size());
+                for (auto& c : ch) bwd.push_back({fs[q], b0, c.first, c.second, nch, first, bbands});
+                bbands++;
+            }
         }
         L.wgemm = make_list(fs, wg, st);
         if (L.wgemm.total) launches_factor++;
-        L.fwd_tiles = make_list(fs, ft, st);
-        L.fwd_rows = make_list(fs, fr, st);
-        L.bwd_tiles = L.fwd_tiles;
-        L.bwd_cols = make_list(fs, bc, st);
-        launches_solve += 5;
+        L.n_fwd = static_cast<int>(fwd.size());
+        L.n_bwd = static_cast<int>(bwd.size());
+        L.d_fwd = upload(fwd, st);
+        L.d_bwd = upload(bwd, st);
+        solve_parts_ = std::max<int64_t>(solve_parts_, std::max(L.n_fwd, L.n_bwd));
+        solve_bands_ = std::max(solve_bands_, std::max(fbands, bbands));
+        launches_solve += 2;
     }
     trsm_nP_.clear();
     for (auto& L : levels_) {
         std::vector<int*> w;
         for (auto& nP : L.trsm_split) w.push_back(nP.empty() ? nullptr : upload(nP, st));
         trsm_nP_.push_back(w);
+    }
+    d_P_ = dalloc(3 * TL * (size_t)solve_parts_);
+    {
+        unsigned* c = nullptr;
+        WRAPD_CUDA(cudaMalloc(&c, std::max(1, solve_bands_) * sizeof(unsigned)));
+        allocs_.push_back(c);
+        device_bytes += std::max(1, solve_bands_) * sizeof(unsigned);
+        d_cnt_ = c;
+        WRAPD_CUDA(cudaMemsetAsync(d_cnt_, 0, std::max(1, solve_bands_) * sizeof(unsigned), st));
     }
     WRAPD_CUDA(cudaStreamSynchronize(st));
 }
@@ -718,7 +757,7 @@ void CholGPU::factor_launches(const double* d_w2, const double* d_Di, int ne, cu
             }
         for (size_t p = 0; p < L.diag.size(); ++p) {
             if (L.diag[p].total) {
-                k_diag<<<L.diag[p].total, 32, 0, st>>>(d_F_, d_Y_, d_desc_, L.diag[p], (int)p, d_status);
+                k_diag<<<L.diag[p].total, 256, 0, st>>>(d_F_, d_Y_, d_desc_, L.diag[p], (int)p, d_status);
                 WRAPD_LAUNCH_CHECK();
             }
             if (L.trsm[p].total) {
@@ -756,20 +795,15 @@ void CholGPU::factor(const double* d_w2, const double* d_Di, int ne, cudaStream_
 }
 
 void CholGPU::solve_launches(double* d_x, cudaStream_t st) {
+    WRAPD_CUDA(cudaMemcpyAsync(d_T_, d_x, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     for (int l = 0; l < nlevels; ++l) {
         Level& L = levels_[l];
-        k_fwd_gather<<<L.all.total, 256, 0, st>>>(d_x, d_T_, d_U_, d_desc_, d_rel_, L.all);
-        WRAPD_LAUNCH_CHECK();
-        k_fwd_tiles<<<L.fwd_tiles.total, 256, 0, st>>>(d_T_, d_Y_, d_W_, d_P_, d_desc_, L.fwd_tiles);
-        WRAPD_LAUNCH_CHECK();
-        k_fwd_reduce<<<L.fwd_rows.total, 128, 0, st>>>(d_x, d_U_, d_P_, d_desc_, L.fwd_rows);
+        k_fwd_level<<<L.n_fwd, 256, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_W_, d_desc_, L.d_fwd, d_P_, d_cnt_);
         WRAPD_LAUNCH_CHECK();
     }
     for (int l = nlevels - 1; l >= 0; --l) {
         Level& L = levels_[l];
-        k_bwd_tiles<<<L.bwd_tiles.total, 256, 0, st>>>(d_x, d_Y_, d_W_, d_rows_, d_P_, d_desc_, L.bwd_tiles);
-        WRAPD_LAUNCH_CHECK();
-        k_bwd_reduce<<<L.bwd_cols.total, 128, 0, st>>>(d_x, d_P_, d_desc_, L.bwd_cols);
+        k_bwd_level<<<L.n_bwd, 256, 0, st>>>(d_x, d_Z_, d_Y_, d_W_, d_rows_, d_desc_, L.d_bwd, d_P_, d_cnt_);
         WRAPD_LAUNCH_CHECK();
     }
 }

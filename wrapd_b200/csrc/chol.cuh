@@ -26,7 +26,7 @@ namespace wrapd {
 
 struct FrontDesc {
     int first, k, r, ld;
-    int64_t f_off, y_off, u_off, rows_off, rel_off, w_off, fp_off, bp_off;
+    int64_t f_off, y_off, u_off, rows_off, rel_off, w_off, inv_off;
     int nchild, child0, child1, pad;
 };
 
@@ -34,6 +34,14 @@ struct FrontDesc {
 // of panel columns.  kind 0: C is F[r0:r1, c0:c1] of the front (lower part
 // where rows and columns overlap), A = F[r0:r1, k0:k1], B' = F[c0:c1, k0:k1];
 // kind 1: C is Y[r0:r1, c0:c1], A = F[r0:r1, k0:k1], B'(j, t) = Y[k0 + t, c0 + j].
+// A solve work item: a 64-wide band starting at b0 (rows forward, columns
+// backward) times the chunk [lo, hi) of the other dimension.  The band's items
+// are contiguous, starting at `first`, `nchunk` of them; `band` indexes the
+// arrival counter.
+struct SolveItem {
+    int front, b0, lo, hi, nchunk, first, band;
+};
+
 struct GemmJob {
     int front, kind, r0, r1, c0, c1, k0, k1;
 };
@@ -96,13 +104,15 @@ private:
         std::vector<JobList> update;     // per panel step: blocked trailing-update jobs (F and Y)
         std::vector<std::vector<int>> trsm_split;  // per step: panel-row tiles per item
         WorkList wgemm;                  // W = L_rs Y tiles
-        WorkList fwd_tiles, fwd_rows;    // solve forward: [Y; W] t tiles, row reduction
-        WorkList bwd_tiles, bwd_cols;    // solve backward: [Y; W]^T in tiles, column reduction
+        SolveItem* d_fwd = nullptr;      // solve forward: (64-row band, column chunk) items
+        SolveItem* d_bwd = nullptr;      // solve backward: (64-column band, row chunk) items
+        int n_fwd = 0, n_bwd = 0;
     };
     std::vector<Level> levels_;
     FrontDesc* d_desc_ = nullptr;
     int* d_rows_ = nullptr;
     int* d_rel_ = nullptr;
+    int64_t* d_inv_ = nullptr;   // per front row: the (up to 2) children's update-vector entries that add into it
     int64_t* d_Apos_ = nullptr;
     int* d_Aptr_ = nullptr;
     int* d_Acon_ = nullptr;
@@ -111,9 +121,13 @@ private:
     double* d_Y_ = nullptr;
     double* d_W_ = nullptr;
     double* d_U_ = nullptr;      // solve update vectors
-    double* d_T_ = nullptr;      // solve temporaries (n x 3)
-    double* d_P_ = nullptr;      // solve tile partial sums
-    int64_t f_pool_ = 0, y_pool_ = 0, u_pool_ = 0, w_pool_ = 0, p_pool_ = 0;
+    double* d_T_ = nullptr;      // solve: copy of the right-hand side (n x 3)
+    double* d_Z_ = nullptr;      // solve: forward result (n x 3)
+    double* d_P_ = nullptr;      // solve: per-item partial sums (64 x 3 per item)
+    unsigned* d_cnt_ = nullptr;  // solve: per-band arrival counters (zero between launches)
+    int64_t solve_parts_ = 0;
+    int solve_bands_ = 0;
+    int64_t f_pool_ = 0, y_pool_ = 0, u_pool_ = 0, w_pool_ = 0;
     cudaGraphExec_t factor_graph_ = nullptr;
     cudaGraphExec_t solve_graph_ = nullptr;
     double* solve_graph_x_ = nullptr;

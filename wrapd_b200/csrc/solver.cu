@@ -103,6 +103,7 @@ SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
 
 SolverGPU::~SolverGPU() {
     if (st_) cudaStreamSynchronize(st_);
+    for (cudaEvent_t e : event_pool_) cudaEventDestroy(e);
     for (void* p : allocs_) cudaFree(p);
     for (auto& e : ev_) if (e) cudaEventDestroy(e);
     if (h_scal_) cudaFreeHost(h_scal_);
@@ -394,10 +395,38 @@ void SolverGPU::factor() {
     n_factor++;
 }
 
+// Profile slots: 0 = local step, 1 = gradient + gather, 2 = two-loop vector
+// kernels, 3 = triangular solves, 4 = x update, 5 = host gaps around syncs.
+void SolverGPU::mark(int slot) {
+    if (!profiling) return;
+    if (event_next_ == event_pool_.size()) {
+        cudaEvent_t e;
+        WRAPD_CUDA(cudaEventCreate(&e));
+        event_pool_.push_back(e);
+    }
+    cudaEvent_t e = event_pool_[event_next_++];
+    WRAPD_CUDA(cudaEventRecord(e, st_));
+    marks_.emplace_back(e, slot);
+}
+
+void SolverGPU::profile_flush() {
+    if (!profiling || marks_.size() < 2) { marks_.clear(); event_next_ = 0; return; }
+    WRAPD_CUDA(cudaEventSynchronize(marks_.back().first));
+    for (size_t i = 1; i < marks_.size(); ++i) {
+        float ms = 0.f;
+        WRAPD_CUDA(cudaEventElapsedTime(&ms, marks_[i - 1].first, marks_[i].first));
+        profile_ms[marks_[i].second] += ms;
+        profile_n[marks_[i].second]++;
+    }
+    marks_.clear();
+    event_next_ = 0;
+}
+
 void SolverGPU::sync_read() {
     WRAPD_CUDA(cudaMemcpyAsync(h_scal_, d_scal_, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st_));
     WRAPD_CUDA(cudaStreamSynchronize(st_));
     n_sync++;
+    mark(5);
 }
 
 void SolverGPU::check_status() {
@@ -458,6 +487,8 @@ void SolverGPU::begin_solve() {
         check_status();
     }
     solving_ = true;
+    marks_.clear();
+    event_next_ = 0;
     runtime_ms[0] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
@@ -489,9 +520,11 @@ int SolverGPU::lbfgs_minimize() {
         }
         WRAPD_LAUNCH_CHECK();
         // q = A^-1 q, three right-hand sides at once
+        mark(2);
         chol.solve(d_q_, st_);
         kernel_launches += chol.launches_solve;
         n_solve++;
+        mark(3);
         // second loop (oldest to newest): c_i = alpha_i - rho_i <y_i, q>, q += c_i s_i; then dir = <grad, q>
         if (it == 0) {
             k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, nullptr, nullptr, 0.0, d_gcur_, nullptr, 1.0,
@@ -511,9 +544,11 @@ int SolverGPU::lbfgs_minimize() {
         k_xupdate<<<vb, 256, 0, st_>>>(n, d_x_, d_q_, d_gcur_, d_scal_ + S_DIR, d_sstage_);
         WRAPD_LAUNCH_CHECK();
         kernel_launches++;
+        mark(2);
         // gradient at the new x; y = grad_new - grad
         grad_at_x(true);
         gather(d_gnew_, d_gcur_, d_ystage_, d_sstage_);
+        mark(1);
         sync_read();
         const double dir = h_scal_[S_DIR];
         const double yy = h_scal_[S_GATHER], sy = h_scal_[S_GATHER + 1];
@@ -558,13 +593,16 @@ int SolverGPU::iterate(int n, bool* conv) {
     while (done < n && iter < cfg.max_iters && !converged_) {
         // ---- local step: polar_update (src/TetElements.cpp:256-356) ----
         WRAPD_CUDA(cudaEventRecord(ev_[0], st_));
+        mark(5);
         local_step(cand_mode_now(), fp32() && !fp64_phase_);
         if (cfg.reweighting) count_++;
+        mark(0);
         WRAPD_CUDA(cudaEventRecord(ev_[1], st_));
         // ---- global step: RotAwareGS::global_step (src/GlobalStepBehavior.hpp:246-258) ----
         if (m_k_ == 0) WRAPD_CUDA(cudaMemsetAsync(d_gold_, 0, 3 * (size_t)nf * sizeof(double), st_));
         grad_at_x(true);
         gather(d_gcur_, d_gold_, nullptr, nullptr);
+        mark(1);
         sync_read();
         const double bef = h_scal_[S_LOCAL], aft = h_scal_[S_LOCAL + 1], pe = h_scal_[S_LOCAL + 2];
         if (h_scal_[S_LOCAL + 3] > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
@@ -598,6 +636,7 @@ int SolverGPU::iterate(int n, bool* conv) {
         }
         WRAPD_CUDA(cudaEventRecord(ev_[3], st_));
         WRAPD_CUDA(cudaEventSynchronize(ev_[3]));
+        profile_flush();
         if (rw) check_status();
         float ml = 0.f, mg = 0.f, mr = 0.f;
         WRAPD_CUDA(cudaEventElapsedTime(&ml, ev_[0], ev_[1]));

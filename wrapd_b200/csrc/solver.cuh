@@ -45,6 +45,12 @@ public:
     void solve_A(const double* b, double* x);
 
     const Logs& logs() const { return logs_; }
+    // Optional per-phase device timeline (CUDA events on the handle's stream):
+    // slots of kProfileNames, accumulated ms and counts.
+    static constexpr int kProfileSlots = 6;
+    bool profiling = false;
+    double profile_ms[kProfileSlots] = {};
+    int64_t profile_n[kProfileSlots] = {};
     double runtime_ms[6] = {0, 0, 0, 0, 0, 0};
     wrapd_settings cfg;
     int nv = 0, ne = 0, np = 0, nf = 0;
@@ -59,6 +65,11 @@ private:
     void* dalloc(size_t bytes);
     template <typename X> X* dupload(const std::vector<X>& v);
     void sync_read();
+    void mark(int slot);          // close the running profile slot at this point of the stream
+    void profile_flush();         // turn recorded event pairs into milliseconds
+    std::vector<std::pair<cudaEvent_t, int>> marks_;
+    std::vector<cudaEvent_t> event_pool_;
+    size_t event_next_ = 0;
     void check_status();
     void grad_at_x(bool write_gel);
     void gather(double* grad, const double* gold, double* ystage, const double* sstage);

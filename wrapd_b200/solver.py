@@ -132,6 +132,15 @@ class Solver:
         self._h.check(self._h.lib.wrapd_get_counters(self._h.h, v))
         return dict(zip(["kernel_launches", "factorizations", "solves", "host_syncs"], list(v)))
 
+    def set_profiling(self, on: bool = True):
+        self._h.check(self._h.lib.wrapd_set_profiling(self._h.h, int(on)))
+
+    def profile(self) -> dict:
+        ms, n = np.zeros(6), (ctypes.c_int64 * 6)()
+        self._h.check(self._h.lib.wrapd_get_profile(self._h.h, capi.dptr(ms), n))
+        names = ["local", "grad_gather", "vector", "solve", "unused", "host_gaps"]
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(names)}
+
     def algorithm_data(self) -> AlgorithmData:
         return AlgorithmData(**{k: self.log(k) for k in capi.LOGS}, runtime_ms=self.runtime())
 
