@@ -72,7 +72,8 @@ typedef struct wrapd_settings {
     int lbfgs_m;          /* global L-BFGS history, 6 (SplitLBFGS.hpp:41) */
     int rw_every;         /* 0: gamma rule; N > 0: reweight (and refactor) every N iterations */
     int precision;        /* 0: FP64 throughout; 1: FP32 local step (SVD + Newton prox), FP64 elsewhere */
-    int prox_mode;        /* 0: L-BFGS prox as the reference (parity mode); 1: Newton prox */
+    int prox_mode;        /* 0: L-BFGS prox as the reference (parity mode); 1: Newton prox;
+                             2: Newton prox warm-started by the prox network (wrapd_set_prox_net) */
     int leaf_size;        /* nested-dissection leaf size for the factorization, 64 */
     int verbose;          /* -p          0 here (1 prints the reference's table) */
     int device;           /* CUDA device ordinal, 0 */
@@ -89,7 +90,8 @@ enum {
     WRAPD_LOG_LS_DELTA_AL = 4,      /* iters entries: |delta AL| of the local step */
     WRAPD_LOG_GS_DELTA_AL = 5,      /* iters entries: |delta AL| of the global step */
     WRAPD_LOG_ACCUMULATED_TIME_S = 6, /* iters + 1 entries: local + global + refactor seconds */
-    WRAPD_LOG_X_ERRORS = 7          /* iters + 1 entries: |x - x_soln| / |x_init - x_soln| */
+    WRAPD_LOG_X_ERRORS = 7,         /* iters + 1 entries: |x - x_soln| / |x_init - x_soln| */
+    WRAPD_LOG_PROX_ITERS = 8        /* iters entries: mean prox iterations per element (extension) */
 };
 
 /* Defaults of wrapd::Settings() + ModelSettings() (src/Settings.hpp:154-162,
@@ -230,6 +232,46 @@ WRAPD_API int wrapd_potential_energy_batch(int n, double mu, double lambda, cons
  *   streams or threads) race and give wrong sums, so serialise them. */
 WRAPD_API int wrapd_potential_energy_batch_noalloc(int n, double mu, double lambda, const double* d_sigma,
                                                    const double* d_vol, double* d_out, void* stream);
+
+/* The Newton prox of prox_mode 1 (no reference counterpart: the reference
+ * keeps mcloptlib's Newton commented out, src/TetElements.cpp:215, 304):
+ * NHProx with x0 = sigma0, w^2/vol = wov, from `start`, until |g| <= tol *
+ * wov * max(1, |x|) or the step is below tol * max(1, |x|); out n x 3, iters n
+ * (nullable). */
+WRAPD_API int wrapd_prox_newton_batch(int n, int fp32, double mu, double lambda, double tol, int max_iters,
+                                      const double* sigma0, const double* wov, const double* start, double* out,
+                                      int* iters);
+
+/* ---- prox network (no reference counterpart) --------------------------------
+ * A 5 -> 64 -> 64 -> 3 GELU MLP that predicts the prox stretches from
+ * (sorted singular values of S_in, log(w^2 / (vol mu)), log(mu / lambda)); it
+ * warm-starts the Newton prox under prox_mode 2.  Parameters are an FP32 blob
+ * of WRAPD_NET_BLOB floats: feature mean[5], 1/std[5], output scale[3], 3 pad,
+ * W1[64][5], b1[64], W2[64][64], b2[64], W3[3][64], b3[3]; the prediction is
+ * sigma_in + scale * y.  Kernels compute with BF16 operands and FP32
+ * accumulation.  Training: features n x 5 (raw, as above), targets n x 3 (the
+ * converged prox stretches); loss = mean squared error of the normalised
+ * output (sigma* - sigma_in) / scale; Adam (0.9, 0.999, 1e-8) with a cosine
+ * rate from lr to lr_end.  Deterministic for a given seed. */
+#define WRAPD_NET_BLOB 4755
+typedef struct wrapd_prox_net wrapd_prox_net;
+WRAPD_API int wrapd_net_create(const float* blob, int n_blob, wrapd_prox_net** out);
+WRAPD_API int wrapd_net_set_data(wrapd_prox_net* h, const float* features, const float* targets, int64_t n);
+/* epoch_loss: `epochs` entries (nullable), the mean loss seen over each epoch. */
+WRAPD_API int wrapd_net_train(wrapd_prox_net* h, int epochs, int batch, float lr, float lr_end, uint64_t seed,
+                              double* epoch_loss);
+/* Loss and gradient (WRAPD_NET_BLOB - 16 floats, the trained part of the blob)
+ * over samples [first, first + n) of the data, without an update. */
+WRAPD_API int wrapd_net_grad(wrapd_prox_net* h, int64_t first, int n, double* loss, float* grad);
+WRAPD_API int wrapd_net_get(wrapd_prox_net* h, float* blob);
+WRAPD_API const char* wrapd_net_last_error(wrapd_prox_net* h);   /* h may be NULL: last create/predict error */
+WRAPD_API void wrapd_net_destroy(wrapd_prox_net* h);
+/* Predicted prox stretches for n samples: sigma_in n x 3 (sorted singular
+ * values), wov n (w^2 / vol); out n x 3. */
+WRAPD_API int wrapd_net_predict(const float* blob, int n_blob, int n, const double* sigma_in, const double* wov,
+                                double mu, double lambda, double* out);
+/* Installs the network used by prox_mode 2 (copied; call before begin_solve). */
+WRAPD_API int wrapd_set_prox_net(wrapd_handle* h, const float* blob, int n_blob);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,133 @@
+"""GPU checks of the prox network: the training kernels' loss and gradient
+against the CPU oracle (same BF16 rounding points; the kernels accumulate in
+FP32, the oracle in float64), the inference kernel against the oracle's
+forward pass, training that lowers the loss, and what the shipped trained
+network gains over starting the Newton prox without it.
+
+Tolerances: gradient blocks within 2e-3 relative (L2), loss within 1e-5
+relative: an FP32 sum of 128-sample tiles against float64, where a value near
+a BF16 rounding boundary can round the other way.  Predictions within 1e-3
+of the output scale: the features pass through logf on the device."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import E_YOUNG, NU
+from oracle import net_oracle as no
+from wrapd_b200 import bars, capi, prox_net
+from wrapd_b200.solver import Solver
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib(lib_built):
+    capi.load()
+
+
+def _data(n, seed, mu, lam):
+    """Prox inputs drawn around the identity and their converged prox stretches."""
+    rng = np.random.default_rng(seed)
+    sig = np.sort(rng.uniform(0.5, 1.6, (n, 3)), axis=1)[:, ::-1].copy()
+    wov = mu * np.exp(rng.uniform(-1.0, 3.0, n))
+    out, its = capi.prox_newton_batch(mu, lam, sig, wov, np.ones_like(sig), tol=1e-10, max_iters=100)
+    assert np.all(its < 100)
+    return prox_net.features(sig, wov, mu, lam), out.astype(np.float32), sig, wov
+
+
+def test_gradient_matches_oracle():
+    mu, lam = prox_net.lame(E_YOUNG, NU)
+    X, T, _, _ = _data(1000, 0, mu, lam)
+    blob = prox_net.init_blob(X, T, seed=3)
+    tr = prox_net.Trainer(blob)
+    tr.set_data(X, T)
+    for first, n in ((0, 1000), (100, 77)):
+        loss, g = tr.grad(first, n)
+        lo, go = no.loss_grad(blob.astype(np.float64), X[first:first + n].astype(np.float64),
+                              T[first:first + n].astype(np.float64), bf=True)
+        assert abs(loss - lo) <= 1e-5 * lo
+        o = -no.B_W1
+        for a, b in ((no.B_W1, no.B_B1), (no.B_B1, no.B_W2), (no.B_W2, no.B_B2), (no.B_B2, no.B_W3),
+                     (no.B_W3, no.B_B3), (no.B_B3, no.N_BLOB)):
+            ref = go[a + o:b + o]
+            err = np.linalg.norm(g[a + o:b + o] - ref) / max(np.linalg.norm(ref), 1e-30)
+            assert err < 2e-3, (a, err)
+    tr.close()
+
+
+def test_prediction_matches_oracle():
+    mu, lam = prox_net.lame(E_YOUNG, NU)
+    X, T, sig, wov = _data(777, 1, mu, lam)
+    blob = prox_net.init_blob(X, T, seed=5)
+    got = prox_net.predict(blob, sig, wov, mu, lam)
+    ref = no.predict(blob.astype(np.float64), sig, wov, mu, lam, bf=True)
+    scale = blob[10:13].astype(np.float64)
+    assert np.all(np.abs(got - ref) <= 1e-3 * scale + 1e-6)
+
+
+def test_training_lowers_loss_and_is_deterministic():
+    mu, lam = prox_net.lame(E_YOUNG, NU)
+    X, T, _, _ = _data(20000, 2, mu, lam)
+    blobs = []
+    for _ in range(2):
+        tr = prox_net.Trainer(prox_net.init_blob(X, T, seed=7))
+        tr.set_data(X, T)
+        l0, _ = tr.grad(0, 8192)
+        losses = tr.train(epochs=6, batch=1024, lr=3e-3, seed=11)
+        l1, _ = tr.grad(0, 8192)
+        blobs.append(tr.blob())
+        tr.close()
+        assert l1 < 0.05 * l0, (l0, l1, losses)
+    np.testing.assert_array_equal(blobs[0], blobs[1])
+
+
+TRAINED = os.path.exists(prox_net.DEFAULT_PATH)
+
+
+@pytest.mark.skipif(not TRAINED, reason="no trained network shipped")
+def test_trained_network_cuts_newton_iterations_on_large_bar():
+    """Prox inputs of a 32 x 32 x 128 bar (360 deg twist, 90 deg bend) after 12
+    FP64 iterations: Newton to 1e-10 from the network's prediction against
+    Newton from the identity; both reach the same stretches."""
+    blob = prox_net.load_default()
+    mu, lam = prox_net.lame(E_YOUNG, NU)
+    bar = bars.config1()
+    s = Solver(youngs=E_YOUNG, poisson=NU, lbfgs_m=5, rw_every=10, prox_mode=1, max_iters=12)
+    s.add_tetmesh(bar.rest, bar.init, bar.tets)
+    s.set_pins(bar.pins)
+    s.initialize()
+    s.begin_solve()
+    s.iterate(12)
+    sig, wov, slast = prox_net.prox_inputs(s)
+    r = prox_net.newton_iterations(blob, sig, wov, slast, mu, lam, tol=1e-10)
+    it_id, it_net = r["identity"].mean(), r["network"].mean()
+    print(f"mean Newton iterations: identity {it_id:.3f}, last stretches {r['last'].mean():.3f}, "
+          f"network {it_net:.3f}")
+    assert it_net <= 0.75 * it_id
+    ok = (r["identity"] < 100) & (r["network"] < 100)
+    assert ok.mean() > 0.999
+    assert np.abs(r["out_network"][ok] - r["out_identity"][ok]).max() < 1e-8
+
+
+@pytest.mark.skipif(not TRAINED, reason="no trained network shipped")
+def test_solver_with_network_matches_newton_solver():
+    """prox_mode 2 (Newton from the better of the network and the last
+    stretches) against prox_mode 1 on the 8 x 8 x 32 bar: the same prox
+    solutions to 1e-12, so the same solve."""
+    bar = bars.config0()
+    res = {}
+    for mode in (1, 2):
+        s = Solver(youngs=E_YOUNG, poisson=NU, lbfgs_m=5, prox_mode=mode, max_iters=120)
+        s.add_tetmesh(bar.rest, bar.init, bar.tets)
+        s.set_pins(bar.pins)
+        if mode == 2:
+            s.set_prox_net(prox_net.load_default())
+        s.initialize()
+        X = s.solve()
+        res[mode] = (X, s.algorithm_data())
+    X1, d1 = res[1]
+    X2, d2 = res[2]
+    assert np.abs(X2 - X1).max() <= 1e-6 * np.abs(X1).max()
+    assert d2.prox_iters.mean() <= d1.prox_iters.mean()
+    print("mean prox iterations: Newton", d1.prox_iters.mean(), "network", d2.prox_iters.mean())

@@ -20,7 +20,8 @@ ERRORS = {
     -9: "WRAPD_E_STATE", -10: "WRAPD_E_UNSUPPORTED",
 }
 LOGS = {"objectives": 0, "reweighted": 1, "flips": 2, "inner_iters": 3, "ls_delta_al": 4,
-        "gs_delta_al": 5, "accumulated_time_s": 6, "x_errors": 7}
+        "gs_delta_al": 5, "accumulated_time_s": 6, "x_errors": 7, "prox_iters": 8}
+NET_BLOB = 4755
 
 
 class WrapdError(RuntimeError):
@@ -44,6 +45,7 @@ class Settings(ctypes.Structure):
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
+_fp = ctypes.POINTER(ctypes.c_float)
 _lib = None
 
 # (name, restype, argtypes) for every entry point of include/wrapd_gpu.h
@@ -84,6 +86,19 @@ SIGNATURES = [
     ("wrapd_potential_energy_batch_noalloc", ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                              ctypes.c_void_p]),
+    ("wrapd_prox_newton_batch", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_double, ctypes.c_int, _dp, _dp, _dp, _dp, _ip]),
+    ("wrapd_net_create", ctypes.c_int, [_fp, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("wrapd_net_set_data", ctypes.c_int, [ctypes.c_void_p, _fp, _fp, ctypes.c_int64]),
+    ("wrapd_net_train", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                        ctypes.c_uint64, _dp]),
+    ("wrapd_net_grad", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, _dp, _fp]),
+    ("wrapd_net_get", ctypes.c_int, [ctypes.c_void_p, _fp]),
+    ("wrapd_net_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
+    ("wrapd_net_destroy", None, [ctypes.c_void_p]),
+    ("wrapd_net_predict", ctypes.c_int, [_fp, ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_double,
+                                          ctypes.c_double, _dp]),
+    ("wrapd_set_prox_net", ctypes.c_int, [ctypes.c_void_p, _fp, ctypes.c_int]),
 ]
 
 
@@ -110,6 +125,18 @@ def prox_batch(mu, lam, sigma0, wov, start, max_iters: int = 20, fp32: bool = Fa
     out, its = np.empty((n, 3)), np.empty(n, dtype=np.int32)
     _check_free(load().wrapd_prox_batch(n, int(fp32), mu, lam, max_iters, dptr(s0), dptr(w), dptr(st), dptr(out),
                                         iptr(its)))
+    return out, its
+
+
+def prox_newton_batch(mu, lam, sigma0, wov, start, tol: float = 1e-10, max_iters: int = 100, fp32: bool = False):
+    """The Newton prox per element; returns (stretches, iteration counts)."""
+    s0 = np.ascontiguousarray(sigma0, dtype=np.float64).reshape(-1, 3)
+    w = np.ascontiguousarray(wov, dtype=np.float64).ravel()
+    st = np.ascontiguousarray(start, dtype=np.float64).reshape(-1, 3)
+    n = s0.shape[0]
+    out, its = np.empty((n, 3)), np.empty(n, dtype=np.int32)
+    _check_free(load().wrapd_prox_newton_batch(n, int(fp32), mu, lam, tol, max_iters, dptr(s0), dptr(w), dptr(st),
+                                               dptr(out), iptr(its)))
     return out, its
 
 
@@ -144,6 +171,10 @@ def load():
         f.argtypes = args
     _lib = lib
     return lib
+
+
+def fptr(a: np.ndarray):
+    return a.ctypes.data_as(_fp)
 
 
 def dptr(a: np.ndarray):

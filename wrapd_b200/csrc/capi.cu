@@ -124,6 +124,11 @@ int wrapd_get_positions(wrapd_handle* h, double* x_out) {
     return guarded(h, [&](wrapd::SolverGPU& s) { s.positions(x_out); });
 }
 
+int wrapd_set_prox_net(wrapd_handle* h, const float* blob, int n_blob) {
+    if (!blob || n_blob != WRAPD_NET_BLOB) return WRAPD_E_INPUT;
+    return guarded(h, [&](wrapd::SolverGPU& s) { s.set_prox_net(blob); });
+}
+
 int wrapd_get_log(wrapd_handle* h, int which, double* out, int cap, int* len) {
     return guarded(h, [&](wrapd::SolverGPU& s) {
         const wrapd::Logs& L = s.logs();
@@ -137,6 +142,7 @@ int wrapd_get_log(wrapd_handle* h, int which, double* out, int cap, int* len) {
             case WRAPD_LOG_GS_DELTA_AL: v = L.gs_dal; break;
             case WRAPD_LOG_ACCUMULATED_TIME_S: v = L.acc_time_s; break;
             case WRAPD_LOG_X_ERRORS: v = L.x_errors; break;
+            case WRAPD_LOG_PROX_ITERS: v = L.prox_iters; break;
             default: throw wrapd::CudaError(WRAPD_E_INPUT, "unknown log channel");
         }
         if (len) *len = static_cast<int>(v.size());

@@ -44,6 +44,25 @@ __global__ void k_prox_batch(int n, double mu, double lambda, int max_iters, con
     for (int i = 0; i < 3; ++i) out[3 * (size_t)e + i] = x[i];
 }
 
+template <typename T>
+__global__ void k_newton_batch(int n, double mu, double lambda, double tol, int max_iters,
+                               const double* __restrict__ s0, const double* __restrict__ wov,
+                               const double* __restrict__ start, double* __restrict__ out, int* __restrict__ iters) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    Prox<T> P;
+    P.nh.mu = T(mu);
+    P.nh.lambda = T(lambda);
+    T x[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { P.x0[i] = T(s0[3 * (size_t)e + i]); x[i] = T(start[3 * (size_t)e + i]); }
+    P.wov = T(wov[e]);
+    const int it = prox_newton(P, x, max_iters, T(tol));
+    if (iters) iters[e] = it;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) out[3 * (size_t)e + i] = x[i];
+}
+
 // potential_energy_x + inversion_count over a batch of stretch triples
 // (src/TetElements.cpp:598-635, 444-468): out[0] = sum vol * psi(sigma),
 // out[1] = number of triples with a negative entry.  Deterministic two-level
@@ -158,6 +177,31 @@ WRAPD_API int wrapd_prox_batch(int n, int fp32, double mu, double lambda, int ma
                                                                   dit.as<int>());
     if ((e = cudaGetLastError()) != cudaSuccess) return finish(e);
     if ((e = cudaMemcpy(out, dout.p, 3 * (size_t)n * 8, cudaMemcpyDeviceToHost)) != cudaSuccess) return finish(e);
+    return finish(cudaMemcpy(iters, dit.p, (size_t)n * 4, cudaMemcpyDeviceToHost));
+}
+
+WRAPD_API int wrapd_prox_newton_batch(int n, int fp32, double mu, double lambda, double tol, int max_iters,
+                                      const double* sigma0, const double* wov, const double* start, double* out,
+                                      int* iters) {
+    if (n < 0 || max_iters < 0 || !(tol > 0.0) || (n > 0 && (!sigma0 || !wov || !start || !out))) return WRAPD_E_INPUT;
+    if (n == 0) return WRAPD_OK;
+    DevBuf d0(3 * (size_t)n * 8), dw((size_t)n * 8), ds(3 * (size_t)n * 8), dout(3 * (size_t)n * 8),
+        dit((size_t)n * 4);
+    if (!d0.p || !dw.p || !ds.p || !dout.p || !dit.p) return WRAPD_E_OOM;
+    cudaError_t e;
+    if ((e = cudaMemcpy(d0.p, sigma0, 3 * (size_t)n * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return finish(e);
+    if ((e = cudaMemcpy(dw.p, wov, (size_t)n * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return finish(e);
+    if ((e = cudaMemcpy(ds.p, start, 3 * (size_t)n * 8, cudaMemcpyHostToDevice)) != cudaSuccess) return finish(e);
+    const int b = (n + 127) / 128;
+    if (fp32)
+        k_newton_batch<float><<<b, 128>>>(n, mu, lambda, tol, max_iters, d0.as<double>(), dw.as<double>(),
+                                          ds.as<double>(), dout.as<double>(), dit.as<int>());
+    else
+        k_newton_batch<double><<<b, 128>>>(n, mu, lambda, tol, max_iters, d0.as<double>(), dw.as<double>(),
+                                           ds.as<double>(), dout.as<double>(), dit.as<int>());
+    if ((e = cudaGetLastError()) != cudaSuccess) return finish(e);
+    if ((e = cudaMemcpy(out, dout.p, 3 * (size_t)n * 8, cudaMemcpyDeviceToHost)) != cudaSuccess) return finish(e);
+    if (!iters) return finish(cudaDeviceSynchronize());
     return finish(cudaMemcpy(iters, dit.p, (size_t)n * 4, cudaMemcpyDeviceToHost));
 }
 

@@ -6,6 +6,7 @@
 #pragma once
 #include "elem_math.cuh"
 #include "elem_types.cuh"
+#include "prox_net.cuh"
 
 namespace wrapd {
 
@@ -191,20 +192,34 @@ static __global__ void __launch_bounds__(256) k_gather(int nf, const int* __rest
 // U update, and the candidate weight (src/TetElements.cpp:391-432).  C is the
 // arithmetic of the SVD and the prox (double, or float in mixed mode); loads,
 // stores, the dual update and every sum are FP64.
-// out[0..3] = bef_penalty, aft_penalty, curr_pe, negative-stretch count.
-// prox_mode 0: the reference's L-BFGS prox; 1: Newton (prox_newton).  The FP32
-// instantiation always uses Newton (see prox_newton).
-template <typename C>
+// out[0..4] = bef_penalty, aft_penalty, curr_pe, negative-stretch count, prox
+// iterations.
+// prox_mode 0: the reference's L-BFGS prox; 1: Newton (prox_newton); 2 (NET):
+// Newton from the better (lower prox objective) of the last stretches and the
+// prox network's prediction.  The FP32 instantiation always uses Newton.
+// NET needs dynamic shared memory: the network image plus one scratch per warp.
+template <typename C, bool NET>
 __global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat, int prox_iters, int cand_mode,
-                                               int prox_mode, double* partials, unsigned* counter, double* out) {
+                                               int prox_mode, const unsigned char* __restrict__ net_img,
+                                               double* partials, unsigned* counter, double* out) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    double red[4] = {0.0, 0.0, 0.0, 0.0};
-    if (e < E.ne) {
-        double S[9], Um[9], Zm[9];
+    const bool valid = e < E.ne;
+    double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    extern __shared__ __align__(16) unsigned char local_smem[];
+    if constexpr (NET) {
+        net::load_image(net_img, local_smem);
+        __syncthreads();
+    }
+    double S[9], Um[9];
+    double w2 = 0.0, vol = 1.0;
+    C sg[3] = {C(1), C(1), C(1)}, Ue[9], Ve[9];
+    if (valid) {
+        double Zm[9];
         load9(E.symF, E.ne, e, S);
         load9(E.U, E.ne, e, Um);
         load9(E.Z, E.ne, e, Zm);
-        const double w2 = E.w2[e], vol = E.vol[e];
+        w2 = E.w2[e];
+        vol = E.vol[e];
         C Sin[9];
         double bef = 0.0;
 #pragma unroll
@@ -216,25 +231,45 @@ __global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat, int 
                 bef += d * d;
             }
         red[0] = 0.5 * w2 * bef;
-        C sg[3], Ue[9], Ve[9];
         svd3(Sin, sg, Ue, Ve);
-        Prox<C> P;
-        P.nh.mu = C(mat.mu);
-        P.nh.lambda = C(mat.lambda);
-        P.x0[0] = sg[0]; P.x0[1] = sg[1]; P.x0[2] = sg[2];
-        P.wov = C(w2 / vol);
-        C xs[3];
+    }
+    Prox<C> P;
+    P.nh.mu = C(mat.mu);
+    P.nh.lambda = C(mat.lambda);
+    P.x0[0] = sg[0]; P.x0[1] = sg[1]; P.x0[2] = sg[2];
+    P.wov = C(w2 / vol);
+    C xs[3] = {C(1), C(1), C(1)};
+    if (valid) {
 #pragma unroll
         for (int i = 0; i < 3; ++i) xs[i] = C(E.slast[(size_t)i * E.ne + e]);
+    }
+    if constexpr (NET) {
+        // warp-collective: every lane runs the network, lanes past the end on dummies
+        const float sf[3] = {float(sg[0]), float(sg[1]), float(sg[2])};
+        float f[net::IN], y[net::OUT], pr[3];
+        net::features(sf, valid ? float(w2 / vol) : float(mat.mu), float(mat.mu), float(mat.lambda), f);
+        net::warp_forward(local_smem, local_smem + net::IMAGE_BYTES + (threadIdx.x >> 5) * net::WARP_SCRATCH, f,
+                          valid, y);
+        net::predict_start(local_smem, sf, y, pr);
+        if (valid) {
+            const C cand[3] = {C(pr[0]), C(pr[1]), C(pr[2])};
+            if (isfinite(cand[0]) && isfinite(cand[1]) && isfinite(cand[2]) && P.value(cand) < P.value(xs)) {
+                xs[0] = cand[0]; xs[1] = cand[1]; xs[2] = cand[2];
+            }
+        }
+    }
+    if (valid) {
+        int iters;
         if constexpr (sizeof(C) == sizeof(double)) {
-            if (prox_mode == 1) {
-                prox_newton(P, xs, prox_iters, C(1e-12));
+            if (NET || prox_mode == 1) {
+                iters = prox_newton(P, xs, prox_iters, C(1e-12));
             } else {
                 extern __shared__ double prox_hist[];   // 48 x blockDim doubles
-                prox_lbfgs(P, xs, prox_iters, ProxHistory<double>{prox_hist + threadIdx.x, (int)blockDim.x});
+                iters = prox_lbfgs(P, xs, prox_iters, ProxHistory<double>{prox_hist + threadIdx.x, (int)blockDim.x});
+                if (iters < 0) iters = prox_iters;
             }
         } else {
-            prox_newton(P, xs, prox_iters, C(8) * Lim<C>::eps());
+            iters = prox_newton(P, xs, prox_iters, C(8) * Lim<C>::eps());
         }
         if (sizeof(C) < sizeof(double) &&
             !(isfinite(xs[0]) && isfinite(xs[1]) && isfinite(xs[2]) && xs[0] >= C(0) && xs[1] >= C(0) && xs[2] >= C(0))) {
@@ -248,10 +283,11 @@ __global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat, int 
             double xd[3];
 #pragma unroll
             for (int i = 0; i < 3; ++i) xd[i] = E.slast[(size_t)i * E.ne + e];
-            prox_newton(Pd, xd, prox_iters, 1e-12);
+            iters += prox_newton(Pd, xd, prox_iters, 1e-12);
 #pragma unroll
             for (int i = 0; i < 3; ++i) xs[i] = C(xd[i]);
         }
+        red[4] = double(iters);
         double xo[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i) { xo[i] = double(xs[i]); E.slast[(size_t)i * E.ne + e] = xo[i]; }
@@ -264,7 +300,7 @@ __global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat, int 
                 M3(Soc, r, c) = M3(Ve, r, 0) * xs[0] * M3(Ue, c, 0) + M3(Ve, r, 1) * xs[1] * M3(Ue, c, 1) +
                                 M3(Ve, r, 2) * xs[2] * M3(Ue, c, 2);
         red[2] = vol * NH<double>{mat.mu, mat.lambda}.psi_plain(xo[0], xo[1], xo[2]);
-        double aft = 0.0;
+        double aft = 0.0, Zm[9];
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
             const double So = double(Soc[i]);
@@ -286,7 +322,7 @@ __global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat, int 
             E.w2c[e] = vol * c;
         }
     }
-    grid_reduce<4>(red, partials, counter, out);
+    grid_reduce<5>(red, partials, counter, out);
 }
 
 // initialize_dual_vars (src/TetElements.cpp:145-166): Z = (V diag(s) V^T)^T of

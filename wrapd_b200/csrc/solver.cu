@@ -17,8 +17,8 @@ namespace {
 enum : int {
     S_GRAD = 0,      // value, pe, flips
     S_GATHER = 4,    // |grad - gold|^2, <s, y>
-    S_LOCAL = 8,     // bef, aft, pe, negative stretches
-    S_INIT = 12,     // polar potential energy after initialize_dual_vars
+    S_LOCAL = 8,     // bef, aft, pe, negative stretches, prox iterations
+    S_INIT = 13,     // polar potential energy after initialize_dual_vars
     S_RATIO = 14,    // max weight ratio
     S_DIR = 16,      // L-BFGS decrement
     S_XERR = 18,     // |x - x_soln|^2
@@ -79,8 +79,8 @@ SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
     if (cfg.rot_aware != 1) throw CudaError(WRAPD_E_UNSUPPORTED, "rotation-unaware global step (-ra 0) is not implemented");
     if (cfg.global_ls != 0) throw CudaError(WRAPD_E_UNSUPPORTED, "global-step line search (-global_ls 1) is not implemented");
     if (cfg.model != 0) throw CudaError(WRAPD_E_UNSUPPORTED, "only the Neo-Hookean model is implemented");
-    if (cfg.prox_mode != 0 && cfg.prox_mode != 1)
-        throw CudaError(WRAPD_E_UNSUPPORTED, "prox_mode must be 0 (L-BFGS) or 1 (Newton)");
+    if (cfg.prox_mode < 0 || cfg.prox_mode > 2)
+        throw CudaError(WRAPD_E_UNSUPPORTED, "prox_mode must be 0 (L-BFGS), 1 (Newton) or 2 (Newton from the prox network)");
     if (cfg.lbfgs_m < 1 || cfg.lbfgs_m > kMaxHistory) throw CudaError(WRAPD_E_INPUT, "lbfgs_m must be in [1, 32]");
     if (cfg.max_iters < 0 || cfg.global_iters < 1 || cfg.prox_iters < 1) throw CudaError(WRAPD_E_INPUT, "bad iteration limits");
     if (!(cfg.poisson > -1.0 && cfg.poisson < 0.5) || !(cfg.youngs > 0.0)) throw CudaError(WRAPD_E_INPUT, "bad material");
@@ -92,7 +92,7 @@ SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
     WRAPD_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     for (auto& e : ev_) WRAPD_CUDA(cudaEventCreate(&e));
     WRAPD_CUDA(cudaMallocHost(&h_scal_, S_COUNT * sizeof(double)));
-    WRAPD_CUDA(cudaFuncSetAttribute(k_local<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLocalHistBytes));
+    WRAPD_CUDA(cudaFuncSetAttribute(k_local<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLocalHistBytes));
     // Lame(E, nu), src/Lame.hpp:50-53; k = 2.0066 mu + 1.0122 lambda, src/TetElements.cpp:84
     mat_.mu = cfg.youngs / (2.0 * (1.0 + cfg.poisson));
     mat_.lambda = cfg.youngs * cfg.poisson / ((1.0 + cfg.poisson) * (1.0 - 2.0 * cfg.poisson));
@@ -105,6 +105,7 @@ SolverGPU::~SolverGPU() {
     if (st_) cudaStreamSynchronize(st_);
     for (cudaEvent_t e : event_pool_) cudaEventDestroy(e);
     for (void* p : allocs_) cudaFree(p);
+    if (d_net_img_) cudaFree(d_net_img_);
     for (auto& e : ev_) if (e) cudaEventDestroy(e);
     if (h_scal_) cudaFreeHost(h_scal_);
     if (st_) cudaStreamDestroy(st_);
@@ -324,7 +325,7 @@ void SolverGPU::initialize() {
     }
     rho_.assign(cfg.lbfgs_m, 0.0);
     const size_t nblk = (size_t)blocks_for(std::max(ne, nf), 128) + 2 * kNumSMs + 8;
-    d_partials_ = static_cast<double*>(dalloc(nblk * 4 * sizeof(double)));
+    d_partials_ = static_cast<double*>(dalloc(nblk * 5 * sizeof(double)));
     d_counter_ = static_cast<unsigned*>(dalloc(sizeof(unsigned)));
     d_scal_ = static_cast<double*>(dalloc(S_COUNT * sizeof(double)));
     WRAPD_CUDA(cudaMemsetAsync(d_counter_, 0, sizeof(unsigned), st_));
@@ -368,15 +369,41 @@ void SolverGPU::gather(double* grad, const double* gold, double* ystage, const d
 }
 
 void SolverGPU::local_step(int cand_mode, bool fp32_compute) {
-    if (fp32_compute)
-        k_local<float><<<blocks_for(ne, 128), 128, 0, st_>>>(view(), mat_, cfg.prox_iters, cand_mode, 1,
+    const int nb = blocks_for(ne, 128);
+    const bool net = cfg.prox_mode == 2;
+    const int net_smem = net::IMAGE_BYTES + 4 * net::WARP_SCRATCH;
+    if (net && !d_net_img_) throw CudaError(WRAPD_E_STATE, "prox_mode 2 needs a network (wrapd_set_prox_net)");
+    if (fp32_compute) {
+        if (net)
+            k_local<float, true><<<nb, 128, net_smem, st_>>>(view(), mat_, cfg.prox_iters, cand_mode, 2, d_net_img_,
                                                              d_partials_, d_counter_, d_scal_ + S_LOCAL);
-    else
-        k_local<double><<<blocks_for(ne, 128), 128, kLocalHistBytes, st_>>>(view(), mat_, cfg.prox_iters, cand_mode,
-                                                              fp32() ? 1 : cfg.prox_mode, d_partials_, d_counter_,
-                                                              d_scal_ + S_LOCAL);
+        else
+            k_local<float, false><<<nb, 128, 0, st_>>>(view(), mat_, cfg.prox_iters, cand_mode, 1, nullptr,
+                                                       d_partials_, d_counter_, d_scal_ + S_LOCAL);
+    } else {
+        if (net)
+            k_local<double, true><<<nb, 128, net_smem, st_>>>(view(), mat_, cfg.prox_iters, cand_mode, 2, d_net_img_,
+                                                              d_partials_, d_counter_, d_scal_ + S_LOCAL);
+        else
+            k_local<double, false><<<nb, 128, kLocalHistBytes, st_>>>(view(), mat_, cfg.prox_iters, cand_mode,
+                                                                      fp32() ? 1 : cfg.prox_mode, nullptr, d_partials_,
+                                                                      d_counter_, d_scal_ + S_LOCAL);
+    }
     WRAPD_LAUNCH_CHECK();
     kernel_launches++;
+}
+
+void SolverGPU::set_prox_net(const float* blob) {
+    if (!d_net_img_) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, net::IMAGE_BYTES + net::N_BLOB * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError();
+            throw CudaError(WRAPD_E_OOM, "cudaMalloc failed (prox network)");
+        }
+        d_net_img_ = static_cast<unsigned char*>(p);
+    }
+    net::upload_image(blob, d_net_img_, reinterpret_cast<float*>(d_net_img_ + net::IMAGE_BYTES), st_);
+    WRAPD_CUDA(cudaStreamSynchronize(st_));
 }
 
 void SolverGPU::mid_candidates(bool from_x, int cand_mode) {
@@ -605,6 +632,7 @@ int SolverGPU::iterate(int n, bool* conv) {
         mark(1);
         sync_read();
         const double bef = h_scal_[S_LOCAL], aft = h_scal_[S_LOCAL + 1], pe = h_scal_[S_LOCAL + 2];
+        const double prox_it = h_scal_[S_LOCAL + 4];
         if (h_scal_[S_LOCAL + 3] > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
         const double dal = aft - bef + pe - curr_pe_;
         curr_pe_ = pe;
@@ -649,6 +677,7 @@ int SolverGPU::iterate(int n, bool* conv) {
         logs_.ls_dal.push_back(std::fabs(dal));
         logs_.gs_dal.push_back(std::fabs(obj_aft - obj_bef));
         logs_.inner.push_back(its);
+        logs_.prox_iters.push_back(prox_it / double(ne));
         logs_.objectives.push_back(pe_x);
         logs_.flips.push_back(flips);
         logs_.acc_time_s.push_back((runtime_ms[1] + runtime_ms[2] + runtime_ms[3]) / 1000.0);

@@ -17,7 +17,7 @@
 namespace wrapd {
 
 struct Logs {
-    std::vector<double> objectives, ls_dal, gs_dal, acc_time_s, x_errors;
+    std::vector<double> objectives, ls_dal, gs_dal, acc_time_s, x_errors, prox_iters;
     std::vector<int> flips, reweighted, inner;
 };
 
@@ -33,6 +33,8 @@ public:
     // runs up to n iterations; returns iterations done; *converged set when the test passes
     int iterate(int n, bool* converged);
     void positions(double* out);
+    // installs the prox network (FP32 blob, net::N_BLOB floats) used by prox_mode 2
+    void set_prox_net(const float* blob);
     void solve(double* out);
 
     // components
@@ -104,6 +106,7 @@ private:
     std::vector<double*> s_, y_;
     std::vector<double> rho_;
     double* d_partials_ = nullptr;
+    unsigned char* d_net_img_ = nullptr;   // prox network image + FP32 blob staging
     unsigned* d_counter_ = nullptr;
     double* d_scal_ = nullptr;
     double* h_scal_ = nullptr;

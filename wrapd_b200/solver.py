@@ -48,6 +48,7 @@ class AlgorithmData:
     gs_delta_al: np.ndarray
     accumulated_time_s: np.ndarray
     x_errors: np.ndarray
+    prox_iters: np.ndarray
     runtime_ms: dict
 
 
@@ -131,6 +132,11 @@ class Solver:
         v = (ctypes.c_int64 * 4)()
         self._h.check(self._h.lib.wrapd_get_counters(self._h.h, v))
         return dict(zip(["kernel_launches", "factorizations", "solves", "host_syncs"], list(v)))
+
+    def set_prox_net(self, blob):
+        """Install the prox network for prox_mode 2 (an FP32 blob, capi.NET_BLOB floats)."""
+        b = np.ascontiguousarray(blob, dtype=np.float32).ravel()
+        self._h.check(self._h.lib.wrapd_set_prox_net(self._h.h, capi.fptr(b), b.size))
 
     def set_profiling(self, on: bool = True):
         self._h.check(self._h.lib.wrapd_set_profiling(self._h.h, int(on)))
