@@ -1,17 +1,20 @@
 """Benchmark of the ADMM solve loop on the 32x32x128 twisted-and-bent bar.
 
-Workload: 786,432 tets / 140,481 vertices (configs[1] of the benchmark
-definition), E = 1e5 Pa, nu = 0.45, global L-BFGS history 5, reweighting (and
-GPU refactorization) every 10 iterations, FP64.  One step = one ADMM iteration
-(local step, global L-BFGS step with its triangular solves, reweight check).
+Workload: 786,432 tets / 140,481 vertices, E = 1e5 Pa, nu = 0.45, global
+L-BFGS history 5, reweighting (and GPU refactorization) every 10 iterations,
+FP64.  One step = one ADMM iteration (local step, global L-BFGS step with its
+triangular solves, reweight check).
 
 Metric: ADMM element-iterations per second (elements x iterations / seconds),
 the throughput behind the time-to-energy-gap metric; `local_elems_per_s` adds
 the local step alone.  Inputs are far larger than L2 (the element state is
-~0.7 GB), so no L2 flush is needed between steps.
+~0.7 GB), so no L2 flush is needed between steps.  The same line carries the
+learned/FP32 form on the same bar and the time to relative energy gap 1e-6 of
+the four solver forms on the 8x8x32 bar (the large bar keeps inverted
+elements and does not reach that gap).
 
 Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-        [--precision fp64|mixed]
+        [--precision fp64|mixed] [--parts main,learned,gap,e2e]
 For N > 1 launch with torchrun: every rank solves its own replica of the bar
 (the path does not shard; replicas only, weak scaling).
 """
@@ -46,6 +49,8 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--parts", default="main,learned,gap,e2e",
+                   help="measurements to run after the main one (main is always run)")
     return p.parse_args()
 
 
@@ -205,6 +210,65 @@ def cpu_baseline():
             "sample": "32x32x16 slice of the bar (98,304 tets), 5 iterations of the C oracle"}
 
 
+# ---- time to energy gap --------------------------------------------------------------
+FORMS = [
+    ("plain_fp64", dict(precision="fp64", prox_mode=0)),        # the reference's method on the GPU
+    ("fp64_newton", dict(precision="fp64", prox_mode=1)),
+    ("fp32_newton", dict(precision="mixed", prox_mode=1)),
+    ("learned_fp32", dict(precision="mixed", prox_mode=2)),     # network warm start, FP32 local step
+]
+
+
+def gap_time(objectives, acc_time_s, e_star, gap=1e-6):
+    """Solver time (local + global + refactor, device events) at the first
+    iterate from which (E_k - E*) / |E*| stays <= gap; None if never."""
+    g = (np.asarray(objectives) - e_star) / abs(e_star)
+    bad = np.nonzero(g > gap)[0]
+    k = 0 if bad.size == 0 else int(bad[-1]) + 1
+    if k >= len(g):
+        return None, None
+    return float(acc_time_s[k]), k
+
+
+def time_to_gap(bar, label, device, base, e_star_iters=20000, gap=1e-6):
+    """E* = lowest energy of a long plain-FP64 run (tol 1e-13); then each form
+    to convergence at tol 1e-13, reporting its time to the gap, iterations and
+    the final positions' error against the plain FP64 run (which matches the
+    FP64 oracle to 1e-8 in the parity tests)."""
+    from wrapd_b200 import prox_net
+    from wrapd_b200.solver import Solver
+
+    def run(kw):
+        s = Solver(**dict(base, **kw, device=device))
+        s.add_tetmesh(bar.rest, bar.init, bar.tets)
+        s.set_pins(bar.pins)
+        if kw.get("prox_mode") == 2:
+            s.set_prox_net(prox_net.load_default())
+        s.initialize()
+        X = s.solve()
+        d = s.algorithm_data()
+        s.close()
+        return X, d
+
+    Xr, dr = run(dict(FORMS[0][1], tol=1e-13, max_iters=e_star_iters))
+    e_star = float(dr.objectives.min())
+    out = {"workload": label, "gap": gap, "e_star": e_star, "e_star_run_iters": int(len(dr.objectives) - 1),
+           "time_source": "solver accumulated_time_s (CUDA events: local + global + refactor)", "forms": {}}
+    for name, kw in FORMS:
+        X, d = (Xr, dr) if name == "plain_fp64" else run(dict(kw, tol=1e-13, max_iters=e_star_iters))
+        t, k = gap_time(d.objectives, d.accumulated_time_s, e_star, gap)
+        out["forms"][name] = {
+            "seconds_to_gap": t, "iterations_to_gap": k, "iterations_run": int(len(d.objectives) - 1),
+            "final_rel_gap": float((d.objectives[-1] - e_star) / abs(e_star)),
+            "x_err_vs_plain_fp64": float(np.abs(X - Xr).max() / np.abs(Xr).max()),
+            "mean_prox_iters": float(np.mean(d.prox_iters)) if len(d.prox_iters) else None,
+        }
+    p0 = out["forms"]["plain_fp64"]["seconds_to_gap"]
+    pl = out["forms"]["learned_fp32"]["seconds_to_gap"]
+    out["speedup_learned_fp32_vs_plain_fp64"] = (p0 / pl) if (p0 and pl) else None
+    return out
+
+
 def profile_traffic():
     """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "k_local_config1.md")
@@ -270,8 +334,9 @@ def run_ours(args, rank, world, local, pg):
     achieved = lbytes / (local_ms / K / 1000.0) / 1e9
     traffic = profile_traffic()
     # e2e: a fresh solve through the C ABI from host buffers, setup included
+    parts = set(args.parts.split(","))
     e2e = None
-    if rank == 0:
+    if rank == 0 and "e2e" in parts:
         t0 = time.perf_counter()
         s2 = Solver(**settings)
         s2.add_tetmesh(bar.rest, bar.init, bar.tets)
@@ -287,6 +352,34 @@ def run_ours(args, rank, world, local, pg):
                "d2h_bytes_per_step": int(X.nbytes // K), "wall_s": e2e_s,
                "includes": "create + add_tetmesh + initialize (symbolic + factor) + begin_solve + K iterations + positions"}
         s2.close()
+    # the learned/FP32 form on the same bar: local step (FP32 SVD + network-started Newton)
+    learned = None
+    if rank == 0 and "learned" in parts:
+        from wrapd_b200 import prox_net
+        s3 = Solver(**dict(settings, precision="mixed", prox_mode=2))
+        s3.add_tetmesh(bar.rest, bar.init, bar.tets)
+        s3.set_pins(bar.pins)
+        s3.set_prox_net(prox_net.load_default())
+        s3.initialize()
+        s3.begin_solve()
+        s3.iterate(args.warmup)
+        r0 = s3.runtime()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s3.iterate(K)
+        wall = time.perf_counter() - t0
+        r1 = s3.runtime()
+        lms = r1["local_ms"] - r0["local_ms"]
+        tot = sum(r1[k] - r0[k] for k in ("local_ms", "global_ms", "refactor_ms"))
+        learned = {"ms_per_step": tot / K, "local_ms_per_step": lms / K,
+                   "local_elems_per_s": ne * K / (lms / 1000.0), "elem_iter_per_s": ne * K / (tot / 1000.0),
+                   "wall_ms_per_step": 1000.0 * wall / K,
+                   "mean_prox_iters": float(np.mean(s3.log("prox_iters")[-K:]))}
+        s3.close()
+    gap = None
+    if rank == 0 and "gap" in parts:
+        gap = time_to_gap(bars.config0(), "bar 8x8x32 cubes x6 tets (12,288 tets), 180 deg twist, E=1e5 nu=0.45",
+                          local, dict(youngs=E_YOUNG, poisson=NU, lbfgs_m=5))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
@@ -303,6 +396,8 @@ def run_ours(args, rank, world, local, pg):
             "local_elems_per_s": world * ne * K / (local_ms / 1000.0),
             "phase_ms_per_step": {"local": local_ms / K, "global": glob_ms / K, "refactor": ref_ms / K},
             "inner_iters_per_step": inner / K,
+            "learned_fp32_same_bar": learned,
+            "time_to_gap": gap,
             "roofline": {"kernel": "k_local (fused local step)", "bound": "hbm", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind, "bytes_per_launch": lbytes},

@@ -73,7 +73,9 @@ typedef struct wrapd_settings {
     int rw_every;         /* 0: gamma rule; N > 0: reweight (and refactor) every N iterations */
     int precision;        /* 0: FP64 throughout; 1: FP32 local step (SVD + Newton prox), FP64 elsewhere */
     int prox_mode;        /* 0: L-BFGS prox as the reference (parity mode); 1: Newton prox;
-                             2: Newton prox warm-started by the prox network (wrapd_set_prox_net) */
+                             2: Newton prox warm-started by the prox network (wrapd_set_prox_net) on
+                             the first local step and the one after each reweight, from the last
+                             stretches elsewhere */
     int leaf_size;        /* nested-dissection leaf size for the factorization, 64 */
     int verbose;          /* -p          0 here (1 prints the reference's table) */
     int device;           /* CUDA device ordinal, 0 */
@@ -104,14 +106,28 @@ WRAPD_API int wrapd_create(const wrapd_settings* s, wrapd_handle** out);
 /* binding::add_tetmesh + System::add_nodes + create_tets_from_mesh +
  * Solver::set_pins (samples/utils/AddMeshes.hpp:61-132, src/System.hpp:75-92,
  * src/TetElements.hpp:250-288, src/System.cpp:33-44).  Pins are vertex ids
- * held in place at init_xyz.  soln_xyz may be NULL.  One mesh per handle. */
+ * held in place at init_xyz.  soln_xyz may be NULL.  Called again before
+ * wrapd_initialize, it appends another mesh (vertex ids of each call are its
+ * own, shifted as add_tetmesh's prev_tet_verts does): the meshes form a batch
+ * solved as one block-diagonal system -- one local-step launch over all their
+ * elements, one factorization holding one tree per mesh.  (The reference's
+ * add_tetmesh replaces the element set on a second call; the batch is an
+ * extension.)  Positions of the batch are returned in the order added. */
 WRAPD_API int wrapd_add_tetmesh(wrapd_handle* h, const double* rest_xyz, const double* init_xyz,
                       const double* soln_xyz, int n_verts, const int32_t* tets, int n_tets,
                       const int32_t* pins, int n_pins);
 
+/* wrapd_add_tetmesh with the mesh's own material (extension): Young's
+ * modulus and Poisson ratio of this mesh in place of the settings' youngs and
+ * poisson, for batches of meshes of different materials. */
+WRAPD_API int wrapd_add_tetmesh_material(wrapd_handle* h, const double* rest_xyz, const double* init_xyz,
+                                         const double* soln_xyz, int n_verts, const int32_t* tets, int n_tets,
+                                         const int32_t* pins, int n_pins, double youngs, double poisson);
+
 /* wrapd::Solver::initialize (src/Solver.cpp:48-60) -> ADMM::initialize
  * (src/ADMM.cpp:34-56): element precompute, initial weights, symbolic
- * analysis and the first numeric factorization, all on the device. */
+ * analysis (one nested dissection per mesh) and the first numeric
+ * factorization, all on the device. */
 WRAPD_API int wrapd_initialize(wrapd_handle* h);
 
 /* wrapd::Solver::solve (src/Solver.cpp:38-46) -> ADMM::solve

@@ -35,7 +35,8 @@ class OracleProblem(ctypes.Structure):
                 ("global_iters", ctypes.c_int), ("kappa", ctypes.c_double),
                 ("reweighting", ctypes.c_int), ("rw_delay", ctypes.c_int), ("gamma", ctypes.c_double),
                 ("beta_static", ctypes.c_double), ("beta_min", ctypes.c_double),
-                ("beta_max", ctypes.c_double), ("rw_every", ctypes.c_int)]
+                ("beta_max", ctypes.c_double), ("rw_every", ctypes.c_int),
+                ("youngs_e", _dp), ("poisson_e", _dp)]
 
 
 _lib = None
@@ -96,7 +97,8 @@ class Oracle:
 
     def __init__(self, rest, init, tets, pins, youngs=1e5, poisson=0.45, max_iters=500, tol=1e-11,
                  lbfgs_m=6, reweighting=1, rw_delay=50, gamma=1.5, rw_every=0, global_iters=100,
-                 kappa=1.0, beta_static=1.0, beta_min=0.1, beta_max=10.0):
+                 kappa=1.0, beta_static=1.0, beta_min=0.1, beta_max=10.0, youngs_e=None, poisson_e=None):
+        """youngs_e / poisson_e: per-element material (a batch of meshes), or None."""
         self.lib = load_oracle()
         self._keep = [np.ascontiguousarray(rest, dtype=np.float64),
                       np.ascontiguousarray(init, dtype=np.float64),
@@ -111,6 +113,10 @@ class Oracle:
         p.reweighting, p.rw_delay, p.gamma, p.rw_every = reweighting, rw_delay, gamma, rw_every
         p.global_iters, p.kappa = global_iters, kappa
         p.beta_static, p.beta_min, p.beta_max = beta_static, beta_min, beta_max
+        if youngs_e is not None:
+            self._keep += [np.ascontiguousarray(youngs_e, dtype=np.float64),
+                           np.ascontiguousarray(poisson_e, dtype=np.float64)]
+            p.youngs_e, p.poisson_e = _d(self._keep[-2]), _d(self._keep[-1])
         self.problem = p
         err = ctypes.c_int(0)
         self.h = self.lib.orc_create(ctypes.byref(p), ctypes.byref(err))

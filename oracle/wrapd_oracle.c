@@ -412,6 +412,7 @@ struct orc_state {
     orc_problem p;
     int ne, nv, nf, np;
     double mu, lambda, k_rest;
+    double *mu_e, *lambda_e;   /* per element (the uniform values unless the problem gives arrays) */
     int* fidx;   /* ne x 4: free index or -1 */
     int* xidx;   /* ne x 4: fixed index or -1 */
     int* tet;    /* ne x 4 */
@@ -453,6 +454,7 @@ void orc_problem_defaults(orc_problem* p) {
 
 void orc_destroy(orc_state* s) {
     if (!s) return;
+    free(s->mu_e); free(s->lambda_e);
     free(s->fidx); free(s->xidx); free(s->tet); free(s->nfree); free(s->free_of_vert); free(s->fix_of_vert);
     free(s->Di); free(s->vol); free(s->w2); free(s->w2c); free(s->DtD); free(s->Dfx);
     free(s->Z); free(s->U); free(s->slast); free(s->F); free(s->sig); free(s->Us); free(s->Vs); free(s->symF);
@@ -481,6 +483,11 @@ orc_state* orc_create(const orc_problem* p, int* err) {
     s->ne = p->n_tets; s->nv = p->n_verts; s->np = p->n_pins; s->nf = p->n_verts - p->n_pins;
     lame(p->youngs, p->poisson, &s->mu, &s->lambda);
     s->k_rest = 2.0066 * s->mu + 1.0122 * s->lambda;   /* src/TetElements.cpp:84 */
+    s->mu_e = NEWD(s->ne); s->lambda_e = NEWD(s->ne);
+    for (int e = 0; e < s->ne; ++e) {
+        if (p->youngs_e && p->poisson_e) lame(p->youngs_e[e], p->poisson_e[e], &s->mu_e[e], &s->lambda_e[e]);
+        else { s->mu_e[e] = s->mu; s->lambda_e[e] = s->lambda; }
+    }
     /* free/fixed maps from the sorted pins, samples/utils/AddMeshes.hpp:268-289 */
     int* sp = NEWI(s->np);
     memcpy(sp, p->pins, sizeof(int) * (size_t)s->np);
@@ -530,7 +537,7 @@ orc_state* orc_create(const orc_problem* p, int* err) {
                 for (int r = 0; r < 3; ++r) v += Di[r + 3 * a] * Di[r + 3 * b];
                 s->DtD[16 * e + a + 4 * b] = v;
             }
-        s->w2[e] = p->beta_static * s->k_rest * s->vol[e];
+        s->w2[e] = p->beta_static * (2.0066 * s->mu_e[e] + 1.0122 * s->lambda_e[e]) * s->vol[e];
         s->slast[3 * e] = s->slast[3 * e + 1] = s->slast[3 * e + 2] = 1.0;
     }
     free(sp);
@@ -609,7 +616,7 @@ void orc_update_defo_cache(orc_state* s) { defo_cache_at(s, s->xfree); }
 
 double orc_potential_energy(const orc_state* s) {
     double pe = 0.0;
-    for (int e = 0; e < s->ne; ++e) pe += s->vol[e] * orc_nh_psi_plain(s->mu, s->lambda, s->sig + 3 * e);
+    for (int e = 0; e < s->ne; ++e) pe += s->vol[e] * orc_nh_psi_plain(s->mu_e[e], s->lambda_e[e], s->sig + 3 * e);
     return pe;
 }
 
@@ -624,18 +631,18 @@ int orc_inversion_count(const orc_state* s) {
 
 /* update_all_candidate_weights, src/TetElements.cpp:391-432 */
 static void candidate_weights(orc_state* s, const double* sig) {
-    double wr = 2.0066 * s->mu + 1.0122 * s->lambda;
-    double wmin = wr * s->p.beta_min, wmax = wr * s->p.beta_max;
     if (s->count > s->p.rw_delay) {
         for (int e = 0; e < s->ne; ++e) {
-            double lm = orc_hess_lmax(s->mu, s->lambda, sig + 3 * e);
+            double wr = 2.0066 * s->mu_e[e] + 1.0122 * s->lambda_e[e];
+            double wmin = wr * s->p.beta_min, wmax = wr * s->p.beta_max;
+            double lm = orc_hess_lmax(s->mu_e[e], s->lambda_e[e], sig + 3 * e);
             double c = lm;
             if (lm < wmin) c = wmin;
             if (lm > wmax) c = wmax;
             s->w2c[e] = s->vol[e] * c;
         }
     } else {
-        for (int e = 0; e < s->ne; ++e) s->w2c[e] = s->vol[e] * wr;
+        for (int e = 0; e < s->ne; ++e) s->w2c[e] = s->vol[e] * (2.0066 * s->mu_e[e] + 1.0122 * s->lambda_e[e]);
     }
     s->count++;
 }
@@ -874,7 +881,7 @@ double orc_polar_update(orc_state* s, int update_candidates) {
         double* x = s->slast + 3 * e;
         double xs[3] = {x[0], x[1], x[2]};
         /* the reference ignores a failed line search and keeps the last iterate */
-        (void)orc_prox_lbfgs(s->mu, s->lambda, sg, s->w2[e] / s->vol[e], xs, 20);
+        (void)orc_prox_lbfgs(s->mu_e[e], s->lambda_e[e], sg, s->w2[e] / s->vol[e], xs, 20);
         memcpy(x, xs, sizeof xs);
         memcpy(tmp + 3 * e, xs, sizeof xs);
         if (xs[0] < 0.0 || xs[1] < 0.0 || xs[2] < 0.0) prox_error = 1;
@@ -885,7 +892,7 @@ double orc_polar_update(orc_state* s, int update_candidates) {
                 for (int k = 0; k < 3; ++k) v += A3(Ve, r, k) * xs[k] * A3(Ue, c, k);
                 A3(So, r, c) = v;
             }
-        pe += s->vol[e] * orc_nh_psi_plain(s->mu, s->lambda, xs);
+        pe += s->vol[e] * orc_nh_psi_plain(s->mu_e[e], s->lambda_e[e], xs);
         double SomU[9];
         for (int i = 0; i < 9; ++i) SomU[i] = So[i] - U[i];
         aft += 0.5 * s->w2[e] * fro2_diff(S, SomU);
@@ -1006,7 +1013,7 @@ static void init_dual(orc_state* s) {
         double Zt[9], sg[3], Uu[9], Vv[9];
         for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c) A3(Zt, r, c) = A3(s->Z + 9 * e, c, r);
         orc_svd3(Zt, sg, Uu, Vv);
-        pe += s->vol[e] * orc_nh_psi_plain(s->mu, s->lambda, sg);
+        pe += s->vol[e] * orc_nh_psi_plain(s->mu_e[e], s->lambda_e[e], sg);
     }
     s->curr_pe = pe;
 }

@@ -42,6 +42,8 @@ typedef struct {
     double gamma;         /* -gamma   (1.5) */
     double beta_static, beta_min, beta_max;  /* (1, 0.1, 10) */
     int rw_every;         /* extension: >0 reweights every rw_every iterations instead of the gamma rule */
+    const double* youngs_e;   /* extension: per-element Young's modulus (a batch of meshes), or NULL */
+    const double* poisson_e;  /* extension: per-element Poisson ratio, or NULL */
 } orc_problem;
 
 void orc_problem_defaults(orc_problem* p);

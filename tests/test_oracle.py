@@ -157,3 +157,18 @@ def test_live_reference_random_inputs(lib):
         x = st[e].copy()
         assert lib.orc_prox_lbfgs(mu, lam, po._d(np.ascontiguousarray(s0[e])), wov[e], po._d(x), 20) == its[e]
         np.testing.assert_array_equal(x, out[e])
+
+
+def test_element_materials_equal_uniform_when_constant():
+    """Per-element material arrays holding one material reproduce the uniform
+    oracle bit for bit (the batch extension of the oracle)."""
+    from wrapd_b200 import bars
+    b = bars.make_bar(3, 3, 6, twist_deg=90.0, noise=0.02, seed=4)
+    kw = dict(youngs=1e5, poisson=0.45, max_iters=8, lbfgs_m=5)
+    o1 = po.Oracle(b.rest, b.init, b.tets, b.pins, **kw)
+    o1.solve()
+    o2 = po.Oracle(b.rest, b.init, b.tets, b.pins, youngs_e=np.full(b.n_tets, 1e5),
+                   poisson_e=np.full(b.n_tets, 0.45), **kw)
+    o2.solve()
+    np.testing.assert_array_equal(o1.get("X"), o2.get("X"))
+    np.testing.assert_array_equal(o1.get("objectives"), o2.get("objectives"))

@@ -170,6 +170,21 @@ def batch_bars(count: int = 64, seed0: int = 0):
     return out
 
 
+def concat(bars_list) -> Bar:
+    """The batch as one mesh: vertices, tets and pins of each bar in turn, ids
+    shifted by the vertices before it (the order a batch's positions come in)."""
+    rest, init, tets, pins, off = [], [], [], [], 0
+    for b in bars_list:
+        rest.append(b.rest)
+        init.append(b.init)
+        tets.append(b.tets + off)
+        pins.append(np.asarray(b.pins) + off)
+        off += b.rest.shape[0]
+    first = bars_list[0]
+    return dataclasses.replace(first, rest=np.concatenate(rest), init=np.concatenate(init),
+                               tets=np.concatenate(tets).astype(np.int32), pins=np.concatenate(pins).astype(np.int32))
+
+
 def write_elenode(path_stem: str, verts: np.ndarray, tets: np.ndarray) -> None:
     """Write ``<stem>.node`` and ``<stem>.ele`` (0-based, exact doubles)."""
     n = verts.shape[0]

@@ -54,6 +54,8 @@ SIGNATURES = [
     ("wrapd_create", ctypes.c_int, [ctypes.POINTER(Settings), ctypes.POINTER(ctypes.c_void_p)]),
     ("wrapd_add_tetmesh", ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_int, _ip, ctypes.c_int, _ip,
                                           ctypes.c_int]),
+    ("wrapd_add_tetmesh_material", ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_int, _ip, ctypes.c_int,
+                                                   _ip, ctypes.c_int, ctypes.c_double, ctypes.c_double]),
     ("wrapd_initialize", ctypes.c_int, [ctypes.c_void_p]),
     ("wrapd_solve", ctypes.c_int, [ctypes.c_void_p, _dp]),
     ("wrapd_begin_solve", ctypes.c_int, [ctypes.c_void_p]),

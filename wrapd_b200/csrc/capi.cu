@@ -98,6 +98,15 @@ int wrapd_add_tetmesh(wrapd_handle* h, const double* rest_xyz, const double* ini
     });
 }
 
+int wrapd_add_tetmesh_material(wrapd_handle* h, const double* rest_xyz, const double* init_xyz,
+                               const double* soln_xyz, int n_verts, const int32_t* tets, int n_tets,
+                               const int32_t* pins, int n_pins, double youngs, double poisson) {
+    if (!(youngs > 0.0) || !(poisson > 0.0)) return WRAPD_E_INPUT;
+    return guarded(h, [&](wrapd::SolverGPU& s) {
+        s.add_mesh(rest_xyz, init_xyz, soln_xyz, n_verts, tets, n_tets, pins, n_pins, youngs, poisson);
+    });
+}
+
 int wrapd_initialize(wrapd_handle* h) {
     return guarded(h, [&](wrapd::SolverGPU& s) { s.initialize(); });
 }

@@ -5,6 +5,11 @@
 
 namespace wrapd {
 
+struct Material {
+    double mu, lambda;
+    double wr, wmin, wmax;   // rest stiffness k and its beta_min / beta_max multiples
+};
+
 struct ElemView {
     int ne;
     const int4* idx;     // per vertex slot: free vertex (dissection order) or -(pin + 1)
@@ -18,11 +23,14 @@ struct ElemView {
     double* sig;         // 3 x ne, cached singular values at the last gradient point
     double* slast;       // 3 x ne, prox warm start (m_last_sigma)
     double* gel;         // 12 x ne, per-element gradient rows g(a, r) at [(r + 3a) * ne + e]
+    const int* mid;      // per element: index into mats (a batch of meshes of several materials), or null
+    const Material* mats;
 };
 
-struct Material {
-    double mu, lambda;
-    double wr, wmin, wmax;   // rest stiffness k and its beta_min / beta_max multiples
-};
+// The material of element e: the batch's per-mesh table when there is one,
+// else the handle's single material m0 (also for lanes past the end).
+__device__ __forceinline__ Material elem_material(const ElemView& E, const Material& m0, int e) {
+    return (E.mid && e < E.ne) ? E.mats[E.mid[e]] : m0;
+}
 
 }  // namespace wrapd

@@ -72,9 +72,10 @@ __device__ __forceinline__ void deformation(const ElemView& E, int e, const doub
 // value 0.5 w^2 |symF - P|^2, the potential energy and the inversion count at
 // x (src/TetElements.cpp:444-468, 598-635).  Outputs out[0..2] = value, pe, flips.
 static __global__ void __launch_bounds__(128) k_grad(ElemView E, const double* __restrict__ x,
-                                              const double* __restrict__ xfix, Material mat, int write_gel,
+                                              const double* __restrict__ xfix, Material mat0, int write_gel,
                                               double* partials, unsigned* counter, double* out) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const Material mat = elem_material(E, mat0, e);
     double red[3] = {0.0, 0.0, 0.0};
     if (e < E.ne) {
         double Fd[9];
@@ -199,17 +200,18 @@ static __global__ void __launch_bounds__(256) k_gather(int nf, const int* __rest
 // prox network's prediction.  The FP32 instantiation always uses Newton.
 // NET needs dynamic shared memory: the network image plus one scratch per warp.
 template <typename C, bool NET>
-__global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat, int prox_iters, int cand_mode,
+__global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat0, int prox_iters, int cand_mode,
                                                int prox_mode, const unsigned char* __restrict__ net_img,
                                                double* partials, unsigned* counter, double* out) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = e < E.ne;
     double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     extern __shared__ __align__(16) unsigned char local_smem[];
     if constexpr (NET) {
         net::load_image(net_img, local_smem);
         __syncthreads();
     }
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const Material mat = elem_material(E, mat0, e);
+    const bool valid = e < E.ne;
     double S[9], Um[9];
     double w2 = 0.0, vol = 1.0;
     C sg[3] = {C(1), C(1), C(1)}, Ue[9], Ve[9];
@@ -230,7 +232,7 @@ __global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat, int 
                 const double d = M3(S, r, c) - (M3(Zm, r, c) - M3(Um, r, c));
                 bef += d * d;
             }
-        red[0] = 0.5 * w2 * bef;
+        red[0] += 0.5 * w2 * bef;
         svd3(Sin, sg, Ue, Ve);
     }
     Prox<C> P;
@@ -287,11 +289,11 @@ __global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat, int 
 #pragma unroll
             for (int i = 0; i < 3; ++i) xs[i] = C(xd[i]);
         }
-        red[4] = double(iters);
+        red[4] += double(iters);
         double xo[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i) { xo[i] = double(xs[i]); E.slast[(size_t)i * E.ne + e] = xo[i]; }
-        red[3] = (xo[0] < 0.0 || xo[1] < 0.0 || xo[2] < 0.0) ? 1.0 : 0.0;
+        red[3] += (xo[0] < 0.0 || xo[1] < 0.0 || xo[2] < 0.0) ? 1.0 : 0.0;
         C Soc[9];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
@@ -299,7 +301,7 @@ __global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat, int 
             for (int c = 0; c < 3; ++c)
                 M3(Soc, r, c) = M3(Ve, r, 0) * xs[0] * M3(Ue, c, 0) + M3(Ve, r, 1) * xs[1] * M3(Ue, c, 1) +
                                 M3(Ve, r, 2) * xs[2] * M3(Ue, c, 2);
-        red[2] = vol * NH<double>{mat.mu, mat.lambda}.psi_plain(xo[0], xo[1], xo[2]);
+        red[2] += vol * NH<double>{mat.mu, mat.lambda}.psi_plain(xo[0], xo[1], xo[2]);
         double aft = 0.0, Zm[9];
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
@@ -309,7 +311,7 @@ __global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat, int 
             Zm[i] = So;
             Um[i] = Um[i] + (S[i] - So);
         }
-        red[1] = 0.5 * w2 * aft;
+        red[1] += 0.5 * w2 * aft;
         store9(E.Z, E.ne, e, Zm);
         store9(E.U, E.ne, e, Um);
         if (cand_mode == CAND_REST) {
@@ -329,9 +331,10 @@ __global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat, int 
 // F(X) with all four slots read from X, U = 0; then polar_potential_energy
 // (src/TetElements.cpp:638-675) of the new Z.  out[0] = that energy.
 static __global__ void __launch_bounds__(128) k_init_dual(ElemView E, const double* __restrict__ x,
-                                                   const double* __restrict__ xfix, Material mat,
+                                                   const double* __restrict__ xfix, Material mat0,
                                                    double* partials, unsigned* counter, double* out) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const Material mat = elem_material(E, mat0, e);
     double red[1] = {0.0};
     if (e < E.ne) {
         double Fd[9];
@@ -362,9 +365,10 @@ static __global__ void __launch_bounds__(128) k_init_dual(ElemView E, const doub
 // Candidate weights of midupdate_weights (src/TetElements.cpp:360-388): from
 // F(X) (from_x = 1) or from the cached singular values.
 static __global__ void __launch_bounds__(128) k_mid_candidates(ElemView E, const double* __restrict__ x,
-                                                        const double* __restrict__ xfix, Material mat,
+                                                        const double* __restrict__ xfix, Material mat0,
                                                         int from_x, int cand_mode) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const Material mat = elem_material(E, mat0, e);
     if (e >= E.ne) return;
     double s[3];
     if (from_x) {

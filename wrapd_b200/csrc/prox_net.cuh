@@ -52,12 +52,21 @@ constexpr int WARP_SCRATCH = 32 * LD1 * 2 + 32 * 8 * 4;   // 2560
 constexpr float kGeluC = 0.7978845608028654f;   // sqrt(2 / pi)
 constexpr float kGeluA = 0.044715f;
 
+// tanh x = 1 - 2 / (e^{2x} + 1), with e^{2x} = 2^{2x log2 e} and the reciprocal
+// on the special-function unit (ex2.approx, rcp.approx): absolute error ~1e-7,
+// far below the BF16 rounding the activations go through next.
+__device__ __forceinline__ float tanh_sfu(float x) {
+    float e, r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(x * 2.8853900817779268f));
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e + 1.0f));
+    return 1.0f - 2.0f * r;
+}
 __device__ __forceinline__ float gelu(float x) {
-    return 0.5f * x * (1.0f + tanhf(kGeluC * (x + kGeluA * x * x * x)));
+    return 0.5f * x * (1.0f + tanh_sfu(kGeluC * (x + kGeluA * x * x * x)));
 }
 __device__ __forceinline__ float gelu_grad(float x) {
     const float x2 = x * x;
-    const float t = tanhf(kGeluC * (x + kGeluA * x2 * x));
+    const float t = tanh_sfu(kGeluC * (x + kGeluA * x2 * x));
     return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * kGeluC * (1.0f + 3.0f * kGeluA * x2);
 }
 

@@ -93,12 +93,18 @@ SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
     for (auto& e : ev_) WRAPD_CUDA(cudaEventCreate(&e));
     WRAPD_CUDA(cudaMallocHost(&h_scal_, S_COUNT * sizeof(double)));
     WRAPD_CUDA(cudaFuncSetAttribute(k_local<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLocalHistBytes));
-    // Lame(E, nu), src/Lame.hpp:50-53; k = 2.0066 mu + 1.0122 lambda, src/TetElements.cpp:84
-    mat_.mu = cfg.youngs / (2.0 * (1.0 + cfg.poisson));
-    mat_.lambda = cfg.youngs * cfg.poisson / ((1.0 + cfg.poisson) * (1.0 - 2.0 * cfg.poisson));
-    mat_.wr = 2.0066 * mat_.mu + 1.0122 * mat_.lambda;
-    mat_.wmin = mat_.wr * cfg.beta_min;
-    mat_.wmax = mat_.wr * cfg.beta_max;
+    mat_ = material(cfg.youngs, cfg.poisson);
+}
+
+// Lame(E, nu), src/Lame.hpp:50-53; k = 2.0066 mu + 1.0122 lambda, src/TetElements.cpp:84
+Material SolverGPU::material(double youngs, double poisson) const {
+    Material m;
+    m.mu = youngs / (2.0 * (1.0 + poisson));
+    m.lambda = youngs * poisson / ((1.0 + poisson) * (1.0 - 2.0 * poisson));
+    m.wr = 2.0066 * m.mu + 1.0122 * m.lambda;
+    m.wmin = m.wr * cfg.beta_min;
+    m.wmax = m.wr * cfg.beta_max;
+    return m;
 }
 
 SolverGPU::~SolverGPU() {
@@ -142,27 +148,46 @@ ElemView SolverGPU::view() {
     v.sig = d_sig_;
     v.slast = d_slast_;
     v.gel = d_gel_;
+    v.mid = d_mid_;
+    v.mats = d_mats_;
     return v;
 }
 
 void SolverGPU::add_mesh(const double* rest, const double* init, const double* soln, int nv_, const int32_t* tets,
-                         int ne_, const int32_t* pins, int np_) {
-    if (initialized_ || nv > 0) throw CudaError(WRAPD_E_STATE, "one mesh per handle");
+                         int ne_, const int32_t* pins, int np_, double youngs, double poisson) {
+    if (initialized_) throw CudaError(WRAPD_E_STATE, "add_tetmesh after initialize");
     if (!rest || !init || !tets || nv_ <= 0 || ne_ <= 0 || np_ < 0 || np_ >= nv_ || (np_ > 0 && !pins))
         throw CudaError(WRAPD_E_INPUT, "bad mesh arguments");
-    nv = nv_; ne = ne_; np = np_; nf = nv - np;
-    rest_.assign(rest, rest + 3 * (size_t)nv);
-    init_.assign(init, init + 3 * (size_t)nv);
-    have_soln_ = soln != nullptr;
-    soln_ = have_soln_ ? std::vector<double>(soln, soln + 3 * (size_t)nv) : rest_;
-    tets_.assign(tets, tets + 4 * (size_t)ne);
-    for (int v : tets_) if (v < 0 || v >= nv) throw CudaError(WRAPD_E_INPUT, "tet vertex id out of range");
-    pins_.assign(pins, pins + np);
-    std::sort(pins_.begin(), pins_.end());
-    for (int j = 0; j < np; ++j)
-        if (pins_[j] < 0 || pins_[j] >= nv || (j > 0 && pins_[j] == pins_[j - 1]))
+    if (!meshes_.empty() && meshes_[0].soln != (soln != nullptr))
+        throw CudaError(WRAPD_E_INPUT, "give a solution mesh for every mesh of a batch or for none");
+    if ((youngs > 0.0) != (poisson > 0.0) || (poisson > 0.0 && !(poisson < 0.5)))
+        throw CudaError(WRAPD_E_INPUT, "bad mesh material");
+    for (int i = 0; i < 4 * ne_; ++i)
+        if (tets[i] < 0 || tets[i] >= nv_) throw CudaError(WRAPD_E_INPUT, "tet vertex id out of range");
+    std::vector<int> p(pins, pins + np_);
+    std::sort(p.begin(), p.end());
+    for (int j = 0; j < np_; ++j)
+        if (p[j] < 0 || p[j] >= nv_ || (j > 0 && p[j] == p[j - 1]))
             throw CudaError(WRAPD_E_INPUT, "pin ids must be distinct vertex ids");
-    // free/fixed maps, samples/utils/AddMeshes.hpp:268-289
+    // the mesh's material: one entry per distinct (mu, lambda)
+    const Material m = youngs > 0.0 ? material(youngs, poisson) : mat_;
+    int mi = 0;
+    while (mi < (int)mats_.size() && !(mats_[mi].mu == m.mu && mats_[mi].lambda == m.lambda)) ++mi;
+    if (mi == (int)mats_.size()) mats_.push_back(m);
+    meshes_.push_back({nv, nv_, ne, ne_, mi, soln != nullptr});
+    // append, vertex ids shifted by the vertices before (binding::add_tetmesh's
+    // prev_tet_verts, samples/utils/AddMeshes.hpp:70-84)
+    rest_.insert(rest_.end(), rest, rest + 3 * (size_t)nv_);
+    init_.insert(init_.end(), init, init + 3 * (size_t)nv_);
+    if (soln) soln_.insert(soln_.end(), soln, soln + 3 * (size_t)nv_);
+    else soln_.insert(soln_.end(), rest, rest + 3 * (size_t)nv_);
+    have_soln_ = soln != nullptr;
+    for (int i = 0; i < 4 * ne_; ++i) tets_.push_back(tets[i] + nv);
+    for (int v : p) pins_.push_back(v + nv);
+    nv += nv_; ne += ne_; np += np_; nf = nv - np;
+    // free/fixed maps over the batch, samples/utils/AddMeshes.hpp:89-110 (meshes
+    // follow each other and pins stay sorted, so each mesh's free vertices are
+    // contiguous)
     free_of_vert_.assign(nv, -1);
     fix_of_vert_.assign(nv, -1);
     for (int i = 0, j = 0, k = 0; i < nv; ++i) {
@@ -185,8 +210,13 @@ void SolverGPU::initialize() {
         if (v < 0.0) throw CudaError(WRAPD_E_INVERTED_REST, "inverted tet " + std::to_string(e) + " in the rest mesh");
         for (int k = 0; k < 12; ++k) Di[(size_t)k * ne + e] = d[k];
         vol[e] = v;
-        w2[e] = cfg.beta_static * mat_.wr * v;
     }
+    std::vector<int> mid(ne);
+    for (const MeshIn& M : meshes_)
+        for (int e = M.e_off; e < M.e_off + M.ne; ++e) {
+            mid[e] = M.mat;
+            w2[e] = cfg.beta_static * mats_[M.mat].wr * vol[e];
+        }
     // ---- free-vertex graph, nested dissection, symbolic factorization ----
     std::vector<std::vector<int>> nb(nf);
     for (int e = 0; e < ne; ++e)
@@ -208,7 +238,22 @@ void SolverGPU::initialize() {
     for (int i = 0; i < nv; ++i)
         if (free_of_vert_[i] >= 0)
             for (int c = 0; c < 3; ++c) coords[3 * (size_t)free_of_vert_[i] + c] = rest_[3 * (size_t)i + c];
-    Symbolic S = analyse(nf, ptr, adj, coords, cfg.leaf_size > 0 ? cfg.leaf_size : 64);
+    // one nested dissection per mesh (their graphs are disjoint), then the forest
+    std::vector<Symbolic> parts;
+    for (const MeshIn& M : meshes_) {
+        int f0 = -1, f1 = -1;
+        for (int i = M.v_off; i < M.v_off + M.nv; ++i)
+            if (free_of_vert_[i] >= 0) { if (f0 < 0) f0 = free_of_vert_[i]; f1 = free_of_vert_[i] + 1; }
+        if (f0 < 0) throw CudaError(WRAPD_E_INPUT, "a mesh without free vertices");
+        const int n = f1 - f0;
+        std::vector<int> p(n + 1), a(adj.begin() + ptr[f0], adj.begin() + ptr[f1]);
+        for (int i = 0; i <= n; ++i) p[i] = ptr[f0 + i] - ptr[f0];
+        for (int& v : a) v -= f0;
+        std::vector<double> c(coords.begin() + 3 * (size_t)f0, coords.begin() + 3 * (size_t)f1);
+        parts.push_back(analyse(n, p, a, c, cfg.leaf_size > 0 ? cfg.leaf_size : 64));
+    }
+    Symbolic S = merge(parts);
+    std::vector<Symbolic>().swap(parts);
     perm_ = S.perm;
     iperm_ = S.iperm;
     // element slots: free -> dissection index, pinned -> -(pin + 1)
@@ -278,6 +323,10 @@ void SolverGPU::initialize() {
     d_Di_ = dupload(Di);
     d_vol_ = dupload(vol);
     d_w2_ = dupload(w2);
+    if (mats_.size() > 1) {
+        d_mid_ = dupload(mid);
+        d_mats_ = dupload(mats_);
+    }
     d_w2c_ = static_cast<double*>(dalloc(ne * sizeof(double)));
     d_Z_ = static_cast<double*>(dalloc(9 * (size_t)ne * TS));
     d_U_ = static_cast<double*>(dalloc(9 * (size_t)ne * TS));
@@ -369,8 +418,12 @@ void SolverGPU::gather(double* grad, const double* gold, double* ystage, const d
 }
 
 void SolverGPU::local_step(int cand_mode, bool fp32_compute) {
+    // prox_mode 2 runs the network where the last stretches are a stale warm
+    // start: the first local step and the one after each reweight (the weight
+    // w^2 / vol, an input of the prox, has just changed); elsewhere the last
+    // stretches start the Newton prox at least as well and cost nothing.
+    const bool net = cfg.prox_mode == 2 && (logs_.reweighted.empty() || logs_.reweighted.back() != 0);
     const int nb = blocks_for(ne, 128);
-    const bool net = cfg.prox_mode == 2;
     const int net_smem = net::IMAGE_BYTES + 4 * net::WARP_SCRATCH;
     if (net && !d_net_img_) throw CudaError(WRAPD_E_STATE, "prox_mode 2 needs a network (wrapd_set_prox_net)");
     if (fp32_compute) {
@@ -386,8 +439,9 @@ void SolverGPU::local_step(int cand_mode, bool fp32_compute) {
                                                               d_partials_, d_counter_, d_scal_ + S_LOCAL);
         else
             k_local<double, false><<<nb, 128, kLocalHistBytes, st_>>>(view(), mat_, cfg.prox_iters, cand_mode,
-                                                                      fp32() ? 1 : cfg.prox_mode, nullptr, d_partials_,
-                                                                      d_counter_, d_scal_ + S_LOCAL);
+                                                                      (fp32() || cfg.prox_mode == 2) ? 1 : cfg.prox_mode,
+                                                                      nullptr, d_partials_, d_counter_,
+                                                                      d_scal_ + S_LOCAL);
     }
     WRAPD_LAUNCH_CHECK();
     kernel_launches++;

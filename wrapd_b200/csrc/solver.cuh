@@ -26,8 +26,12 @@ public:
     explicit SolverGPU(const wrapd_settings& s);
     ~SolverGPU();
 
+    // Appends one mesh (pins: its own vertex ids).  Several meshes make a
+    // batch solved as one block-diagonal system; youngs/poisson > 0 give the
+    // mesh its own material (else the settings').
+    Material material(double youngs, double poisson) const;
     void add_mesh(const double* rest, const double* init, const double* soln, int nv, const int32_t* tets, int ne,
-                  const int32_t* pins, int np);
+                  const int32_t* pins, int np, double youngs = 0.0, double poisson = 0.0);
     void initialize();
     void begin_solve();
     // runs up to n iterations; returns iterations done; *converged set when the test passes
@@ -87,11 +91,16 @@ private:
 
     // host mesh
     std::vector<double> rest_, init_, soln_;
-    std::vector<int> tets_, pins_;         // pins sorted
+    std::vector<int> tets_, pins_;         // pins sorted (batch vertex ids)
+    struct MeshIn { int v_off, nv, e_off, ne, mat; bool soln; };
+    std::vector<MeshIn> meshes_;
+    std::vector<Material> mats_;           // distinct materials of the batch
     std::vector<int> free_of_vert_, fix_of_vert_;
     std::vector<int> perm_, iperm_;        // dissection order over free vertices
     bool have_soln_ = false;
     Material mat_{};
+    int* d_mid_ = nullptr;                 // per-element material index (several materials only)
+    Material* d_mats_ = nullptr;
     // device
     cudaStream_t st_ = nullptr;
     cudaEvent_t ev_[4] = {};

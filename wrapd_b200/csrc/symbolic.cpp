@@ -186,4 +186,38 @@ Symbolic analyse(int n, const std::vector<int>& adj_ptr, const std::vector<int>&
     return S;
 }
 
+Symbolic merge(const std::vector<Symbolic>& parts) {
+    if (parts.size() == 1) return parts[0];
+    Symbolic S;
+    int off = 0, foff = 0;
+    int64_t fo = 0, yo = 0, uo = 0, ro = 0;
+    for (const Symbolic& P : parts) {
+        for (int v : P.perm) S.perm.push_back(v + off);
+        if (S.levels.size() < P.levels.size()) S.levels.resize(P.levels.size());
+        for (size_t l = 0; l < P.levels.size(); ++l)
+            for (int f : P.levels[l]) S.levels[l].push_back(f + foff);
+        for (const Front& F : P.fronts) {
+            Front G = F;
+            G.first += off;
+            for (int& r : G.rows) r += off;
+            if (G.parent >= 0) G.parent += foff;
+            for (int& c : G.children) c += foff;
+            G.f_off += fo; G.y_off += yo; G.u_off += uo; G.rel_off += ro;
+            S.fronts.push_back(std::move(G));
+        }
+        S.relmap.insert(S.relmap.end(), P.relmap.begin(), P.relmap.end());
+        off += P.n;
+        foff += static_cast<int>(P.fronts.size());
+        fo += P.f_pool; yo += P.y_pool; uo += P.u_pool; ro += static_cast<int64_t>(P.relmap.size());
+        S.nnz_L += P.nnz_L;
+        S.flops += P.flops;
+        S.max_children = std::max(S.max_children, P.max_children);
+    }
+    S.n = off;
+    S.f_pool = fo; S.y_pool = yo; S.u_pool = uo;
+    S.iperm.assign(S.n, -1);
+    for (int i = 0; i < S.n; ++i) S.iperm[S.perm[i]] = i;
+    return S;
+}
+
 }  // namespace wrapd

@@ -51,4 +51,9 @@ struct Symbolic {
 Symbolic analyse(int n, const std::vector<int>& adj_ptr, const std::vector<int>& adj,
                  const std::vector<double>& coords, int leaf);
 
+// The analysis of a block-diagonal matrix from the analyses of its blocks (one
+// per mesh of a batch), block p taking the columns after blocks 0..p-1: the
+// forest of their trees, level l holding every block's level-l fronts.
+Symbolic merge(const std::vector<Symbolic>& parts);
+
 }  // namespace wrapd

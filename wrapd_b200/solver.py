@@ -57,34 +57,46 @@ class Solver:
         self.settings = settings if settings is not None else Settings(**kw)
         self._h = capi.Handle(self.settings)
         self.n_verts = 0
-        self._mesh = None
-        self._pins = None
+        self._meshes = []
 
     # -- mesh ---------------------------------------------------------------
-    def add_tetmesh(self, rest, init, tets, soln=None):
+    def add_tetmesh(self, rest, init, tets, soln=None, pins=None, youngs=None, poisson=None):
+        """Add a mesh; call again for a batch (meshes solved as one block-diagonal
+        system, positions returned in the order added).  youngs/poisson give this
+        mesh its own material (both or neither)."""
         rest = np.ascontiguousarray(rest, dtype=np.float64).reshape(-1, 3)
         init = np.ascontiguousarray(init, dtype=np.float64).reshape(-1, 3)
         tets = np.ascontiguousarray(tets, dtype=np.int32).reshape(-1, 4)
         if rest.shape != init.shape:
             raise WrapdError(-1, "Rest mesh and init mesh do not have the same number of vertices.")
+        if (youngs is None) != (poisson is None):
+            raise ValueError("give both youngs and poisson, or neither")
         soln = None if soln is None else np.ascontiguousarray(soln, dtype=np.float64).reshape(-1, 3)
-        self._mesh = (rest, init, tets, soln)
-        self.n_verts = rest.shape[0]
+        self._meshes.append(dict(rest=rest, init=init, tets=tets, soln=soln, pins=None, youngs=youngs,
+                                 poisson=poisson))
+        if pins is not None:
+            self.set_pins(pins)
+        self.n_verts += rest.shape[0]
 
     def set_pins(self, inds):
-        """Pin vertices in place (src/System.cpp:33-44)."""
-        self._pins = np.ascontiguousarray(inds, dtype=np.int32).ravel()
+        """Pin vertices of the last added mesh in place (src/System.cpp:33-44)."""
+        if not self._meshes:
+            raise WrapdError(-9, "set_pins before add_tetmesh")
+        self._meshes[-1]["pins"] = np.ascontiguousarray(inds, dtype=np.int32).ravel()
 
     def initialize(self):
-        if self._mesh is None:
+        if not self._meshes:
             raise WrapdError(-9, "initialize before add_tetmesh")
-        rest, init, tets, soln = self._mesh
-        pins = self._pins if self._pins is not None else np.zeros(0, dtype=np.int32)
         h = self._h
-        h.check(h.lib.wrapd_add_tetmesh(h.h, capi.dptr(rest), capi.dptr(init),
-                                        capi.dptr(soln) if soln is not None else None,
-                                        rest.shape[0], capi.iptr(tets), tets.shape[0], capi.iptr(pins),
-                                        pins.shape[0]))
+        for m in self._meshes:
+            pins = m["pins"] if m["pins"] is not None else np.zeros(0, dtype=np.int32)
+            args = (h.h, capi.dptr(m["rest"]), capi.dptr(m["init"]),
+                    capi.dptr(m["soln"]) if m["soln"] is not None else None, m["rest"].shape[0],
+                    capi.iptr(m["tets"]), m["tets"].shape[0], capi.iptr(pins), pins.shape[0])
+            if m["youngs"] is None:
+                h.check(h.lib.wrapd_add_tetmesh(*args))
+            else:
+                h.check(h.lib.wrapd_add_tetmesh_material(*args, float(m["youngs"]), float(m["poisson"])))
         h.check(h.lib.wrapd_initialize(h.h))
         return True
 
