@@ -289,6 +289,12 @@ WRAPD_API int wrapd_net_predict(const float* blob, int n_blob, int n, const doub
 /* Installs the network used by prox_mode 2 (copied; call before begin_solve). */
 WRAPD_API int wrapd_set_prox_net(wrapd_handle* h, const float* blob, int n_blob);
 
+/* Measured FP64 tensor-core throughput of this GPU (TFLOP/s): back-to-back
+ * mma.sync m8n8k4 f64 from registers on every SM for `iters` rounds, timed by
+ * CUDA events.  The roofline denominator of the factorization (no reference
+ * counterpart). */
+WRAPD_API int wrapd_dmma_peak(int iters, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT, "libwrapd_gpu.so")
-SOURCES = ["symbolic.cpp", "chol.cu", "solver.cu", "capi.cu", "elem_batch.cu", "prox_net.cu"]
+SOURCES = ["symbolic.cpp", "chol.cu", "solver.cu", "capi.cu", "elem_batch.cu", "prox_net.cu", "dmma_peak.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-lineinfo",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", f"-I{os.path.join(ROOT, 'include')}"]
 

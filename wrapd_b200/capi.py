@@ -101,6 +101,7 @@ SIGNATURES = [
     ("wrapd_net_predict", ctypes.c_int, [_fp, ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_double,
                                           ctypes.c_double, _dp]),
     ("wrapd_set_prox_net", ctypes.c_int, [ctypes.c_void_p, _fp, ctypes.c_int]),
+    ("wrapd_dmma_peak", ctypes.c_int, [ctypes.c_int, _dp]),
 ]
 
 
@@ -157,6 +158,13 @@ def hess_lmax_batch(mu, lam, sigma):
     out = np.empty(s.shape[0])
     _check_free(load().wrapd_hess_lmax_batch(s.shape[0], mu, lam, dptr(s), dptr(out)))
     return out
+
+
+def dmma_peak(iters: int = 20000) -> float:
+    """Measured FP64 tensor-core throughput (TFLOP/s)."""
+    v = ctypes.c_double(0.0)
+    _check_free(load().wrapd_dmma_peak(iters, ctypes.byref(v)))
+    return v.value
 
 
 def load():

@@ -109,6 +109,97 @@ __device__ __forceinline__ void tile_store(double* C, int64_t crs, int64_t ccs, 
             }
 }
 
+// ---- pipelined GEMM core ------------------------------------------------------
+// Operand tiles are staged by cp.async in one of two layouts, chosen by which
+// index is contiguous in global memory so that both the staging writes and the
+// DMMA fragment reads hit every shared-memory bank evenly:
+//   t-major S[t * TP + i] for sources with i contiguous (columns of F),
+//   i-major S[i * SLD + t] for sources with t contiguous (row blocks of Y).
+// Two stages: chunk c + 1 is in flight while chunk c is multiplied.
+constexpr int TP = TL + 8;            // t-major pitch: 8 mod 16 doubles
+constexpr int TILE_D = TL * SLD;      // doubles per staged operand tile
+static_assert(NB * TP == TILE_D, "both layouts take the same space");
+constexpr int GEMM_SMEM = 2 * 2 * TILE_D * (int)sizeof(double);   // 2 stages x (A, B)
+
+__device__ __forceinline__ void cp_async8(double* s, const double* g, bool valid) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(s));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(g), "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Element (i, t), i < rows, t < K, of a source with (TMAJOR) i contiguous:
+// base[i + t * ld], or t contiguous: base[i * ld + t]; zeros up to K4.
+template <bool TMAJOR>
+__device__ __forceinline__ void stage_tile(double* S, const double* base, int64_t ld, int rows, int K, int K4) {
+    const int total = TL * K4;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        if constexpr (TMAJOR) {
+            const int i = idx % TL, t = idx / TL;
+            const bool v = i < rows && t < K;
+            cp_async8(S + t * TP + i, v ? base + i + (int64_t)t * ld : base, v);
+        } else {
+            const int t = idx % K4, i = idx / K4;
+            const bool v = i < rows && t < K;
+            cp_async8(S + i * SLD + t, v ? base + (int64_t)i * ld + t : base, v);
+        }
+    }
+}
+
+template <bool AT, bool BT>
+__device__ __forceinline__ void tile_mma2(const double* As, const double* Bs, int K4, double (&acc)[4][4][2]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int r = lane >> 2, c = lane & 3;
+    for (int kk = 0; kk < K4; kk += 4) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int row = wm * 32 + i * 8 + r;
+            a[i] = AT ? As[(kk + c) * TP + row] : As[row * SLD + kk + c];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int col = wn * 32 + j * 8 + r;
+            b[j] = BT ? Bs[(kk + c) * TP + col] : Bs[col * SLD + kk + c];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+}
+
+// acc += A B'^T over t in [0, K): A(i, t) = A0[i + t * lda] (i < M), B'(j, t) =
+// B0[j + t * ldb] when BT, else B0[j * ldb + t] (j < N).
+template <bool BT>
+__device__ __forceinline__ void gemm_pipelined(const double* A0, int64_t lda, int M, const double* B0, int64_t ldb,
+                                               int N, int K, double* smem, double (&acc)[4][4][2]) {
+    const int nch = (K + NB - 1) / NB;
+    auto issue = [&](int c) {
+        const int k0 = c * NB, Kc = min(NB, K - k0), K4 = (Kc + 3) & ~3;
+        double* st = smem + (c & 1) * 2 * TILE_D;
+        stage_tile<true>(st, A0 + (int64_t)k0 * lda, lda, M, Kc, K4);
+        stage_tile<BT>(st + TILE_D, BT ? B0 + (int64_t)k0 * ldb : B0 + k0, ldb, N, Kc, K4);
+        cp_async_commit();
+    };
+    if (nch > 0) issue(0);
+    for (int c = 0; c < nch; ++c) {
+        if (c + 1 < nch) {
+            issue(c + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const int Kc = min(NB, K - c * NB), K4 = (Kc + 3) & ~3;
+        const double* st = smem + (c & 1) * 2 * TILE_D;
+        tile_mma2<true, BT>(st, st + TILE_D, K4, acc);
+        __syncthreads();
+    }
+}
+
 // ---- assembly ----------------------------------------------------------------
 __global__ void k_assemble_A(double* __restrict__ F, const int64_t* __restrict__ pos, const int* __restrict__ ptr,
                              const int* __restrict__ con, int nA, const double* __restrict__ w2,
@@ -259,8 +350,7 @@ __device__ __forceinline__ void job_tile(const GemmJob& jb, int t, int& ti, int&
 
 __global__ void __launch_bounds__(GEMM_THREADS) k_update(double* __restrict__ F, double* __restrict__ Y,
                                                          const FrontDesc* __restrict__ desc, JobList jl) {
-    __shared__ double As[TL * SLD];
-    __shared__ double Bs[TL * SLD];
+    extern __shared__ __align__(16) double gemm_smem[];
     const int item = find_item(jl.d_prefix, jl.n, blockIdx.x);
     const GemmJob jb = jl.d_jobs[item];
     const FrontDesc d = desc[jb.front];
@@ -269,15 +359,13 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_update(double* __restrict__ F,
     const int r0 = jb.r0 + ti * TL, c0 = jb.c0 + tj * TL;
     const int M = min(TL, jb.r1 - r0), N = min(TL, jb.c1 - c0);
     double acc[4][4][2] = {};
-    for (int k0 = jb.k0; k0 < jb.k1; k0 += NB) {
-        const int K = min(NB, jb.k1 - k0), K4 = (K + 3) & ~3;
-        load_tile(As, F + d.f_off + r0 + (int64_t)k0 * d.ld, 1, d.ld, M, K, K4);
-        if (jb.kind == 0) load_tile(Bs, F + d.f_off + c0 + (int64_t)k0 * d.ld, 1, d.ld, N, K, K4);
-        else load_tile(Bs, Y + d.y_off + k0 + (int64_t)c0 * d.k, d.k, 1, N, K, K4);
-        __syncthreads();
-        tile_mma(As, Bs, K4, acc);
-        __syncthreads();
-    }
+    const double* A0 = F + d.f_off + r0 + (int64_t)jb.k0 * d.ld;
+    if (jb.kind == 0)
+        gemm_pipelined<true>(A0, d.ld, M, F + d.f_off + c0 + (int64_t)jb.k0 * d.ld, d.ld, N, jb.k1 - jb.k0,
+                             gemm_smem, acc);
+    else   // B'(j, t) = Y(k0 + t, c0 + j)
+        gemm_pipelined<false>(A0, d.ld, M, Y + d.y_off + jb.k0 + (int64_t)c0 * d.k, d.k, N, jb.k1 - jb.k0,
+                              gemm_smem, acc);
     if (jb.kind == 0) {
         // on tiles crossing the diagonal keep only row >= column (global indices)
         double* C = F + d.f_off + r0 + (int64_t)c0 * d.ld;
@@ -304,8 +392,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_update(double* __restrict__ F,
 __global__ void __launch_bounds__(GEMM_THREADS) k_wgemm(const double* __restrict__ F, const double* __restrict__ Y,
                                                         double* __restrict__ W, const FrontDesc* __restrict__ desc,
                                                         WorkList wl) {
-    __shared__ double As[TL * SLD];
-    __shared__ double Bs[TL * SLD];
+    extern __shared__ __align__(16) double gemm_smem[];
     const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
     const FrontDesc d = desc[wl.d_fronts[item]];
     const int t = blockIdx.x - wl.d_prefix[item];
@@ -314,14 +401,9 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_wgemm(const double* __restrict
     const int M = min(TL, d.r - r0), N = min(TL, d.k - c0);
     const double* A = F + d.f_off + d.k + r0;   // L_rs(i, t) at A[i + t ld]
     double acc[4][4][2] = {};
-    for (int k0 = c0; k0 < d.k; k0 += NB) {
-        const int K = min(NB, d.k - k0), K4 = (K + 3) & ~3;
-        load_tile(As, A + (int64_t)k0 * d.ld, 1, d.ld, M, K, K4);
-        load_tile(Bs, Y + d.y_off + k0 + (int64_t)c0 * d.k, d.k, 1, N, K, K4);   // Y(k0 + t, c0 + j)
-        __syncthreads();
-        tile_mma(As, Bs, K4, acc);
-        __syncthreads();
-    }
+    // t over [c0, k): Y(k0 + t, c0 + j) vanishes above the diagonal
+    gemm_pipelined<false>(A + (int64_t)c0 * d.ld, d.ld, M, Y + d.y_off + c0 + (int64_t)c0 * d.k, d.k, N, d.k - c0,
+                          gemm_smem, acc);
     tile_store(W + d.w_off + r0 + (int64_t)c0 * d.r, 1, d.r, M, N, EPI_SET, acc);
 }
 
@@ -566,6 +648,8 @@ WorkList CholGPU::make_list(const std::vector<int>& fronts, const std::vector<in
 
 void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const std::vector<int>& A_ptr,
                     const std::vector<int>& A_contrib, cudaStream_t st) {
+    WRAPD_CUDA(cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
+    WRAPD_CUDA(cudaFuncSetAttribute(k_wgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
     n = S.n;
     nfronts = static_cast<int>(S.fronts.size());
     nlevels = static_cast<int>(S.levels.size());
@@ -765,12 +849,12 @@ void CholGPU::factor_launches(const double* d_w2, const double* d_Di, int ne, cu
                 WRAPD_LAUNCH_CHECK();
             }
             if (L.update[p].total) {
-                k_update<<<L.update[p].total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_desc_, L.update[p]);
+                k_update<<<L.update[p].total, GEMM_THREADS, GEMM_SMEM, st>>>(d_F_, d_Y_, d_desc_, L.update[p]);
                 WRAPD_LAUNCH_CHECK();
             }
         }
         if (L.wgemm.total) {
-            k_wgemm<<<L.wgemm.total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_W_, d_desc_, L.wgemm);
+            k_wgemm<<<L.wgemm.total, GEMM_THREADS, GEMM_SMEM, st>>>(d_F_, d_Y_, d_W_, d_desc_, L.wgemm);
             WRAPD_LAUNCH_CHECK();
         }
     }
