@@ -447,6 +447,7 @@ void orc_problem_defaults(orc_problem* p) {
     p->max_iters = 5000; p->tol = 1e-11; p->lbfgs_m = 6; p->global_iters = 100; p->kappa = 1.0;
     p->reweighting = 1; p->rw_delay = 50; p->gamma = 1.5;
     p->beta_static = 1.0; p->beta_min = 0.1; p->beta_max = 10.0; p->rw_every = 0;
+    p->rot_aware = 1; p->model = 0;
 }
 
 #define NEWD(n) ((double*)calloc((size_t)(n) ? (size_t)(n) : 1, sizeof(double)))
@@ -537,7 +538,9 @@ orc_state* orc_create(const orc_problem* p, int* err) {
                 for (int r = 0; r < 3; ++r) v += Di[r + 3 * a] * Di[r + 3 * b];
                 s->DtD[16 * e + a + 4 * b] = v;
             }
-        s->w2[e] = p->beta_static * (2.0066 * s->mu_e[e] + 1.0122 * s->lambda_e[e]) * s->vol[e];
+        /* k = 1 for ARAP, 2.0066 mu + 1.0122 lambda for NH (src/TetElements.cpp:80-87) */
+        const double k = p->model == 1 ? 1.0 : 2.0066 * s->mu_e[e] + 1.0122 * s->lambda_e[e];
+        s->w2[e] = p->beta_static * k * s->vol[e];
         s->slast[3 * e] = s->slast[3 * e + 1] = s->slast[3 * e + 2] = 1.0;
     }
     free(sp);
@@ -614,8 +617,29 @@ static void defo_cache_at(orc_state* s, const double* xfree) {
 
 void orc_update_defo_cache(orc_state* s) { defo_cache_at(s, s->xfree); }
 
+/* rot(F) = U V^T of the sign-fixed SVD, math::polar (src/Math.hpp:218-225) */
+static void rot3(const double* F, double* R) {
+    double sg[3], Uu[9], Vv[9];
+    orc_svd3(F, sg, Uu, Vv);
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            double v = 0.0;
+            for (int k = 0; k < 3; ++k) v += A3(Uu, r, k) * A3(Vv, c, k);
+            A3(R, r, c) = v;
+        }
+}
+
+/* potential_energy_x, src/TetElements.cpp:598-635 (ARAP: k = 1) */
 double orc_potential_energy(const orc_state* s) {
     double pe = 0.0;
+    if (s->p.model == 1) {
+        for (int e = 0; e < s->ne; ++e) {
+            double R[9];
+            rot3(s->F + 9 * e, R);
+            pe += 0.5 * 1.0 * s->vol[e] * fro2_diff(s->F + 9 * e, R);
+        }
+        return pe;
+    }
     for (int e = 0; e < s->ne; ++e) pe += s->vol[e] * orc_nh_psi_plain(s->mu_e[e], s->lambda_e[e], s->sig + 3 * e);
     return pe;
 }
@@ -865,8 +889,27 @@ static int prox_error;
 
 double orc_polar_update(orc_state* s, int update_candidates) {
     double bef_pe = s->curr_pe, pe = 0.0, bef = 0.0, aft = 0.0;
-    double* tmp = NEWD(3 * s->ne);
     prox_error = 0;
+    if (s->p.model == 1) {   /* ARAP branch, src/TetElements.cpp:265-282 */
+        for (int e = 0; e < s->ne; ++e) {
+            double *Z = s->Z + 9 * e, *U = s->U + 9 * e;
+            const double* S = s->symF + 9 * e;
+            double Sio[9], ZmU[9], SmI[9], SmU[9];
+            for (int i = 0; i < 9; ++i) { Sio[i] = S[i] + U[i]; ZmU[i] = Z[i] - U[i]; SmI[i] = S[i]; }
+            bef += 0.5 * s->w2[e] * fro2_diff(S, ZmU);
+            for (int i = 0; i < 9; ++i) Sio[i] = 0.5 * Sio[i];
+            for (int d = 0; d < 3; ++d) { Sio[4 * d] += 0.5; SmI[4 * d] -= 1.0; }
+            double n2 = 0.0;
+            for (int i = 0; i < 9; ++i) n2 += SmI[i] * SmI[i];
+            pe += 0.5 * 1.0 * s->vol[e] * n2;
+            for (int i = 0; i < 9; ++i) SmU[i] = Sio[i] - U[i];
+            aft += 0.5 * s->w2[e] * fro2_diff(S, SmU);
+            for (int i = 0; i < 9; ++i) { Z[i] = Sio[i]; U[i] += S[i] - Sio[i]; }
+        }
+        s->curr_pe = pe;
+        return aft - bef + pe - bef_pe;
+    }
+    double* tmp = NEWD(3 * s->ne);
     for (int e = 0; e < s->ne; ++e) {
         double *Z = s->Z + 9 * e, *U = s->U + 9 * e;
         const double* S = s->symF + 9 * e;
@@ -982,6 +1025,76 @@ static int lbfgs_minimize(orc_state* s, int* err) {
     return breaking ? global_iter : global_iter - 1;
 }
 
+/* ---- rotation-unaware ADMM (-ra 0) ----------------------------------------- */
+/* TetElements::update, src/TetElements.cpp:193-254: from F at the current x
+ * (update_defo_cache), Ft = F^T + U; NH: SVD of Ft^T, prox from the last
+ * stretches, Ft = V sigma* U^T; ARAP: Ft = (F' + rot(F'))^T / 2 with F' = Ft^T;
+ * then U += F^T - Ft, Z = Ft. */
+static void local_update_unaware(orc_state* s, int update_candidates) {
+    double* tmp = NEWD(3 * s->ne);
+    prox_error = 0;
+    for (int e = 0; e < s->ne; ++e) {
+        double *Z = s->Z + 9 * e, *U = s->U + 9 * e;
+        const double* F = s->F + 9 * e;
+        double Dx[9], Fp[9], Ft[9];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) A3(Dx, r, c) = A3(F, c, r);
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) A3(Fp, r, c) = A3(Dx, c, r) + A3(U, c, r);   /* (Dx + U)^T */
+        if (s->p.model == 1) {
+            double R[9];
+            rot3(Fp, R);
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) A3(Ft, r, c) = 0.5 * (A3(Fp, c, r) + A3(R, c, r));
+        } else {
+            double sg[3], Ue[9], Ve[9];
+            orc_svd3(Fp, sg, Ue, Ve);
+            double* x = s->slast + 3 * e;
+            double xs[3] = {x[0], x[1], x[2]};
+            (void)orc_prox_lbfgs(s->mu_e[e], s->lambda_e[e], sg, s->w2[e] / s->vol[e], xs, 20);
+            memcpy(x, xs, sizeof xs);
+            memcpy(tmp + 3 * e, xs, sizeof xs);
+            if (xs[0] < 0.0 || xs[1] < 0.0 || xs[2] < 0.0) prox_error = 1;
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) {
+                    double v = 0.0;
+                    for (int k = 0; k < 3; ++k) v += A3(Ve, r, k) * xs[k] * A3(Ue, c, k);
+                    A3(Ft, r, c) = v;
+                }
+        }
+        for (int i = 0; i < 9; ++i) { U[i] += Dx[i] - Ft[i]; Z[i] = Ft[i]; }
+    }
+    if (update_candidates && s->p.reweighting) candidate_weights(s, tmp);
+    free(tmp);
+}
+
+/* UnawareGS::global_step, src/GlobalStepBehavior.hpp:162-180: b = sum_e w^2
+ * Di^T (Z - U - Dfix xfix) (TetElements::add_to_b, src/TetElements.cpp:470-481),
+ * x = A^-1 b per column, then the defo cache at the new x. */
+static void global_step_unaware(orc_state* s) {
+    const int n = 3 * s->nf;
+    double* b = NEWD(n);
+    for (int e = 0; e < s->ne; ++e) {
+        const double* Di = s->Di + 12 * e;
+        double T[9];
+        for (int i = 0; i < 9; ++i) T[i] = s->Z[9 * e + i] - s->U[9 * e + i];
+        if (s->nfree[e] < 4)
+            for (int i = 0; i < 9; ++i) T[i] -= s->Dfx[9 * e + i];
+        for (int a = 0; a < 4; ++a) {
+            const int j = s->fidx[4 * e + a];
+            if (j < 0) continue;
+            for (int r = 0; r < 3; ++r) {
+                double v = 0.0;
+                for (int c = 0; c < 3; ++c) v += Di[c + 3 * a] * A3(T, c, r);
+                b[3 * j + r] += s->w2[e] * v;
+            }
+        }
+    }
+    orc_solve_A(s, b, s->xfree);
+    free(b);
+    defo_cache_at(s, s->xfree);
+}
+
 /* ---- ADMM driver --------------------------------------------------------- */
 static void load_positions(orc_state* s) {
     const orc_problem* p = &s->p;
@@ -999,17 +1112,31 @@ static void init_dual(orc_state* s) {
     for (int e = 0; e < s->ne; ++e) {
         double F[9], sg[3], Uu[9], Vv[9];
         F_from_X(s, e, s->p.init, F);
-        orc_svd3(F, sg, Uu, Vv);
         double* Z = s->Z + 9 * e;
+        memset(s->U + 9 * e, 0, 9 * sizeof(double));
+        if (!s->p.rot_aware) {   /* Z = Di x = F^T (src/TetElements.cpp:167-181) */
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) A3(Z, r, c) = A3(F, c, r);
+            continue;
+        }
+        orc_svd3(F, sg, Uu, Vv);
         for (int r = 0; r < 3; ++r)   /* Z = S^T with S = V diag(s) V^T */
             for (int c = 0; c < 3; ++c) {
                 double v = 0.0;
                 for (int k = 0; k < 3; ++k) v += A3(Vv, c, k) * sg[k] * A3(Vv, r, k);
                 A3(Z, r, c) = v;
             }
-        memset(s->U + 9 * e, 0, 9 * sizeof(double));
     }
+    if (!s->p.rot_aware) return;
     for (int e = 0; e < s->ne; ++e) {
+        if (s->p.model == 1) {   /* ARAP polar_potential_energy, src/TetElements.cpp:640-646 */
+            const double* Z = s->Z + 9 * e;
+            double n2 = 0.0;
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) { const double d = A3(Z, r, c) - (r == c ? 1.0 : 0.0); n2 += d * d; }
+            pe += 0.5 * 1.0 * s->vol[e] * n2;
+            continue;
+        }
         double Zt[9], sg[3], Uu[9], Vv[9];
         for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c) A3(Zt, r, c) = A3(s->Z + 9 * e, c, r);
         orc_svd3(Zt, sg, Uu, Vv);
@@ -1029,6 +1156,8 @@ void orc_init_state(orc_state* s) {
 int orc_setup(orc_state* s) {
     const orc_problem* p = &s->p;
     int rc;
+    /* update_all_candidate_weights throws for any model but NH (src/TetElements.cpp:393-395) */
+    if (p->reweighting && p->model != 0) return E_INPUT;
     load_positions(s);
     /* GlobalStepBehavior ctor: midupdate_weights(X_init), src/TetElements.cpp:360-381 */
     if (p->reweighting) {
@@ -1070,14 +1199,24 @@ int orc_iterate(orc_state* s) {
     int rc;
     if (!s->setup_done) return E_INPUT;
     if (s->iter >= p->max_iters) return E_INPUT;
-    double dal = orc_polar_update(s, 1);
-    if (prox_error) return E_PROX_NEG;
-    defo_cache_at(s, s->xfree);
-    double obj_bef = global_value(s, s->xfree);
-    s->m_tol = fabs(dal);
-    int its = lbfgs_minimize(s, &rc);
-    if (rc != E_OK) return rc;
-    double obj_aft = global_value(s, s->xfree);
+    double dal = 0.0, obj_bef = 0.0, obj_aft = 0.0;
+    int its = 1;
+    if (!p->rot_aware) {
+        /* local_update, update_defo_cache, UnawareGS::global_step (ADMM.cpp:117-133) */
+        local_update_unaware(s, 1);
+        if (prox_error) return E_PROX_NEG;
+        global_step_unaware(s);
+        obj_aft = 1.e8;   /* UnawareGS::last_step_delta_auglag */
+    } else {
+        dal = orc_polar_update(s, 1);
+        if (prox_error) return E_PROX_NEG;
+        defo_cache_at(s, s->xfree);
+        obj_bef = global_value(s, s->xfree);
+        s->m_tol = fabs(dal);
+        its = lbfgs_minimize(s, &rc);
+        if (rc != E_OK) return rc;
+        obj_aft = global_value(s, s->xfree);
+    }
     int rw = 0;
     if (p->reweighting) {
         if (p->rw_every > 0) rw = ((s->iter + 1) % p->rw_every) == 0;

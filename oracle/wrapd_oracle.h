@@ -44,6 +44,8 @@ typedef struct {
     int rw_every;         /* extension: >0 reweights every rw_every iterations instead of the gamma rule */
     const double* youngs_e;   /* extension: per-element Young's modulus (a batch of meshes), or NULL */
     const double* poisson_e;  /* extension: per-element Poisson ratio, or NULL */
+    int rot_aware;        /* -ra      (1); 0 = UnawareGS (src/GlobalStepBehavior.hpp:118-193) */
+    int model;            /* -model   (0 = nh, 1 = arap) */
 } orc_problem;
 
 void orc_problem_defaults(orc_problem* p);

@@ -12,6 +12,10 @@ Outputs (all seeded, reproducible):
   tiny_step.npz     one setup + local step + gradient of TetElements on a small bar
   solve_small.npz   full reference solves of small bars (default and rw_delay 5)
   solve_config0.npz the reference solve of the 8x8x32 bar (E = 1e5, nu = 0.45)
+  solve_modes.npz   reference solves of a small bar with -ra 0, -model arap -rw 0
+                    and -model arap -rw 0 -ra 0
+
+    python tests/golden/make_golden.py [--only modes]
 """
 from __future__ import annotations
 
@@ -131,14 +135,32 @@ def solves():
                         ls_dal=r["ls_delta_al"], gs_dal=r["gs_delta_al"])
 
 
+def modes():
+    b = bars.make_bar(3, 3, 8, twist_deg=90.0, noise=0.02, seed=5)
+    out = {}
+    for tag, extra in [("ra0", ("-ra", "0")), ("arap", ("-model", "arap", "-rw", "0")),
+                       ("arap_ra0", ("-model", "arap", "-rw", "0", "-ra", "0"))]:
+        r = ref_solve(b, 60, extra)
+        out.update({f"{tag}_objectives": r["objectives"], f"{tag}_inner": r["inner_iters"],
+                    f"{tag}_reweighted": r["reweighted"], f"{tag}_x": r["x"],
+                    f"{tag}_ls_dal": r["ls_delta_al"], f"{tag}_gs_dal": r["gs_delta_al"]})
+    np.savez_compressed(os.path.join(HERE, "solve_modes.npz"), rest=b.rest, init=b.init, tets=b.tets,
+                        pins=b.pins, **out)
+
+
 def main():
     if not po.ref_available():
         raise SystemExit("oracle/_ref is not built: run `make -C oracle ref` (needs the reference sources)")
+    if sys.argv[1:] == ["--only", "modes"]:
+        modes()
+        print("golden vectors written to", HERE)
+        return
     ref = po.load_ref_elem()
     rng = np.random.default_rng(20240611)
     elem_cases(ref, rng)
     tiny_step(ref)
     solves()
+    modes()
     print("golden vectors written to", HERE)
 
 

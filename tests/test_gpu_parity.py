@@ -220,8 +220,8 @@ def test_bad_input_is_rejected():
         s.initialize()
     assert ei.value.name == "WRAPD_E_INPUT"
     with pytest.raises(capi.WrapdError) as ei:
-        Solver(Settings(rot_aware=0))
-    assert ei.value.name == "WRAPD_E_UNSUPPORTED"
+        Solver(Settings(rot_aware=2))
+    assert ei.value.name == "WRAPD_E_INPUT"
     s2 = Solver(youngs=E_YOUNG)
     with pytest.raises(capi.WrapdError) as ei:
         s2.begin_solve()

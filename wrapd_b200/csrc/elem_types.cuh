@@ -5,9 +5,13 @@
 
 namespace wrapd {
 
+enum : int { MODEL_NH = 0, MODEL_ARAP = 1 };
+
 struct Material {
     double mu, lambda;
     double wr, wmin, wmax;   // rest stiffness k and its beta_min / beta_max multiples
+    int model;               // MODEL_NH or MODEL_ARAP (ARAP: psi = |F - R|^2 / 2, k = 1)
+    int pad;
 };
 
 struct ElemView {

@@ -65,6 +65,15 @@ __device__ __forceinline__ void deformation(const ElemView& E, int e, const doub
     }
 }
 
+// potential_energy_x per element (src/TetElements.cpp:598-635) from the
+// sign-fixed singular values: NH psi(sigma); ARAP |F - R|^2 / 2 with
+// R = U V^T, i.e. sum (sigma_i - 1)^2 / 2 (k = 1).
+__device__ __forceinline__ double elastic_energy(const Material& m, const double* s) {
+    if (m.model == MODEL_ARAP)
+        return 0.5 * ((s[0] - 1.0) * (s[0] - 1.0) + (s[1] - 1.0) * (s[1] - 1.0) + (s[2] - 1.0) * (s[2] - 1.0));
+    return NH<double>{m.mu, m.lambda}.psi_plain(s[0], s[1], s[2]);
+}
+
 // ---- the defo cache + gradient of the global AL objective -------------------
 // update_defo_cache (src/TetElements.cpp:564-596) fused with
 // global_obj_grad (src/TetElements.cpp:691-738): F, SVD, symF, Q = V^T P V,
@@ -108,7 +117,7 @@ static __global__ void __launch_bounds__(128) k_grad(ElemView E, const double* _
             for (int i = 0; i < 9; ++i) { const double d = double(S[i]) - double(P[i]); v += d * d; }
             red[0] = (0.5 * w2) * v;
         }
-        red[1] = E.vol[e] * NH<double>{mat.mu, mat.lambda}.psi_plain(double(s[0]), double(s[1]), double(s[2]));
+        red[1] = E.vol[e] * elastic_energy(mat, s);
         red[2] = (s[0] < double(0) || s[1] < double(0) || s[2] < double(0)) ? 1.0 : 0.0;
         if (write_gel) {
             double Tm[9], Q[9], K[9], Mm[9];
@@ -356,8 +365,18 @@ static __global__ void __launch_bounds__(128) k_init_dual(ElemView E, const doub
         for (int r = 0; r < 3; ++r)
 #pragma unroll
             for (int c = 0; c < 3; ++c) M3(Zt, r, c) = M3(Zm, c, r);
-        svd3(Zt, s, Us, Vs);
-        red[0] = E.vol[e] * NH<double>{mat.mu, mat.lambda}.psi_plain(double(s[0]), double(s[1]), double(s[2]));
+        if (mat.model == MODEL_ARAP) {
+            // ARAP polar_potential_energy (src/TetElements.cpp:640-646): |Z - I|^2 / 2
+            double n2 = 0.0;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) { const double d = M3(Zm, r, c) - (r == c ? 1.0 : 0.0); n2 += d * d; }
+            red[0] = 0.5 * E.vol[e] * n2;
+        } else {
+            svd3(Zt, s, Us, Vs);
+            red[0] = E.vol[e] * NH<double>{mat.mu, mat.lambda}.psi_plain(double(s[0]), double(s[1]), double(s[2]));
+        }
     }
     grid_reduce<1>(red, partials, counter, out);
 }
@@ -449,6 +468,199 @@ static __global__ void __launch_bounds__(256) k_xupdate(int n, double* __restric
         s[i] = xn - xo;
         x[i] = xn;
     }
+}
+
+// ---- ARAP local step (rotation-aware) ------------------------------------------
+// polar_update, ARAP branch (src/TetElements.cpp:265-282): S = symF + U (both
+// symmetric), Z = (S + I) / 2, U += symF - Z; curr_pe = sum vol |symF - I|^2 / 2.
+// out[0..4] as k_local (no prox: [3] = [4] = 0).
+static __global__ void __launch_bounds__(128) k_local_arap(ElemView E, double* partials, unsigned* counter,
+                                                         double* out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (e < E.ne) {
+        double S[9], Um[9], Zm[9];
+        load9(E.symF, E.ne, e, S);
+        load9(E.U, E.ne, e, Um);
+        load9(E.Z, E.ne, e, Zm);
+        const double w2 = E.w2[e], vol = E.vol[e];
+        double bef = 0.0, aft = 0.0, n2 = 0.0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const double d = S[i] - (Zm[i] - Um[i]);
+            bef += d * d;
+        }
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const double id = (i % 4 == 0) ? 1.0 : 0.0;
+            const double So = 0.5 * ((S[i] + Um[i]) + id);
+            n2 += (S[i] - id) * (S[i] - id);
+            const double d = S[i] - (So - Um[i]);
+            aft += d * d;
+            Zm[i] = So;
+            Um[i] = Um[i] + (S[i] - So);
+        }
+        red[0] = 0.5 * w2 * bef;
+        red[1] = 0.5 * w2 * aft;
+        red[2] = 0.5 * vol * n2;
+        store9(E.Z, E.ne, e, Zm);
+        store9(E.U, E.ne, e, Um);
+    }
+    grid_reduce<5>(red, partials, counter, out);
+}
+
+// ---- rotation-unaware ADMM (-ra 0) -----------------------------------------------
+// initialize_dual_vars, rotation-unaware branch (src/TetElements.cpp:167-181):
+// Z = Di x = F^T with all four slots read from X, U = 0.
+static __global__ void __launch_bounds__(128) k_init_dual_unaware(ElemView E, const double* __restrict__ x,
+                                                                const double* __restrict__ xfix) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E.ne) return;
+    double F[9], Zm[9], zero[9] = {};
+    deformation(E, e, x, xfix, false, F);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) M3(Zm, r, c) = F[c + 3 * r];
+    store9(E.Z, E.ne, e, Zm);
+    store9(E.U, E.ne, e, zero);
+}
+
+// TetElements::update (src/TetElements.cpp:193-254) from F at the current x
+// (the defo cache): Dx = F^T, F' = (Dx + U)^T; NH: SVD of F', the prox from the
+// last stretches, Z = V diag(sigma*) U^T; ARAP: Z = (F' + rot(F'))^T / 2; then
+// U += Dx - Z.  C: arithmetic of the SVD and prox as in k_local (float in mixed
+// mode, with the same FP64 rescue).  out[0..4] = 0, 0, 0, negative stretches,
+// prox iterations.
+template <typename C>
+__global__ void __launch_bounds__(128, 4) k_local_unaware(ElemView E, const double* __restrict__ x,
+                                                       const double* __restrict__ xfix, Material mat0, int prox_iters,
+                                                       int cand_mode, int prox_mode, double* partials,
+                                                       unsigned* counter, double* out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (e < E.ne) {
+        const Material mat = elem_material(E, mat0, e);
+        double F[9], Um[9], Zn[9];
+        deformation(E, e, x, xfix, true, F);
+        load9(E.U, E.ne, e, Um);
+        C Fp[9];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) M3(Fp, r, c) = C(F[r + 3 * c] + M3(Um, c, r));   // (F^T + U)^T
+        C sg[3], Ue[9], Ve[9];
+        svd3(Fp, sg, Ue, Ve);
+        if (mat.model == MODEL_ARAP) {
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    // rot(F') = Ue Ve^T; Z(r, c) = (F'(c, r) + R(c, r)) / 2
+                    const double Rcr = double(M3(Ue, c, 0) * M3(Ve, r, 0) + M3(Ue, c, 1) * M3(Ve, r, 1) +
+                                              M3(Ue, c, 2) * M3(Ve, r, 2));
+                    M3(Zn, r, c) = 0.5 * (double(M3(Fp, c, r)) + Rcr);
+                }
+        } else {
+            const double w2 = E.w2[e], vol = E.vol[e];
+            Prox<C> P;
+            P.nh.mu = C(mat.mu);
+            P.nh.lambda = C(mat.lambda);
+            P.x0[0] = sg[0]; P.x0[1] = sg[1]; P.x0[2] = sg[2];
+            P.wov = C(w2 / vol);
+            C xs[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) xs[i] = C(E.slast[(size_t)i * E.ne + e]);
+            int iters;
+            if constexpr (sizeof(C) == sizeof(double)) {
+                if (prox_mode != 0) {
+                    iters = prox_newton(P, xs, prox_iters, C(1e-12));
+                } else {
+                    extern __shared__ double prox_hist[];
+                    iters = prox_lbfgs(P, xs, prox_iters, ProxHistory<double>{prox_hist + threadIdx.x, (int)blockDim.x});
+                    if (iters < 0) iters = prox_iters;
+                }
+            } else {
+                iters = prox_newton(P, xs, prox_iters, C(8) * Lim<C>::eps());
+                if (!(isfinite(xs[0]) && isfinite(xs[1]) && isfinite(xs[2]) && xs[0] >= C(0) && xs[1] >= C(0) &&
+                      xs[2] >= C(0))) {
+                    Prox<double> Pd;
+                    Pd.nh.mu = mat.mu;
+                    Pd.nh.lambda = mat.lambda;
+                    Pd.x0[0] = double(sg[0]); Pd.x0[1] = double(sg[1]); Pd.x0[2] = double(sg[2]);
+                    Pd.wov = w2 / vol;
+                    double xd[3];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) xd[i] = E.slast[(size_t)i * E.ne + e];
+                    iters += prox_newton(Pd, xd, prox_iters, 1e-12);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) xs[i] = C(xd[i]);
+                }
+            }
+            red[4] = double(iters);
+            double xo[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) { xo[i] = double(xs[i]); E.slast[(size_t)i * E.ne + e] = xo[i]; }
+            red[3] = (xo[0] < 0.0 || xo[1] < 0.0 || xo[2] < 0.0) ? 1.0 : 0.0;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    M3(Zn, r, c) = double(M3(Ve, r, 0) * xs[0] * M3(Ue, c, 0) + M3(Ve, r, 1) * xs[1] * M3(Ue, c, 1) +
+                                          M3(Ve, r, 2) * xs[2] * M3(Ue, c, 2));
+            if (cand_mode == CAND_REST) {
+                E.w2c[e] = vol * mat.wr;
+            } else if (cand_mode == CAND_HESSIAN) {
+                const double lm = NH<double>{mat.mu, mat.lambda}.hess_lmax(xo);
+                double cnd = lm;
+                if (lm < mat.wmin) cnd = mat.wmin;
+                if (lm > mat.wmax) cnd = mat.wmax;
+                E.w2c[e] = vol * cnd;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) M3(Um, r, c) = M3(Um, r, c) + (F[c + 3 * r] - M3(Zn, r, c));
+        store9(E.Z, E.ne, e, Zn);
+        store9(E.U, E.ne, e, Um);
+    }
+    grid_reduce<5>(red, partials, counter, out);
+}
+
+// UnawareGS right-hand side per element (TetElements::add_to_b,
+// src/TetElements.cpp:470-481): b_e(a, r) = w^2 sum_c Di(c, a) (Z - U - Dfix xfix)(c, r),
+// into the gradient rows gel (the gather adds the free slots).
+static __global__ void __launch_bounds__(128) k_rhs_unaware(ElemView E, const double* __restrict__ xfix) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E.ne) return;
+    double Zm[9], Um[9], Ffix[9] = {};
+    load9(E.Z, E.ne, e, Zm);
+    load9(E.U, E.ne, e, Um);
+    const int4 id = E.idx[e];
+    const int s[4] = {id.x, id.y, id.z, id.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        if (s[a] >= 0) continue;
+        const double* p = xfix + 3 * (size_t)(-s[a] - 1);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double d = E.Di[(size_t)(c + 3 * a) * E.ne + e];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) Ffix[c + 3 * r] += d * p[r];   // (Dfix xfix)(c, r)
+        }
+    }
+    const double w2 = E.w2[e];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            double v = 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                v += E.Di[(size_t)(c + 3 * a) * E.ne + e] * (M3(Zm, c, r) - M3(Um, c, r) - Ffix[c + 3 * r]);
+            E.gel[(size_t)(r + 3 * a) * E.ne + e] = w2 * v;
+        }
 }
 
 }  // namespace wrapd

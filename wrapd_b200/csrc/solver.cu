@@ -76,9 +76,9 @@ void element_geometry(const double* p0, const double* p1, const double* p2, cons
 }  // namespace
 
 SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
-    if (cfg.rot_aware != 1) throw CudaError(WRAPD_E_UNSUPPORTED, "rotation-unaware global step (-ra 0) is not implemented");
+    if (cfg.rot_aware != 0 && cfg.rot_aware != 1) throw CudaError(WRAPD_E_INPUT, "rot_aware must be 0 or 1");
     if (cfg.global_ls != 0) throw CudaError(WRAPD_E_UNSUPPORTED, "global-step line search (-global_ls 1) is not implemented");
-    if (cfg.model != 0) throw CudaError(WRAPD_E_UNSUPPORTED, "only the Neo-Hookean model is implemented");
+    if (cfg.model != MODEL_NH && cfg.model != MODEL_ARAP) throw CudaError(WRAPD_E_INPUT, "model must be 0 (nh) or 1 (arap)");
     if (cfg.prox_mode < 0 || cfg.prox_mode > 2)
         throw CudaError(WRAPD_E_UNSUPPORTED, "prox_mode must be 0 (L-BFGS), 1 (Newton) or 2 (Newton from the prox network)");
     if (cfg.lbfgs_m < 1 || cfg.lbfgs_m > kMaxHistory) throw CudaError(WRAPD_E_INPUT, "lbfgs_m must be in [1, 32]");
@@ -93,15 +93,19 @@ SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
     for (auto& e : ev_) WRAPD_CUDA(cudaEventCreate(&e));
     WRAPD_CUDA(cudaMallocHost(&h_scal_, S_COUNT * sizeof(double)));
     WRAPD_CUDA(cudaFuncSetAttribute(k_local<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLocalHistBytes));
+    WRAPD_CUDA(cudaFuncSetAttribute(k_local_unaware<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kLocalHistBytes));
     mat_ = material(cfg.youngs, cfg.poisson);
 }
 
 // Lame(E, nu), src/Lame.hpp:50-53; k = 2.0066 mu + 1.0122 lambda, src/TetElements.cpp:84
 Material SolverGPU::material(double youngs, double poisson) const {
-    Material m;
+    Material m{};
     m.mu = youngs / (2.0 * (1.0 + poisson));
     m.lambda = youngs * poisson / ((1.0 + poisson) * (1.0 - 2.0 * poisson));
-    m.wr = 2.0066 * m.mu + 1.0122 * m.lambda;
+    m.model = cfg.model;
+    // rest stiffness k: 1 for ARAP (src/TetElements.cpp:80-87)
+    m.wr = cfg.model == MODEL_ARAP ? 1.0 : 2.0066 * m.mu + 1.0122 * m.lambda;
     m.wmin = m.wr * cfg.beta_min;
     m.wmax = m.wr * cfg.beta_max;
     return m;
@@ -199,6 +203,9 @@ void SolverGPU::add_mesh(const double* rest, const double* init, const double* s
 void SolverGPU::initialize() {
     if (nv == 0) throw CudaError(WRAPD_E_STATE, "initialize before add_tetmesh");
     if (initialized_) throw CudaError(WRAPD_E_STATE, "already initialized");
+    // update_all_candidate_weights (src/TetElements.cpp:393-395)
+    if (cfg.model != MODEL_NH && cfg.reweighting)
+        throw CudaError(WRAPD_E_INPUT, "Adaptive weights are only supported for the NH model (use reweighting = 0)");
     auto t0 = std::chrono::steady_clock::now();
     // ---- element geometry (TetElements ctor, src/TetElements.cpp:90-142) ----
     std::vector<double> Di(12 * (size_t)ne), vol(ne), w2(ne);
@@ -418,6 +425,12 @@ void SolverGPU::gather(double* grad, const double* gold, double* ystage, const d
 }
 
 void SolverGPU::local_step(int cand_mode, bool fp32_compute) {
+    if (cfg.model == MODEL_ARAP) {
+        k_local_arap<<<blocks_for(ne, 128), 128, 0, st_>>>(view(), d_partials_, d_counter_, d_scal_ + S_LOCAL);
+        WRAPD_LAUNCH_CHECK();
+        kernel_launches++;
+        return;
+    }
     // prox_mode 2 runs the network where the last stretches are a stale warm
     // start: the first local step and the one after each reweight (the weight
     // w^2 / vol, an input of the prox, has just changed); elsewhere the last
@@ -445,6 +458,33 @@ void SolverGPU::local_step(int cand_mode, bool fp32_compute) {
     }
     WRAPD_LAUNCH_CHECK();
     kernel_launches++;
+}
+
+void SolverGPU::local_step_unaware(int cand_mode, bool fp32_compute) {
+    const int nb = blocks_for(ne, 128);
+    if (fp32_compute && cfg.model == MODEL_NH)
+        k_local_unaware<float><<<nb, 128, 0, st_>>>(view(), d_x_, d_xfix_, mat_, cfg.prox_iters, cand_mode, 1,
+                                                    d_partials_, d_counter_, d_scal_ + S_LOCAL);
+    else
+        k_local_unaware<double><<<nb, 128, kLocalHistBytes, st_>>>(view(), d_x_, d_xfix_, mat_, cfg.prox_iters,
+                                                                   cand_mode, (fp32() || cfg.prox_mode != 0) ? 1 : 0,
+                                                                   d_partials_, d_counter_, d_scal_ + S_LOCAL);
+    WRAPD_LAUNCH_CHECK();
+    kernel_launches++;
+}
+
+void SolverGPU::global_step_unaware() {
+    WRAPD_ELEM_LAUNCH(k_rhs_unaware, blocks_for(ne, 128), 128, d_xfix_);
+    gather(d_q_, nullptr, nullptr, nullptr);
+    mark(1);
+    chol.solve(d_q_, st_);
+    kernel_launches += chol.launches_solve;
+    n_solve++;
+    mark(3);
+    WRAPD_CUDA(cudaMemcpyAsync(d_x_, d_q_, 3 * (size_t)nf * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    // update_defo_cache(x, true): singular values for the energy and flips
+    grad_at_x(false);
+    mark(1);
 }
 
 void SolverGPU::set_prox_net(const float* blob) {
@@ -547,10 +587,14 @@ void SolverGPU::begin_solve() {
     // setup_solve (src/ADMM.cpp:89-107): X = X_init, defo cache, dual variables
     WRAPD_CUDA(cudaMemcpyAsync(d_x_, d_xinit_, 3 * (size_t)nf * sizeof(double), cudaMemcpyDeviceToDevice, st_));
     grad_at_x(false);
-    WRAPD_ELEM_LAUNCH(k_init_dual, blocks_for(ne, 128), 128, d_x_, d_xfix_, mat_, d_partials_, d_counter_,
-                      d_scal_ + S_INIT);
+    if (cfg.rot_aware) {
+        WRAPD_ELEM_LAUNCH(k_init_dual, blocks_for(ne, 128), 128, d_x_, d_xfix_, mat_, d_partials_, d_counter_,
+                          d_scal_ + S_INIT);
+    } else {
+        WRAPD_ELEM_LAUNCH(k_init_dual_unaware, blocks_for(ne, 128), 128, d_x_, d_xfix_);
+    }
     sync_read();
-    curr_pe_ = h_scal_[S_INIT];
+    curr_pe_ = cfg.rot_aware ? h_scal_[S_INIT] : 0.0;
     // log_initial_data (src/AlgorithmData.cpp:50-64)
     logs_.objectives.push_back(h_scal_[S_GRAD + 1]);
     logs_.flips.push_back((int)h_scal_[S_GRAD + 2]);
@@ -672,29 +716,45 @@ int SolverGPU::iterate(int n, bool* conv) {
     int done = 0;
     *conv = converged_;
     while (done < n && iter < cfg.max_iters && !converged_) {
-        // ---- local step: polar_update (src/TetElements.cpp:256-356) ----
         WRAPD_CUDA(cudaEventRecord(ev_[0], st_));
         mark(5);
-        local_step(cand_mode_now(), fp32() && !fp64_phase_);
-        if (cfg.reweighting) count_++;
-        mark(0);
-        WRAPD_CUDA(cudaEventRecord(ev_[1], st_));
-        // ---- global step: RotAwareGS::global_step (src/GlobalStepBehavior.hpp:246-258) ----
-        if (m_k_ == 0) WRAPD_CUDA(cudaMemsetAsync(d_gold_, 0, 3 * (size_t)nf * sizeof(double), st_));
-        grad_at_x(true);
-        gather(d_gcur_, d_gold_, nullptr, nullptr);
-        mark(1);
-        sync_read();
-        const double bef = h_scal_[S_LOCAL], aft = h_scal_[S_LOCAL + 1], pe = h_scal_[S_LOCAL + 2];
-        const double prox_it = h_scal_[S_LOCAL + 4];
-        if (h_scal_[S_LOCAL + 3] > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
-        const double dal = aft - bef + pe - curr_pe_;
-        curr_pe_ = pe;
-        const double obj_bef = h_scal_[S_GRAD];
-        m_tol_ = std::fabs(dal);
-        int its = 0;
-        if (!(h_scal_[S_GATHER] < 1.e-13)) its = lbfgs_minimize();
-        const double obj_aft = h_scal_[S_GRAD];
+        double dal = 0.0, obj_bef = 0.0, obj_aft = 0.0, prox_it = 0.0;
+        int its = 1;
+        if (cfg.rot_aware) {
+            // ---- local step: polar_update (src/TetElements.cpp:256-356) ----
+            local_step(cand_mode_now(), fp32() && !fp64_phase_);
+            if (cfg.reweighting) count_++;
+            mark(0);
+            WRAPD_CUDA(cudaEventRecord(ev_[1], st_));
+            // ---- global step: RotAwareGS::global_step (src/GlobalStepBehavior.hpp:246-258) ----
+            if (m_k_ == 0) WRAPD_CUDA(cudaMemsetAsync(d_gold_, 0, 3 * (size_t)nf * sizeof(double), st_));
+            grad_at_x(true);
+            gather(d_gcur_, d_gold_, nullptr, nullptr);
+            mark(1);
+            sync_read();
+            const double bef = h_scal_[S_LOCAL], aft = h_scal_[S_LOCAL + 1], pe = h_scal_[S_LOCAL + 2];
+            prox_it = h_scal_[S_LOCAL + 4];
+            if (h_scal_[S_LOCAL + 3] > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
+            dal = aft - bef + pe - curr_pe_;
+            curr_pe_ = pe;
+            obj_bef = h_scal_[S_GRAD];
+            m_tol_ = std::fabs(dal);
+            its = 0;
+            if (!(h_scal_[S_GATHER] < 1.e-13)) its = lbfgs_minimize();
+            obj_aft = h_scal_[S_GRAD];
+        } else {
+            // ---- local_update: TetElements::update (src/TetElements.cpp:193-254) ----
+            local_step_unaware(cand_mode_now(), fp32() && !fp64_phase_);
+            if (cfg.reweighting) count_++;
+            mark(0);
+            WRAPD_CUDA(cudaEventRecord(ev_[1], st_));
+            // ---- UnawareGS::global_step (src/GlobalStepBehavior.hpp:162-180): x = A^-1 b ----
+            global_step_unaware();
+            sync_read();
+            prox_it = h_scal_[S_LOCAL + 4];
+            if (h_scal_[S_LOCAL + 3] > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
+            obj_aft = 1.e8;   // UnawareGS::last_step_delta_auglag (src/GlobalStepBehavior.hpp:102)
+        }
         const double pe_x = h_scal_[S_GRAD + 1];
         const int flips = (int)h_scal_[S_GRAD + 2];
         WRAPD_CUDA(cudaEventRecord(ev_[2], st_));

@@ -79,6 +79,8 @@ private:
     void check_status();
     void grad_at_x(bool write_gel);
     void gather(double* grad, const double* gold, double* ystage, const double* sstage);
+    void local_step_unaware(int cand_mode, bool fp32_compute);
+    void global_step_unaware();
     void local_step(int cand_mode, bool fp32_compute);
     void mid_candidates(bool from_x, int cand_mode);
     void apply_weights();
