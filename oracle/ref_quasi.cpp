@@ -8,7 +8,9 @@
 //   * outputs go to `-out DIR` instead of the compiled-in WRAPD_OUTPUT_DIR;
 //   * besides the reference's logs it writes the inner L-BFGS iteration
 //     counts, the local/global delta-AL columns, the run times and the final
-//     positions as raw little-endian doubles (final_x.bin, n x 3 row-major).
+//     positions as raw little-endian doubles (final_x.bin, n x 3 row-major);
+//   * the final mesh files (final_mesh.node/.ele/.obj) are written with the
+//     reference's own MeshIO calls, as quasi.cpp:113-130 does.
 // Every other flag is handed to wrapd::Settings::parse_args unchanged.
 //
 // Only tests, the CPU baseline of bench.py and fixture generation run it.
@@ -123,6 +125,19 @@ int main(int argc, char** argv) {
         FILE* f = std::fopen((outdir + "/final_x.bin").c_str(), "wb");
         std::fwrite(rowmajor.data(), sizeof(double), rowmajor.size(), f);
         std::fclose(f);
+    }
+    {
+        auto final_mesh = mcl::TetMesh::create();
+        final_mesh->tets = init_mesh->tets;
+        const wrapd::math::MatX3& X = solver->m_system->X();
+        final_mesh->vertices.resize(init_mesh->vertices.size());
+        for (int i = 0; i < static_cast<int>(final_mesh->vertices.size()); i++) final_mesh->vertices[i] = X.row(i);
+        mcl::meshio::save_elenode(final_mesh.get(), outdir + "/final_mesh");
+        final_mesh->need_faces(true);
+        auto obj = mcl::TriangleMesh::create();
+        obj->vertices = final_mesh->vertices;
+        obj->faces = final_mesh->faces;
+        mcl::meshio::save_obj(obj.get(), outdir + "/final_mesh.obj");
     }
     return EXIT_SUCCESS;
 }

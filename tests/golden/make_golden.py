@@ -14,8 +14,10 @@ Outputs (all seeded, reproducible):
   solve_config0.npz the reference solve of the 8x8x32 bar (E = 1e5, nu = 0.45)
   solve_modes.npz   reference solves of a small bar with -ra 0, -model arap -rw 0
                     and -model arap -rw 0 -ra 0
+  quasi_small.npz   the reference front end's output files for a small bar: the
+                    logs, final_mesh.node/.ele/.obj, without and with -soln
 
-    python tests/golden/make_golden.py [--only modes]
+    python tests/golden/make_golden.py [--only modes|quasi]
 """
 from __future__ import annotations
 
@@ -148,11 +150,30 @@ def modes():
                         pins=b.pins, **out)
 
 
+def quasi_files():
+    b = bars.make_bar(3, 3, 8, twist_deg=90.0, noise=0.02, seed=5)
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        files = bars.write_bar(b, d, "q")
+        for tag, extra, it in [("plain", (), 40), ("soln", ("-soln", d + "/plain/final_mesh"), 200)]:
+            od = os.path.join(d, tag)
+            po.run_quasi_ref(files, E_YOUNG, NU, it, threads=1, extra=list(extra), outdir=od)
+            for name in ("objectives", "x_errors", "reweighted", "final_mesh.node", "final_mesh.ele",
+                         "final_mesh.obj"):
+                fn = os.path.join(od, name if "." in name else name + ".txt")
+                out[f"{tag}/{name}"] = np.frombuffer(open(fn, "rb").read(), dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, "quasi_small.npz"), **out)
+
+
 def main():
     if not po.ref_available():
         raise SystemExit("oracle/_ref is not built: run `make -C oracle ref` (needs the reference sources)")
     if sys.argv[1:] == ["--only", "modes"]:
         modes()
+        print("golden vectors written to", HERE)
+        return
+    if sys.argv[1:] == ["--only", "quasi"]:
+        quasi_files()
         print("golden vectors written to", HERE)
         return
     ref = po.load_ref_elem()
@@ -161,6 +182,7 @@ def main():
     tiny_step(ref)
     solves()
     modes()
+    quasi_files()
     print("golden vectors written to", HERE)
 
 

@@ -1,4 +1,5 @@
-"""Build the CUDA library in-tree: wrapd_b200/_lib/libwrapd_gpu.so (sm_100a).
+"""Build the CUDA library in-tree: wrapd_b200/_lib/libwrapd_gpu.so (sm_100a),
+and the command-line front end wrapd_b200/_lib/quasi that links it.
 
 Run as ``python -m wrapd_b200.build`` or through ``__graft_entry__.build()``.
 Objects are rebuilt only when a source or header is newer than them.
@@ -16,6 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT, "libwrapd_gpu.so")
+QUASI = os.path.join(OUT, "quasi")
 SOURCES = ["symbolic.cpp", "chol.cu", "solver.cu", "capi.cu", "elem_batch.cu", "prox_net.cu", "dmma_peak.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-lineinfo",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", f"-I{os.path.join(ROOT, 'include')}"]
@@ -54,6 +56,13 @@ def build(verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    quasi_src = os.path.join(CSRC, "quasi.cpp")
+    if not os.path.exists(QUASI) or os.path.getmtime(QUASI) < max(os.path.getmtime(LIB), os.path.getmtime(quasi_src)):
+        cmd = ["g++", "-O2", "-std=c++17", quasi_src, "-o", QUASI, f"-L{OUT}", "-lwrapd_gpu",
+               "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"quasi build failed:\n{r.stdout}\n{r.stderr}")
     if verbose:
         print(LIB)
     return LIB

@@ -90,6 +90,7 @@ private:
     void download_elem(const double* d, int comps, std::vector<double>& out);
     void upload_elem(double* d, int comps, const double* in);
     double x_error();
+    void x_error_launch();
 
     // host mesh
     std::vector<double> rest_, init_, soln_;
