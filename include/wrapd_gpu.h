@@ -54,14 +54,14 @@ enum {
 typedef struct wrapd_settings {
     int max_iters;        /* -it         5000  */
     double tol;           /* -tol        1e-11 */
-    int rot_aware;        /* -ra         1 (0 is not implemented: WRAPD_E_UNSUPPORTED) */
+    int rot_aware;        /* -ra         1 (0: rotation-unaware global step, x = A^-1 b) */
     int reweighting;      /* -rw         1     */
     int rw_delay;         /* -rw_delay   50    */
     double gamma;         /* -gamma      1.5   */
     int global_iters;     /* -global_it  100   */
     int global_ls;        /* -global_ls  0 (1 is not implemented: WRAPD_E_UNSUPPORTED) */
     double kappa;         /* -kappa      1     */
-    int model;            /* -model      0 = nh (1 = arap: WRAPD_E_UNSUPPORTED) */
+    int model;            /* -model      0 = nh, 1 = arap */
     double poisson;       /* -poisson    0.45  */
     double beta_static;   /* -beta_static 1    */
     double beta_min;      /* -beta_min   0.1   */

@@ -36,7 +36,8 @@ class OracleProblem(ctypes.Structure):
                 ("reweighting", ctypes.c_int), ("rw_delay", ctypes.c_int), ("gamma", ctypes.c_double),
                 ("beta_static", ctypes.c_double), ("beta_min", ctypes.c_double),
                 ("beta_max", ctypes.c_double), ("rw_every", ctypes.c_int),
-                ("youngs_e", _dp), ("poisson_e", _dp), ("rot_aware", ctypes.c_int), ("model", ctypes.c_int)]
+                ("youngs_e", _dp), ("poisson_e", _dp), ("rot_aware", ctypes.c_int), ("model", ctypes.c_int),
+                ("global_ls", ctypes.c_int)]
 
 
 _lib = None
@@ -98,7 +99,7 @@ class Oracle:
     def __init__(self, rest, init, tets, pins, youngs=1e5, poisson=0.45, max_iters=500, tol=1e-11,
                  lbfgs_m=6, reweighting=1, rw_delay=50, gamma=1.5, rw_every=0, global_iters=100,
                  kappa=1.0, beta_static=1.0, beta_min=0.1, beta_max=10.0, youngs_e=None, poisson_e=None,
-                 rot_aware=1, model=0):
+                 rot_aware=1, model=0, global_ls=0):
         """youngs_e / poisson_e: per-element material (a batch of meshes), or None."""
         self.lib = load_oracle()
         self._keep = [np.ascontiguousarray(rest, dtype=np.float64),
@@ -114,7 +115,7 @@ class Oracle:
         p.reweighting, p.rw_delay, p.gamma, p.rw_every = reweighting, rw_delay, gamma, rw_every
         p.global_iters, p.kappa = global_iters, kappa
         p.beta_static, p.beta_min, p.beta_max = beta_static, beta_min, beta_max
-        p.rot_aware, p.model = rot_aware, model
+        p.rot_aware, p.model, p.global_ls = rot_aware, model, global_ls
         if youngs_e is not None:
             self._keep += [np.ascontiguousarray(youngs_e, dtype=np.float64),
                            np.ascontiguousarray(poisson_e, dtype=np.float64)]

@@ -447,7 +447,7 @@ void orc_problem_defaults(orc_problem* p) {
     p->max_iters = 5000; p->tol = 1e-11; p->lbfgs_m = 6; p->global_iters = 100; p->kappa = 1.0;
     p->reweighting = 1; p->rw_delay = 50; p->gamma = 1.5;
     p->beta_static = 1.0; p->beta_min = 0.1; p->beta_max = 10.0; p->rw_every = 0;
-    p->rot_aware = 1; p->model = 0;
+    p->rot_aware = 1; p->model = 0; p->global_ls = 0;
 }
 
 #define NEWD(n) ((double*)calloc((size_t)(n) ? (size_t)(n) : 1, sizeof(double)))
@@ -956,6 +956,29 @@ static double dotn(const double* a, const double* b, int n) {
 
 static double* hist(double** v, int head, int M, int i) { return v[(head + i) % M]; }
 
+/* Backtracking::search (deps/mcloptlib/include/MCL/Backtracking.hpp:71-98),
+ * called by SplitMinimizer::linesearch for -global_ls 1 with p = -q: Armijo
+ * sufficient decrease 1e-4, step factor 0.7, from alpha0; a direction of norm
+ * <= machine epsilon returns the decrease constant.  `work` holds n doubles. */
+static double backtracking(orc_state* s, const double* x, const double* q, double alpha0, double* work) {
+    const int n = 3 * s->nf;
+    const double decrease = 1.e-4, tau = 0.7;
+    if (sqrt(dotn(q, q, n)) <= DBL_EPSILON) return decrease;
+    double* g = NEWD(n);
+    const double fx0 = orc_global_grad(s, x, g);
+    const double gtp = -dotn(g, q, n);
+    free(g);
+    double alpha = alpha0;
+    int iter = 0;
+    for (; iter < 100000; ++iter) {
+        for (int k = 0; k < n; ++k) work[k] = x[k] + alpha * -q[k];
+        const double fxa = global_value(s, work);
+        if (fxa <= fx0 + alpha * decrease * gtp) break;
+        alpha *= tau;
+    }
+    return iter >= 100000 ? -1.0 : alpha;
+}
+
 static int lbfgs_minimize(orc_state* s, int* err) {
     int n = 3 * s->nf, M = s->M;
     double *q = s->q, *grad = s->grad, *gold = s->grad_old, *xo = s->x_old, *x = s->xfree;
@@ -992,12 +1015,21 @@ static int lbfgs_minimize(orc_state* s, int* err) {
         }
         double dir = dotn(grad, q, n);
         if (isnan(dir)) { *err = E_NAN; free(st); free(yt); return global_iter; }
+        double alpha_init = 1.0;
         if (dir <= 0.0) {
             memcpy(q, grad, sizeof(double) * (size_t)n);
             max_iters -= s->m_k;
             s->m_k = 0;
+            double gmax = 0.0;
+            for (int k = 0; k < n; ++k) gmax = fabs(grad[k]) > gmax ? fabs(grad[k]) : gmax;
+            alpha_init = 1.0 / gmax < 1.0 ? 1.0 / gmax : 1.0;
         }
-        for (int k = 0; k < n; ++k) x[k] -= 1.0 * q[k];   /* LSMethod::None -> rate 1 */
+        double rate = 1.0;   /* LSMethod::None -> rate 1 */
+        if (s->p.global_ls && s->m_tol > 1.e-12) {
+            rate = backtracking(s, x, q, alpha_init, st);
+            if (rate <= 0.0) { free(st); free(yt); return -1; }   /* SplitMinimizer::FAILURE */
+        }
+        for (int k = 0; k < n; ++k) x[k] -= rate * q[k];
         orc_global_grad(s, x, grad);
         for (int k = 0; k < n; ++k) { st[k] = x[k] - xo[k]; yt[k] = grad[k] - gold[k]; }
         if (s->m_k < M) {

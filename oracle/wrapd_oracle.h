@@ -46,6 +46,7 @@ typedef struct {
     const double* poisson_e;  /* extension: per-element Poisson ratio, or NULL */
     int rot_aware;        /* -ra      (1); 0 = UnawareGS (src/GlobalStepBehavior.hpp:118-193) */
     int model;            /* -model   (0 = nh, 1 = arap) */
+    int global_ls;        /* -global_ls (0); 1 = Backtracking Armijo line search in the global step */
 } orc_problem;
 
 void orc_problem_defaults(orc_problem* p);

@@ -14,10 +14,13 @@ Outputs (all seeded, reproducible):
   solve_config0.npz the reference solve of the 8x8x32 bar (E = 1e5, nu = 0.45)
   solve_modes.npz   reference solves of a small bar with -ra 0, -model arap -rw 0
                     and -model arap -rw 0 -ra 0
+  solve_gls.npz     the reference solve of a strongly twisted small bar with
+                    -global_ls 1 -rw 0 (the global step's backtracking line
+                    search shortens steps from iteration 33 on)
   quasi_small.npz   the reference front end's output files for a small bar: the
                     logs, final_mesh.node/.ele/.obj, without and with -soln
 
-    python tests/golden/make_golden.py [--only modes|quasi]
+    python tests/golden/make_golden.py [--only modes|gls|quasi]
 """
 from __future__ import annotations
 
@@ -150,6 +153,14 @@ def modes():
                         pins=b.pins, **out)
 
 
+def global_ls():
+    b = bars.make_bar(3, 3, 8, twist_deg=720.0, noise=0.4, seed=7)
+    r = ref_solve(b, 80, ("-global_ls", "1", "-rw", "0"))
+    np.savez_compressed(os.path.join(HERE, "solve_gls.npz"), rest=b.rest, init=b.init, tets=b.tets, pins=b.pins,
+                        objectives=r["objectives"], inner=r["inner_iters"], reweighted=r["reweighted"], x=r["x"],
+                        ls_dal=r["ls_delta_al"], gs_dal=r["gs_delta_al"])
+
+
 def quasi_files():
     b = bars.make_bar(3, 3, 8, twist_deg=90.0, noise=0.02, seed=5)
     out = {}
@@ -172,6 +183,10 @@ def main():
         modes()
         print("golden vectors written to", HERE)
         return
+    if sys.argv[1:] == ["--only", "gls"]:
+        global_ls()
+        print("golden vectors written to", HERE)
+        return
     if sys.argv[1:] == ["--only", "quasi"]:
         quasi_files()
         print("golden vectors written to", HERE)
@@ -182,6 +197,7 @@ def main():
     tiny_step(ref)
     solves()
     modes()
+    global_ls()
     quasi_files()
     print("golden vectors written to", HERE)
 

@@ -197,3 +197,29 @@ def test_modes_match_reference_golden(golden, tag):
     # late global-step decrements are differences of nearly equal values
     gs = g[f"{tag}_gs_dal"]
     np.testing.assert_allclose(o.get("gs_dal"), gs, rtol=1e-6, atol=1e-9 * np.abs(gs).max())
+
+
+def test_global_line_search_matches_reference_golden(golden):
+    """-global_ls 1 (Backtracking::search in the global L-BFGS step,
+    deps/mcloptlib/include/MCL/Backtracking.hpp:71-98) against the reference's
+    own solve of a 720-degree-twisted small bar with -rw 0
+    (tests/golden/solve_gls.npz), where the line search shortens the step from
+    iteration 33 on: final positions within 1e-9 of max |x|, identical
+    inner-iteration log, energies within 1e-9 of the largest and 1e-6 of
+    each (the energy falls 13 orders, from 1e10 at the inverted start to 1e-3
+    near rest, so the last iterates' energies carry the first ones' rounding)."""
+    g = golden("solve_gls.npz")
+    o = po.Oracle(g["rest"], g["init"], g["tets"], g["pins"], youngs=E_YOUNG, poisson=NU, max_iters=80,
+                  reweighting=0, global_ls=1)
+    o.solve()
+    ob, ref = o.get("objectives"), g["objectives"]
+    assert np.abs(ob - ref).max() <= 1e-9 * np.abs(ref).max()
+    np.testing.assert_allclose(ob, ref, rtol=1e-6)
+    X = o.get("X").reshape(-1, 3)
+    assert np.abs(X - g["x"]).max() <= 1e-9 * np.abs(g["x"]).max()
+    np.testing.assert_array_equal(o.get("inner_iters"), g["inner"])
+    # without the line search the trajectory leaves the reference's after iteration 33
+    o0 = po.Oracle(g["rest"], g["init"], g["tets"], g["pins"], youngs=E_YOUNG, poisson=NU, max_iters=80,
+                   reweighting=0)
+    o0.solve()
+    assert np.abs(o0.get("objectives")[:80] - g["objectives"][:80]).max() > 1e-6 * np.abs(g["objectives"]).max()
