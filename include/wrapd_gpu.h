@@ -59,7 +59,7 @@ typedef struct wrapd_settings {
     int rw_delay;         /* -rw_delay   50    */
     double gamma;         /* -gamma      1.5   */
     int global_iters;     /* -global_it  100   */
-    int global_ls;        /* -global_ls  0 (1 is not implemented: WRAPD_E_UNSUPPORTED) */
+    int global_ls;        /* -global_ls  0 (1: backtracking line search in the global step) */
     double kappa;         /* -kappa      1     */
     int model;            /* -model      0 = nh, 1 = arap */
     double poisson;       /* -poisson    0.45  */

@@ -1,7 +1,8 @@
 """GPU parity of the solver modes beside the default: the rotation-unaware
-global step (-ra 0, UnawareGS: x = A^-1 b every iteration) and the ARAP model
-(-model arap, with -rw 0 as the reference requires), each against the
-reference's own solve (tests/golden/solve_modes.npz) and against the oracle.
+global step (-ra 0, UnawareGS: x = A^-1 b every iteration), the ARAP model
+(-model arap, with -rw 0 as the reference requires) and the global step's
+backtracking line search (-global_ls 1), each against the reference's own
+solve (tests/golden/solve_modes.npz, solve_gls.npz) and against the oracle.
 FP64: energies and positions within 1e-8 relative, identical logs."""
 import numpy as np
 import pytest
@@ -62,3 +63,25 @@ def test_arap_with_reweighting_is_rejected(golden):
     with pytest.raises(capi.WrapdError) as e:
         s.initialize()
     assert e.value.name == "WRAPD_E_INPUT"
+
+
+def test_global_line_search_matches_reference(golden):
+    """-global_ls 1 on a 720-degree-twisted bar (-rw 0) where the search
+    shortens the step from iteration 33 on: the reference's energies within
+    1e-8 of the largest (1e-6 of each: they fall from 1e10 to 1e-3), final
+    positions within 1e-8 of max |x|, identical inner-iteration log; and the
+    oracle's trajectory to 1e-9 of the largest energy."""
+    g = golden("solve_gls.npz")
+    X, d = _solve(g, 80, reweighting=0, global_ls=1)
+    ref = g["objectives"]
+    assert np.abs(d.objectives - ref).max() <= 1e-8 * np.abs(ref).max()
+    np.testing.assert_allclose(d.objectives, ref, rtol=1e-6)
+    assert np.abs(X - g["x"]).max() <= 1e-8 * np.abs(g["x"]).max()
+    np.testing.assert_array_equal(d.inner_iters, g["inner"])
+    o = po.Oracle(g["rest"], g["init"], g["tets"], g["pins"], youngs=E_YOUNG, poisson=NU, max_iters=80,
+                  reweighting=0, global_ls=1)
+    o.solve()
+    assert np.abs(d.objectives - o.get("objectives")).max() <= 1e-9 * np.abs(ref).max()
+    # the search is live: plain rate-1 steps leave this trajectory
+    X0, d0 = _solve(g, 80, reweighting=0)
+    assert np.abs(d0.objectives[:60] - ref[:60]).max() > 1e-6 * np.abs(ref).max()

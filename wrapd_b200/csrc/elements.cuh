@@ -456,18 +456,48 @@ static __global__ void __launch_bounds__(256) k_axpy_dot(int n, double* __restri
     grid_reduce<1>(red, partials, counter, out, base, scale);
 }
 
-// x <- x - step with step = q, or grad when the decrement dir <= 0 (the
-// steepest-descent restart of SplitLBFGS.hpp:189-194); s = x_new - x_old.
+// x <- x - rate * step with step = q, or grad when the decrement dir <= 0
+// (the steepest-descent restart of SplitLBFGS.hpp:189-194); s = x_new - x_old.
+// rate is 1 unless the global line search chose another (SplitLBFGS.hpp:196-206).
 static __global__ void __launch_bounds__(256) k_xupdate(int n, double* __restrict__ x, const double* __restrict__ q,
                                                  const double* __restrict__ grad, const double* __restrict__ dir,
-                                                 double* __restrict__ s) {
+                                                 double rate, double* __restrict__ s) {
     const bool restart = !(*dir > 0.0);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double xo = x[i];
-        const double xn = xo - (restart ? grad[i] : q[i]);
+        const double xn = xo - rate * (restart ? grad[i] : q[i]);
         s[i] = xn - xo;
         x[i] = xn;
     }
+}
+
+// Inputs of the global line search (Backtracking::search,
+// deps/mcloptlib/include/MCL/Backtracking.hpp:71-98): out[0] = <q, q>,
+// out[1] = <grad, grad> (sums); then, in k_ls_gmax, out[0] = max |grad|.
+static __global__ void __launch_bounds__(256) k_ls_norms(int n, const double* __restrict__ q,
+                                                  const double* __restrict__ grad, double* partials,
+                                                  unsigned* counter, double* out) {
+    double red[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        red[0] += q[i] * q[i];
+        red[1] += grad[i] * grad[i];
+    }
+    grid_reduce<2>(red, partials, counter, out);
+}
+
+static __global__ void __launch_bounds__(256) k_ls_gmax(int n, const double* __restrict__ grad, double* partials,
+                                                 unsigned* counter, double* out) {
+    double red[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        red[0] = fmax(red[0], fabs(grad[i]));
+    grid_reduce<1, true>(red, partials, counter, out);
+}
+
+// Trial point of the line search: xt = x + alpha * p with p = -step.
+static __global__ void __launch_bounds__(256) k_ls_trial(int n, double* __restrict__ xt, const double* __restrict__ x,
+                                                  const double* __restrict__ step, double alpha) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        xt[i] = x[i] + alpha * -step[i];
 }
 
 // ---- ARAP local step (rotation-aware) ------------------------------------------

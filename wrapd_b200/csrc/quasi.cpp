@@ -183,7 +183,7 @@ void help() {
         "\nArgs (as the reference's quasi):\n"
         " -rest, -init, -soln <stem>   .node/.ele meshes; -handles <file>: pinned vertex ids\n"
         " -it N (5000)  -tol T (1e-11)  -ra 0|1 (1)  -rw 0|1 (1)  -rw_delay N (50)  -gamma G (1.5)\n"
-        " -global_it N (100)  -global_ls 0  -kappa K (1)  -model nh|arap  -poisson P (0.45)\n"
+        " -global_it N (100)  -global_ls 0|1  -kappa K (1)  -model nh|arap  -poisson P (0.45)\n"
         " -beta_static B (1)  -beta_min B (0.1)  -beta_max B (10)  -p 0|1  -s 0|1 (1)\n"
         "Extensions: -youngs E (1e7)  -out DIR (.)  -lbfgs_m M (6)  -rw_every N  -precision fp64|mixed\n"
         "            -prox lbfgs|newton|net  -net FILE  -leaf N  -device D\n\n");

@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <numeric>
 
 namespace wrapd {
@@ -26,7 +27,10 @@ enum : int {
     S_ALPHA = 20,    // alpha_i, up to 32 entries
     S_C = 52,        // alpha_i - beta_i, up to 32 entries
     S_ONE = 84,      // constant 1 (a device-side coefficient)
-    S_COUNT = 85
+    S_LSN = 85,      // line search: <q, q>, <grad, grad>
+    S_LSM = 87,      // line search: max |grad|
+    S_LSV = 88,      // line search: AL value, pe, flips at the trial point
+    S_COUNT = 91
 };
 constexpr int kMaxHistory = 32;
 // Dynamic shared memory of k_local<double>: the prox L-BFGS history, 48 doubles
@@ -78,7 +82,7 @@ void element_geometry(const double* p0, const double* p1, const double* p2, cons
 
 SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
     if (cfg.rot_aware != 0 && cfg.rot_aware != 1) throw CudaError(WRAPD_E_INPUT, "rot_aware must be 0 or 1");
-    if (cfg.global_ls != 0) throw CudaError(WRAPD_E_UNSUPPORTED, "global-step line search (-global_ls 1) is not implemented");
+    if (cfg.global_ls != 0 && cfg.global_ls != 1) throw CudaError(WRAPD_E_INPUT, "global_ls must be 0 or 1");
     if (cfg.model != MODEL_NH && cfg.model != MODEL_ARAP) throw CudaError(WRAPD_E_INPUT, "model must be 0 (nh) or 1 (arap)");
     if (cfg.prox_mode < 0 || cfg.prox_mode > 2)
         throw CudaError(WRAPD_E_UNSUPPORTED, "prox_mode must be 0 (L-BFGS), 1 (Newton) or 2 (Newton from the prox network)");
@@ -628,6 +632,48 @@ void SolverGPU::begin_solve() {
 // SplitLBFGS::minimize (deps/mcloptlib/include/MCL/SplitLBFGS.hpp:114-256) with
 // LSMethod::None (rate 1).  On entry the gradient at x is in d_gcur_ and the
 // |grad - grad_old|^2 early-return test has passed.
+// Backtracking::search (deps/mcloptlib/include/MCL/Backtracking.hpp:71-98) as
+// SplitLBFGS::minimize calls it for -global_ls 1: p = -q, or -grad with
+// alpha0 = min(1, 1 / max|grad|) after a non-descent restart; Armijo decrease
+// 1e-4, step factor 0.7; a direction of norm <= machine epsilon returns 1e-4.
+// fx0 is the AL value of the last gradient evaluation, which was at x.  Each
+// trial value is one gradient-kernel pass (no gradient rows) at x + alpha p
+// into a staging vector; the element cache it leaves is refreshed by the
+// gradient at the accepted x.  On a non-descent restart the history reset of
+// SplitLBFGS.hpp:189-194 is applied here, before the search.
+double SolverGPU::line_search() {
+    const int n = 3 * nf, vb = vec_blocks(n);
+    k_ls_norms<<<vb, 256, 0, st_>>>(n, d_q_, d_gcur_, d_partials_, d_counter_, d_scal_ + S_LSN);
+    k_ls_gmax<<<vb, 256, 0, st_>>>(n, d_gcur_, d_partials_, d_counter_, d_scal_ + S_LSM);
+    WRAPD_LAUNCH_CHECK();
+    kernel_launches += 2;
+    sync_read();
+    const double dir = h_scal_[S_DIR];
+    if (std::isnan(dir)) throw CudaError(WRAPD_E_NAN, "L-BFGS decrement is NaN");
+    const bool restart = !(dir > 0.0);
+    ls_restart_ = restart;
+    const double alpha0 = restart ? std::min(1.0, 1.0 / h_scal_[S_LSM]) : 1.0;
+    const double pnorm = std::sqrt(restart ? h_scal_[S_LSN + 1] : h_scal_[S_LSN]);
+    const double decrease = 1.e-4, tau = 0.7;
+    if (pnorm <= std::numeric_limits<double>::epsilon()) return decrease;
+    const double fx0 = h_scal_[S_GRAD];
+    const double gtp = restart ? -h_scal_[S_LSN + 1] : -dir;
+    const double* step = restart ? d_gcur_ : d_q_;
+    double alpha = alpha0;
+    for (int it = 0; it < 100000; ++it) {
+        k_ls_trial<<<vb, 256, 0, st_>>>(n, d_sstage_, d_x_, step, alpha);
+        WRAPD_LAUNCH_CHECK();
+        kernel_launches++;
+        WRAPD_ELEM_LAUNCH(k_grad, blocks_for(ne, 128), 128, d_sstage_, d_xfix_, mat_, 0, d_partials_, d_counter_,
+                          d_scal_ + S_LSV);
+        sync_read();
+        const double fxa = h_scal_[S_LSV];
+        if (fxa <= fx0 + alpha * decrease * gtp) return alpha;
+        alpha *= tau;
+    }
+    return -1.0;
+}
+
 int SolverGPU::lbfgs_minimize() {
     const int M = cfg.lbfgs_m, n = 3 * nf, vb = vec_blocks(n);
     int max_iters = cfg.global_iters, global_iter = 1;
@@ -673,8 +719,17 @@ int SolverGPU::lbfgs_minimize() {
                                             d_partials_, d_counter_, d_scal_ + S_DIR);
             kernel_launches += it + 1;
         }
-        // x -= q (or grad on a non-descent direction); s = x_new - x_old
-        k_xupdate<<<vb, 256, 0, st_>>>(n, d_x_, d_q_, d_gcur_, d_scal_ + S_DIR, d_sstage_);
+        // -global_ls 1: Backtracking::search along p = -q (SplitLBFGS.hpp:196-206)
+        double rate = 1.0;
+        if (cfg.global_ls && m_tol_ > 1.e-12) {
+            rate = line_search();
+            if (rate <= 0.0) {   // SplitMinimizer::FAILURE, after the restart's history reset
+                if (ls_restart_) m_k_ = 0;
+                return -1;
+            }
+        }
+        // x -= rate q (or rate grad on a non-descent direction); s = x_new - x_old
+        k_xupdate<<<vb, 256, 0, st_>>>(n, d_x_, d_q_, d_gcur_, d_scal_ + S_DIR, rate, d_sstage_);
         WRAPD_LAUNCH_CHECK();
         kernel_launches++;
         mark(2);

@@ -86,6 +86,7 @@ private:
     void apply_weights();
     void factor();
     int lbfgs_minimize();
+    double line_search();
     int cand_mode_now() const;
     void download_elem(const double* d, int comps, std::vector<double>& out);
     void upload_elem(double* d, int comps, const double* in);
@@ -126,6 +127,7 @@ private:
     int count_ = 0;          // reweight-delay counter (src/TetElements.cpp:404)
     int m_k_ = 0;
     double m_tol_ = 1e-15;
+    bool ls_restart_ = false;   // the last line search followed a non-descent restart
     double curr_pe_ = 0.0;
     double init_xerr_ = 1.0;
     bool initialized_ = false, solving_ = false, converged_ = false;
