@@ -4,10 +4,11 @@
 //   extend-add   children's update matrices into the fronts (one launch per
 //                child slot, so two children never write one entry at once);
 //   then per panel of NB = 32 columns (right-looking partial Cholesky):
-//   diag         one CTA per front: Cholesky of the NB x NB diagonal block and
-//                its inverse Li (stored as a diagonal block of Y);
-//   trsm         the panel rows below the block, P <- P Li^T, and the inverse
-//                row block Y[p, 0:p0] <- Li Y[p, 0:p0] (FP64 DMMA tiles);
+//   panel        every CTA factors the NB x NB diagonal block in registers
+//                (one warp) and forms its inverse Li (also stored as a diagonal
+//                block of Y), then applies it to one tile: the panel rows
+//                below the block, P <- P Li^T, or the inverse row block
+//                Y[p, 0:p0] <- Li Y[p, 0:p0] (FP64 DMMA tiles);
 //   update       blocked right-looking: inside the current OB-column block,
 //                F[j0:, j0:be] -= P P^T and Y[j0:be, 0:j0] -= P Y[p, 0:j0];
 //                after a block's last panel, the deferred trailing update
@@ -34,6 +35,7 @@ constexpr int TL = 64;        // output tile of the DMMA kernels
 constexpr int SLD = NB + 4;   // smem row pitch (doubles) for [row][k] operand tiles
 constexpr int GEMM_THREADS = 128;
 constexpr int ROWS_PER_CTA = 128;  // solve row tiles
+constexpr int kFusedPanelCtas = 4 * 148;   // panel steps up to one wave (4 CTAs per SM) run fused
 constexpr int COLS_PER_CTA = 8;    // solve / extend-add column groups (one warp each)
 
 __device__ __forceinline__ int find_item(const int* prefix, int n, int b) {
@@ -243,66 +245,99 @@ __global__ void k_extend_add(double* __restrict__ F, const FrontDesc* __restrict
 }
 
 // ---- panel factorization -------------------------------------------------------
-// One CTA per front: Cholesky of the NB x NB diagonal block in shared memory
-// and its inverse Li, written as the diagonal block of Y.
-__global__ void __launch_bounds__(256) k_diag(double* __restrict__ F, double* __restrict__ Y,
-                                              const FrontDesc* __restrict__ desc, WorkList wl, int p,
-                                              int* __restrict__ status) {
-    __shared__ double L[NB][NB + 1];
-    __shared__ double Li[NB][NB + 1];
-    const FrontDesc d = desc[wl.d_fronts[blockIdx.x]];
-    const int p0 = p * NB;
-    const int nb = min(NB, d.k - p0);
-    if (nb <= 0) return;
+// Cholesky of the nb x nb (nb <= NB = 32) diagonal block at Fd (column-major,
+// lower part read) and its inverse, by a CTA of 128 threads in shared memory.
+// Right-looking: at pivot j every thread updates a fixed slice of 8 entries
+// of row i = tid % 32 (columns tid / 32 + 4m), with all its operands loaded
+// before the first store, so one barrier per pivot is the only serial step.
+// L(i, j) = A'(i, j) rsqrt(d) goes to Lsm (pitch lp), rsqrt(d) to D.  The
+// inverse is right-looking by rows: row s of inv(L) is (e_s - P(s, :)) / L(s, s)
+// and the rows below add L(r, s) times it to their partial sums P (kept in S).
+// Row s of inv(L) is written to X (pitch xp), columns < nb.  A non-positive
+// (or NaN) pivot sets *bad and continues with a unit pivot.
+constexpr int LSP = NB + 1;
+static_assert(GEMM_THREADS == 128 && NB == 32, "cta_chol_inv maps 128 threads onto 32 rows x 4 column slices");
+__device__ __forceinline__ void cta_chol_inv(const double* __restrict__ Fd, int64_t ld, int nb, double* S,
+                                             double* Lsm, int lp, double* D, double* X, int xp, bool* bad) {
     const int tid = threadIdx.x;
-    double* Fd = F + d.f_off + p0 + (int64_t)p0 * d.ld;
-    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-        const int i = idx % NB, j = idx / NB;
-        L[i][j] = (i < nb && j < nb && i >= j) ? Fd[i + (int64_t)j * d.ld] : 0.0;
-        Li[i][j] = 0.0;
+    for (int idx = tid; idx < NB * NB; idx += GEMM_THREADS) {
+        const int i = idx & 31, c = idx >> 5;
+        S[i * LSP + c] = (i < nb && c <= i) ? Fd[i + (int64_t)c * ld] : 0.0;
     }
     __syncthreads();
+    const int i = tid & 31, q = tid >> 5;
+    bool b = false;
     for (int j = 0; j < nb; ++j) {
-        if (tid == 0) {
-            double v = L[j][j];
-            if (!(v > 0.0)) {   // non-SPD or NaN pivot: flag it and continue with a unit pivot
-                atomicExch(status, WRAPD_E_NOT_SPD);
-                v = 1.0;
-            }
-            L[j][j] = sqrt(v);
+        double piv = S[j * LSP + j];
+        const double sij = S[i * LSP + j];
+        double cj[8], ic[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            cj[m] = S[(q + 4 * m) * LSP + j];
+            ic[m] = S[i * LSP + q + 4 * m];
         }
-        __syncthreads();
-        for (int i = j + 1 + tid; i < nb; i += blockDim.x) L[i][j] /= L[j][j];
-        __syncthreads();
-        const int m = nb - j - 1;
-        for (int idx = tid; idx < m * m; idx += blockDim.x) {
-            const int i = j + 1 + idx % m, c = j + 1 + idx / m;
-            if (c <= i) L[i][c] -= L[i][j] * L[c][j];
+        if (!(piv > 0.0)) { b = true; piv = 1.0; }
+        const double rs = rsqrt(piv);
+        if (q == 0 && i >= j && i < nb) Lsm[i * lp + j] = i == j ? piv * rs : sij * rs;
+        if (tid == 0) D[j] = rs;
+        const double t = sij * (rs * rs);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int c = q + 4 * m;
+            if (c > j && c <= i && i < nb) S[i * LSP + c] = fma(-t, cj[m], ic[m]);
         }
         __syncthreads();
     }
-    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
-        const int i = idx % nb, j = idx / nb;
-        if (i >= j) Fd[i + (int64_t)j * d.ld] = L[i][j];
-    }
-    if (tid < nb) {   // column tid of inv(L) by forward substitution
-        const int c = tid;
-        for (int i = c; i < nb; ++i) {
-            double v = (i == c) ? 1.0 : 0.0;
-            for (int t = c; t < i; ++t) v -= L[i][t] * Li[t][c];
-            Li[i][c] = v / L[i][i];
-        }
-    }
+    for (int idx = tid; idx < NB * NB; idx += GEMM_THREADS) S[(idx >> 5) * LSP + (idx & 31)] = 0.0;
     __syncthreads();
+    const int c = tid & 31;
+    for (int s = 0; s < nb; ++s) {
+        const double ps = S[s * LSP + c];
+        const double ds = D[s];
+        double lr[8], pr[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            lr[m] = Lsm[(q + 4 * m) * lp + s];
+            pr[m] = S[(q + 4 * m) * LSP + c];
+        }
+        const double f = (c <= s) ? ((c == s ? 1.0 : 0.0) - ps) * ds : 0.0;
+        if (q == 0 && c < nb) X[s * xp + c] = f;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int r = q + 4 * m;
+            if (r > s && r < nb) S[r * LSP + c] = fma(lr[m], f, pr[m]);
+        }
+        __syncthreads();
+    }
+    *bad = b;
+}
+
+// Diagonal step alone, for panel steps with many CTAs (where redoing the
+// block in every CTA would cost more than a launch): one CTA per front
+// factors the block and writes Li as the diagonal block of Y.
+__global__ void __launch_bounds__(GEMM_THREADS) k_diag(const double* __restrict__ F, double* __restrict__ Y,
+                                                       const FrontDesc* __restrict__ desc, WorkList wl, int p,
+                                                       int* __restrict__ status) {
+    __shared__ double S[NB * LSP];
+    __shared__ double Lsm[NB * LSP];
+    __shared__ double X[NB * LSP];
+    __shared__ double D[NB];
+    const FrontDesc d = desc[wl.d_fronts[blockIdx.x]];
+    const int p0 = p * NB, nb = min(NB, d.k - p0);
+    if (nb <= 0) return;
+    bool bad = false;
+    cta_chol_inv(F + d.f_off + p0 + (int64_t)p0 * d.ld, d.ld, nb, S, Lsm, LSP, D, X, LSP, &bad);
+    if (bad && threadIdx.x == 0) atomicExch(status, WRAPD_E_NOT_SPD);
     double* Yp = Y + d.y_off + p0;   // row block p of Y (column-major, ld = k)
-    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
-        const int i = idx % nb, j = idx / nb;
-        Yp[i + (int64_t)(p0 + j) * d.k] = Li[i][j];
+    for (int idx = threadIdx.x; idx < NB * NB; idx += GEMM_THREADS) {
+        const int i = idx & 31, c = idx >> 5;
+        if (i < nb && c < nb) Yp[i + (int64_t)(p0 + c) * d.k] = c <= i ? X[i * LSP + c] : 0.0;
     }
 }
 
-// Items per front: nP panel-row tiles (P <- P Li^T below the diagonal block),
-// then the inverse row-block tiles Y[p, c0:c0+64] <- Li Y[p, c0:c0+64], c0 < p0.
+// The tiles of a panel step after k_diag: nP panel-row tiles (P <- P Li^T),
+// then the inverse row-block tiles Y[p, c0:c0+64] <- Li Y[p, c0:c0+64], with
+// Li read back from Y's diagonal block.
 __global__ void __launch_bounds__(GEMM_THREADS) k_trsm(double* __restrict__ F, double* __restrict__ Y,
                                                        const FrontDesc* __restrict__ desc, WorkList wl,
                                                        const int* __restrict__ nP_of_item, int p) {
@@ -315,23 +350,104 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_trsm(double* __restrict__ F, d
     const int p0 = p * NB, nb = min(NB, d.k - p0), j0 = p0 + nb;
     if (nb <= 0) return;
     const int K4 = (nb + 3) & ~3;
+    const double* Li = Y + d.y_off + p0 + (int64_t)p0 * d.k;   // Li(i, t) at Li[i + t k]
     double acc[4][4][2] = {};
     if (tile < nP) {
-        const int m = d.ld - j0 - tile * TL;
+        const int m = min(d.ld - j0 - tile * TL, TL);
         double* A = F + d.f_off + j0 + tile * TL + (int64_t)p0 * d.ld;
-        load_tile(As, A, 1, d.ld, min(m, TL), nb, K4);
-        load_tile(Bs, Y + d.y_off + p0 + (int64_t)p0 * d.k, 1, d.k, nb, nb, K4);
+        load_tile(As, A, 1, d.ld, m, nb, K4);
+        load_tile(Bs, Li, 1, d.k, nb, nb, K4);
         __syncthreads();
         tile_mma(As, Bs, K4, acc);
-        tile_store(A, 1, d.ld, min(m, TL), nb, EPI_SET, acc);
+        tile_store(A, 1, d.ld, m, nb, EPI_SET, acc);
     } else {
         const int c0 = (tile - nP) * TL;
+        if (c0 >= p0) return;
         double* Yr = Y + d.y_off + p0 + (int64_t)c0 * d.k;   // Y[p0 + t, c0 + j] at Yr[t + j k]
-        load_tile(As, Y + d.y_off + p0 + (int64_t)p0 * d.k, 1, d.k, nb, nb, K4);   // Li(i, t)
-        load_tile(Bs, Yr, d.k, 1, min(p0 - c0, TL), nb, K4);                      // Y_p(t, c0 + j)
+        load_tile(As, Li, 1, d.k, nb, nb, K4);
+        load_tile(Bs, Yr, d.k, 1, min(p0 - c0, TL), nb, K4);
         __syncthreads();
         tile_mma(As, Bs, K4, acc);
         tile_store(Yr, 1, d.k, nb, min(p0 - c0, TL), EPI_SET, acc);
+    }
+}
+
+// Panel steps with few CTAs (the upper levels: a few large fronts, where the
+// step is latency-bound) run as one launch: every CTA first factors the
+// front's NB x NB diagonal block itself (warp 0, registers) and keeps its
+// inverse Li in shared memory, so no separate diagonal launch precedes it.  Items per front: nP
+// panel-row tiles (P <- P Li^T below the diagonal block), then the inverse
+// row-block tiles Y[p, c0:c0+64] <- Li Y[p, c0:c0+64], c0 < p0; a front with
+// neither has one item that only factors.  The front's first item writes Li
+// as the diagonal block of Y.  F's diagonal block is read, never written: the
+// solve and the later steps use only Y, W and the panels below it.
+__global__ void __launch_bounds__(GEMM_THREADS) k_panel(double* __restrict__ F, double* __restrict__ Y,
+                                                        const FrontDesc* __restrict__ desc, WorkList wl,
+                                                        const int* __restrict__ nP_of_item, int p,
+                                                        int* __restrict__ status) {
+    __shared__ __align__(16) double As[TL * SLD];
+    __shared__ __align__(16) double Bs[TL * SLD];
+    __shared__ double S[NB * LSP];
+    __shared__ double D[NB];
+    const int item = find_item(wl.d_prefix, wl.n, blockIdx.x);
+    const FrontDesc d = desc[wl.d_fronts[item]];
+    const int tile = blockIdx.x - wl.d_prefix[item];
+    const int nP = nP_of_item[item];
+    const int p0 = p * NB, nb = min(NB, d.k - p0), j0 = p0 + nb;
+    if (nb <= 0) return;
+    const int K4 = (nb + 3) & ~3;
+    const bool ptile = tile < nP;
+    const int c0 = (tile - nP) * TL;
+    const bool ytile = !ptile && c0 < p0;
+    // The other operand is staged asynchronously while the diagonal block is
+    // factored: the panel rows (A(i, t) = P(i, t)) or the Y row block (B'(j, t)
+    // = Y(p0 + t, c0 + j)).
+    const int tid = threadIdx.x;
+    if (ptile) {
+        const int m = min(d.ld - j0 - tile * TL, TL);
+        const double* A = F + d.f_off + j0 + tile * TL + (int64_t)p0 * d.ld;
+        for (int idx = tid; idx < TL * K4; idx += GEMM_THREADS) {
+            const int i = idx % TL, t = idx / TL;
+            const bool v = i < m && t < nb;
+            cp_async8(As + i * SLD + t, v ? A + i + (int64_t)t * d.ld : A, v);
+        }
+    } else if (ytile) {
+        const int n = min(p0 - c0, TL);
+        const double* Yr = Y + d.y_off + p0 + (int64_t)c0 * d.k;
+        for (int idx = tid; idx < TL * K4; idx += GEMM_THREADS) {
+            const int t = idx % K4, j = idx / K4;
+            const bool v = j < n && t < nb;
+            cp_async8(Bs + j * SLD + t, v ? Yr + t + (int64_t)j * d.k : Yr, v);
+        }
+    }
+    cp_async_commit();
+    // Li lands in the operand slot of the product: B for panel tiles (B'(j, t) =
+    // Li(j, t)), A for inverse row-block tiles (A(i, t) = Li(i, t)); rows 32..63
+    // of that slot hold L meanwhile and are cleared afterwards.
+    double* Ls = ptile ? Bs : As;
+    for (int idx = tid; idx < NB * SLD; idx += GEMM_THREADS) Ls[idx] = 0.0;
+    bool bad = false;
+    cta_chol_inv(F + d.f_off + p0 + (int64_t)p0 * d.ld, d.ld, nb, S, Ls + NB * SLD, SLD, D, Ls, SLD, &bad);
+    if (tile == 0) {
+        if (bad && tid == 0) atomicExch(status, WRAPD_E_NOT_SPD);
+        double* Yp = Y + d.y_off + p0;   // row block p of Y (column-major, ld = k)
+        for (int idx = tid; idx < NB * NB; idx += GEMM_THREADS) {
+            const int i = idx & 31, c = idx >> 5;
+            if (i < nb && c < nb) Yp[i + (int64_t)(p0 + c) * d.k] = Ls[i * SLD + c];
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < NB * SLD; idx += GEMM_THREADS) Ls[NB * SLD + idx] = 0.0;
+    cp_async_wait<0>();
+    __syncthreads();
+    if (!ptile && !ytile) return;
+    double acc[4][4][2] = {};
+    tile_mma(As, Bs, K4, acc);
+    if (ptile) {
+        const int m = min(d.ld - j0 - tile * TL, TL);
+        tile_store(F + d.f_off + j0 + tile * TL + (int64_t)p0 * d.ld, 1, d.ld, m, nb, EPI_SET, acc);
+    } else {
+        tile_store(Y + d.y_off + p0 + (int64_t)c0 * d.k, 1, d.k, nb, min(p0 - c0, TL), EPI_SET, acc);
     }
 }
 
@@ -440,6 +556,8 @@ __device__ __forceinline__ void front_rhs(const double* __restrict__ B, const do
 // partial sums; the last one to arrive adds them in chunk order (deterministic)
 // and writes the band's result, then resets the band counter.
 constexpr int SCH = 256;
+constexpr int SCH_MIN = 32;
+constexpr int kSolveCtas = 8 * 148;   // eight 256-thread CTAs per SM of a B200
 
 __device__ __forceinline__ bool band_arrive(unsigned* counter, int nchunk) {
     __shared__ bool last;
@@ -737,7 +855,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         }
         const int steps = ceil_div(L.kmax, NB);
         for (int p = 0; p < steps; ++p) {
-            std::vector<int> act, cd, ct, nP;
+            std::vector<int> act, ct, nP;
             std::vector<GemmJob> jobs;
             for (int f : fs) {
                 const FrontDesc& d = h_desc_[f];
@@ -747,7 +865,6 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
                 const int m = d.ld - j0;
                 const int bs = (p0 / OB) * OB, be = std::min(d.k, bs + OB);
                 act.push_back(f);
-                cd.push_back(1);
                 nP.push_back(ceil_div(m, TL));
                 ct.push_back(ceil_div(m, TL) + ceil_div(p0, TL));
                 if (j0 < be) {
@@ -760,40 +877,73 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
                     jobs.push_back(GemmJob{f, 1, be, d.k, 0, be, bs, be});
                 }
             }
-            L.diag.push_back(make_list(act, cd, st));
-            std::vector<int> actt, ct2, nP2;
-            for (size_t i = 0; i < act.size(); ++i)
-                if (ct[i] > 0) { actt.push_back(act[i]); ct2.push_back(ct[i]); nP2.push_back(nP[i]); }
-            L.trsm.push_back(make_list(actt, ct2, st));
-            L.trsm_split.push_back(nP2);
+            // every active front gets at least one item (its diagonal block is factored there)
+            int total = 0;
+            for (int& c : ct) { c = std::max(c, 1); total += c; }
+            const bool fused = total <= kFusedPanelCtas;
+            L.fused.push_back(fused ? 1 : 0);
+            if (!fused) {
+                WorkList dl = make_list(act, std::vector<int>(act.size(), 1), st);
+                L.diag.push_back(dl);
+            } else {
+                L.diag.push_back(WorkList{});
+            }
+            L.trsm.push_back(make_list(act, ct, st));
+            L.trsm_split.push_back(nP);
             L.update.push_back(make_jobs(jobs, st));
-            launches_factor += 1 + (L.trsm.back().total ? 1 : 0) + (L.update.back().total ? 1 : 0);
+            launches_factor += (fused ? 0 : 1) + (L.trsm.back().total ? 1 : 0) + (L.update.back().total ? 1 : 0);
         }
         std::vector<int> wg(fs.size());
-        std::vector<SolveItem> fwd, bwd;
-        int fbands = 0, bbands = 0;
         for (size_t q = 0; q < fs.size(); ++q) {
             const FrontDesc& d = h_desc_[fs[q]];
-            const int T = ceil_div(d.k, TL), nW = ceil_div(d.r, TL);
-            wg[q] = nW * T;
-            const int R = d.k + d.r;
-            // forward: row bands; Y bands use columns up to their last row
-            for (int b0 = 0; b0 < R; b0 += TL) {
-                const int cend = b0 < d.k ? std::min(d.k, b0 + TL) : d.k;
-                const int nch = ceil_div(cend, SCH), first = static_cast<int>(fwd.size());
-                for (int c = 0; c < nch; ++c)
-                    fwd.push_back({fs[q], b0, c * SCH, std::min(cend, (c + 1) * SCH), nch, first, fbands});
-                fbands++;
+            wg[q] = ceil_div(d.r, TL) * ceil_div(d.k, TL);
+        }
+        // Solve items with chunks of `sch` (<= SCH) along the streamed dimension.
+        auto fwd_items = [&](int sch, std::vector<SolveItem>& fwd, int& fbands) {
+            fwd.clear();
+            fbands = 0;
+            for (int f : fs) {
+                const FrontDesc& d = h_desc_[f];
+                const int R = d.k + d.r;
+                // forward: row bands; Y bands use columns up to their last row
+                for (int b0 = 0; b0 < R; b0 += TL) {
+                    const int cend = b0 < d.k ? std::min(d.k, b0 + TL) : d.k;
+                    const int nch = ceil_div(cend, sch), first = static_cast<int>(fwd.size());
+                    for (int c = 0; c < nch; ++c)
+                        fwd.push_back({f, b0, c * sch, std::min(cend, (c + 1) * sch), nch, first, fbands});
+                    fbands++;
+                }
             }
-            // backward: column bands over rows [b0, k) of Y, then the W rows; no chunk crosses k
-            for (int b0 = 0; b0 < d.k; b0 += TL) {
-                std::vector<std::pair<int, int>> ch;
-                for (int lo = b0; lo < d.k; lo += SCH) ch.push_back({lo, std::min(d.k, lo + SCH)});
-                for (int lo = d.k; lo < R; lo += SCH) ch.push_back({lo, std::min(R, lo + SCH)});
-                const int nch = static_cast<int>(ch.size()), first = static_cast<int>(bwd.size());
-                for (auto& c : ch) bwd.push_back({fs[q], b0, c.first, c.second, nch, first, bbands});
-                bbands++;
+        };
+        auto bwd_items = [&](int sch, std::vector<SolveItem>& bwd, int& bbands) {
+            bwd.clear();
+            bbands = 0;
+            for (int f : fs) {
+                const FrontDesc& d = h_desc_[f];
+                const int R = d.k + d.r;
+                // backward: column bands over rows [b0, k) of Y, then the W rows; no chunk crosses k
+                for (int b0 = 0; b0 < d.k; b0 += TL) {
+                    std::vector<std::pair<int, int>> ch;
+                    for (int lo = b0; lo < d.k; lo += sch) ch.push_back({lo, std::min(d.k, lo + sch)});
+                    for (int lo = d.k; lo < R; lo += sch) ch.push_back({lo, std::min(R, lo + sch)});
+                    const int nch = static_cast<int>(ch.size()), first = static_cast<int>(bwd.size());
+                    for (auto& c : ch) bwd.push_back({f, b0, c.first, c.second, nch, first, bbands});
+                    bbands++;
+                }
             }
+        };
+        // Chunks as long as possible (fewer partial sums) while the launch still
+        // has kSolveCtas CTAs: the upper levels hold a few large fronts, and
+        // long chunks there leave most SMs idle with each CTA latency-bound.
+        std::vector<SolveItem> fwd, bwd;
+        int fbands = 0, bbands = 0;
+        for (int sch = SCH; ; sch /= 2) {
+            fwd_items(sch, fwd, fbands);
+            if ((int)fwd.size() >= kSolveCtas || sch <= SCH_MIN) break;
+        }
+        for (int sch = SCH; ; sch /= 2) {
+            bwd_items(sch, bwd, bbands);
+            if ((int)bwd.size() >= kSolveCtas || sch <= SCH_MIN) break;
         }
         L.wgemm = make_list(fs, wg, st);
         if (L.wgemm.total) launches_factor++;
@@ -839,14 +989,23 @@ void CholGPU::factor_launches(const double* d_w2, const double* d_Di, int ne, cu
                 k_extend_add<<<L.extend[slot].total, 32 * COLS_PER_CTA, 0, st>>>(d_F_, d_desc_, d_rel_, L.extend[slot], slot);
                 WRAPD_LAUNCH_CHECK();
             }
-        for (size_t p = 0; p < L.diag.size(); ++p) {
-            if (L.diag[p].total) {
-                k_diag<<<L.diag[p].total, 256, 0, st>>>(d_F_, d_Y_, d_desc_, L.diag[p], (int)p, d_status);
-                WRAPD_LAUNCH_CHECK();
-            }
-            if (L.trsm[p].total) {
-                k_trsm<<<L.trsm[p].total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_desc_, L.trsm[p], trsm_nP_[l][p], (int)p);
-                WRAPD_LAUNCH_CHECK();
+        for (size_t p = 0; p < L.trsm.size(); ++p) {
+            if (L.fused[p]) {
+                if (L.trsm[p].total) {
+                    k_panel<<<L.trsm[p].total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_desc_, L.trsm[p],
+                                                                      trsm_nP_[l][p], (int)p, d_status);
+                    WRAPD_LAUNCH_CHECK();
+                }
+            } else {
+                if (L.diag[p].n) {
+                    k_diag<<<L.diag[p].n, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_desc_, L.diag[p], (int)p, d_status);
+                    WRAPD_LAUNCH_CHECK();
+                }
+                if (L.trsm[p].total) {
+                    k_trsm<<<L.trsm[p].total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_desc_, L.trsm[p],
+                                                                     trsm_nP_[l][p], (int)p);
+                    WRAPD_LAUNCH_CHECK();
+                }
             }
             if (L.update[p].total) {
                 k_update<<<L.update[p].total, GEMM_THREADS, GEMM_SMEM, st>>>(d_F_, d_Y_, d_desc_, L.update[p]);

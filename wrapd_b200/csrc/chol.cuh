@@ -99,8 +99,9 @@ private:
         int kmax = 0;
         WorkList all;                    // one CTA per front (gather, diag...)
         std::vector<WorkList> extend;    // per child slot: CTAs over child columns
-        std::vector<WorkList> diag;      // per panel step
-        std::vector<WorkList> trsm;      // per panel step (panel row tiles + Y row-block tiles)
+        std::vector<char> fused;         // per panel step: diagonal block factored inside the panel launch
+        std::vector<WorkList> diag;      // per panel step (steps not fused): one warp per front
+        std::vector<WorkList> trsm;      // per panel step: panel row tiles + Y row-block tiles
         std::vector<JobList> update;     // per panel step: blocked trailing-update jobs (F and Y)
         std::vector<std::vector<int>> trsm_split;  // per step: panel-row tiles per item
         WorkList wgemm;                  // W = L_rs Y tiles
