@@ -224,7 +224,7 @@ __global__ void k_y_identity(double* __restrict__ Y, const FrontDesc* __restrict
     const int f = blockIdx.x;
     if (f >= nfronts) return;
     const FrontDesc d = desc[f];
-    for (int i = threadIdx.x; i < d.k; i += blockDim.x) Y[d.y_off + i + (int64_t)i * d.k] = 1.0;
+    for (int i = threadIdx.x; i < d.k; i += blockDim.x) Y[d.y_off + i + (int64_t)i * d.ldy] = 1.0;
 }
 
 // children slot `slot` of each front in the list: F_s[rel[i], rel[j]] += U_c[i, j], i >= j
@@ -328,10 +328,10 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_diag(const double* __restrict_
     bool bad = false;
     cta_chol_inv(F + d.f_off + p0 + (int64_t)p0 * d.ld, d.ld, nb, S, Lsm, LSP, D, X, LSP, &bad);
     if (bad && threadIdx.x == 0) atomicExch(status, WRAPD_E_NOT_SPD);
-    double* Yp = Y + d.y_off + p0;   // row block p of Y (column-major, ld = k)
+    double* Yp = Y + d.y_off + p0;   // row block p of Y (column-major, ld = ldy)
     for (int idx = threadIdx.x; idx < NB * NB; idx += GEMM_THREADS) {
         const int i = idx & 31, c = idx >> 5;
-        if (i < nb && c < nb) Yp[i + (int64_t)(p0 + c) * d.k] = c <= i ? X[i * LSP + c] : 0.0;
+        if (i < nb && c < nb) Yp[i + (int64_t)(p0 + c) * d.ldy] = c <= i ? X[i * LSP + c] : 0.0;
     }
 }
 
@@ -350,25 +350,25 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_trsm(double* __restrict__ F, d
     const int p0 = p * NB, nb = min(NB, d.k - p0), j0 = p0 + nb;
     if (nb <= 0) return;
     const int K4 = (nb + 3) & ~3;
-    const double* Li = Y + d.y_off + p0 + (int64_t)p0 * d.k;   // Li(i, t) at Li[i + t k]
+    const double* Li = Y + d.y_off + p0 + (int64_t)p0 * d.ldy;   // Li(i, t) at Li[i + t ldy]
     double acc[4][4][2] = {};
     if (tile < nP) {
         const int m = min(d.ld - j0 - tile * TL, TL);
         double* A = F + d.f_off + j0 + tile * TL + (int64_t)p0 * d.ld;
         load_tile(As, A, 1, d.ld, m, nb, K4);
-        load_tile(Bs, Li, 1, d.k, nb, nb, K4);
+        load_tile(Bs, Li, 1, d.ldy, nb, nb, K4);
         __syncthreads();
         tile_mma(As, Bs, K4, acc);
         tile_store(A, 1, d.ld, m, nb, EPI_SET, acc);
     } else {
         const int c0 = (tile - nP) * TL;
         if (c0 >= p0) return;
-        double* Yr = Y + d.y_off + p0 + (int64_t)c0 * d.k;   // Y[p0 + t, c0 + j] at Yr[t + j k]
-        load_tile(As, Li, 1, d.k, nb, nb, K4);
-        load_tile(Bs, Yr, d.k, 1, min(p0 - c0, TL), nb, K4);
+        double* Yr = Y + d.y_off + p0 + (int64_t)c0 * d.ldy;   // Y[p0 + t, c0 + j] at Yr[t + j ldy]
+        load_tile(As, Li, 1, d.ldy, nb, nb, K4);
+        load_tile(Bs, Yr, d.ldy, 1, min(p0 - c0, TL), nb, K4);
         __syncthreads();
         tile_mma(As, Bs, K4, acc);
-        tile_store(Yr, 1, d.k, nb, min(p0 - c0, TL), EPI_SET, acc);
+        tile_store(Yr, 1, d.ldy, nb, min(p0 - c0, TL), EPI_SET, acc);
     }
 }
 
@@ -413,11 +413,11 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_panel(double* __restrict__ F, 
         }
     } else if (ytile) {
         const int n = min(p0 - c0, TL);
-        const double* Yr = Y + d.y_off + p0 + (int64_t)c0 * d.k;
+        const double* Yr = Y + d.y_off + p0 + (int64_t)c0 * d.ldy;
         for (int idx = tid; idx < TL * K4; idx += GEMM_THREADS) {
             const int t = idx % K4, j = idx / K4;
             const bool v = j < n && t < nb;
-            cp_async8(Bs + j * SLD + t, v ? Yr + t + (int64_t)j * d.k : Yr, v);
+            cp_async8(Bs + j * SLD + t, v ? Yr + t + (int64_t)j * d.ldy : Yr, v);
         }
     }
     cp_async_commit();
@@ -430,10 +430,10 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_panel(double* __restrict__ F, 
     cta_chol_inv(F + d.f_off + p0 + (int64_t)p0 * d.ld, d.ld, nb, S, Ls + NB * SLD, SLD, D, Ls, SLD, &bad);
     if (tile == 0) {
         if (bad && tid == 0) atomicExch(status, WRAPD_E_NOT_SPD);
-        double* Yp = Y + d.y_off + p0;   // row block p of Y (column-major, ld = k)
+        double* Yp = Y + d.y_off + p0;   // row block p of Y (column-major, ld = ldy)
         for (int idx = tid; idx < NB * NB; idx += GEMM_THREADS) {
             const int i = idx & 31, c = idx >> 5;
-            if (i < nb && c < nb) Yp[i + (int64_t)(p0 + c) * d.k] = Ls[i * SLD + c];
+            if (i < nb && c < nb) Yp[i + (int64_t)(p0 + c) * d.ldy] = Ls[i * SLD + c];
         }
     }
     __syncthreads();
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_panel(double* __restrict__ F, 
         const int m = min(d.ld - j0 - tile * TL, TL);
         tile_store(F + d.f_off + j0 + tile * TL + (int64_t)p0 * d.ld, 1, d.ld, m, nb, EPI_SET, acc);
     } else {
-        tile_store(Y + d.y_off + p0 + (int64_t)c0 * d.k, 1, d.k, nb, min(p0 - c0, TL), EPI_SET, acc);
+        tile_store(Y + d.y_off + p0 + (int64_t)c0 * d.ldy, 1, d.ldy, nb, min(p0 - c0, TL), EPI_SET, acc);
     }
 }
 
@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_update(double* __restrict__ F,
         gemm_pipelined<true>(A0, d.ld, M, F + d.f_off + c0 + (int64_t)jb.k0 * d.ld, d.ld, N, jb.k1 - jb.k0,
                              gemm_smem, acc);
     else   // B'(j, t) = Y(k0 + t, c0 + j)
-        gemm_pipelined<false>(A0, d.ld, M, Y + d.y_off + jb.k0 + (int64_t)c0 * d.k, d.k, N, jb.k1 - jb.k0,
+        gemm_pipelined<false>(A0, d.ld, M, Y + d.y_off + jb.k0 + (int64_t)c0 * d.ldy, d.ldy, N, jb.k1 - jb.k0,
                               gemm_smem, acc);
     if (jb.kind == 0) {
         // on tiles crossing the diagonal keep only row >= column (global indices)
@@ -499,7 +499,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_update(double* __restrict__ F,
                     C[row + (int64_t)col * d.ld] -= acc[i][j][h];
                 }
     } else {
-        tile_store(Y + d.y_off + r0 + (int64_t)c0 * d.k, 1, d.k, M, N, EPI_SUB, acc);
+        tile_store(Y + d.y_off + r0 + (int64_t)c0 * d.ldy, 1, d.ldy, M, N, EPI_SUB, acc);
     }
 }
 
@@ -518,17 +518,17 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_wgemm(const double* __restrict
     const double* A = F + d.f_off + d.k + r0;   // L_rs(i, t) at A[i + t ld]
     double acc[4][4][2] = {};
     // t over [c0, k): Y(k0 + t, c0 + j) vanishes above the diagonal
-    gemm_pipelined<false>(A + (int64_t)c0 * d.ld, d.ld, M, Y + d.y_off + c0 + (int64_t)c0 * d.k, d.k, N, d.k - c0,
+    gemm_pipelined<false>(A + (int64_t)c0 * d.ld, d.ld, M, Y + d.y_off + c0 + (int64_t)c0 * d.ldy, d.ldy, N, d.k - c0,
                           gemm_smem, acc);
-    tile_store(W + d.w_off + r0 + (int64_t)c0 * d.r, 1, d.r, M, N, EPI_SET, acc);
+    tile_store(W + d.y_off + d.k + r0 + (int64_t)c0 * d.ldy, 1, d.ldy, M, N, EPI_SET, acc);
 }
 
 // ---- solve -----------------------------------------------------------------------
 // Per level, one launch per direction.  Forward: a CTA owns a band of 64 rows of
-// M = [Y; W] ((k + r) x k) and streams all its columns (Y rows only up to the
-// diagonal): rows < k give z_s = Y t_s, rows >= k give u_s = v_s - W t_s.
-// Backward: a CTA owns a band of 64 columns and streams the rows below the
-// diagonal plus all W rows: y_s = Y^T z_s - W^T y_rows.  The right-hand side is
+// the front's M = [Y; W] ((k + r) x k, leading dimension ldy) and a chunk of its
+// columns (Y rows only up to the diagonal): rows < k give z_s = Y t_s, rows >= k
+// give u_s = v_s - W t_s.  Backward: a CTA owns a band of 64 columns and a chunk
+// of the rows below the diagonal and of the W rows: y_s = Y^T z_s - W^T y_rows.  The right-hand side is
 // read from B (a copy of the input), z from Zb, and y written to x, so no CTA
 // reads what another CTA of the same launch writes.
 
@@ -556,8 +556,8 @@ __device__ __forceinline__ void front_rhs(const double* __restrict__ B, const do
 // partial sums; the last one to arrive adds them in chunk order (deterministic)
 // and writes the band's result, then resets the band counter.
 constexpr int SCH = 256;
-constexpr int SCH_MIN = 32;
-constexpr int kSolveCtas = 8 * 148;   // eight 256-thread CTAs per SM of a B200
+constexpr int SCH_MIN = 64;
+constexpr int kSolveCtas = 2 * 148;   // two 256-thread CTAs per SM of a B200
 
 __device__ __forceinline__ bool band_arrive(unsigned* counter, int nchunk) {
     __shared__ bool last;
@@ -573,18 +573,20 @@ __device__ __forceinline__ bool band_arrive(unsigned* counter, int nchunk) {
     return last;
 }
 
+// Forward: lane l of warp w holds rows b0 + 2l and b0 + 2l + 1 of the band (one
+// 16-byte load per column: the block's leading dimension and the band start are
+// even) and takes columns lo + w, lo + w + 8, ...; the eight warps' sums are
+// added in warp order.
 __global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B, double* __restrict__ Zb,
                                                    double* __restrict__ U, const int64_t* __restrict__ inv,
-                                                   const double* __restrict__ Y, const double* __restrict__ W,
-                                                   const FrontDesc* __restrict__ desc, const SolveItem* __restrict__ items,
-                                                   double* __restrict__ P, unsigned* __restrict__ counters) {
+                                                   const double* __restrict__ YW, const FrontDesc* __restrict__ desc,
+                                                   const SolveItem* __restrict__ items, double* __restrict__ P,
+                                                   unsigned* __restrict__ counters) {
     __shared__ double tv[SCH * 3];
-    __shared__ double part[4][TL][3];
+    __shared__ double part[8][TL][3];
     const SolveItem it = items[blockIdx.x];
     const FrontDesc d = desc[it.front];
     const int R = d.k + d.r;
-    const int row = threadIdx.x & (TL - 1), grp = threadIdx.x >> 6;
-    const int i = it.b0 + row;
     const int nc = it.hi - it.lo;
     for (int j = threadIdx.x; j < nc; j += blockDim.x) {
         double v0, v1, v2;
@@ -592,32 +594,36 @@ __global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B,
         tv[3 * j] = v0; tv[3 * j + 1] = v1; tv[3 * j + 2] = v2;
     }
     __syncthreads();
-    const bool wrow = i >= d.k;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    if (i < R) {
-        const int64_t ld = wrow ? d.r : d.k;
-        const double* M = (wrow ? W + d.w_off + (i - d.k) : Y + d.y_off + i) + (int64_t)it.lo * ld;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i0 = it.b0 + 2 * lane;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0;
+    if (i0 < R) {
+        const double* M = YW + d.y_off + i0 + (int64_t)it.lo * d.ldy;
 #pragma unroll 4
-        for (int j = grp; j < nc; j += 4) {
-            const double m = M[(int64_t)j * ld];
-            a0 += m * tv[3 * j]; a1 += m * tv[3 * j + 1]; a2 += m * tv[3 * j + 2];
+        for (int j = warp; j < nc; j += 8) {
+            const double2 m = __ldg(reinterpret_cast<const double2*>(M + (int64_t)j * d.ldy));
+            const double t0 = tv[3 * j], t1 = tv[3 * j + 1], t2 = tv[3 * j + 2];
+            a0 = fma(m.x, t0, a0); a1 = fma(m.x, t1, a1); a2 = fma(m.x, t2, a2);
+            b0 = fma(m.y, t0, b0); b1 = fma(m.y, t1, b1); b2 = fma(m.y, t2, b2);
         }
     }
-    part[grp][row][0] = a0; part[grp][row][1] = a1; part[grp][row][2] = a2;
+    part[warp][2 * lane][0] = a0; part[warp][2 * lane][1] = a1; part[warp][2 * lane][2] = a2;
+    part[warp][2 * lane + 1][0] = b0; part[warp][2 * lane + 1][1] = b1; part[warp][2 * lane + 1][2] = b2;
     __syncthreads();
+    const int row = threadIdx.x;
+    const int i = it.b0 + row;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    if (threadIdx.x < TL) {
-        s0 = ((part[0][row][0] + part[1][row][0]) + part[2][row][0]) + part[3][row][0];
-        s1 = ((part[0][row][1] + part[1][row][1]) + part[2][row][1]) + part[3][row][1];
-        s2 = ((part[0][row][2] + part[1][row][2]) + part[2][row][2]) + part[3][row][2];
+    if (row < TL) {
+#pragma unroll
+        for (int w = 0; w < 8; ++w) { s0 += part[w][row][0]; s1 += part[w][row][1]; s2 += part[w][row][2]; }
     }
     if (it.nchunk > 1) {
-        if (threadIdx.x < TL) {
+        if (row < TL) {
             double* p = P + 3 * ((int64_t)blockIdx.x * TL + row);
             p[0] = s0; p[1] = s1; p[2] = s2;
         }
         if (!band_arrive(counters + it.band, it.nchunk)) return;
-        if (threadIdx.x < TL) {
+        if (row < TL) {
             s0 = s1 = s2 = 0.0;
             for (int q = 0; q < it.nchunk; ++q) {
                 const double* p = P + 3 * ((int64_t)(it.first + q) * TL + row);
@@ -625,8 +631,8 @@ __global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B,
             }
         }
     }
-    if (threadIdx.x < TL && i < R) {
-        if (!wrow) {
+    if (row < TL && i < R) {
+        if (i < d.k) {
             double* o = Zb + 3 * ((int64_t)d.first + i);
             o[0] = s0; o[1] = s1; o[2] = s2;
         } else {
@@ -638,53 +644,89 @@ __global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B,
     }
 }
 
-// Backward: one warp per column of the band, lanes along the rows of the chunk.
+// Backward: a CTA owns a band of 64 columns and a chunk [lo, hi) of the rows
+// (lo even; a chunk may cross row k): the input of row i is z_i for i < k and
+// minus the solution at the front's row i - k for i >= k.  Warp w takes the
+// eight columns b0 + w + 8m; lane l loads rows lo + 2l + 64t and the next one
+// of each as one 16-byte load.  The 8 x 3 lane sums are then added across the
+// warp by a butterfly that halves the values each lane keeps (12, 6, 3) before
+// two plain exchange steps, so the eight columns share 27 shuffles.
 __global__ void __launch_bounds__(256) k_bwd_level(double* __restrict__ x, const double* __restrict__ Zb,
-                                                   const double* __restrict__ Y, const double* __restrict__ W,
-                                                   const int* __restrict__ rows, const FrontDesc* __restrict__ desc,
+                                                   const double* __restrict__ YW, const int* __restrict__ rows,
+                                                   const FrontDesc* __restrict__ desc,
                                                    const SolveItem* __restrict__ items, double* __restrict__ P,
                                                    unsigned* __restrict__ counters) {
-    __shared__ double in[SCH * 3];
+    __shared__ double in[(SCH + 1) * 3];
     __shared__ double res[TL][3];
     const SolveItem it = items[blockIdx.x];
     const FrontDesc d = desc[it.front];
     const int nr = it.hi - it.lo;
     const int nc = min(TL, d.k - it.b0);
-    for (int t = threadIdx.x; t < nr; t += blockDim.x) {
+    for (int t = threadIdx.x; t < nr + 1; t += blockDim.x) {
         const int i = it.lo + t;
-        double v0, v1, v2;
-        if (i < d.k) {
-            const double* z = Zb + 3 * ((int64_t)d.first + i);
-            v0 = z[0]; v1 = z[1]; v2 = z[2];
-        } else {
-            const double* y = x + 3 * (int64_t)rows[d.rows_off + i - d.k];
-            v0 = -y[0]; v1 = -y[1]; v2 = -y[2];
+        double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+        if (t < nr) {
+            if (i < d.k) {
+                const double* z = Zb + 3 * ((int64_t)d.first + i);
+                v0 = z[0]; v1 = z[1]; v2 = z[2];
+            } else {
+                const double* y = x + 3 * (int64_t)rows[d.rows_off + i - d.k];
+                v0 = -y[0]; v1 = -y[1]; v2 = -y[2];
+            }
         }
         in[3 * t] = v0; in[3 * t + 1] = v1; in[3 * t + 2] = v2;
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // the chunk lies entirely in Y rows or entirely in W rows
-    const bool wpart = it.lo >= d.k;
-    const int64_t ld = wpart ? d.r : d.k;
-    const double* base = wpart ? W + d.w_off + (it.lo - d.k) : Y + d.y_off + it.lo;
-    for (int jj = warp; jj < TL; jj += 8) {
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        if (jj < nc) {
-            const double* M = base + (int64_t)(it.b0 + jj) * ld;
-#pragma unroll 4
-            for (int t = lane; t < nr; t += 32) {
-                const double m = M[t];
-                a0 += m * in[3 * t]; a1 += m * in[3 * t + 1]; a2 += m * in[3 * t + 2];
+    double v[24];
+#pragma unroll
+    for (int q = 0; q < 24; ++q) v[q] = 0.0;
+    const double* M0 = YW + d.y_off + it.lo + (int64_t)(it.b0 + warp) * d.ldy;
+    for (int t = 2 * lane; t < nr; t += 64) {
+        const double x0 = in[3 * t], x1 = in[3 * t + 1], x2 = in[3 * t + 2];
+        const double y0 = in[3 * t + 3], y1 = in[3 * t + 4], y2 = in[3 * t + 5];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            if (warp + 8 * m < nc) {
+                const double2 a = __ldg(reinterpret_cast<const double2*>(M0 + (int64_t)(8 * m) * d.ldy + t));
+                v[3 * m] = fma(a.y, y0, fma(a.x, x0, v[3 * m]));
+                v[3 * m + 1] = fma(a.y, y1, fma(a.x, x1, v[3 * m + 1]));
+                v[3 * m + 2] = fma(a.y, y2, fma(a.x, x2, v[3 * m + 2]));
             }
         }
+    }
+    // reduce-scatter: after the offsets 16, 8, 4 lane l keeps the 3 sums of
+    // column slot m = 4 (l>>4 & 1) + 2 (l>>3 & 1) + (l>>2 & 1) over 8 lanes
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            a0 += __shfl_down_sync(0xffffffffu, a0, o);
-            a1 += __shfl_down_sync(0xffffffffu, a1, o);
-            a2 += __shfl_down_sync(0xffffffffu, a2, o);
-        }
-        if (lane == 0) { res[jj][0] = a0; res[jj][1] = a1; res[jj][2] = a2; }
+    for (int q = 0; q < 12; ++q) {
+        const bool hi = lane & 16;
+        const double send = hi ? v[q] : v[q + 12];
+        const double keep = hi ? v[q + 12] : v[q];
+        v[q] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const bool hi = lane & 8;
+        const double send = hi ? v[q] : v[q + 6];
+        const double keep = hi ? v[q + 6] : v[q];
+        v[q] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const bool hi = lane & 4;
+        const double send = hi ? v[q] : v[q + 3];
+        const double keep = hi ? v[q + 3] : v[q];
+        v[q] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        v[q] += __shfl_xor_sync(0xffffffffu, v[q], 2);
+        v[q] += __shfl_xor_sync(0xffffffffu, v[q], 1);
+    }
+    if ((lane & 3) == 0) {
+        const int m = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+        const int jj = warp + 8 * m;
+        res[jj][0] = v[0]; res[jj][1] = v[1]; res[jj][2] = v[2];
     }
     __syncthreads();
     const int j = threadIdx.x;
@@ -776,7 +818,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
     if (S.max_children > 2) throw CudaError(WRAPD_E_INPUT, "assembly tree with more than 2 children");
     h_desc_.resize(nfronts);
     std::vector<int> rows;
-    int64_t roff = 0, woff = 0, ioff = 0;
+    int64_t roff = 0, ioff = 0;
     for (int f = 0; f < nfronts; ++f) {
         const Front& F = S.fronts[f];
         FrontDesc& d = h_desc_[f];
@@ -785,12 +827,11 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         d.rows_off = roff;
         rows.insert(rows.end(), F.rows.begin(), F.rows.end());
         roff += F.nrows();
-        d.w_off = woff; woff += (int64_t)d.r * d.k;
         d.inv_off = ioff; ioff += 2 * ((int64_t)d.k + d.r);
         d.nchild = static_cast<int>(F.children.size());
         d.child0 = d.nchild > 0 ? F.children[0] : -1;
         d.child1 = d.nchild > 1 ? F.children[1] : -1;
-        d.pad = 0;
+        d.ldy = static_cast<int>(yw_ld(d.k, d.r));
     }
     std::vector<int64_t> inv(ioff, -1);
     for (int f = 0; f < nfronts; ++f) {
@@ -809,7 +850,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
     d_Apos_ = upload(A_pos, st);
     d_Aptr_ = upload(A_ptr, st);
     d_Acon_ = upload(A_contrib, st);
-    f_pool_ = S.f_pool; y_pool_ = S.y_pool; u_pool_ = S.u_pool; w_pool_ = woff;
+    f_pool_ = S.f_pool; y_pool_ = S.y_pool; u_pool_ = S.u_pool;
     auto dalloc = [&](size_t count) {
         double* p = nullptr;
         if (cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(double)) != cudaSuccess) {
@@ -822,7 +863,6 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
     };
     d_F_ = dalloc(f_pool_);
     d_Y_ = dalloc(y_pool_);
-    d_W_ = dalloc(w_pool_);
     d_U_ = dalloc(u_pool_);
     d_T_ = dalloc(3 * (size_t)n);
     d_Z_ = dalloc(3 * (size_t)n);
@@ -921,13 +961,10 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
             for (int f : fs) {
                 const FrontDesc& d = h_desc_[f];
                 const int R = d.k + d.r;
-                // backward: column bands over rows [b0, k) of Y, then the W rows; no chunk crosses k
+                // backward: column bands over rows [b0, R) (Y rows below the band, then the W rows)
                 for (int b0 = 0; b0 < d.k; b0 += TL) {
-                    std::vector<std::pair<int, int>> ch;
-                    for (int lo = b0; lo < d.k; lo += sch) ch.push_back({lo, std::min(d.k, lo + sch)});
-                    for (int lo = d.k; lo < R; lo += sch) ch.push_back({lo, std::min(R, lo + sch)});
-                    const int nch = static_cast<int>(ch.size()), first = static_cast<int>(bwd.size());
-                    for (auto& c : ch) bwd.push_back({f, b0, c.first, c.second, nch, first, bbands});
+                    const int nch = ceil_div(R - b0, sch), first = static_cast<int>(bwd.size());
+                    for (int lo = b0; lo < R; lo += sch) bwd.push_back({f, b0, lo, std::min(R, lo + sch), nch, first, bbands});
                     bbands++;
                 }
             }
@@ -1013,7 +1050,7 @@ void CholGPU::factor_launches(const double* d_w2, const double* d_Di, int ne, cu
             }
         }
         if (L.wgemm.total) {
-            k_wgemm<<<L.wgemm.total, GEMM_THREADS, GEMM_SMEM, st>>>(d_F_, d_Y_, d_W_, d_desc_, L.wgemm);
+            k_wgemm<<<L.wgemm.total, GEMM_THREADS, GEMM_SMEM, st>>>(d_F_, d_Y_, d_Y_, d_desc_, L.wgemm);
             WRAPD_LAUNCH_CHECK();
         }
     }
@@ -1041,12 +1078,12 @@ void CholGPU::solve_launches(double* d_x, cudaStream_t st) {
     WRAPD_CUDA(cudaMemcpyAsync(d_T_, d_x, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     for (int l = 0; l < nlevels; ++l) {
         Level& L = levels_[l];
-        k_fwd_level<<<L.n_fwd, 256, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_W_, d_desc_, L.d_fwd, d_P_, d_cnt_);
+        k_fwd_level<<<L.n_fwd, 256, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_desc_, L.d_fwd, d_P_, d_cnt_);
         WRAPD_LAUNCH_CHECK();
     }
     for (int l = nlevels - 1; l >= 0; --l) {
         Level& L = levels_[l];
-        k_bwd_level<<<L.n_bwd, 256, 0, st>>>(d_x, d_Z_, d_Y_, d_W_, d_rows_, d_desc_, L.d_bwd, d_P_, d_cnt_);
+        k_bwd_level<<<L.n_bwd, 256, 0, st>>>(d_x, d_Z_, d_Y_, d_rows_, d_desc_, L.d_bwd, d_P_, d_cnt_);
         WRAPD_LAUNCH_CHECK();
     }
 }

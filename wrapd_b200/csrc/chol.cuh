@@ -9,9 +9,10 @@
 //           factoring, columns 0..k-1 hold the front's panel of L
 //           (L_ss on top, L_rs below) and the trailing r x r block holds the
 //           update matrix that the parent assembles.
-//   Y pool  one k x k lower-triangular block per front: inv(L_ss), built
-//           during the factorization;
-//   W pool  one r x k block per front: W = L_rs inv(L_ss).
+//   Y pool  one (k + r) x k block per front, column-major with an even
+//           leading dimension ldy >= k + r: rows 0..k-1 hold Y = inv(L_ss)
+//           (lower triangular, built during the factorization), rows k..k+r-1
+//           hold W = L_rs inv(L_ss).
 //   With Y and W the solve needs no serial substitution: per front, forward
 //   x_s = Y t_s and u_s = v_s - W t_s, backward y_s = Y^T z_s - W^T y_rows,
 //   i.e. one pass of 2D-tiled matrix-vector products over [Y; W] per level.
@@ -26,8 +27,8 @@ namespace wrapd {
 
 struct FrontDesc {
     int first, k, r, ld;
-    int64_t f_off, y_off, u_off, rows_off, rel_off, w_off, inv_off;
-    int nchild, child0, child1, pad;
+    int64_t f_off, y_off, u_off, rows_off, rel_off, inv_off;
+    int nchild, child0, child1, ldy;   // ldy: leading dimension of the front's [Y; W] block
 };
 
 // A trailing-update job of the blocked factorization: C -= A B'^T over a K range
@@ -120,7 +121,6 @@ private:
     int nA_ = 0;
     double* d_F_ = nullptr;
     double* d_Y_ = nullptr;
-    double* d_W_ = nullptr;
     double* d_U_ = nullptr;      // solve update vectors
     double* d_T_ = nullptr;      // solve: copy of the right-hand side (n x 3)
     double* d_Z_ = nullptr;      // solve: forward result (n x 3)
@@ -128,7 +128,7 @@ private:
     unsigned* d_cnt_ = nullptr;  // solve: per-band arrival counters (zero between launches)
     int64_t solve_parts_ = 0;
     int solve_bands_ = 0;
-    int64_t f_pool_ = 0, y_pool_ = 0, u_pool_ = 0, w_pool_ = 0;
+    int64_t f_pool_ = 0, y_pool_ = 0, u_pool_ = 0;
     cudaGraphExec_t factor_graph_ = nullptr;
     cudaGraphExec_t solve_graph_ = nullptr;
     double* solve_graph_x_ = nullptr;

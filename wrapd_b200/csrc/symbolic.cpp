@@ -150,7 +150,7 @@ Symbolic analyse(int n, const std::vector<int>& adj_ptr, const std::vector<int>&
     for (Front& f : S.fronts) {
         const int64_t k = f.ncols, r = f.nrows(), ld = k + r;
         f.f_off = fo; fo += ld * ld;
-        f.y_off = yo; yo += k * k;
+        f.y_off = yo; yo += yw_ld(k, r) * k;
         f.u_off = uo; uo += r * 3;
         f.rel_off = ro; ro += r;
         S.nnz_L += k * (k + 1) / 2 + k * r;

@@ -25,12 +25,16 @@ struct Front {
     std::vector<int> children;
     int level = 0;
     int64_t f_off = 0;         // F pool: (k + r) x (k + r) column-major, ld = k + r
-    int64_t y_off = 0;         // Y pool: k x k column-major (inverse of the diagonal factor)
+    int64_t y_off = 0;         // Y pool: [inv(L_ss); L_rs inv(L_ss)], (k + r) x k column-major, ld yw_ld(k, r)
     int64_t u_off = 0;         // solve update pool: r x 3
     int64_t rel_off = 0;       // this front's map of `rows` into the parent's front rows
     int ld() const { return ncols + static_cast<int>(rows.size()); }
     int nrows() const { return static_cast<int>(rows.size()); }
 };
+
+// Leading dimension of a front's block in the Y pool: k + r rounded up to even,
+// so every 64-row band of a column starts on a 16-byte boundary.
+inline int64_t yw_ld(int64_t k, int64_t r) { return (k + r + 1) & ~int64_t(1); }
 
 struct Symbolic {
     int n = 0;
