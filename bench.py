@@ -44,7 +44,7 @@ E_YOUNG, NU = 1e5, 0.45
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
@@ -56,7 +56,8 @@ def parse():
 
 # ---- clocks ----------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms during the
+    timed region (one nvidia-smi process in loop mode, stopped afterwards)."""
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
@@ -64,30 +65,33 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.samples = []
-        self._stop = threading.Event()
+        self._p = None
         self._t = None
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                if out.returncode == 0 and out.stdout.strip():
-                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._p.stdout:
+            f = [x.strip() for x in line.strip().split(",")]
+            if len(f) >= 7:
+                self.samples.append(f)
 
     def __enter__(self):
         if shutil.which("nvidia-smi"):
-            self._t = threading.Thread(target=self._run, daemon=True)
+            self._p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                        "--format=csv,noheader,nounits", "-lms", "100"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            time.sleep(0.3)   # first sample before the timed work starts
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        if self._t:
-            self._t.join(timeout=10)
+        if self._p:
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._p.kill()
+            self._t.join(timeout=5)
 
     def summary(self):
         if not self.samples:
@@ -333,6 +337,31 @@ def run_ours(args, rank, world, local, pg):
     lbytes = local_step_bytes(ne, fp)
     achieved = lbytes / (local_ms / K / 1000.0) / 1e9
     traffic = profile_traffic()
+    # Secondary rooflines, from K more iterations with the per-phase device
+    # timeline on (outside the timed region): the factorization against the
+    # FP64 tensor-core peak measured here, the 3-RHS solve against HBM.
+    info = s.info()
+    p0, rp0, cp0 = s.profile(), s.runtime(), s.counters()
+    s.set_profiling(True)
+    s.iterate(K)
+    s.set_profiling(False)
+    p1, rp1, cp1 = s.profile(), s.runtime(), s.counters()
+    n_solves = p1["solve"][1] - p0["solve"][1]
+    solve_ms = (p1["solve"][0] - p0["solve"][0]) / max(1, n_solves)
+    n_fact = cp1["factorizations"] - cp0["factorizations"]
+    fact_ms = (rp1["refactor_ms"] - rp0["refactor_ms"]) / max(1, n_fact)
+    dmma = capi.dmma_peak()
+    solve_bytes = 16.0 * info["nnz_L"]   # [Y; W] read once forward and once backward, FP64
+    solve_gbs = solve_bytes / (solve_ms / 1000.0) / 1e9
+    fact_tflops = info["factor_flops"] / (fact_ms / 1000.0) / 1e12
+    roof_solve = {"kernel": "k_fwd_level + k_bwd_level (3-RHS triangular solve, all levels)", "bound": "hbm",
+                  "achieved": solve_gbs, "peak": peak, "unit": "GB/s", "frac": solve_gbs / peak, "traffic": None,
+                  "peak_source": peak_kind, "bytes_per_solve": solve_bytes, "ms_per_solve": solve_ms}
+    roof_fact = {"kernel": "numeric factorization (k_panel, k_diag, k_trsm, k_update, k_wgemm; FP64 DMMA)",
+                 "bound": "tensor", "achieved": fact_tflops, "peak": dmma, "unit": "TFLOP/s",
+                 "frac": fact_tflops / dmma, "traffic": None,
+                 "peak_source": "FP64 mma.sync m8n8k4 throughput measured on this GPU (wrapd_dmma_peak)",
+                 "flops_per_factorization": info["factor_flops"], "ms_per_factorization": fact_ms}
     # e2e: a fresh solve through the C ABI from host buffers, setup included
     parts = set(args.parts.split(","))
     e2e = None
@@ -401,6 +430,8 @@ def run_ours(args, rank, world, local, pg):
             "roofline": {"kernel": "k_local (fused local step)", "bound": "hbm", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind, "bytes_per_launch": lbytes},
+            "roofline_solve": roof_solve,
+            "roofline_factorization": roof_fact,
             "gpu_launches": int(c1["kernel_launches"] - c0["kernel_launches"]),
             "factorizations": int(c1["factorizations"] - c0["factorizations"]),
             "clocks": clk.summary(),
@@ -413,12 +444,14 @@ def run_ours(args, rank, world, local, pg):
 
 def main():
     args = parse()
+    if args.impl == "reference":
+        # the reference's CPU solver: rank 0 alone runs it (no process group);
+        # the other ranks of a multi-GPU launch exit without work
+        run_reference(args, int(os.environ.get("RANK", "0")))
+        return
     rank, world, local, pg = dist_setup(args.gpus)
     try:
-        if args.impl == "reference":
-            run_reference(args, rank)
-        else:
-            run_ours(args, rank, world, local, pg)
+        run_ours(args, rank, world, local, pg)
     finally:
         if pg is not None:
             pg.barrier()

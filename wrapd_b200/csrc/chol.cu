@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B,
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0;
     if (i0 < R) {
         const double* M = YW + d.y_off + i0 + (int64_t)it.lo * d.ldy;
-#pragma unroll 4
+#pragma unroll 8
         for (int j = warp; j < nc; j += 8) {
             const double2 m = __ldg(reinterpret_cast<const double2*>(M + (int64_t)j * d.ldy));
             const double t0 = tv[3 * j], t1 = tv[3 * j + 1], t2 = tv[3 * j + 2];
