@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 #include <numeric>
@@ -212,6 +213,14 @@ void SolverGPU::initialize() {
     if (cfg.model != MODEL_NH && cfg.reweighting)
         throw CudaError(WRAPD_E_INPUT, "Adaptive weights are only supported for the NH model (use reweighting = 0)");
     auto t0 = std::chrono::steady_clock::now();
+    // host phase timings, printed to stderr with verbose >= 2
+    std::vector<std::pair<const char*, double>> laps;
+    auto tl = t0;
+    auto lap = [&](const char* name) {
+        const auto now = std::chrono::steady_clock::now();
+        laps.emplace_back(name, std::chrono::duration<double, std::milli>(now - tl).count());
+        tl = now;
+    };
     // ---- element geometry (TetElements ctor, src/TetElements.cpp:90-142) ----
     std::vector<double> Di(12 * (size_t)ne), vol(ne), w2(ne);
     for (int e = 0; e < ne; ++e) {
@@ -229,27 +238,51 @@ void SolverGPU::initialize() {
             mid[e] = M.mat;
             w2[e] = cfg.beta_static * mats_[M.mat].wr * vol[e];
         }
+    lap("element geometry");
     // ---- free-vertex graph, nested dissection, symbolic factorization ----
-    std::vector<std::vector<int>> nb(nf);
+    // element incidences per free vertex (free numbering), in element order:
+    // entry e * 4 + a for vertex slot a of element e
+    std::vector<int> vinc_ptr(nf + 1, 0), vinc;
     for (int e = 0; e < ne; ++e)
-        for (int a = 0; a < 4; ++a)
-            for (int b = 0; b < 4; ++b) {
-                const int i = free_of_vert_[tets_[4 * (size_t)e + a]], j = free_of_vert_[tets_[4 * (size_t)e + b]];
-                if (i >= 0 && j >= 0 && i != j) nb[i].push_back(j);
+        for (int a = 0; a < 4; ++a) {
+            const int i = free_of_vert_[tets_[4 * (size_t)e + a]];
+            if (i >= 0) vinc_ptr[i + 1]++;
+        }
+    for (int i = 0; i < nf; ++i) vinc_ptr[i + 1] += vinc_ptr[i];
+    vinc.resize(vinc_ptr[nf]);
+    {
+        std::vector<int> fill(vinc_ptr.begin(), vinc_ptr.end() - 1);
+        for (int e = 0; e < ne; ++e)
+            for (int a = 0; a < 4; ++a) {
+                const int i = free_of_vert_[tets_[4 * (size_t)e + a]];
+                if (i >= 0) vinc[fill[i]++] = e * 4 + a;
             }
-    std::vector<int> ptr(nf + 1, 0), adj;
-    for (int i = 0; i < nf; ++i) {
-        auto& v = nb[i];
-        std::sort(v.begin(), v.end());
-        v.erase(std::unique(v.begin(), v.end()), v.end());
-        ptr[i + 1] = ptr[i] + (int)v.size();
     }
-    adj.reserve(ptr[nf]);
-    for (auto& v : nb) { adj.insert(adj.end(), v.begin(), v.end()); std::vector<int>().swap(v); }
+    // adjacency: the other free vertices of the incident elements, sorted and unique
+    std::vector<int> ptr(nf + 1, 0), adj;
+    {
+        std::vector<int> cand;
+        adj.reserve(16 * (size_t)nf);
+        for (int i = 0; i < nf; ++i) {
+            cand.clear();
+            for (int q = vinc_ptr[i]; q < vinc_ptr[i + 1]; ++q) {
+                const int e = vinc[q] >> 2;
+                for (int b = 0; b < 4; ++b) {
+                    const int j = free_of_vert_[tets_[4 * (size_t)e + b]];
+                    if (j >= 0 && j != i) cand.push_back(j);
+                }
+            }
+            std::sort(cand.begin(), cand.end());
+            cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+            adj.insert(adj.end(), cand.begin(), cand.end());
+            ptr[i + 1] = (int)adj.size();
+        }
+    }
     std::vector<double> coords(3 * (size_t)nf);
     for (int i = 0; i < nv; ++i)
         if (free_of_vert_[i] >= 0)
             for (int c = 0; c < 3; ++c) coords[3 * (size_t)free_of_vert_[i] + c] = rest_[3 * (size_t)i + c];
+    lap("free-vertex graph");
     // one nested dissection per mesh (their graphs are disjoint), then the forest
     std::vector<Symbolic> parts;
     for (const MeshIn& M : meshes_) {
@@ -265,6 +298,7 @@ void SolverGPU::initialize() {
         parts.push_back(analyse(n, p, a, c, cfg.leaf_size > 0 ? cfg.leaf_size : 64));
     }
     Symbolic S = merge(parts);
+    lap("nested dissection + symbolic");
     std::vector<Symbolic>().swap(parts);
     perm_ = S.perm;
     iperm_ = S.iperm;
@@ -282,38 +316,83 @@ void SolverGPU::initialize() {
     std::vector<int> col2front(nf, -1);
     for (size_t f = 0; f < S.fronts.size(); ++f)
         for (int j = 0; j < S.fronts[f].ncols; ++j) col2front[S.fronts[f].first + j] = (int)f;
-    std::vector<std::pair<int64_t, int>> contrib;
-    contrib.reserve(10 * (size_t)ne);
-    for (int e = 0; e < ne; ++e) {
-        const int s[4] = {idx[e].x, idx[e].y, idx[e].z, idx[e].w};
-        for (int a = 0; a < 4; ++a)
-            for (int b = 0; b < 4; ++b) {
-                if (s[a] < 0 || s[b] < 0) continue;
-                // one contribution per unordered pair: the reference's (i <= j) triplet
-                const int fa = free_of_vert_[tets_[4 * (size_t)e + a]], fb = free_of_vert_[tets_[4 * (size_t)e + b]];
-                if (fa > fb || (fa == fb && a != b)) continue;
-                const int r = std::max(s[a], s[b]), c = std::min(s[a], s[b]);
-                const Front& F = S.fronts[col2front[c]];
-                int lr;
-                if (r < F.first + F.ncols) lr = r - F.first;
-                else lr = F.ncols + (int)(std::lower_bound(F.rows.begin(), F.rows.end(), r) - F.rows.begin());
-                const int64_t pos = F.f_off + lr + (int64_t)(c - F.first) * F.ld();
-                contrib.emplace_back(pos, e * 16 + a * 4 + b);
-            }
+    // Entries of A (unordered free-vertex pairs {i, j}, i <= j): entry ids
+    // base[i] + rank of j in {i} + {neighbours > i} (sorted).  Contributions
+    // are counted per entry, then filled in element order (e, a, b), so each
+    // entry sums its contributions in the order of the reference's triplet
+    // list; each entry's pool position is looked up once.
+    std::vector<int64_t> ebase(nf + 1, 0);
+    for (int i = 0; i < nf; ++i) {
+        const int* lo = adj.data() + ptr[i];
+        const int* hi = adj.data() + ptr[i + 1];
+        ebase[i + 1] = ebase[i] + 1 + (hi - std::upper_bound(lo, hi, i));
     }
-    std::sort(contrib.begin(), contrib.end());
-    std::vector<int64_t> A_pos;
-    std::vector<int> A_ptr(1, 0), A_con;
-    A_con.reserve(contrib.size());
-    for (size_t i = 0; i < contrib.size(); ++i) {
-        if (i == 0 || contrib[i].first != contrib[i - 1].first) {
-            if (i > 0) A_ptr.push_back((int)A_con.size());
-            A_pos.push_back(contrib[i].first);
+    const int64_t nentries = ebase[nf];
+    auto entry_of = [&](int fa, int fb) -> int64_t {   // fa <= fb
+        if (fa == fb) return ebase[fa];
+        const int* lo = adj.data() + ptr[fa];
+        const int* hi = adj.data() + ptr[fa + 1];
+        const int* up = std::upper_bound(lo, hi, fa);
+        return ebase[fa] + 1 + (std::lower_bound(up, hi, fb) - up);
+    };
+    // Contributions of entry {i, j}: the elements holding both vertices, in
+    // element order (a merge of the two incidence lists), as e * 16 + a * 4 + b
+    // with a the slot of the lower free index and b the other's.
+    auto entry_contribs = [&](int i, int j, auto&& out) {
+        if (i == j) {
+            for (int q = vinc_ptr[i]; q < vinc_ptr[i + 1]; ++q) out((vinc[q] >> 2) * 16 + (vinc[q] & 3) * 5);
+            return;
         }
-        A_con.push_back(contrib[i].second);
+        int p = vinc_ptr[i], q = vinc_ptr[j];
+        while (p < vinc_ptr[i + 1] && q < vinc_ptr[j + 1]) {
+            const int ep = vinc[p] >> 2, eq = vinc[q] >> 2;
+            if (ep < eq) ++p;
+            else if (eq < ep) ++q;
+            else { out(ep * 16 + (vinc[p] & 3) * 4 + (vinc[q] & 3)); ++p; ++q; }
+        }
+    };
+    std::vector<int> A_ptr(nentries + 1, 0), A_con;
+    for (int i = 0; i < nf; ++i) {
+        int64_t id = ebase[i];
+        int n = 0;
+        entry_contribs(i, i, [&](int) { ++n; });
+        A_ptr[id + 1] = n;
+        for (int q = ptr[i]; q < ptr[i + 1]; ++q) {
+            if (adj[q] <= i) continue;
+            n = 0;
+            entry_contribs(i, adj[q], [&](int) { ++n; });
+            A_ptr[++id + 1] = n;
+        }
     }
-    A_ptr.push_back((int)A_con.size());
-    std::vector<std::pair<int64_t, int>>().swap(contrib);
+    for (int64_t t = 0; t < nentries; ++t) A_ptr[t + 1] += A_ptr[t];
+    A_con.resize(A_ptr[nentries]);
+    for (int i = 0; i < nf; ++i) {
+        int64_t id = ebase[i];
+        int w = A_ptr[id];
+        entry_contribs(i, i, [&](int c) { A_con[w++] = c; });
+        for (int q = ptr[i]; q < ptr[i + 1]; ++q) {
+            if (adj[q] <= i) continue;
+            w = A_ptr[++id];
+            entry_contribs(i, adj[q], [&](int c) { A_con[w++] = c; });
+        }
+    }
+    // pool position of each entry: lower triangle in the dissection order
+    std::vector<int64_t> A_pos(nentries);
+    for (int i = 0; i < nf; ++i) {
+        auto put = [&](int j) {
+            const int si = iperm_[i], sj = iperm_[j];
+            const int r = std::max(si, sj), c = std::min(si, sj);
+            const Front& F = S.fronts[col2front[c]];
+            int lr;
+            if (r < F.first + F.ncols) lr = r - F.first;
+            else lr = F.ncols + (int)(std::lower_bound(F.rows.begin(), F.rows.end(), r) - F.rows.begin());
+            A_pos[entry_of(i, j)] = F.f_off + lr + (int64_t)(c - F.first) * F.ld();
+        };
+        put(i);
+        for (int q = ptr[i]; q < ptr[i + 1]; ++q)
+            if (adj[q] > i) put(adj[q]);
+    }
+    lap("A pattern (scatter map)");
     // gather incidences, element order per free vertex
     std::vector<int> inc_ptr(nf + 1, 0), inc;
     for (int e = 0; e < ne; ++e) {
@@ -329,6 +408,7 @@ void SolverGPU::initialize() {
             for (int a = 0; a < 4; ++a) if (s[a] >= 0) inc[fill[s[a]]++] = e * 4 + a;
         }
     }
+    lap("gather incidences");
     // ---- device state ----
     const size_t TS = sizeof(double);
     d_idx_ = dupload(idx);
@@ -395,7 +475,10 @@ void SolverGPU::initialize() {
         static const double one = 1.0;
         WRAPD_CUDA(cudaMemcpyAsync(d_scal_ + S_ONE, &one, sizeof(double), cudaMemcpyHostToDevice, st_));
     }
+    lap("element state upload");
     chol.build(S, A_pos, A_ptr, A_con, st_);
+    WRAPD_CUDA(cudaStreamSynchronize(st_));
+    lap("factor structures upload");
     // ---- GlobalStepBehavior ctor: midupdate_weights(X_init) and the first factorization ----
     if (cfg.reweighting) {
         mid_candidates(true, cand_mode_now());
@@ -405,8 +488,11 @@ void SolverGPU::initialize() {
     factor();
     m_k_ = 0;
     check_status();
+    lap("first factorization (graph capture + run)");
     initialized_ = true;
     runtime_ms[0] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (cfg.verbose >= 2)
+        for (const auto& l : laps) std::fprintf(stderr, "wrapd setup: %-42s %9.1f ms\n", l.first, l.second);
 }
 
 int SolverGPU::cand_mode_now() const {
