@@ -34,7 +34,6 @@ constexpr int OB = 128;       // outer block: trailing updates beyond it are def
 constexpr int TL = 64;        // output tile of the DMMA kernels
 constexpr int SLD = NB + 4;   // smem row pitch (doubles) for [row][k] operand tiles
 constexpr int GEMM_THREADS = 128;
-constexpr int ROWS_PER_CTA = 128;  // solve row tiles
 constexpr int kFusedPanelCtas = 4 * 148;   // panel steps up to one wave (4 CTAs per SM) run fused
 constexpr int COLS_PER_CTA = 8;    // solve / extend-add column groups (one warp each)
 
@@ -119,13 +118,28 @@ __device__ __forceinline__ void tile_store(double* C, int64_t crs, int64_t ccs, 
 //   i-major S[i * SLD + t] for sources with t contiguous (row blocks of Y).
 // Two stages: chunk c + 1 is in flight while chunk c is multiplied.
 constexpr int TP = TL + 8;            // t-major pitch: 8 mod 16 doubles
-constexpr int TILE_D = TL * SLD;      // doubles per staged operand tile
-static_assert(NB * TP == TILE_D, "both layouts take the same space");
-constexpr int GEMM_SMEM = 2 * 2 * TILE_D * (int)sizeof(double);   // 2 stages x (A, B)
+#ifndef WRAPD_GEMM_KC
+#define WRAPD_GEMM_KC 16
+#endif
+constexpr int KC = WRAPD_GEMM_KC;     // K columns per staged chunk of the trailing-update GEMMs
+constexpr int GSLD = KC + 4;          // i-major pitch (KC + 4 = 4 mod 8 doubles: conflict-free fragment reads)
+constexpr int TILE_D = (KC * TP > TL * GSLD) ? KC * TP : TL * GSLD;   // doubles per staged operand tile
+static_assert(KC % 4 == 0 && KC <= NB, "chunks of whole DMMA k-steps");
+#ifndef WRAPD_GEMM_STAGES
+#define WRAPD_GEMM_STAGES 2
+#endif
+constexpr int GEMM_STAGES = WRAPD_GEMM_STAGES;   // cp.async pipeline depth of the trailing-update GEMMs
+constexpr int GEMM_SMEM = GEMM_STAGES * 2 * TILE_D * (int)sizeof(double);   // stages x (A, B)
 
 __device__ __forceinline__ void cp_async8(double* s, const double* g, bool valid) {
     const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(s));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(g), "r"(valid ? 8 : 0));
+}
+// 16-byte copy of which the first src_bytes (16, 8 or 0) come from global
+// memory and the rest is zero-filled; both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(double* s, const double* g, int src_bytes) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(s));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(g), "r"(src_bytes));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
@@ -133,8 +147,30 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 // Element (i, t), i < rows, t < K, of a source with (TMAJOR) i contiguous:
 // base[i + t * ld], or t contiguous: base[i * ld + t]; zeros up to K4.
+// Where the source is 16-byte aligned and ld even (every front's F and Y
+// blocks have an even leading dimension; a job's row offset may still be odd),
+// element pairs move as one 16-byte copy: along i in the t-major layout, along
+// t in the i-major one.
 template <bool TMAJOR>
 __device__ __forceinline__ void stage_tile(double* S, const double* base, int64_t ld, int rows, int K, int K4) {
+    if ((reinterpret_cast<uintptr_t>(base) & 15) == 0 && (ld & 1) == 0) {
+        if constexpr (TMAJOR) {
+            const int total = (TL / 2) * K4;
+            for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+                const int i = 2 * (idx % (TL / 2)), t = idx / (TL / 2);
+                const int nbytes = (t < K && i < rows) ? (i + 1 < rows ? 16 : 8) : 0;
+                cp_async16(S + t * TP + i, nbytes ? base + i + (int64_t)t * ld : base, nbytes);
+            }
+        } else {
+            const int total = TL * (K4 / 2);
+            for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+                const int t = 2 * (idx % (K4 / 2)), i = idx / (K4 / 2);
+                const int nbytes = (i < rows && t < K) ? (t + 1 < K ? 16 : 8) : 0;
+                cp_async16(S + i * GSLD + t, nbytes ? base + (int64_t)i * ld + t : base, nbytes);
+            }
+        }
+        return;
+    }
     const int total = TL * K4;
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
         if constexpr (TMAJOR) {
@@ -144,7 +180,7 @@ __device__ __forceinline__ void stage_tile(double* S, const double* base, int64_
         } else {
             const int t = idx % K4, i = idx / K4;
             const bool v = i < rows && t < K;
-            cp_async8(S + i * SLD + t, v ? base + (int64_t)i * ld + t : base, v);
+            cp_async8(S + i * GSLD + t, v ? base + (int64_t)i * ld + t : base, v);
         }
     }
 }
@@ -159,12 +195,12 @@ __device__ __forceinline__ void tile_mma2(const double* As, const double* Bs, in
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int row = wm * 32 + i * 8 + r;
-            a[i] = AT ? As[(kk + c) * TP + row] : As[row * SLD + kk + c];
+            a[i] = AT ? As[(kk + c) * TP + row] : As[row * GSLD + kk + c];
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int col = wn * 32 + j * 8 + r;
-            b[j] = BT ? Bs[(kk + c) * TP + col] : Bs[col * SLD + kk + c];
+            b[j] = BT ? Bs[(kk + c) * TP + col] : Bs[col * GSLD + kk + c];
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i)
@@ -178,25 +214,24 @@ __device__ __forceinline__ void tile_mma2(const double* As, const double* Bs, in
 template <bool BT>
 __device__ __forceinline__ void gemm_pipelined(const double* A0, int64_t lda, int M, const double* B0, int64_t ldb,
                                                int N, int K, double* smem, double (&acc)[4][4][2]) {
-    const int nch = (K + NB - 1) / NB;
+    const int nch = (K + KC - 1) / KC;
     auto issue = [&](int c) {
-        const int k0 = c * NB, Kc = min(NB, K - k0), K4 = (Kc + 3) & ~3;
-        double* st = smem + (c & 1) * 2 * TILE_D;
-        stage_tile<true>(st, A0 + (int64_t)k0 * lda, lda, M, Kc, K4);
-        stage_tile<BT>(st + TILE_D, BT ? B0 + (int64_t)k0 * ldb : B0 + k0, ldb, N, Kc, K4);
-        cp_async_commit();
-    };
-    if (nch > 0) issue(0);
-    for (int c = 0; c < nch; ++c) {
-        if (c + 1 < nch) {
-            issue(c + 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
+        if (c < nch) {
+            const int k0 = c * KC, Kc = min(KC, K - k0), K4 = (Kc + 3) & ~3;
+            double* st = smem + (c % GEMM_STAGES) * 2 * TILE_D;
+            stage_tile<true>(st, A0 + (int64_t)k0 * lda, lda, M, Kc, K4);
+            stage_tile<BT>(st + TILE_D, BT ? B0 + (int64_t)k0 * ldb : B0 + k0, ldb, N, Kc, K4);
         }
+        cp_async_commit();   // an empty group past the last chunk keeps the wait count uniform
+    };
+#pragma unroll
+    for (int c = 0; c < GEMM_STAGES - 1; ++c) issue(c);
+    for (int c = 0; c < nch; ++c) {
+        issue(c + GEMM_STAGES - 1);
+        cp_async_wait<GEMM_STAGES - 1>();
         __syncthreads();
-        const int Kc = min(NB, K - c * NB), K4 = (Kc + 3) & ~3;
-        const double* st = smem + (c & 1) * 2 * TILE_D;
+        const int Kc = min(KC, K - c * KC), K4 = (Kc + 3) & ~3;
+        const double* st = smem + (c % GEMM_STAGES) * 2 * TILE_D;
         tile_mma2<true, BT>(st, st + TILE_D, K4, acc);
         __syncthreads();
     }
@@ -464,7 +499,10 @@ __device__ __forceinline__ void job_tile(const GemmJob& jb, int t, int& ti, int&
     ti = Tr;   // not reached for valid t
 }
 
-__global__ void __launch_bounds__(GEMM_THREADS) k_update(double* __restrict__ F, double* __restrict__ Y,
+#ifndef WRAPD_GEMM_MINB
+#define WRAPD_GEMM_MINB 5
+#endif
+__global__ void __launch_bounds__(GEMM_THREADS, WRAPD_GEMM_MINB) k_update(double* __restrict__ F, double* __restrict__ Y,
                                                          const FrontDesc* __restrict__ desc, JobList jl) {
     extern __shared__ __align__(16) double gemm_smem[];
     const int item = find_item(jl.d_prefix, jl.n, blockIdx.x);

@@ -456,6 +456,104 @@ static __global__ void __launch_bounds__(256) k_axpy_dot(int n, double* __restri
     grid_reduce<1>(red, partials, counter, out, base, scale);
 }
 
+// ---- the two-loop recursion in one CTA, for small systems -------------------------
+// With n <= kTwoLoopMaxN the chain of short reductions above is latency-bound:
+// one 1024-thread CTA runs each half of the recursion, q in registers
+// (kTwoLoopPerThread entries per thread), each inner product a block sum in a
+// fixed order.  Same formulas and the same alpha_i, c_i and decrement slots.
+constexpr int kMaxHistory = 32;   // longest global L-BFGS history (lbfgs_m)
+constexpr int kTwoLoopThreads = 1024;
+constexpr int kTwoLoopPerThread = 16;
+constexpr int kTwoLoopMaxN = kTwoLoopThreads * kTwoLoopPerThread;
+struct HistPtrs { const double* p[kMaxHistory]; };
+struct HistRho { double r[kMaxHistory]; };
+
+__device__ __forceinline__ double cta_sum_all(double v, double* sm) {
+    __shared__ double total;
+    const double r = block_sum(v, sm);
+    if (threadIdx.x == 0) total = r;
+    __syncthreads();
+    return total;
+}
+
+// First loop (SplitLBFGS.hpp:152-158): q = g; for i = it-1 .. 0:
+// alpha_i = rho_i <s_i, q>, q -= alpha_i y_i.
+static __global__ void __launch_bounds__(kTwoLoopThreads) k_two_loop_first(int n, double* __restrict__ q,
+                                                                           const double* __restrict__ g,
+                                                                           HistPtrs S, HistPtrs Yh, HistRho rho,
+                                                                           int it, double* __restrict__ alpha) {
+    __shared__ double sm[32];
+    double qr[kTwoLoopPerThread];
+#pragma unroll
+    for (int k = 0; k < kTwoLoopPerThread; ++k) {
+        const int i = threadIdx.x + k * kTwoLoopThreads;
+        qr[k] = i < n ? g[i] : 0.0;
+    }
+    for (int h = it - 1; h >= 0; --h) {
+        double d = 0.0;
+#pragma unroll
+        for (int k = 0; k < kTwoLoopPerThread; ++k) {
+            const int i = threadIdx.x + k * kTwoLoopThreads;
+            if (i < n) d += S.p[h][i] * qr[k];
+        }
+        const double a = rho.r[h] * cta_sum_all(d, sm);
+        if (threadIdx.x == 0) alpha[h] = a;
+#pragma unroll
+        for (int k = 0; k < kTwoLoopPerThread; ++k) {
+            const int i = threadIdx.x + k * kTwoLoopThreads;
+            if (i < n) qr[k] = qr[k] + (-a) * Yh.p[h][i];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kTwoLoopPerThread; ++k) {
+        const int i = threadIdx.x + k * kTwoLoopThreads;
+        if (i < n) q[i] = qr[k];
+    }
+}
+
+// Second loop (SplitLBFGS.hpp:170-173) after q = A^-1 q: for i = 0 .. it-1:
+// c_i = alpha_i - rho_i <y_i, q>, q += c_i s_i; then dir = <g, q>.
+static __global__ void __launch_bounds__(kTwoLoopThreads) k_two_loop_second(int n, double* __restrict__ q,
+                                                                            const double* __restrict__ g,
+                                                                            HistPtrs S, HistPtrs Yh, HistRho rho,
+                                                                            int it, const double* __restrict__ alpha,
+                                                                            double* __restrict__ C,
+                                                                            double* __restrict__ dir) {
+    __shared__ double sm[32];
+    double qr[kTwoLoopPerThread];
+#pragma unroll
+    for (int k = 0; k < kTwoLoopPerThread; ++k) {
+        const int i = threadIdx.x + k * kTwoLoopThreads;
+        qr[k] = i < n ? q[i] : 0.0;
+    }
+    for (int h = 0; h < it; ++h) {
+        double d = 0.0;
+#pragma unroll
+        for (int k = 0; k < kTwoLoopPerThread; ++k) {
+            const int i = threadIdx.x + k * kTwoLoopThreads;
+            if (i < n) d += Yh.p[h][i] * qr[k];
+        }
+        const double c = alpha[h] + (-rho.r[h]) * cta_sum_all(d, sm);
+        if (threadIdx.x == 0) C[h] = c;
+#pragma unroll
+        for (int k = 0; k < kTwoLoopPerThread; ++k) {
+            const int i = threadIdx.x + k * kTwoLoopThreads;
+            if (i < n) qr[k] = qr[k] + c * S.p[h][i];
+        }
+    }
+    double d = 0.0;
+#pragma unroll
+    for (int k = 0; k < kTwoLoopPerThread; ++k) {
+        const int i = threadIdx.x + k * kTwoLoopThreads;
+        if (i < n) {
+            q[i] = qr[k];
+            d += g[i] * qr[k];
+        }
+    }
+    const double dd = cta_sum_all(d, sm);
+    if (threadIdx.x == 0) *dir = dd;
+}
+
 // x <- x - rate * step with step = q, or grad when the decrement dir <= 0
 // (the steepest-descent restart of SplitLBFGS.hpp:189-194); s = x_new - x_old.
 // rate is 1 unless the global line search chose another (SplitLBFGS.hpp:196-206).

@@ -33,7 +33,6 @@ enum : int {
     S_LSV = 88,      // line search: AL value, pe, flips at the trial point
     S_COUNT = 91
 };
-constexpr int kMaxHistory = 32;
 // Dynamic shared memory of k_local<double>: the prox L-BFGS history, 48 doubles
 // per thread of a 128-thread block.
 constexpr int kLocalHistBytes = 48 * 128 * (int)sizeof(double);
@@ -768,8 +767,16 @@ int SolverGPU::lbfgs_minimize() {
     double* C = d_scal_ + S_C;
     for (; global_iter <= max_iters; ++global_iter) {
         const int it = std::min(M, m_k_);
+        const bool small = n <= kTwoLoopMaxN;
+        HistPtrs hs{}, hy{};
+        HistRho hr{};
+        if (small)
+            for (int i = 0; i < it; ++i) { hs.p[i] = s_[i]; hy.p[i] = y_[i]; hr.r[i] = rho_[i]; }
         // first loop (newest to oldest): alpha_i = rho_i <s_i, q>, q -= alpha_i y_i
-        if (it == 0) {
+        if (small) {
+            k_two_loop_first<<<1, kTwoLoopThreads, 0, st_>>>(n, d_q_, d_gcur_, hs, hy, hr, it, A);
+            kernel_launches++;
+        } else if (it == 0) {
             k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, d_gcur_, nullptr, nullptr, 0.0, nullptr, nullptr, 1.0,
                                             d_partials_, d_counter_, d_scal_ + S_DUMMY);
             kernel_launches++;
@@ -791,7 +798,11 @@ int SolverGPU::lbfgs_minimize() {
         n_solve++;
         mark(3);
         // second loop (oldest to newest): c_i = alpha_i - rho_i <y_i, q>, q += c_i s_i; then dir = <grad, q>
-        if (it == 0) {
+        if (small) {
+            k_two_loop_second<<<1, kTwoLoopThreads, 0, st_>>>(n, d_q_, d_gcur_, hs, hy, hr, it, A, C,
+                                                              d_scal_ + S_DIR);
+            kernel_launches++;
+        } else if (it == 0) {
             k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, nullptr, nullptr, 0.0, d_gcur_, nullptr, 1.0,
                                             d_partials_, d_counter_, d_scal_ + S_DIR);
             kernel_launches++;

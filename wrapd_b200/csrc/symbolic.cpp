@@ -148,8 +148,8 @@ Symbolic analyse(int n, const std::vector<int>& adj_ptr, const std::vector<int>&
     // Pools, relative maps, statistics.
     int64_t fo = 0, yo = 0, uo = 0, ro = 0;
     for (Front& f : S.fronts) {
-        const int64_t k = f.ncols, r = f.nrows(), ld = k + r;
-        f.f_off = fo; fo += ld * ld;
+        const int64_t k = f.ncols, r = f.nrows(), ld = k + r, ldp = f.ld();
+        f.f_off = fo; fo += ldp * ldp;
         f.y_off = yo; yo += yw_ld(k, r) * k;
         f.u_off = uo; uo += r * 3;
         f.rel_off = ro; ro += r;

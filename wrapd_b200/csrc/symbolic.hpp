@@ -24,11 +24,13 @@ struct Front {
     int parent = -1;
     std::vector<int> children;
     int level = 0;
-    int64_t f_off = 0;         // F pool: (k + r) x (k + r) column-major, ld = k + r
+    int64_t f_off = 0;         // F pool: (k + r) x (k + r) column-major, leading dimension ld()
     int64_t y_off = 0;         // Y pool: [inv(L_ss); L_rs inv(L_ss)], (k + r) x k column-major, ld yw_ld(k, r)
     int64_t u_off = 0;         // solve update pool: r x 3
     int64_t rel_off = 0;       // this front's map of `rows` into the parent's front rows
-    int ld() const { return ncols + static_cast<int>(rows.size()); }
+    // leading dimension of the front's F-pool block: k + r rounded up to even (the
+    // padding row and column stay zero), so columns start on 16-byte boundaries
+    int ld() const { return (ncols + static_cast<int>(rows.size()) + 1) & ~1; }
     int nrows() const { return static_cast<int>(rows.size()); }
 };
 
