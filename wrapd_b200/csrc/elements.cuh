@@ -164,8 +164,9 @@ static __global__ void __launch_bounds__(128) k_grad(ElemView E, const double* _
     grid_reduce<3>(red, partials, counter, out);
 }
 
-// Free-vertex gather of the element gradients (atomic-free; incidences are in
-// element order, the reference's single-thread accumulation order):
+// Free-vertex gather of the element gradients (atomic-free; each vertex's
+// incidences, in element order, are added by eight lanes in a fixed order, so
+// the sum is deterministic):
 //   grad[i] = sum over (e, a) incident to i of gel(a, :)[e].
 // With gold: d = grad - gold; ystage <- d (if given); out[0] = |d|^2 and
 // out[1] = <sstage, d> (if sstage given).
@@ -174,17 +175,28 @@ static __global__ void __launch_bounds__(256) k_gather(int nf, const int* __rest
                                                 const double* __restrict__ gold, double* __restrict__ ystage,
                                                 const double* __restrict__ sstage, double* partials,
                                                 unsigned* counter, double* out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    // eight lanes per vertex: lane s of the group adds incidences s, s + 8, ...
+    // of the vertex, then the group adds its lanes in a fixed xor tree
+    const int gidx = (blockIdx.x * blockDim.x + threadIdx.x) >> 3, sub = threadIdx.x & 7;
+    const int i = gidx;
     double red[2] = {0.0, 0.0};
+    double g0 = 0.0, g1 = 0.0, g2 = 0.0;
     if (i < nf) {
-        double g0 = 0.0, g1 = 0.0, g2 = 0.0;
-        for (int t = inc_ptr[i]; t < inc_ptr[i + 1]; ++t) {
+        for (int t = inc_ptr[i] + sub; t < inc_ptr[i + 1]; t += 8) {
             const int c = inc[t];
             const int e = c >> 2, a = c & 3;
             g0 += gel[(size_t)(0 + 3 * a) * ne + e];
             g1 += gel[(size_t)(1 + 3 * a) * ne + e];
             g2 += gel[(size_t)(2 + 3 * a) * ne + e];
         }
+    }
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+        g0 += __shfl_xor_sync(0xffffffffu, g0, o);
+        g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+        g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+    }
+    if (i < nf && sub == 0) {
         grad[3 * (size_t)i] = g0; grad[3 * (size_t)i + 1] = g1; grad[3 * (size_t)i + 2] = g2;
         if (gold) {
             const double d0 = g0 - gold[3 * (size_t)i], d1 = g1 - gold[3 * (size_t)i + 1], d2 = g2 - gold[3 * (size_t)i + 2];

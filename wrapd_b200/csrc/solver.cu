@@ -464,7 +464,8 @@ void SolverGPU::initialize() {
         y_[i] = static_cast<double*>(dalloc(vb));
     }
     rho_.assign(cfg.lbfgs_m, 0.0);
-    const size_t nblk = (size_t)blocks_for(std::max(ne, nf), 128) + 2 * kNumSMs + 8;
+    const size_t nblk = (size_t)std::max(blocks_for(std::max(ne, nf), 128), blocks_for(8 * (int64_t)nf, 256)) +
+                        2 * kNumSMs + 8;
     d_partials_ = static_cast<double*>(dalloc(nblk * 5 * sizeof(double)));
     d_counter_ = static_cast<unsigned*>(dalloc(sizeof(unsigned)));
     d_scal_ = static_cast<double*>(dalloc(S_COUNT * sizeof(double)));
@@ -512,7 +513,7 @@ void SolverGPU::grad_at_x(bool write_gel) {
 }
 
 void SolverGPU::gather(double* grad, const double* gold, double* ystage, const double* sstage) {
-    k_gather<<<blocks_for(nf, 256), 256, 0, st_>>>(nf, d_inc_ptr_, d_inc_, d_gel_, ne, grad, gold, ystage, sstage,
+    k_gather<<<blocks_for(8 * (int64_t)nf, 256), 256, 0, st_>>>(nf, d_inc_ptr_, d_inc_, d_gel_, ne, grad, gold, ystage, sstage,
                                                    d_partials_, d_counter_, d_scal_ + S_GATHER);
     WRAPD_LAUNCH_CHECK();
     kernel_launches++;
