@@ -626,19 +626,38 @@ __global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B,
     const FrontDesc d = desc[it.front];
     const int R = d.k + d.r;
     const int nc = it.hi - it.lo;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i0 = it.b0 + 2 * lane;
+    const double* M = YW + d.y_off + i0 + (int64_t)it.lo * d.ldy;
+    // the first eight columns of each warp are in flight while the right-hand
+    // side is gathered
+    constexpr int PRE = 8;
+    double2 pre[PRE];
+#pragma unroll
+    for (int u = 0; u < PRE; ++u) {
+        const int j = warp + 8 * u;
+        pre[u] = (i0 < R && j < nc) ? __ldg(reinterpret_cast<const double2*>(M + (int64_t)j * d.ldy))
+                                    : make_double2(0.0, 0.0);
+    }
     for (int j = threadIdx.x; j < nc; j += blockDim.x) {
         double v0, v1, v2;
         front_rhs(B, U, inv, d, it.lo + j, v0, v1, v2);
         tv[3 * j] = v0; tv[3 * j + 1] = v1; tv[3 * j + 2] = v2;
     }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i0 = it.b0 + 2 * lane;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0;
+#pragma unroll
+    for (int u = 0; u < PRE; ++u) {
+        const int j = warp + 8 * u;
+        if (j < nc) {
+            const double t0 = tv[3 * j], t1 = tv[3 * j + 1], t2 = tv[3 * j + 2];
+            a0 = fma(pre[u].x, t0, a0); a1 = fma(pre[u].x, t1, a1); a2 = fma(pre[u].x, t2, a2);
+            b0 = fma(pre[u].y, t0, b0); b1 = fma(pre[u].y, t1, b1); b2 = fma(pre[u].y, t2, b2);
+        }
+    }
     if (i0 < R) {
-        const double* M = YW + d.y_off + i0 + (int64_t)it.lo * d.ldy;
 #pragma unroll 8
-        for (int j = warp; j < nc; j += 8) {
+        for (int j = warp + 8 * PRE; j < nc; j += 8) {
             const double2 m = __ldg(reinterpret_cast<const double2*>(M + (int64_t)j * d.ldy));
             const double t0 = tv[3 * j], t1 = tv[3 * j + 1], t2 = tv[3 * j + 2];
             a0 = fma(m.x, t0, a0); a1 = fma(m.x, t1, a1); a2 = fma(m.x, t2, a2);
@@ -700,6 +719,16 @@ __global__ void __launch_bounds__(256) k_bwd_level(double* __restrict__ x, const
     const FrontDesc d = desc[it.front];
     const int nr = it.hi - it.lo;
     const int nc = min(TL, d.k - it.b0);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const double* M0 = YW + d.y_off + it.lo + (int64_t)(it.b0 + warp) * d.ldy;
+    // the first row pair of each of the warp's columns is in flight while the
+    // input rows are gathered
+    double2 pre[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+        pre[m] = (2 * lane < nr && warp + 8 * m < nc)
+                     ? __ldg(reinterpret_cast<const double2*>(M0 + (int64_t)(8 * m) * d.ldy + 2 * lane))
+                     : make_double2(0.0, 0.0);
     for (int t = threadIdx.x; t < nr + 1; t += blockDim.x) {
         const int i = it.lo + t;
         double v0 = 0.0, v1 = 0.0, v2 = 0.0;
@@ -715,12 +744,21 @@ __global__ void __launch_bounds__(256) k_bwd_level(double* __restrict__ x, const
         in[3 * t] = v0; in[3 * t + 1] = v1; in[3 * t + 2] = v2;
     }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double v[24];
 #pragma unroll
     for (int q = 0; q < 24; ++q) v[q] = 0.0;
-    const double* M0 = YW + d.y_off + it.lo + (int64_t)(it.b0 + warp) * d.ldy;
-    for (int t = 2 * lane; t < nr; t += 64) {
+    if (2 * lane < nr) {
+        const int t = 2 * lane;
+        const double x0 = in[3 * t], x1 = in[3 * t + 1], x2 = in[3 * t + 2];
+        const double y0 = in[3 * t + 3], y1 = in[3 * t + 4], y2 = in[3 * t + 5];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            v[3 * m] = fma(pre[m].y, y0, fma(pre[m].x, x0, v[3 * m]));
+            v[3 * m + 1] = fma(pre[m].y, y1, fma(pre[m].x, x1, v[3 * m + 1]));
+            v[3 * m + 2] = fma(pre[m].y, y2, fma(pre[m].x, x2, v[3 * m + 2]));
+        }
+    }
+    for (int t = 2 * lane + 64; t < nr; t += 64) {
         const double x0 = in[3 * t], x1 = in[3 * t + 1], x2 = in[3 * t + 2];
         const double y0 = in[3 * t + 3], y1 = in[3 * t + 4], y2 = in[3 * t + 5];
 #pragma unroll
