@@ -14,7 +14,7 @@ the four solver forms on the 8x8x32 bar (the large bar keeps inverted
 elements and does not reach that gap).
 
 Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-        [--precision fp64|mixed] [--parts main,learned,gap,e2e]
+        [--precision fp64|mixed] [--parts main,learned,gap,e2e,batch]
 For N > 1 launch with torchrun: every rank solves its own replica of the bar
 (the path does not shard; replicas only, weak scaling).
 """
@@ -49,7 +49,7 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--parts", default="main,learned,gap,e2e",
+    p.add_argument("--parts", default="main,learned,gap,e2e,batch",
                    help="measurements to run after the main one (main is always run)")
     return p.parse_args()
 
@@ -277,6 +277,48 @@ def time_to_gap(bar, label, device, base, e_star_iters=20000, gap=1e-6):
     return out
 
 
+def batch_throughput(device, K):
+    """64 uneven bars (n_a, n_b in U{4..16}, n_L in U{8..64}, per-bar E and nu),
+    FP32 local / FP64 global, solved as one batch (one handle, one block-diagonal
+    system) and one bar after another (64 handles); device time of K iterations
+    after 2 warm-up ones, setup excluded and reported apart."""
+    from wrapd_b200 import bars
+    from wrapd_b200.solver import Solver
+    triples = bars.batch_bars(64, 0)
+    ne_total = sum(b.n_tets for b, _, _ in triples)
+    base = dict(youngs=E_YOUNG, poisson=NU, lbfgs_m=5, max_iters=100000, precision="mixed", prox_mode=1,
+                device=device)
+
+    def run(group):
+        t0 = time.perf_counter()
+        s = Solver(**base)
+        for b, E, nu in group:
+            s.add_tetmesh(b.rest, b.init, b.tets, pins=b.pins, youngs=E, poisson=nu)
+        s.initialize()
+        s.begin_solve()
+        setup = time.perf_counter() - t0
+        s.iterate(2)
+        r0 = s.runtime()
+        done, _ = s.iterate(K)
+        r1 = s.runtime()
+        ms = sum(r1[k] - r0[k] for k in ("local_ms", "global_ms", "refactor_ms"))
+        s.close()
+        return ms, done, setup
+
+    ms_b, done_b, setup_b = run(triples)
+    ms_s, setup_s, elem_iter_s = 0.0, 0.0, 0
+    for tr in triples:
+        ms, done, setup = run([tr])
+        ms_s += ms
+        setup_s += setup
+        elem_iter_s += tr[0].n_tets * done
+    return {"workload": "64 uneven bars (seeds 0-63), %d tets in total" % ne_total, "iterations": K,
+            "batch_elem_iter_per_s": ne_total * done_b / (ms_b / 1000.0), "batch_ms_per_iter": ms_b / max(1, done_b),
+            "one_by_one_elem_iter_per_s": elem_iter_s / (ms_s / 1000.0),
+            "batch_speedup": (ne_total * done_b / ms_b) / (elem_iter_s / ms_s),
+            "setup_s": {"batch": setup_b, "one_by_one": setup_s}}
+
+
 def profile_traffic():
     """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "k_local_config1.md")
@@ -413,6 +455,9 @@ def run_ours(args, rank, world, local, pg):
     if rank == 0 and "gap" in parts:
         gap = time_to_gap(bars.config0(), "bar 8x8x32 cubes x6 tets (12,288 tets), 180 deg twist, E=1e5 nu=0.45",
                           local, dict(youngs=E_YOUNG, poisson=NU, lbfgs_m=5))
+    batch = None
+    if rank == 0 and "batch" in parts:
+        batch = batch_throughput(local, min(K, 20))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
@@ -431,6 +476,7 @@ def run_ours(args, rank, world, local, pg):
             "inner_iters_per_step": inner / K,
             "learned_fp32_same_bar": learned,
             "time_to_gap": gap,
+            "batch_64_bars": batch,
             "roofline": {"kernel": "k_local (fused local step)", "bound": "hbm", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind, "bytes_per_launch": lbytes},
