@@ -79,6 +79,10 @@ typedef struct wrapd_settings {
     int leaf_size;        /* nested-dissection leaf size for the factorization, 64 */
     int verbose;          /* -p          0 here (1 prints the reference's table) */
     int device;           /* CUDA device ordinal, 0 */
+    int autotune;         /* 0; 1: wrapd_initialize times the candidate tile shapes of the triangular
+                             solve (chunk length per level and direction) and of the factorization's
+                             panel steps (fused or split, by the number of tiles) on this system and
+                             keeps the fastest (see wrapd_get_tuning) */
 } wrapd_settings;
 
 typedef struct wrapd_handle wrapd_handle;
@@ -161,6 +165,13 @@ WRAPD_API int wrapd_get_info(wrapd_handle* h, double out[8]);
  * handle, numeric factorizations, triangular solves (3 RHS each), host
  * synchronisations.  (No reference counterpart: instrumentation.) */
 WRAPD_API int wrapd_get_counters(wrapd_handle* h, int64_t out[4]);
+
+/* The tile shapes in use (no reference counterpart): out[0] = the largest
+ * panel step (in tiles) whose diagonal block is factored inside the tile
+ * launch, out[1] = levels L, then L forward and L backward solve chunk
+ * lengths.  *len receives 2 + 2 L.  Chosen by timing when autotune = 1, by
+ * fixed rules otherwise. */
+WRAPD_API int wrapd_get_tuning(wrapd_handle* h, int* out, int cap, int* len);
 
 /* Per-phase device timeline (no reference counterpart; the reference's
  * MicroTimer splits only local/global/refactor).  wrapd_set_profiling(h, 1)

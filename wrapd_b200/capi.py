@@ -40,7 +40,8 @@ class Settings(ctypes.Structure):
                 ("beta_min", ctypes.c_double), ("beta_max", ctypes.c_double), ("prox_iters", ctypes.c_int),
                 ("youngs", ctypes.c_double), ("lbfgs_m", ctypes.c_int), ("rw_every", ctypes.c_int),
                 ("precision", ctypes.c_int), ("prox_mode", ctypes.c_int), ("leaf_size", ctypes.c_int),
-                ("verbose", ctypes.c_int), ("device", ctypes.c_int)]
+                ("verbose", ctypes.c_int), ("device", ctypes.c_int),
+                ("autotune", ctypes.c_int)]
 
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -69,6 +70,8 @@ SIGNATURES = [
     ("wrapd_get_counters", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
     ("wrapd_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wrapd_get_profile", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_int64)]),
+    ("wrapd_get_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_int)]),
     ("wrapd_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("wrapd_destroy", None, [ctypes.c_void_p]),
     ("wrapd_get_state", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, _dp, ctypes.c_int64,

@@ -65,6 +65,7 @@ int wrapd_settings_default(wrapd_settings* s) {
     s->leaf_size = 64;
     s->verbose = 0;
     s->device = 0;
+    s->autotune = 0;
     return WRAPD_OK;
 }
 
@@ -183,6 +184,15 @@ int wrapd_get_counters(wrapd_handle* h, int64_t out[4]) {
 
 int wrapd_set_profiling(wrapd_handle* h, int on) {
     return guarded(h, [&](wrapd::SolverGPU& s) { s.profiling = on != 0; });
+}
+
+int wrapd_get_tuning(wrapd_handle* h, int* out, int cap, int* len) {
+    if (!len || (cap > 0 && !out)) return WRAPD_E_INPUT;
+    return guarded(h, [&](wrapd::SolverGPU& s) {
+        const std::vector<int> t = s.chol.tuning();
+        *len = (int)t.size();
+        for (int i = 0; i < (int)t.size() && i < cap; ++i) out[i] = t[i];
+    });
 }
 
 int wrapd_get_profile(wrapd_handle* h, double ms[6], int64_t counts[6]) {

@@ -949,8 +949,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
     WRAPD_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
 
     levels_.assign(nlevels, Level());
-    launches_factor = 4;  // memsets + assembly + identity
-    launches_solve = 0;
+    fused_ctas_ = kFusedPanelCtas;
     for (int l = 0; l < nlevels; ++l) {
         Level& L = levels_[l];
         L.fronts_sorted = S.levels[l];
@@ -967,7 +966,6 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
                 cnt[i] = c < 0 ? 0 : ceil_div(h_desc_[c].r, COLS_PER_CTA);
             }
             L.extend.push_back(make_list(fs, cnt, st));
-            if (L.extend.back().total) launches_factor++;
         }
         const int steps = ceil_div(L.kmax, NB);
         for (int p = 0; p < steps; ++p) {
@@ -994,20 +992,12 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
                 }
             }
             // every active front gets at least one item (its diagonal block is factored there)
-            int total = 0;
-            for (int& c : ct) { c = std::max(c, 1); total += c; }
-            const bool fused = total <= kFusedPanelCtas;
-            L.fused.push_back(fused ? 1 : 0);
-            if (!fused) {
-                WorkList dl = make_list(act, std::vector<int>(act.size(), 1), st);
-                L.diag.push_back(dl);
-            } else {
-                L.diag.push_back(WorkList{});
-            }
+            for (int& c : ct) c = std::max(c, 1);
+            // both forms of the step are kept; factor_launches picks one by the step's size
+            L.diag.push_back(make_list(act, std::vector<int>(act.size(), 1), st));
             L.trsm.push_back(make_list(act, ct, st));
             L.trsm_split.push_back(nP);
             L.update.push_back(make_jobs(jobs, st));
-            launches_factor += (fused ? 0 : 1) + (L.trsm.back().total ? 1 : 0) + (L.update.back().total ? 1 : 0);
         }
         std::vector<int> wg(fs.size());
         for (size_t q = 0; q < fs.size(); ++q) {
@@ -1045,28 +1035,30 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
                 }
             }
         };
-        // Chunks as long as possible (fewer partial sums) while the launch still
-        // has kSolveCtas CTAs: the upper levels hold a few large fronts, and
-        // long chunks there leave most SMs idle with each CTA latency-bound.
+        // Candidate chunk lengths SCH, SCH/2, ..., SCH_MIN, all uploaded.  The fixed
+        // rule takes chunks as long as possible (fewer partial sums) while the
+        // launch still has kSolveCtas CTAs: the upper levels of a large system
+        // hold a few large fronts, and long chunks there leave most SMs idle with
+        // each CTA latency-bound.  When not even the shortest chunks fill the GPU
+        // (a small system) the longest are kept.  autotune() may pick another
+        // candidate by timing.
         std::vector<SolveItem> fwd, bwd;
         int fbands = 0, bbands = 0;
-        for (int sch = SCH; ; sch /= 2) {
+        L.cfwd = -1;
+        L.cbwd = -1;
+        for (int sch = SCH, c = 0; sch >= SCH_MIN; sch /= 2, ++c) {
             fwd_items(sch, fwd, fbands);
-            if ((int)fwd.size() >= kSolveCtas || sch <= SCH_MIN) break;
-        }
-        for (int sch = SCH; ; sch /= 2) {
             bwd_items(sch, bwd, bbands);
-            if ((int)bwd.size() >= kSolveCtas || sch <= SCH_MIN) break;
+            L.cand.push_back({sch, upload(fwd, st), static_cast<int>(fwd.size()), upload(bwd, st),
+                              static_cast<int>(bwd.size())});
+            if (L.cfwd < 0 && (int)fwd.size() >= kSolveCtas) L.cfwd = c;
+            if (L.cbwd < 0 && (int)bwd.size() >= kSolveCtas) L.cbwd = c;
+            solve_parts_ = std::max<int64_t>(solve_parts_, std::max<int64_t>(fwd.size(), bwd.size()));
+            solve_bands_ = std::max(solve_bands_, std::max(fbands, bbands));
         }
+        if (L.cfwd < 0) L.cfwd = 0;
+        if (L.cbwd < 0) L.cbwd = 0;
         L.wgemm = make_list(fs, wg, st);
-        if (L.wgemm.total) launches_factor++;
-        L.n_fwd = static_cast<int>(fwd.size());
-        L.n_bwd = static_cast<int>(bwd.size());
-        L.d_fwd = upload(fwd, st);
-        L.d_bwd = upload(bwd, st);
-        solve_parts_ = std::max<int64_t>(solve_parts_, std::max(L.n_fwd, L.n_bwd));
-        solve_bands_ = std::max(solve_bands_, std::max(fbands, bbands));
-        launches_solve += 2;
     }
     trsm_nP_.clear();
     for (auto& L : levels_) {
@@ -1074,6 +1066,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         for (auto& nP : L.trsm_split) w.push_back(nP.empty() ? nullptr : upload(nP, st));
         trsm_nP_.push_back(w);
     }
+    count_launches();
     d_P_ = dalloc(3 * TL * (size_t)solve_parts_);
     {
         unsigned* c = nullptr;
@@ -1084,6 +1077,79 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         WRAPD_CUDA(cudaMemsetAsync(d_cnt_, 0, std::max(1, solve_bands_) * sizeof(unsigned), st));
     }
     WRAPD_CUDA(cudaStreamSynchronize(st));
+}
+
+void CholGPU::count_launches() {
+    launches_factor = 4;   // memsets + assembly + identity
+    launches_solve = 1;    // the right-hand side copy
+    for (const Level& L : levels_) {
+        for (const WorkList& e : L.extend) launches_factor += e.total ? 1 : 0;
+        for (size_t p = 0; p < L.trsm.size(); ++p) {
+            if (L.trsm[p].total > fused_ctas_) launches_factor += L.diag[p].n ? 1 : 0;
+            launches_factor += (L.trsm[p].total ? 1 : 0) + (L.update[p].total ? 1 : 0);
+        }
+        launches_factor += L.wgemm.total ? 1 : 0;
+        launches_solve += 2;
+    }
+}
+
+std::vector<int> CholGPU::tuning() const {
+    std::vector<int> t{fused_ctas_, nlevels};
+    for (const Level& L : levels_) t.push_back(L.cand.empty() ? 0 : L.cand[L.cfwd].sch);
+    for (const Level& L : levels_) t.push_back(L.cand.empty() ? 0 : L.cand[L.cbwd].sch);
+    return t;
+}
+
+// Each candidate is timed by CUDA events on the handle's stream: one level's
+// solve launch (the mean of three after one untimed), or one whole
+// factorization launched directly (after one untimed at the fixed rule).  The
+// solve launches run on scratch vectors; the factorizations on the current
+// weights, so the factor is valid afterwards whatever the choice.
+void CholGPU::autotune(const double* d_w2, const double* d_Di, int ne, cudaStream_t st) {
+    cudaEvent_t e0, e1;
+    WRAPD_CUDA(cudaEventCreate(&e0));
+    WRAPD_CUDA(cudaEventCreate(&e1));
+    auto timed = [&](int reps, auto&& launch) {
+        launch();
+        WRAPD_CUDA(cudaEventRecord(e0, st));
+        for (int r = 0; r < reps; ++r) launch();
+        WRAPD_CUDA(cudaEventRecord(e1, st));
+        WRAPD_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        WRAPD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return ms / reps;
+    };
+    for (Level& L : levels_) {
+        float best_f = 1e30f, best_b = 1e30f;
+        for (int c = 0; c < (int)L.cand.size(); ++c) {
+            const Level::SolveCand& C = L.cand[c];
+            const float tf = timed(3, [&] {
+                k_fwd_level<<<C.nfwd, 256, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_desc_, C.fwd, d_P_, d_cnt_);
+            });
+            const float tb = timed(3, [&] {
+                k_bwd_level<<<C.nbwd, 256, 0, st>>>(d_T_, d_Z_, d_Y_, d_rows_, d_desc_, C.bwd, d_P_, d_cnt_);
+            });
+            WRAPD_LAUNCH_CHECK();
+            if (tf < best_f) { best_f = tf; L.cfwd = c; }
+            if (tb < best_b) { best_b = tb; L.cbwd = c; }
+        }
+    }
+    const int candidates[] = {0, kNumSMs, kFusedPanelCtas, 4 * kFusedPanelCtas, 1 << 30};
+    float best = 1e30f;
+    int pick = kFusedPanelCtas;
+    fused_ctas_ = kFusedPanelCtas;
+    factor_launches(d_w2, d_Di, ne, st);   // untimed first run
+    for (int c : candidates) {
+        fused_ctas_ = c;
+        const float t = timed(1, [&] { factor_launches(d_w2, d_Di, ne, st); });
+        if (t < best) { best = t; pick = c; }
+    }
+    fused_ctas_ = pick;
+    count_launches();
+    WRAPD_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+    WRAPD_CUDA(cudaStreamSynchronize(st));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
 }
 
 void CholGPU::factor_launches(const double* d_w2, const double* d_Di, int ne, cudaStream_t st) {
@@ -1103,7 +1169,7 @@ void CholGPU::factor_launches(const double* d_w2, const double* d_Di, int ne, cu
                 WRAPD_LAUNCH_CHECK();
             }
         for (size_t p = 0; p < L.trsm.size(); ++p) {
-            if (L.fused[p]) {
+            if (L.trsm[p].total <= fused_ctas_) {
                 if (L.trsm[p].total) {
                     k_panel<<<L.trsm[p].total, GEMM_THREADS, 0, st>>>(d_F_, d_Y_, d_desc_, L.trsm[p],
                                                                       trsm_nP_[l][p], (int)p, d_status);
@@ -1154,12 +1220,14 @@ void CholGPU::solve_launches(double* d_x, cudaStream_t st) {
     WRAPD_CUDA(cudaMemcpyAsync(d_T_, d_x, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     for (int l = 0; l < nlevels; ++l) {
         Level& L = levels_[l];
-        k_fwd_level<<<L.n_fwd, 256, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_desc_, L.d_fwd, d_P_, d_cnt_);
+        const Level::SolveCand& c = L.cand[L.cfwd];
+        k_fwd_level<<<c.nfwd, 256, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_desc_, c.fwd, d_P_, d_cnt_);
         WRAPD_LAUNCH_CHECK();
     }
     for (int l = nlevels - 1; l >= 0; --l) {
         Level& L = levels_[l];
-        k_bwd_level<<<L.n_bwd, 256, 0, st>>>(d_x, d_Z_, d_Y_, d_rows_, d_desc_, L.d_bwd, d_P_, d_cnt_);
+        const Level::SolveCand& c = L.cand[L.cbwd];
+        k_bwd_level<<<c.nbwd, 256, 0, st>>>(d_x, d_Z_, d_Y_, d_rows_, d_desc_, c.bwd, d_P_, d_cnt_);
         WRAPD_LAUNCH_CHECK();
     }
 }

@@ -85,6 +85,13 @@ public:
     // In place: x <- A^-1 x for an n x 3 block in the dissection order
     // (graph-replayed per vector pointer).
     void solve(double* d_x, cudaStream_t st);
+    // Times the candidate tile shapes on this system (the solve's chunk length
+    // per level and direction; the largest panel step, in tiles, that factors
+    // its diagonal block inside the tile launch) and keeps the fastest.  Runs
+    // real factorizations of the current weights; call before the first factor.
+    void autotune(const double* d_w2, const double* d_Di, int ne, cudaStream_t st);
+    // [fused panel-step limit, levels, forward chunk per level..., backward chunk per level...]
+    std::vector<int> tuning() const;
 
     int n = 0;
     int* d_status = nullptr;
@@ -100,15 +107,16 @@ private:
         int kmax = 0;
         WorkList all;                    // one CTA per front (gather, diag...)
         std::vector<WorkList> extend;    // per child slot: CTAs over child columns
-        std::vector<char> fused;         // per panel step: diagonal block factored inside the panel launch
-        std::vector<WorkList> diag;      // per panel step (steps not fused): one warp per front
+        std::vector<WorkList> diag;      // per panel step (steps not fused): one CTA per front
         std::vector<WorkList> trsm;      // per panel step: panel row tiles + Y row-block tiles
         std::vector<JobList> update;     // per panel step: blocked trailing-update jobs (F and Y)
         std::vector<std::vector<int>> trsm_split;  // per step: panel-row tiles per item
         WorkList wgemm;                  // W = L_rs Y tiles
-        SolveItem* d_fwd = nullptr;      // solve forward: (64-row band, column chunk) items
-        SolveItem* d_bwd = nullptr;      // solve backward: (64-column band, row chunk) items
-        int n_fwd = 0, n_bwd = 0;
+        // solve items for each candidate chunk length: forward (64-row band,
+        // column chunk) and backward (64-column band, row chunk)
+        struct SolveCand { int sch; SolveItem* fwd; int nfwd; SolveItem* bwd; int nbwd; };
+        std::vector<SolveCand> cand;
+        int cfwd = 0, cbwd = 0;          // the candidates in use
     };
     std::vector<Level> levels_;
     FrontDesc* d_desc_ = nullptr;
@@ -132,6 +140,8 @@ private:
     cudaGraphExec_t factor_graph_ = nullptr;
     cudaGraphExec_t solve_graph_ = nullptr;
     double* solve_graph_x_ = nullptr;
+    int fused_ctas_ = 0;                 // panel steps of at most this many tiles run fused (k_panel)
+    void count_launches();
     void factor_launches(const double* d_w2, const double* d_Di, int ne, cudaStream_t st);
     void solve_launches(double* d_x, cudaStream_t st);
     std::vector<void*> allocs_;

@@ -18,7 +18,7 @@
 // Extensions: -youngs E (the reference hard-codes 1e7 Pa, src/Lame.hpp:38),
 // -out DIR, -lbfgs_m M, -rw_every N, -precision fp64|mixed,
 // -prox lbfgs|newton|net (net: the prox network from -net FILE, a raw
-// little-endian float32 blob), -leaf N, -device D.
+// little-endian float32 blob), -leaf N, -device D, -autotune 0|1.
 #include <algorithm>
 #include <array>
 #include <cerrno>
@@ -186,7 +186,7 @@ void help() {
         " -global_it N (100)  -global_ls 0|1  -kappa K (1)  -model nh|arap  -poisson P (0.45)\n"
         " -beta_static B (1)  -beta_min B (0.1)  -beta_max B (10)  -p 0|1  -s 0|1 (1)\n"
         "Extensions: -youngs E (1e7)  -out DIR (.)  -lbfgs_m M (6)  -rw_every N  -precision fp64|mixed\n"
-        "            -prox lbfgs|newton|net  -net FILE  -leaf N  -device D\n\n");
+        "            -prox lbfgs|newton|net  -net FILE  -leaf N  -device D  -autotune 0|1\n\n");
 }
 
 int run(int argc, char** argv) {
@@ -259,6 +259,7 @@ int run(int argc, char** argv) {
         } else if (a == "-net") net = gets();
         else if (a == "-leaf") s.leaf_size = geti();
         else if (a == "-device") s.device = geti();
+        else if (a == "-autotune") s.autotune = geti();
         else fail("Error: Unrecognized command-line argument: " + a);
     }
     const std::vector<int32_t> pins = load_handles(handles);

@@ -90,6 +90,7 @@ SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
     if (cfg.max_iters < 0 || cfg.global_iters < 1 || cfg.prox_iters < 1) throw CudaError(WRAPD_E_INPUT, "bad iteration limits");
     if (!(cfg.poisson > -1.0 && cfg.poisson < 0.5) || !(cfg.youngs > 0.0)) throw CudaError(WRAPD_E_INPUT, "bad material");
     if (cfg.precision != 0 && cfg.precision != 1) throw CudaError(WRAPD_E_INPUT, "precision must be 0 or 1");
+    if (cfg.autotune != 0 && cfg.autotune != 1) throw CudaError(WRAPD_E_INPUT, "autotune must be 0 or 1");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) throw CudaError(WRAPD_E_CUDA, "no CUDA device");
     if (cfg.device < 0 || cfg.device >= ndev) throw CudaError(WRAPD_E_INPUT, "bad device ordinal");
@@ -484,6 +485,10 @@ void SolverGPU::initialize() {
         mid_candidates(true, cand_mode_now());
         count_++;
         apply_weights();
+    }
+    if (cfg.autotune) {
+        chol.autotune(d_w2_, d_Di_, ne, st_);
+        lap("autotune (solve chunks, panel steps)");
     }
     factor();
     m_k_ = 0;

@@ -145,6 +145,17 @@ class Solver:
         self._h.check(self._h.lib.wrapd_get_counters(self._h.h, v))
         return dict(zip(["kernel_launches", "factorizations", "solves", "host_syncs"], list(v)))
 
+    def tuning(self) -> dict:
+        """Tile shapes in use (wrapd_get_tuning): the fused panel-step limit and
+        the solve chunk length per level and direction."""
+        n = ctypes.c_int(0)
+        self._h.check(self._h.lib.wrapd_get_tuning(self._h.h, None, 0, ctypes.byref(n)))
+        out = (ctypes.c_int * n.value)()
+        self._h.check(self._h.lib.wrapd_get_tuning(self._h.h, out, n.value, ctypes.byref(n)))
+        v = list(out)
+        L = v[1]
+        return {"fused_panel_ctas": v[0], "levels": L, "solve_chunk_fwd": v[2:2 + L], "solve_chunk_bwd": v[2 + L:]}
+
     def set_prox_net(self, blob):
         """Install the prox network for prox_mode 2 (an FP32 blob, capi.NET_BLOB floats)."""
         b = np.ascontiguousarray(blob, dtype=np.float32).ravel()
