@@ -4,6 +4,7 @@ few ADMM iterations through the C ABI.
     python -m wrapd_b200.profile_case [--grid 32 32 64] [--iters 2]
         [--precision fp64|mixed] [--prox-mode 0|1|2]
     python -m wrapd_b200.profile_case --bar config4 --rw-every 20 --warmup 2 --iters 20 --report
+    python -m wrapd_b200.profile_case --net 1000000
 
 The default 32x32x64 bar holds ~0.2 GB of element state (larger than the
 126 MB L2) and ~1.5 GB on the device in total, so a profiler capture of one
@@ -11,7 +12,9 @@ launch stays small.  ``--bar config1|config4`` takes the 786,432-tet or the
 3,932,160-tet bar instead.  ``--report`` prints one JSON line: device memory
 held by the solver (cudaMemGetInfo before create minus after initialize),
 setup time, and per-iteration local/global/refactor milliseconds over the
-``--iters`` iterations that follow ``--warmup`` ones.
+``--iters`` iterations that follow ``--warmup`` ones.  ``--net N`` instead
+runs the prox network's kernels on N seeded synthetic samples: one training
+epoch (batch 4096) from the shipped blob, then one inference pass.
 """
 from __future__ import annotations
 
@@ -39,7 +42,23 @@ def main(argv=None):
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--prox-mode", type=int, default=0)
     ap.add_argument("--report", action="store_true")
+    ap.add_argument("--net", type=int, default=0)
     a = ap.parse_args(argv)
+    if a.net:
+        import numpy as np
+        rng = np.random.default_rng(0)
+        mu, lam = prox_net.lame(1e5, 0.45)
+        sig = np.sort(rng.uniform(0.5, 1.5, (a.net, 3)), axis=1)[:, ::-1].copy()
+        wov = 10.0 ** rng.uniform(3.0, 6.0, a.net)
+        X = np.column_stack([sig, np.log(wov / mu), np.full(a.net, np.log(mu / lam))]).astype(np.float32)
+        T = (sig + 0.01 * rng.standard_normal(sig.shape)).astype(np.float32)
+        tr = prox_net.Trainer(prox_net.load_default())
+        tr.set_data(X, T)
+        losses = tr.train(epochs=1, batch=4096, lr=1e-4, lr_end=1e-5, seed=1)
+        out = prox_net.predict(tr.blob(), sig, wov, mu, lam)
+        tr.close()
+        print(f"net samples {a.net} loss {losses[0]:.3e} predicted {out.shape[0]} finite {bool(np.isfinite(out).all())}")
+        return
     if a.bar == "config1":
         bar = bars.config1()
     elif a.bar == "config4":
