@@ -453,8 +453,15 @@ def run_ours(args, rank, world, local, pg):
         s3.close()
     gap = None
     if rank == 0 and "gap" in parts:
-        gap = time_to_gap(bars.config0(), "bar 8x8x32 cubes x6 tets (12,288 tets), 180 deg twist, E=1e5 nu=0.45",
-                          local, dict(youngs=E_YOUNG, poisson=NU, lbfgs_m=5))
+        # the 8x8x32 bar, and a 786,432-tet bar with the same 180 deg twist (no
+        # bend): config 1's bent bar keeps inverted elements and its energy does
+        # not settle to a 1e-6 gap
+        base = dict(youngs=E_YOUNG, poisson=NU, lbfgs_m=5)
+        gap = {"bar_8x8x32": time_to_gap(bars.config0(), "bar 8x8x32 cubes x6 tets (12,288 tets), 180 deg twist, "
+                                         "E=1e5 nu=0.45", local, base),
+               "bar_32x32x128": time_to_gap(bars.make_bar(32, 32, 128, twist_deg=180.0, noise=0.02, seed=0),
+                                            "bar 32x32x128 cubes x6 tets (786,432 tets), 180 deg twist, E=1e5 "
+                                            "nu=0.45", local, base, e_star_iters=4000)}
     batch = None
     if rank == 0 and "batch" in parts:
         batch = batch_throughput(local, min(K, 20))
