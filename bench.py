@@ -9,9 +9,10 @@ Metric: ADMM element-iterations per second (elements x iterations / seconds),
 the throughput behind the time-to-energy-gap metric; `local_elems_per_s` adds
 the local step alone.  Inputs are far larger than L2 (the element state is
 ~0.7 GB), so no L2 flush is needed between steps.  The same line carries the
-learned/FP32 form on the same bar and the time to relative energy gap 1e-6 of
-the four solver forms on the 8x8x32 bar (the large bar keeps inverted
-elements and does not reach that gap).
+learned/FP32 form on the same bar, the time to relative energy gap 1e-6 of the
+four solver forms on the 8x8x32 bar and on a 786,432-tet bar with a 180 deg
+twist (the bent bar above keeps inverted elements and does not reach that gap),
+and 64 uneven bars solved as one batch and one by one.
 
 Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
         [--precision fp64|mixed] [--parts main,learned,gap,e2e,batch]
