@@ -276,7 +276,24 @@ __global__ void k_extend_add(double* __restrict__ F, const FrontDesc* __restrict
     const int* rc = rel + dc.rel_off;
     const double* Uc = F + dc.f_off + dc.k + (int64_t)(dc.k + j) * dc.ld;
     double* Fs = F + ds.f_off + (int64_t)rc[j] * ds.ld;
-    for (int i = j + lane; i < dc.r; i += 32) Fs[rc[i]] += Uc[i];
+    // Uc and Fs live in one pool, so the loads are batched by hand ahead of the
+    // stores (rel maps a column's rows to distinct parent rows)
+    constexpr int U = 4;
+    for (int i0 = j + lane; i0 < dc.r; i0 += 32 * U) {
+        double u[U], f[U];
+        int ri[U];
+#pragma unroll
+        for (int q = 0; q < U; ++q) {
+            const int i = i0 + 32 * q;
+            ri[q] = i < dc.r ? rc[i] : 0;
+            u[q] = i < dc.r ? Uc[i] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < U; ++q) f[q] = (i0 + 32 * q < dc.r) ? Fs[ri[q]] : 0.0;
+#pragma unroll
+        for (int q = 0; q < U; ++q)
+            if (i0 + 32 * q < dc.r) Fs[ri[q]] = f[q] + u[q];
+    }
 }
 
 // ---- panel factorization -------------------------------------------------------
@@ -957,8 +974,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
                          [&](int a, int b) { return h_desc_[a].k > h_desc_[b].k; });
         const auto& fs = L.fronts_sorted;
         L.kmax = fs.empty() ? 0 : h_desc_[fs[0]].k;
-        std::vector<int> one(fs.size(), 1), cnt(fs.size());
-        L.all = make_list(fs, one, st);
+        std::vector<int> cnt(fs.size());
         for (int slot = 0; slot < 2; ++slot) {
             for (size_t i = 0; i < fs.size(); ++i) {
                 const FrontDesc& d = h_desc_[fs[i]];

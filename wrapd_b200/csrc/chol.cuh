@@ -105,7 +105,6 @@ private:
     struct Level {
         std::vector<int> fronts_sorted;   // by k descending
         int kmax = 0;
-        WorkList all;                    // one CTA per front (gather, diag...)
         std::vector<WorkList> extend;    // per child slot: CTAs over child columns
         std::vector<WorkList> diag;      // per panel step (steps not fused): one CTA per front
         std::vector<WorkList> trsm;      // per panel step: panel row tiles + Y row-block tiles

@@ -169,17 +169,19 @@ static __global__ void __launch_bounds__(128) k_grad(ElemView E, const double* _
 // the sum is deterministic):
 //   grad[i] = sum over (e, a) incident to i of gel(a, :)[e].
 // With gold: d = grad - gold; ystage <- d (if given); out[0] = |d|^2 and
-// out[1] = <sstage, d> (if sstage given).
+// out[1] = <sstage, d> (if sstage given).  With x: out[2] = |x - xs|^2 (the
+// x error of AlgorithmData, at the point the gradient was taken).
 static __global__ void __launch_bounds__(256) k_gather(int nf, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
                                                 const double* __restrict__ gel, int ne, double* __restrict__ grad,
                                                 const double* __restrict__ gold, double* __restrict__ ystage,
-                                                const double* __restrict__ sstage, double* partials,
+                                                const double* __restrict__ sstage, const double* __restrict__ x,
+                                                const double* __restrict__ xs, double* partials,
                                                 unsigned* counter, double* out) {
     // eight lanes per vertex: lane s of the group adds incidences s, s + 8, ...
     // of the vertex, then the group adds its lanes in a fixed xor tree
     const int gidx = (blockIdx.x * blockDim.x + threadIdx.x) >> 3, sub = threadIdx.x & 7;
     const int i = gidx;
-    double red[2] = {0.0, 0.0};
+    double red[3] = {0.0, 0.0, 0.0};
     double g0 = 0.0, g1 = 0.0, g2 = 0.0;
     if (i < nf) {
         for (int t = inc_ptr[i] + sub; t < inc_ptr[i + 1]; t += 8) {
@@ -204,8 +206,13 @@ static __global__ void __launch_bounds__(256) k_gather(int nf, const int* __rest
             red[0] = d0 * d0 + d1 * d1 + d2 * d2;
             if (sstage) red[1] = sstage[3 * (size_t)i] * d0 + sstage[3 * (size_t)i + 1] * d1 + sstage[3 * (size_t)i + 2] * d2;
         }
+        if (x) {
+            const double e0 = x[3 * (size_t)i] - xs[3 * (size_t)i], e1 = x[3 * (size_t)i + 1] - xs[3 * (size_t)i + 1],
+                         e2 = x[3 * (size_t)i + 2] - xs[3 * (size_t)i + 2];
+            red[2] = e0 * e0 + e1 * e1 + e2 * e2;
+        }
     }
-    grid_reduce<2>(red, partials, counter, out);
+    grid_reduce<3>(red, partials, counter, out);
 }
 
 // ---- local step ---------------------------------------------------------------

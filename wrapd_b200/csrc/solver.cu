@@ -18,7 +18,7 @@ namespace {
 // Slots of the device scalar block (one pinned download per sync point).
 enum : int {
     S_GRAD = 0,      // value, pe, flips
-    S_GATHER = 4,    // |grad - gold|^2, <s, y>
+    S_GATHER = 4,    // |grad - gold|^2, <s, y>, |x - x_soln|^2
     S_LOCAL = 8,     // bef, aft, pe, negative stretches, prox iterations
     S_INIT = 13,     // polar potential energy after initialize_dual_vars
     S_RATIO = 14,    // max weight ratio
@@ -96,7 +96,8 @@ SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
     if (cfg.device < 0 || cfg.device >= ndev) throw CudaError(WRAPD_E_INPUT, "bad device ordinal");
     WRAPD_CUDA(cudaSetDevice(cfg.device));
     WRAPD_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
-    for (auto& e : ev_) WRAPD_CUDA(cudaEventCreate(&e));
+    for (auto& set : evs_)
+        for (auto& e : set) WRAPD_CUDA(cudaEventCreate(&e));
     WRAPD_CUDA(cudaMallocHost(&h_scal_, S_COUNT * sizeof(double)));
     WRAPD_CUDA(cudaFuncSetAttribute(k_local<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLocalHistBytes));
     WRAPD_CUDA(cudaFuncSetAttribute(k_local_unaware<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -122,7 +123,8 @@ SolverGPU::~SolverGPU() {
     for (cudaEvent_t e : event_pool_) cudaEventDestroy(e);
     for (void* p : allocs_) cudaFree(p);
     if (d_net_img_) cudaFree(d_net_img_);
-    for (auto& e : ev_) if (e) cudaEventDestroy(e);
+    for (auto& set : evs_)
+        for (auto& e : set) if (e) cudaEventDestroy(e);
     if (h_scal_) cudaFreeHost(h_scal_);
     if (st_) cudaStreamDestroy(st_);
 }
@@ -517,9 +519,10 @@ void SolverGPU::grad_at_x(bool write_gel) {
                       d_counter_, d_scal_ + S_GRAD);
 }
 
-void SolverGPU::gather(double* grad, const double* gold, double* ystage, const double* sstage) {
+void SolverGPU::gather(double* grad, const double* gold, double* ystage, const double* sstage, bool xerr) {
     k_gather<<<blocks_for(8 * (int64_t)nf, 256), 256, 0, st_>>>(nf, d_inc_ptr_, d_inc_, d_gel_, ne, grad, gold, ystage, sstage,
-                                                   d_partials_, d_counter_, d_scal_ + S_GATHER);
+                                                   xerr ? d_x_ : nullptr, d_xsoln_, d_partials_, d_counter_,
+                                                   d_scal_ + S_GATHER);
     WRAPD_LAUNCH_CHECK();
     kernel_launches++;
 }
@@ -683,6 +686,7 @@ void SolverGPU::begin_solve() {
     if (!initialized_) throw CudaError(WRAPD_E_STATE, "begin_solve before initialize");
     auto t0 = std::chrono::steady_clock::now();
     logs_ = Logs();
+    pend_ = PendingTiming{};
     iter = 0;
     converged_ = false;
     fp64_phase_ = false;
@@ -838,7 +842,7 @@ int SolverGPU::lbfgs_minimize() {
         mark(2);
         // gradient at the new x; y = grad_new - grad
         grad_at_x(true);
-        gather(d_gnew_, d_gcur_, d_ystage_, d_sstage_);
+        gather(d_gnew_, d_gcur_, d_ystage_, d_sstage_, true);
         mark(1);
         sync_read();
         const double dir = h_scal_[S_DIR];
@@ -882,6 +886,7 @@ int SolverGPU::iterate(int n, bool* conv) {
     int done = 0;
     *conv = converged_;
     while (done < n && iter < cfg.max_iters && !converged_) {
+        cudaEvent_t* ev_ = evs_[iter & 1];
         WRAPD_CUDA(cudaEventRecord(ev_[0], st_));
         mark(5);
         double dal = 0.0, obj_bef = 0.0, obj_aft = 0.0, prox_it = 0.0;
@@ -895,9 +900,10 @@ int SolverGPU::iterate(int n, bool* conv) {
             // ---- global step: RotAwareGS::global_step (src/GlobalStepBehavior.hpp:246-258) ----
             if (m_k_ == 0) WRAPD_CUDA(cudaMemsetAsync(d_gold_, 0, 3 * (size_t)nf * sizeof(double), st_));
             grad_at_x(true);
-            gather(d_gcur_, d_gold_, nullptr, nullptr);
+            gather(d_gcur_, d_gold_, nullptr, nullptr, true);
             mark(1);
             sync_read();
+            settle_timing(false);   // the previous iteration's events are behind this synchronisation
             const double bef = h_scal_[S_LOCAL], aft = h_scal_[S_LOCAL + 1], pe = h_scal_[S_LOCAL + 2];
             prox_it = h_scal_[S_LOCAL + 4];
             if (h_scal_[S_LOCAL + 3] > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
@@ -943,15 +949,20 @@ int SolverGPU::iterate(int n, bool* conv) {
             }
         }
         WRAPD_CUDA(cudaEventRecord(ev_[3], st_));
-        x_error_launch();   // outside the timed region, as the reference logs it
-        sync_read();
-        profile_flush();
+        // The x error of the final x: the rotation-aware step's last gradient
+        // gather computed it (outside the timed phases, as the reference logs it);
+        // the rotation-unaware step computes it here.
+        if (!cfg.rot_aware) {
+            x_error_launch();
+            sync_read();
+        }
+        const double xerr2 = cfg.rot_aware ? h_scal_[S_GATHER + 2] : h_scal_[S_XERR];
+        if (profiling) {
+            sync_read();
+            profile_flush();
+        }
         if (rw) check_status();
-        float ml = 0.f, mg = 0.f, mr = 0.f;
-        WRAPD_CUDA(cudaEventElapsedTime(&ml, ev_[0], ev_[1]));
-        WRAPD_CUDA(cudaEventElapsedTime(&mg, ev_[1], ev_[2]));
-        WRAPD_CUDA(cudaEventElapsedTime(&mr, ev_[2], ev_[3]));
-        runtime_ms[1] += ml; runtime_ms[2] += mg; runtime_ms[3] += mr; runtime_ms[5] += its;
+        runtime_ms[5] += its;
         // ---- AlgorithmData::update_per_iter_* (src/AlgorithmData.cpp:66-83) ----
         const int k = iter;
         logs_.reweighted.push_back(rw ? 1 : 0);
@@ -961,8 +972,11 @@ int SolverGPU::iterate(int n, bool* conv) {
         logs_.prox_iters.push_back(prox_it / double(ne));
         logs_.objectives.push_back(pe_x);
         logs_.flips.push_back(flips);
-        logs_.acc_time_s.push_back((runtime_ms[1] + runtime_ms[2] + runtime_ms[3]) / 1000.0);
-        const double xe = std::sqrt(h_scal_[S_XERR]) / init_xerr_;
+        // phase times: read once a later synchronisation has passed the events
+        logs_.acc_time_s.push_back(0.0);
+        pend_ = PendingTiming{true, k, ev_};
+        if (!cfg.rot_aware || profiling || rw) settle_timing(false);
+        const double xe = std::sqrt(xerr2) / init_xerr_;
         logs_.x_errors.push_back(xe);
         iter = k + 1;
         done++;
@@ -974,8 +988,24 @@ int SolverGPU::iterate(int n, bool* conv) {
         if ((logs_.flips[k + 1] == 0 && logs_.flips[k] == 0 && res < cfg.tol) || (have_soln_ && xe < 1.e-4))
             converged_ = true;
     }
+    settle_timing(true);
     *conv = converged_;
     return done;
+}
+
+// Adds a finished iteration's phase times (CUDA events) to the runtime and its
+// accumulated-time log entry.  wait = false: a host synchronisation of the
+// stream has already passed the events.
+void SolverGPU::settle_timing(bool wait) {
+    if (!pend_.on) return;
+    if (wait) WRAPD_CUDA(cudaEventSynchronize(pend_.ev[3]));
+    float ml = 0.f, mg = 0.f, mr = 0.f;
+    WRAPD_CUDA(cudaEventElapsedTime(&ml, pend_.ev[0], pend_.ev[1]));
+    WRAPD_CUDA(cudaEventElapsedTime(&mg, pend_.ev[1], pend_.ev[2]));
+    WRAPD_CUDA(cudaEventElapsedTime(&mr, pend_.ev[2], pend_.ev[3]));
+    runtime_ms[1] += ml; runtime_ms[2] += mg; runtime_ms[3] += mr;
+    logs_.acc_time_s[pend_.k + 1] = (runtime_ms[1] + runtime_ms[2] + runtime_ms[3]) / 1000.0;
+    pend_.on = false;
 }
 
 void SolverGPU::positions(double* out) {

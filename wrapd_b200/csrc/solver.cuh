@@ -78,7 +78,7 @@ private:
     size_t event_next_ = 0;
     void check_status();
     void grad_at_x(bool write_gel);
-    void gather(double* grad, const double* gold, double* ystage, const double* sstage);
+    void gather(double* grad, const double* gold, double* ystage, const double* sstage, bool xerr = false);
     void local_step_unaware(int cand_mode, bool fp32_compute);
     void global_step_unaware();
     void local_step(int cand_mode, bool fp32_compute);
@@ -107,7 +107,12 @@ private:
     Material* d_mats_ = nullptr;
     // device
     cudaStream_t st_ = nullptr;
-    cudaEvent_t ev_[4] = {};
+    // phase events of two consecutive iterations (local, global, reweight): an
+    // iteration's times are read once a later host synchronisation has passed them
+    cudaEvent_t evs_[2][4] = {};
+    struct PendingTiming { bool on = false; int k = 0; cudaEvent_t* ev = nullptr; };
+    PendingTiming pend_;
+    void settle_timing(bool wait);
     std::vector<void*> allocs_;
     int4* d_idx_ = nullptr;
     double *d_Di_ = nullptr, *d_vol_ = nullptr, *d_w2_ = nullptr, *d_w2c_ = nullptr;
