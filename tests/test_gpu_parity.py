@@ -6,7 +6,7 @@ Tolerances (FP64 mode):
   * the prox: it stops when |dx| < 1e-8 (src/TetElements.hpp:40-42), so its
     output is defined to ~1e-9 and a last-ulp difference can move the stop by
     one iteration: stretches within 5e-8, iteration counts equal in >= 97%;
-  * full solves: final positions within 1e-8 of max |x|,
+  * full solves: final positions within 1e-8 of max |x| (the FP64 parity bar),
     energy trajectory within 1e-8 relative, identical iteration counts.
 Mixed mode (FP32 element math): final positions within 1e-5 of max |x|.
 """
