@@ -160,7 +160,7 @@ def run_reference(args, rank):
     if not os.path.exists(po.QUASI_REF):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/quasi_ref not built (no reference sources)"}))
         return
-    bar = bars.config1()
+    bar = bars.bar_32x32x128_bent()
     # a bounded sample: the reference's own setup (AMD ordering + first
     # SimplicialLDLT factorization of 138k unknowns) already takes minutes, and
     # each of its iterations about 2 s, so at most 10 iterations are timed
@@ -183,7 +183,7 @@ def run_reference(args, rank):
                    "solver": "reference quasi (Eigen SimplicialLDLT), -rw 0, L-BFGS history 6",
                    "timed": f"ADMM iterations {W}..{W + K - 1} from the reference's accumulated_time_s"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"config-1 bar, {W + K} ADMM iterations, last {K} timed; setup "
+                         "sample": f"the bent 32x32x128 bar, {W + K} ADMM iterations, last {K} timed; setup "
                                    f"{r['runtime']['setup_ms'] / 1000:.1f} s untimed; wall {wall:.1f} s"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -322,7 +322,7 @@ def batch_throughput(device, K):
 
 def profile_traffic():
     """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_local_config1.md")
+    path = os.path.join(ROOT, "profiles", "k_local_32x32x128.md")
     if not os.path.exists(path):
         return None
     m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
@@ -331,7 +331,7 @@ def profile_traffic():
 
 def profile_fp64_pipe():
     """FP64 pipe utilisation of the local step from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_local_config1.md")
+    path = os.path.join(ROOT, "profiles", "k_local_32x32x128.md")
     if not os.path.exists(path):
         return None
     m = re.search(r"FP64 pipe active \(sm__pipe_fp64_cycles_active\) \| ([0-9.]+) %", open(path).read())
@@ -353,7 +353,7 @@ def run_ours(args, rank, world, local, pg):
     import torch
 
     torch.cuda.set_device(local)
-    bar = bars.config1(seed=rank)
+    bar = bars.bar_32x32x128_bent(seed=rank)
     settings = dict(youngs=E_YOUNG, poisson=NU, lbfgs_m=5, rw_every=10, max_iters=100000,
                     precision=args.precision, device=local)
     s = Solver(**settings)
@@ -464,10 +464,10 @@ def run_ours(args, rank, world, local, pg):
     gap = None
     if rank == 0 and "gap" in parts:
         # the 8x8x32 bar, and a 786,432-tet bar with the same 180 deg twist (no
-        # bend): config 1's bent bar keeps inverted elements and its energy does
+        # bend): the bent bar keeps inverted elements and its energy does
         # not settle to a 1e-6 gap
         base = dict(youngs=E_YOUNG, poisson=NU, lbfgs_m=5)
-        gap = {"bar_8x8x32": time_to_gap(bars.config0(), "bar 8x8x32 cubes x6 tets (12,288 tets), 180 deg twist, "
+        gap = {"bar_8x8x32": time_to_gap(bars.bar_8x8x32(), "bar 8x8x32 cubes x6 tets (12,288 tets), 180 deg twist, "
                                          "E=1e5 nu=0.45", local, base),
                "bar_32x32x128": time_to_gap(bars.make_bar(32, 32, 128, twist_deg=180.0, noise=0.02, seed=0),
                                             "bar 32x32x128 cubes x6 tets (786,432 tets), 180 deg twist, E=1e5 "
@@ -500,7 +500,7 @@ def run_ours(args, rank, world, local, pg):
                          "fp64_pipe_active_ncu": profile_fp64_pipe(),
                          "note": "FP64-arithmetic-bound (Jacobi SVD + L-BFGS prox per element); the HBM "
                                  "fraction is low by design, the FP64 pipe share comes from the ncu capture "
-                                 "in profiles/k_local_config1.md"},
+                                 "in profiles/k_local_32x32x128.md"},
             "roofline_solve": roof_solve,
             "roofline_factorization": roof_fact,
             "gpu_launches": int(c1["kernel_launches"] - c0["kernel_launches"]),

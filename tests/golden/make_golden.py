@@ -11,7 +11,7 @@ Outputs (all seeded, reproducible):
                     the candidate-stiffness eigenvalue, on random and edge inputs
   tiny_step.npz     one setup + local step + gradient of TetElements on a small bar
   solve_small.npz   full reference solves of small bars (default and rw_delay 5)
-  solve_config0.npz the reference solve of the 8x8x32 bar (E = 1e5, nu = 0.45)
+  solve_bar_8x8x32.npz the reference solve of the 8x8x32 bar (E = 1e5, nu = 0.45)
   solve_modes.npz   reference solves of a small bar with -ra 0, -model arap -rw 0
                     and -model arap -rw 0 -ra 0
   solve_gls.npz     the reference solve of a strongly twisted small bar with
@@ -133,9 +133,9 @@ def solves():
                     f"{tag}_ls_dal": r["ls_delta_al"], f"{tag}_gs_dal": r["gs_delta_al"]})
     np.savez_compressed(os.path.join(HERE, "solve_small.npz"), rest=small.rest, init=small.init,
                         tets=small.tets, pins=small.pins, **out)
-    c0 = bars.config0()
+    c0 = bars.bar_8x8x32()
     r = ref_solve(c0, 500)
-    np.savez_compressed(os.path.join(HERE, "solve_config0.npz"), objectives=r["objectives"],
+    np.savez_compressed(os.path.join(HERE, "solve_bar_8x8x32.npz"), objectives=r["objectives"],
                         inner=r["inner_iters"], reweighted=r["reweighted"], x=r["x"],
                         ls_dal=r["ls_delta_al"], gs_dal=r["gs_delta_al"])
 

@@ -21,7 +21,7 @@ def _lib(lib_built):
 
 
 def _solve(autotune, iters=500):
-    bar = bars.config0()
+    bar = bars.bar_8x8x32()
     s = Solver(youngs=E_YOUNG, poisson=NU, max_iters=iters, autotune=autotune)
     s.add_tetmesh(bar.rest, bar.init, bar.tets)
     s.set_pins(bar.pins)
@@ -31,7 +31,7 @@ def _solve(autotune, iters=500):
 
 
 def test_autotuned_solve_matches_reference(golden):
-    g = golden("solve_config0.npz")
+    g = golden("solve_bar_8x8x32.npz")
     X, d, t, info = _solve(1)
     assert len(d.objectives) == len(g["objectives"])
     np.testing.assert_array_equal(d.inner_iters, g["inner"])

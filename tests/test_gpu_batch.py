@@ -72,7 +72,7 @@ def test_batch_of_materials_matches_oracle_with_element_materials():
 
 
 def test_batch_of_one_equals_single_mesh_path():
-    b = bars.config0()
+    b = bars.bar_8x8x32()
     X1, d1, _ = _solve_batch([b], iters=30)
     s = Solver(youngs=E_YOUNG, poisson=NU, lbfgs_m=5, max_iters=30)
     s.add_tetmesh(b.rest, b.init, b.tets)

@@ -162,24 +162,24 @@ def test_solve_small_bars_match_reference(golden):
         _compare_solve(s, g[f"{tag}_objectives"], g[f"{tag}_inner"], g[f"{tag}_reweighted"], g[f"{tag}_x"], 1e-8)
 
 
-def test_solve_config0_matches_reference(golden):
-    g = golden("solve_config0.npz")
-    s = make_solver(bars.config0(), max_iters=500)
+def test_solve_bar_8x8x32_matches_reference(golden):
+    g = golden("solve_bar_8x8x32.npz")
+    s = make_solver(bars.bar_8x8x32(), max_iters=500)
     _compare_solve(s, g["objectives"], g["inner"], g["reweighted"], g["x"], 1e-8)
 
 
-def test_solve_config0_mixed_precision(golden):
-    g = golden("solve_config0.npz")
-    s = make_solver(bars.config0(), max_iters=500, precision=1)
+def test_solve_bar_8x8x32_mixed_precision(golden):
+    g = golden("solve_bar_8x8x32.npz")
+    s = make_solver(bars.bar_8x8x32(), max_iters=500, precision=1)
     X = s.solve()
     assert rel_max(X, g["x"]) < 1e-5
     assert s.log("objectives")[-1] == pytest.approx(g["objectives"][-1], rel=1e-6)
 
 
-def test_solve_config0_newton_prox(golden):
+def test_solve_bar_8x8x32_newton_prox(golden):
     """prox_mode 1 (Newton) reaches the reference's solution to its convergence level."""
-    g = golden("solve_config0.npz")
-    s = make_solver(bars.config0(), max_iters=500, prox_mode=1)
+    g = golden("solve_bar_8x8x32.npz")
+    s = make_solver(bars.bar_8x8x32(), max_iters=500, prox_mode=1)
     X = s.solve()
     assert rel_max(X, g["x"]) < 1e-6
     assert s.log("objectives")[-1] == pytest.approx(g["objectives"][-1], rel=1e-9)
@@ -248,12 +248,12 @@ def test_nan_input_reports_an_error_and_the_context_survives():
 # ---- full-size properties (786,432 tets) ---------------------------------------------
 @pytest.fixture(scope="module")
 def big():
-    bar = bars.config1()
+    bar = bars.bar_32x32x128_bent()
     s = make_solver(bar, lbfgs_m=5, rw_every=10)
     return bar, s
 
 
-def test_config1_solve_A_residual(big):
+def test_large_bar_solve_A_residual(big):
     """A (A^-1 b) = b for the 138,303-unknown weighted Laplacian, A built on the host."""
     import scipy.sparse as sp
     bar, s = big
@@ -278,7 +278,7 @@ def test_config1_solve_A_residual(big):
     assert np.abs(r).max() / np.abs(b).max() < 1e-9
 
 
-def test_config1_gradient_matches_oracle(big):
+def test_large_bar_gradient_matches_oracle(big):
     """The global gradient at full size for seeded dual variables (at the initial
     state Z = sym(F), U = 0 the gradient vanishes, so Z and U are perturbed)."""
     bar, s = big
@@ -296,7 +296,7 @@ def test_config1_gradient_matches_oracle(big):
     assert rel_max(g, go) < 1e-10
 
 
-def test_config1_iterations_decrease_energy(big):
+def test_large_bar_iterations_decrease_energy(big):
     bar, s = big
     s.begin_solve()
     done, _ = s.iterate(12)

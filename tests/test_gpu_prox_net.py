@@ -92,7 +92,7 @@ def test_trained_network_cuts_newton_iterations_on_large_bar():
     Newton from the identity; both reach the same stretches."""
     blob = prox_net.load_default()
     mu, lam = prox_net.lame(E_YOUNG, NU)
-    bar = bars.config1()
+    bar = bars.bar_32x32x128_bent()
     s = Solver(youngs=E_YOUNG, poisson=NU, lbfgs_m=5, rw_every=10, prox_mode=1, max_iters=12)
     s.add_tetmesh(bar.rest, bar.init, bar.tets)
     s.set_pins(bar.pins)
@@ -115,7 +115,7 @@ def test_solver_with_network_matches_newton_solver():
     """prox_mode 2 (Newton from the better of the network and the last
     stretches) against prox_mode 1 on the 8 x 8 x 32 bar: the same prox
     solutions to 1e-12, so the same solve."""
-    bar = bars.config0()
+    bar = bars.bar_8x8x32()
     res = {}
     for mode in (1, 2):
         s = Solver(youngs=E_YOUNG, poisson=NU, lbfgs_m=5, prox_mode=mode, max_iters=120)

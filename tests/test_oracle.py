@@ -103,9 +103,9 @@ def test_solve_small_bars_match_reference(golden):
                      tol_x=1e-9, tol_obj=1e-9)
 
 
-def test_solve_config0_matches_reference(golden):
-    g = golden("solve_config0.npz")
-    b = bars.config0()
+def test_solve_bar_8x8x32_matches_reference(golden):
+    g = golden("solve_bar_8x8x32.npz")
+    b = bars.bar_8x8x32()
     o = po.Oracle(b.rest, b.init, b.tets, b.pins, youngs=E_YOUNG, poisson=NU, max_iters=500)
     _check_solve(o, g["objectives"], g["inner"], g["reweighted"], g["x"], tol_x=1e-9, tol_obj=1e-9)
 

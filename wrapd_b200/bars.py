@@ -139,17 +139,17 @@ def make_bar(n_a: int, n_b: int, n_L: int, *, twist_deg: float = 180.0,
 
 
 # The bar workloads, by the sizes they are quoted at.
-def config0(seed: int = 0) -> Bar:
+def bar_8x8x32(seed: int = 0) -> Bar:
     """8x8x32 cubes (12,288 tets, 2,673 verts), 180 deg twist, noise 0.02 h."""
     return make_bar(8, 8, 32, twist_deg=180.0, noise=0.02, seed=seed)
 
 
-def config1(seed: int = 0) -> Bar:
+def bar_32x32x128_bent(seed: int = 0) -> Bar:
     """32x32x128 cubes (786,432 tets, 140,481 verts), 360 deg twist + 90 deg bend, noise 0.01 h."""
     return make_bar(32, 32, 128, twist_deg=360.0, bend_deg=90.0, noise=0.01, seed=seed)
 
 
-def config4(seed: int = 0) -> Bar:
+def bar_64x64x160(seed: int = 0) -> Bar:
     """64x64x160 cubes (3,932,160 tets, 680,225 verts), 720 deg twist, noise 0.005 h."""
     return make_bar(64, 64, 160, twist_deg=720.0, noise=0.005, seed=seed)
 

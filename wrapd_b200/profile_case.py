@@ -3,12 +3,12 @@ few ADMM iterations through the C ABI.
 
     python -m wrapd_b200.profile_case [--grid 32 32 64] [--iters 2]
         [--precision fp64|mixed] [--prox-mode 0|1|2]
-    python -m wrapd_b200.profile_case --bar config4 --rw-every 20 --warmup 2 --iters 20 --report
+    python -m wrapd_b200.profile_case --bar 64x64x160 --rw-every 20 --warmup 2 --iters 20 --report
     python -m wrapd_b200.profile_case --net 1000000
 
 The default 32x32x64 bar holds ~0.2 GB of element state (larger than the
 126 MB L2) and ~1.5 GB on the device in total, so a profiler capture of one
-launch stays small.  ``--bar config1|config4`` takes the 786,432-tet or the
+launch stays small.  ``--bar 32x32x128-bent|64x64x160`` takes the 786,432-tet or the
 3,932,160-tet bar instead.  ``--report`` prints one JSON line: device memory
 held by the solver (cudaMemGetInfo before create minus after initialize),
 setup time, and per-iteration local/global/refactor milliseconds over the
@@ -35,7 +35,7 @@ def device_free_bytes() -> int:
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--grid", type=int, nargs=3, default=[32, 32, 64])
-    ap.add_argument("--bar", choices=["grid", "config1", "config4"], default="grid")
+    ap.add_argument("--bar", choices=["grid", "32x32x128-bent", "64x64x160"], default="grid")
     ap.add_argument("--iters", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=0)
     ap.add_argument("--rw-every", type=int, default=10)
@@ -59,10 +59,10 @@ def main(argv=None):
         tr.close()
         print(f"net samples {a.net} loss {losses[0]:.3e} predicted {out.shape[0]} finite {bool(np.isfinite(out).all())}")
         return
-    if a.bar == "config1":
-        bar = bars.config1()
-    elif a.bar == "config4":
-        bar = bars.config4()
+    if a.bar == "32x32x128-bent":
+        bar = bars.bar_32x32x128_bent()
+    elif a.bar == "64x64x160":
+        bar = bars.bar_64x64x160()
     else:
         na, nb, nl = a.grid
         bar = bars.make_bar(na, nb, nl, twist_deg=360.0 * nl / 128.0, bend_deg=90.0 * nl / 128.0, noise=0.01,

@@ -156,7 +156,7 @@ def prox_inputs(solver):
     return sig, w2 / vol, slast
 
 
-def _config2_run(seed: int):
+def _harvest_run(seed: int):
     """Twist angle and Poisson ratio of one harvesting run (seeded)."""
     u = bars.uniform01(0x5EED0000 + seed, 2)
     return 540.0 * float(u[0]), 0.3 + 0.19 * float(u[1])
@@ -171,7 +171,7 @@ def harvest(runs: int = 200, seed0: int = 1000, every: int = 4, per_snapshot: in
     Xs, Ts = [], []
     for r in range(runs):
         seed = seed0 + r
-        twist, nu = _config2_run(seed)
+        twist, nu = _harvest_run(seed)
         mu, lam = lame(youngs, nu)
         bar = bars.make_bar(8, 8, 32, twist_deg=twist, bend_deg=0.0, noise=0.02, seed=seed)
         s = Solver(youngs=youngs, poisson=nu, lbfgs_m=5, max_iters=max_iters, prox_mode=1)
