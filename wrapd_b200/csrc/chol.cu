@@ -87,10 +87,8 @@ __device__ __forceinline__ void tile_mma(const double* As, const double* Bs, int
     }
 }
 
-enum { EPI_SUB = 0, EPI_SUB_LOWER = 1, EPI_SET = 2 };
-
-// C[row*crs + col*ccs] (op)= acc for row < M, col < N.
-__device__ __forceinline__ void tile_store(double* C, int64_t crs, int64_t ccs, int M, int N, int mode,
+// C[row*crs + col*ccs] = acc for row < M, col < N.
+__device__ __forceinline__ void tile_store(double* C, int64_t crs, int64_t ccs, int M, int N,
                                            const double (&acc)[4][4][2]) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wm = warp & 1, wn = warp >> 1;
@@ -102,11 +100,7 @@ __device__ __forceinline__ void tile_store(double* C, int64_t crs, int64_t ccs, 
             for (int h = 0; h < 2; ++h) {
                 const int row = wm * 32 + i * 8 + (lane >> 2);
                 const int col = wn * 32 + j * 8 + 2 * (lane & 3) + h;
-                if (row >= M || col >= N) continue;
-                if (mode == EPI_SUB_LOWER && row < col) continue;
-                double* p = C + row * crs + col * ccs;
-                if (mode == EPI_SET) *p = acc[i][j][h];
-                else *p -= acc[i][j][h];
+                if (row < M && col < N) C[row * crs + col * ccs] = acc[i][j][h];
             }
 }
 
@@ -411,7 +405,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_trsm(double* __restrict__ F, d
         load_tile(Bs, Li, 1, d.ldy, nb, nb, K4);
         __syncthreads();
         tile_mma(As, Bs, K4, acc);
-        tile_store(A, 1, d.ld, m, nb, EPI_SET, acc);
+        tile_store(A, 1, d.ld, m, nb, acc);
     } else {
         const int c0 = (tile - nP) * TL;
         if (c0 >= p0) return;
@@ -420,7 +414,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_trsm(double* __restrict__ F, d
         load_tile(Bs, Yr, d.ldy, 1, min(p0 - c0, TL), nb, K4);
         __syncthreads();
         tile_mma(As, Bs, K4, acc);
-        tile_store(Yr, 1, d.ldy, nb, min(p0 - c0, TL), EPI_SET, acc);
+        tile_store(Yr, 1, d.ldy, nb, min(p0 - c0, TL), acc);
     }
 }
 
@@ -497,9 +491,60 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_panel(double* __restrict__ F, 
     tile_mma(As, Bs, K4, acc);
     if (ptile) {
         const int m = min(d.ld - j0 - tile * TL, TL);
-        tile_store(F + d.f_off + j0 + tile * TL + (int64_t)p0 * d.ld, 1, d.ld, m, nb, EPI_SET, acc);
+        tile_store(F + d.f_off + j0 + tile * TL + (int64_t)p0 * d.ld, 1, d.ld, m, nb, acc);
     } else {
-        tile_store(Y + d.y_off + p0 + (int64_t)c0 * d.ldy, 1, d.ldy, nb, min(p0 - c0, TL), EPI_SET, acc);
+        tile_store(Y + d.y_off + p0 + (int64_t)c0 * d.ldy, 1, d.ldy, nb, min(p0 - c0, TL), acc);
+    }
+}
+
+#ifndef WRAPD_EPI_BATCH
+#define WRAPD_EPI_BATCH 8
+#endif
+constexpr int EPI_BATCH = WRAPD_EPI_BATCH;   // columns per thread whose reads the staged epilogue issues together
+constexpr int EPI_P = TL + 2;   // pitch of the staged output tile: lanes' (row, 2-column) fragments hit distinct banks
+static_assert(TL * EPI_P <= 2 * GEMM_STAGES * TILE_D, "the staged output tile reuses the operand stages");
+static_assert(TL == 2 * 32 && GEMM_THREADS == 2 * TL, "the staged epilogue maps two threads per row");
+
+// C[row + col*ld] -= acc for row < M, col < N and row + diag >= col, through
+// shared memory: the fragments go to a column-major tile, then each warp
+// updates 32 consecutive rows of a column (coalesced) with EPI_BATCH columns'
+// reads in flight before their writes.  Direct read-modify-writes from the
+// fragments would be serialised, since a store through C may alias the next
+// read as far as the compiler can tell.  `smem` (the operand stages) must have
+// no reads pending from other threads; the call's first barrier ensures that.
+__device__ __forceinline__ void tile_sub_staged(double* __restrict__ C, int64_t ld, int M, int N, int diag,
+                                                const double (&acc)[4][4][2], double* smem) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wm = warp & 1, wn = warp >> 1;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int row = wm * 32 + i * 8 + (lane >> 2);
+                const int col = wn * 32 + j * 8 + 2 * (lane & 3) + h;
+                smem[col * EPI_P + row] = acc[i][j][h];
+            }
+    __syncthreads();
+    const int row = threadIdx.x & (TL - 1), cg = threadIdx.x >> 6;
+    if (row >= M) return;
+    // columns cg, cg + 2, ... below N and with row + diag >= col
+    const int cend = min(N, row + diag + 1);
+#pragma unroll 1
+    for (int c0 = cg; c0 < cend; c0 += 2 * EPI_BATCH) {
+        double v[EPI_BATCH];
+#pragma unroll
+        for (int q = 0; q < EPI_BATCH; ++q) {
+            const int col = c0 + 2 * q;
+            v[q] = col < cend ? C[row + (int64_t)col * ld] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < EPI_BATCH; ++q) {
+            const int col = c0 + 2 * q;
+            if (col < cend) C[row + (int64_t)col * ld] = v[q] - smem[col * EPI_P + row];
+        }
     }
 }
 
@@ -537,25 +582,11 @@ __global__ void __launch_bounds__(GEMM_THREADS, WRAPD_GEMM_MINB) k_update(double
     else   // B'(j, t) = Y(k0 + t, c0 + j)
         gemm_pipelined<false>(A0, d.ld, M, Y + d.y_off + jb.k0 + (int64_t)c0 * d.ldy, d.ldy, N, jb.k1 - jb.k0,
                               gemm_smem, acc);
-    if (jb.kind == 0) {
-        // on tiles crossing the diagonal keep only row >= column (global indices)
-        double* C = F + d.f_off + r0 + (int64_t)c0 * d.ld;
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        const int wm = warp & 1, wn = warp >> 1;
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int row = wm * 32 + i * 8 + (lane >> 2);
-                    const int col = wn * 32 + j * 8 + 2 * (lane & 3) + h;
-                    if (row >= M || col >= N || r0 + row < c0 + col) continue;
-                    C[row + (int64_t)col * d.ld] -= acc[i][j][h];
-                }
-    } else {
-        tile_store(Y + d.y_off + r0 + (int64_t)c0 * d.ldy, 1, d.ldy, M, N, EPI_SUB, acc);
-    }
+    // on tiles of kind 0 crossing the diagonal keep only row >= column (global indices)
+    if (jb.kind == 0)
+        tile_sub_staged(F + d.f_off + r0 + (int64_t)c0 * d.ld, d.ld, M, N, r0 - c0, acc, gemm_smem);
+    else
+        tile_sub_staged(Y + d.y_off + r0 + (int64_t)c0 * d.ldy, d.ldy, M, N, TL, acc, gemm_smem);
 }
 
 // W = L_rs Y (r x k) with Y lower triangular: tile (ti, tj) of 64 x 64 sums
@@ -575,7 +606,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_wgemm(const double* __restrict
     // t over [c0, k): Y(k0 + t, c0 + j) vanishes above the diagonal
     gemm_pipelined<false>(A + (int64_t)c0 * d.ld, d.ld, M, Y + d.y_off + c0 + (int64_t)c0 * d.ldy, d.ldy, N, d.k - c0,
                           gemm_smem, acc);
-    tile_store(W + d.y_off + d.k + r0 + (int64_t)c0 * d.ldy, 1, d.ldy, M, N, EPI_SET, acc);
+    tile_store(W + d.y_off + d.k + r0 + (int64_t)c0 * d.ldy, 1, d.ldy, M, N, acc);
 }
 
 // ---- solve -----------------------------------------------------------------------
