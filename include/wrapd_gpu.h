@@ -44,7 +44,7 @@ enum {
     WRAPD_E_OOM = -7,            /* device allocation failed */
     WRAPD_E_CUDA = -8,           /* any other CUDA error, or no device */
     WRAPD_E_STATE = -9,          /* call out of order (e.g. solve before initialize) */
-    WRAPD_E_UNSUPPORTED = -10    /* an option this build does not implement */
+    WRAPD_E_UNSUPPORTED = -10    /* an option this library does not implement */
 };
 
 /* Solver options.  Field meanings and defaults follow wrapd::Settings
