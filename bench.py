@@ -117,7 +117,7 @@ def dist_setup(n):
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         pg = dist
     return rank, world, local, pg
 
@@ -127,13 +127,23 @@ def barrier(pg):
         pg.barrier()
 
 
-def max_over_ranks(pg, v: float) -> float:
-    if pg is None:
-        return v
+def _all_reduce(pg, v: float, op) -> float:
     import torch
-    t = torch.tensor([v], device="cuda", dtype=torch.float64)
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    # NCCL reduces device tensors; gloo (the CPU tests of this harness) host ones
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], device=dev, dtype=torch.float64)
+    pg.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(pg, v: float) -> float:
+    """The slowest rank's time: every rank calls it at the same point."""
+    return v if pg is None else _all_reduce(pg, v, pg.ReduceOp.MAX)
+
+
+def sum_over_ranks(pg, v: float) -> float:
+    """The units all ranks processed: every rank calls it at the same point."""
+    return v if pg is None else _all_reduce(pg, v, pg.ReduceOp.SUM)
 
 
 # ---- bytes / flops model (algorithmic, per launch) -----------------------------------
@@ -377,11 +387,12 @@ def run_ours(args, rank, world, local, pg):
     barrier(pg)
     ms = ev0.elapsed_time(ev1)
     ms = max_over_ranks(pg, ms)
+    ne, nf = bar.n_tets, bar.n_verts - len(bar.pins)
+    units = sum_over_ranks(pg, float(ne * done))   # element-iterations of all replicas
     rt1, c1 = s.runtime(), s.counters()
     if done != K:
         raise RuntimeError(f"only {done} of {K} iterations ran")
-    ne, nf = bar.n_tets, bar.n_verts - len(bar.pins)
-    value = world * ne * K / (ms / 1000.0)
+    value = units / (ms / 1000.0)
     local_ms = rt1["local_ms"] - rt0["local_ms"]
     glob_ms = rt1["global_ms"] - rt0["global_ms"]
     ref_ms = rt1["refactor_ms"] - rt0["refactor_ms"]
