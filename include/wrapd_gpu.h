@@ -306,6 +306,42 @@ WRAPD_API int wrapd_set_prox_net(wrapd_handle* h, const float* blob, int n_blob)
  * counterpart). */
 WRAPD_API int wrapd_dmma_peak(int iters, double* tflops);
 
+/* ---- Host-only planning: no CUDA call, no device memory ------------------
+ * The symbolic analysis that wrapd_initialize runs on the host, for one mesh,
+ * with no GPU needed: the nested-dissection order of the free vertices, the
+ * assembly tree of dense fronts, and the sizes of the factor's device pools,
+ * so a job can be sized against the GPU's memory before a handle exists.
+ * Stands for the analyzePattern step of the reference's SimplicialLDLT
+ * (deps/mcloptlib/include/MCL/LinearSolver.hpp:279-298, AMD ordering there;
+ * geometric nested dissection here).  Errors: wrapd_last_error(NULL). */
+typedef struct wrapd_plan wrapd_plan;
+
+/* Mesh arguments as wrapd_add_tetmesh (rest positions n_verts x 3, tets
+ * n_tets x 4 0-based, distinct pinned vertex ids); leaf_size <= 0 takes the
+ * default of the settings (64).  Free vertices are numbered in ascending
+ * vertex id order with the pinned ones skipped, as the solver numbers them. */
+WRAPD_API int wrapd_plan_create(const double* rest_xyz, int n_verts, const int32_t* tets, int n_tets,
+                                const int32_t* pins, int n_pins, int leaf_size, wrapd_plan** out);
+
+/* out[0..7] = free vertices, fronts, levels, stored factor entries (dense
+ * fronts: k(k+1)/2 + k r each), F-pool bytes and Y-pool bytes (FP64; the two
+ * largest device allocations of a solve), total front rows (the length of
+ * the row and relative-index arrays), factorization flops (rounded). */
+WRAPD_API int wrapd_plan_info(const wrapd_plan* p, int64_t out[8]);
+
+/* perm (free vertices): the free index of the vertex in each column of the
+ * new order.  Per front, in post-order (children before their parent): first
+ * column, column count, parent front (-1 for a root), level (one more than
+ * its highest child, 0 for a leaf); row_ptr (fronts + 1) delimits its rows
+ * (new numbering, sorted, after its own columns) in `rows`, and `relmap`
+ * gives where each row lands in the parent's front (t < k_parent: the
+ * parent's column t; k_parent + t: the parent's row t).  Any output may be
+ * NULL. */
+WRAPD_API int wrapd_plan_fronts(const wrapd_plan* p, int32_t* perm, int32_t* first, int32_t* ncols,
+                                int32_t* parent, int32_t* level, int64_t* row_ptr, int32_t* rows,
+                                int32_t* relmap);
+WRAPD_API void wrapd_plan_destroy(wrapd_plan* p);
+
 #ifdef __cplusplus
 }
 #endif

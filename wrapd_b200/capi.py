@@ -105,6 +105,12 @@ SIGNATURES = [
                                           ctypes.c_double, _dp]),
     ("wrapd_set_prox_net", ctypes.c_int, [ctypes.c_void_p, _fp, ctypes.c_int]),
     ("wrapd_dmma_peak", ctypes.c_int, [ctypes.c_int, _dp]),
+    ("wrapd_plan_create", ctypes.c_int, [_dp, ctypes.c_int, _ip, ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_void_p)]),
+    ("wrapd_plan_info", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    ("wrapd_plan_fronts", ctypes.c_int, [ctypes.c_void_p, _ip, _ip, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_int64),
+                                          _ip, _ip]),
+    ("wrapd_plan_destroy", None, [ctypes.c_void_p]),
 ]
 
 
@@ -168,6 +174,41 @@ def dmma_peak(iters: int = 20000) -> float:
     v = ctypes.c_double(0.0)
     _check_free(load().wrapd_dmma_peak(iters, ctypes.byref(v)))
     return v.value
+
+
+PLAN_INFO = ("n_free", "fronts", "levels", "nnz_L", "f_pool_bytes", "y_pool_bytes", "total_rows", "flops")
+
+
+def plan(rest, tets, pins, leaf_size: int = 0) -> dict:
+    """Host-only symbolic analysis of one mesh (wrapd_plan_*; needs no GPU):
+    the sizes of PLAN_INFO, the order `perm` (free index per new column) and
+    per front `first`, `ncols`, `parent`, `level`, `row_ptr`, `rows`, `relmap`."""
+    lib = load()
+    X = np.ascontiguousarray(rest, dtype=np.float64).reshape(-1, 3)
+    T = np.ascontiguousarray(tets, dtype=np.int32).reshape(-1, 4)
+    P = np.ascontiguousarray(pins, dtype=np.int32).ravel()
+    h = ctypes.c_void_p()
+    rc = lib.wrapd_plan_create(dptr(X), X.shape[0], iptr(T), T.shape[0], iptr(P), P.size, leaf_size,
+                               ctypes.byref(h))
+    if rc != WRAPD_OK:
+        raise WrapdError(rc, lib.wrapd_last_error(None).decode())
+    try:
+        info = np.zeros(8, dtype=np.int64)
+        lib.wrapd_plan_info(h, info.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+        out = dict(zip(PLAN_INFO, (int(v) for v in info)))
+        nf, nfr, nr = out["n_free"], out["fronts"], out["total_rows"]
+        arr = {k: np.zeros(n, dtype=np.int32) for k, n in
+               (("perm", nf), ("first", nfr), ("ncols", nfr), ("parent", nfr), ("level", nfr), ("rows", nr),
+                ("relmap", nr))}
+        arr["row_ptr"] = np.zeros(nfr + 1, dtype=np.int64)
+        _check_free(lib.wrapd_plan_fronts(h, iptr(arr["perm"]), iptr(arr["first"]), iptr(arr["ncols"]),
+                                          iptr(arr["parent"]), iptr(arr["level"]),
+                                          arr["row_ptr"].ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                          iptr(arr["rows"]), iptr(arr["relmap"])))
+        out.update(arr)
+        return out
+    finally:
+        lib.wrapd_plan_destroy(h)
 
 
 def load():

@@ -1,5 +1,6 @@
 // extern "C" entry points declared in include/wrapd_gpu.h.  Every entry
 // catches C++ exceptions and returns a WRAPD_E_* code.
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -10,6 +11,10 @@
 struct wrapd_handle {
     wrapd::SolverGPU* s = nullptr;
     std::string err;
+};
+
+struct wrapd_plan {
+    wrapd::Symbolic S;
 };
 
 namespace {
@@ -201,6 +206,97 @@ int wrapd_get_profile(wrapd_handle* h, double ms[6], int64_t counts[6]) {
         for (int i = 0; i < 6; ++i) { ms[i] = s.profile_ms[i]; counts[i] = s.profile_n[i]; }
     });
 }
+
+int wrapd_plan_create(const double* rest_xyz, int n_verts, const int32_t* tets, int n_tets, const int32_t* pins,
+                      int n_pins, int leaf_size, wrapd_plan** out) {
+    if (!out) return WRAPD_E_INPUT;
+    *out = nullptr;
+    try {
+        // the argument checks of wrapd_add_tetmesh (SolverGPU::add_mesh)
+        if (!rest_xyz || !tets || n_verts <= 0 || n_tets <= 0 || n_pins < 0 || n_pins >= n_verts ||
+            (n_pins > 0 && !pins))
+            throw wrapd::CudaError(WRAPD_E_INPUT, "bad mesh arguments");
+        for (int64_t i = 0; i < 4 * (int64_t)n_tets; ++i)
+            if (tets[i] < 0 || tets[i] >= n_verts) throw wrapd::CudaError(WRAPD_E_INPUT, "tet vertex id out of range");
+        std::vector<int> p(pins, pins + n_pins);
+        std::sort(p.begin(), p.end());
+        for (int j = 0; j < n_pins; ++j)
+            if (p[j] < 0 || p[j] >= n_verts || (j > 0 && p[j] == p[j - 1]))
+                throw wrapd::CudaError(WRAPD_E_INPUT, "pin ids must be distinct vertex ids");
+        // free numbering: ascending vertex id, pinned vertices skipped
+        std::vector<int> free_of_vert(n_verts, -1);
+        for (int i = 0, j = 0, k = 0; i < n_verts; ++i) {
+            if (j < n_pins && i == p[j]) ++j;
+            else free_of_vert[i] = k++;
+        }
+        const int nf = n_verts - n_pins;
+        std::vector<int> vinc_ptr, vinc, ptr, adj;
+        wrapd::free_vertex_graph(nf, n_tets, tets, free_of_vert.data(), vinc_ptr, vinc, ptr, adj);
+        std::vector<double> coords(3 * (size_t)nf);
+        for (int i = 0; i < n_verts; ++i)
+            if (free_of_vert[i] >= 0)
+                for (int c = 0; c < 3; ++c) coords[3 * (size_t)free_of_vert[i] + c] = rest_xyz[3 * (size_t)i + c];
+        auto* pl = new wrapd_plan();
+        try {
+            pl->S = wrapd::analyse(nf, ptr, adj, coords, leaf_size > 0 ? leaf_size : 64);
+        } catch (...) {
+            delete pl;
+            throw;
+        }
+        *out = pl;
+        g_create_error.clear();
+        return WRAPD_OK;
+    } catch (const wrapd::CudaError& e) {
+        g_create_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_create_error = "host allocation failed";
+        return WRAPD_E_OOM;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        return WRAPD_E_INPUT;
+    }
+}
+
+int wrapd_plan_info(const wrapd_plan* p, int64_t out[8]) {
+    if (!p || !out) return WRAPD_E_INPUT;
+    const wrapd::Symbolic& S = p->S;
+    out[0] = S.n;
+    out[1] = (int64_t)S.fronts.size();
+    out[2] = (int64_t)S.levels.size();
+    out[3] = S.nnz_L;
+    out[4] = S.f_pool * (int64_t)sizeof(double);
+    out[5] = S.y_pool * (int64_t)sizeof(double);
+    out[6] = (int64_t)S.relmap.size();
+    out[7] = (int64_t)(S.flops + 0.5);
+    return WRAPD_OK;
+}
+
+int wrapd_plan_fronts(const wrapd_plan* p, int32_t* perm, int32_t* first, int32_t* ncols, int32_t* parent,
+                      int32_t* level, int64_t* row_ptr, int32_t* rows, int32_t* relmap) {
+    if (!p) return WRAPD_E_INPUT;
+    const wrapd::Symbolic& S = p->S;
+    if (perm)
+        for (int i = 0; i < S.n; ++i) perm[i] = S.perm[i];
+    int64_t at = 0;
+    for (size_t f = 0; f < S.fronts.size(); ++f) {
+        const wrapd::Front& F = S.fronts[f];
+        if (first) first[f] = F.first;
+        if (ncols) ncols[f] = F.ncols;
+        if (parent) parent[f] = F.parent;
+        if (level) level[f] = F.level;
+        if (row_ptr) row_ptr[f] = at;
+        for (int t = 0; t < F.nrows(); ++t) {
+            if (rows) rows[at + t] = F.rows[t];
+            if (relmap) relmap[at + t] = S.relmap[F.rel_off + t];
+        }
+        at += F.nrows();
+    }
+    if (row_ptr) row_ptr[S.fronts.size()] = at;
+    return WRAPD_OK;
+}
+
+void wrapd_plan_destroy(wrapd_plan* p) { delete p; }
 
 const char* wrapd_last_error(const wrapd_handle* h) {
     if (!h) return g_create_error.c_str();

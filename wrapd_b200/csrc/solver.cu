@@ -242,44 +242,11 @@ void SolverGPU::initialize() {
         }
     lap("element geometry");
     // ---- free-vertex graph, nested dissection, symbolic factorization ----
-    // element incidences per free vertex (free numbering), in element order:
-    // entry e * 4 + a for vertex slot a of element e
-    std::vector<int> vinc_ptr(nf + 1, 0), vinc;
-    for (int e = 0; e < ne; ++e)
-        for (int a = 0; a < 4; ++a) {
-            const int i = free_of_vert_[tets_[4 * (size_t)e + a]];
-            if (i >= 0) vinc_ptr[i + 1]++;
-        }
-    for (int i = 0; i < nf; ++i) vinc_ptr[i + 1] += vinc_ptr[i];
-    vinc.resize(vinc_ptr[nf]);
-    {
-        std::vector<int> fill(vinc_ptr.begin(), vinc_ptr.end() - 1);
-        for (int e = 0; e < ne; ++e)
-            for (int a = 0; a < 4; ++a) {
-                const int i = free_of_vert_[tets_[4 * (size_t)e + a]];
-                if (i >= 0) vinc[fill[i]++] = e * 4 + a;
-            }
-    }
-    // adjacency: the other free vertices of the incident elements, sorted and unique
-    std::vector<int> ptr(nf + 1, 0), adj;
-    {
-        std::vector<int> cand;
-        adj.reserve(16 * (size_t)nf);
-        for (int i = 0; i < nf; ++i) {
-            cand.clear();
-            for (int q = vinc_ptr[i]; q < vinc_ptr[i + 1]; ++q) {
-                const int e = vinc[q] >> 2;
-                for (int b = 0; b < 4; ++b) {
-                    const int j = free_of_vert_[tets_[4 * (size_t)e + b]];
-                    if (j >= 0 && j != i) cand.push_back(j);
-                }
-            }
-            std::sort(cand.begin(), cand.end());
-            cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
-            adj.insert(adj.end(), cand.begin(), cand.end());
-            ptr[i + 1] = (int)adj.size();
-        }
-    }
+    // element incidences per free vertex (free numbering), in element order
+    // (entry e * 4 + a for vertex slot a of element e), and the adjacency: the
+    // other free vertices of the incident elements, sorted and unique
+    std::vector<int> vinc_ptr, vinc, ptr, adj;
+    free_vertex_graph(nf, ne, tets_.data(), free_of_vert_.data(), vinc_ptr, vinc, ptr, adj);
     std::vector<double> coords(3 * (size_t)nf);
     for (int i = 0; i < nv; ++i)
         if (free_of_vert_[i] >= 0)

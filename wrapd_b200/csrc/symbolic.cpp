@@ -99,6 +99,43 @@ struct Dissector {
 
 }  // namespace
 
+void free_vertex_graph(int nf, int ne, const int* tets, const int* free_of_vert, std::vector<int>& vinc_ptr,
+                       std::vector<int>& vinc, std::vector<int>& ptr, std::vector<int>& adj) {
+    vinc_ptr.assign(nf + 1, 0);
+    for (int64_t t = 0; t < 4 * (int64_t)ne; ++t) {
+        const int i = free_of_vert[tets[t]];
+        if (i >= 0) vinc_ptr[i + 1]++;
+    }
+    for (int i = 0; i < nf; ++i) vinc_ptr[i + 1] += vinc_ptr[i];
+    vinc.resize(vinc_ptr[nf]);
+    {
+        std::vector<int> fill(vinc_ptr.begin(), vinc_ptr.end() - 1);
+        for (int e = 0; e < ne; ++e)
+            for (int a = 0; a < 4; ++a) {
+                const int i = free_of_vert[tets[4 * (int64_t)e + a]];
+                if (i >= 0) vinc[fill[i]++] = e * 4 + a;
+            }
+    }
+    ptr.assign(nf + 1, 0);
+    adj.clear();
+    adj.reserve(16 * (size_t)nf);
+    std::vector<int> cand;
+    for (int i = 0; i < nf; ++i) {
+        cand.clear();
+        for (int q = vinc_ptr[i]; q < vinc_ptr[i + 1]; ++q) {
+            const int e = vinc[q] >> 2;
+            for (int b = 0; b < 4; ++b) {
+                const int j = free_of_vert[tets[4 * (int64_t)e + b]];
+                if (j >= 0 && j != i) cand.push_back(j);
+            }
+        }
+        std::sort(cand.begin(), cand.end());
+        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+        adj.insert(adj.end(), cand.begin(), cand.end());
+        ptr[i + 1] = static_cast<int>(adj.size());
+    }
+}
+
 Symbolic analyse(int n, const std::vector<int>& adj_ptr, const std::vector<int>& adj,
                  const std::vector<double>& coords, int leaf) {
     if (n <= 0) throw std::invalid_argument("analyse: empty matrix");

@@ -52,6 +52,15 @@ struct Symbolic {
     double flops = 0.0;       // factorization flops (dense front model)
 };
 
+// The free-vertex graph of a tet mesh (the sparsity of A, src/TetElements.cpp:
+// 483-510).  free_of_vert[v] is vertex v's free index (ascending vertex id,
+// pinned vertices skipped) or -1 for a pinned vertex.  Outputs, per free vertex
+// i: vinc[vinc_ptr[i] .. vinc_ptr[i+1]) its element incidences e * 4 + a (slot
+// a of element e) in element order, and adj[ptr[i] .. ptr[i+1]) the other free
+// vertices of those elements, sorted and unique.
+void free_vertex_graph(int nf, int ne, const int* tets, const int* free_of_vert, std::vector<int>& vinc_ptr,
+                       std::vector<int>& vinc, std::vector<int>& ptr, std::vector<int>& adj);
+
 // adj_ptr/adj: symmetric adjacency of the n free vertices (no self loops).
 // coords: n x 3 positions used for the geometric cuts.  leaf: max leaf size.
 Symbolic analyse(int n, const std::vector<int>& adj_ptr, const std::vector<int>& adj,
