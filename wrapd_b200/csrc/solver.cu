@@ -281,86 +281,11 @@ void SolverGPU::initialize() {
         }
         idx[e] = make_int4(s[0], s[1], s[2], s[3]);
     }
-    // lower-triangle entries of A in front storage, with their element contributions
-    std::vector<int> col2front(nf, -1);
-    for (size_t f = 0; f < S.fronts.size(); ++f)
-        for (int j = 0; j < S.fronts[f].ncols; ++j) col2front[S.fronts[f].first + j] = (int)f;
-    // Entries of A (unordered free-vertex pairs {i, j}, i <= j): entry ids
-    // base[i] + rank of j in {i} + {neighbours > i} (sorted).  Contributions
-    // are counted per entry, then filled in element order (e, a, b), so each
-    // entry sums its contributions in the order of the reference's triplet
-    // list; each entry's pool position is looked up once.
-    std::vector<int64_t> ebase(nf + 1, 0);
-    for (int i = 0; i < nf; ++i) {
-        const int* lo = adj.data() + ptr[i];
-        const int* hi = adj.data() + ptr[i + 1];
-        ebase[i + 1] = ebase[i] + 1 + (hi - std::upper_bound(lo, hi, i));
-    }
-    const int64_t nentries = ebase[nf];
-    auto entry_of = [&](int fa, int fb) -> int64_t {   // fa <= fb
-        if (fa == fb) return ebase[fa];
-        const int* lo = adj.data() + ptr[fa];
-        const int* hi = adj.data() + ptr[fa + 1];
-        const int* up = std::upper_bound(lo, hi, fa);
-        return ebase[fa] + 1 + (std::lower_bound(up, hi, fb) - up);
-    };
-    // Contributions of entry {i, j}: the elements holding both vertices, in
-    // element order (a merge of the two incidence lists), as e * 16 + a * 4 + b
-    // with a the slot of the lower free index and b the other's.
-    auto entry_contribs = [&](int i, int j, auto&& out) {
-        if (i == j) {
-            for (int q = vinc_ptr[i]; q < vinc_ptr[i + 1]; ++q) out((vinc[q] >> 2) * 16 + (vinc[q] & 3) * 5);
-            return;
-        }
-        int p = vinc_ptr[i], q = vinc_ptr[j];
-        while (p < vinc_ptr[i + 1] && q < vinc_ptr[j + 1]) {
-            const int ep = vinc[p] >> 2, eq = vinc[q] >> 2;
-            if (ep < eq) ++p;
-            else if (eq < ep) ++q;
-            else { out(ep * 16 + (vinc[p] & 3) * 4 + (vinc[q] & 3)); ++p; ++q; }
-        }
-    };
-    std::vector<int> A_ptr(nentries + 1, 0), A_con;
-    for (int i = 0; i < nf; ++i) {
-        int64_t id = ebase[i];
-        int n = 0;
-        entry_contribs(i, i, [&](int) { ++n; });
-        A_ptr[id + 1] = n;
-        for (int q = ptr[i]; q < ptr[i + 1]; ++q) {
-            if (adj[q] <= i) continue;
-            n = 0;
-            entry_contribs(i, adj[q], [&](int) { ++n; });
-            A_ptr[++id + 1] = n;
-        }
-    }
-    for (int64_t t = 0; t < nentries; ++t) A_ptr[t + 1] += A_ptr[t];
-    A_con.resize(A_ptr[nentries]);
-    for (int i = 0; i < nf; ++i) {
-        int64_t id = ebase[i];
-        int w = A_ptr[id];
-        entry_contribs(i, i, [&](int c) { A_con[w++] = c; });
-        for (int q = ptr[i]; q < ptr[i + 1]; ++q) {
-            if (adj[q] <= i) continue;
-            w = A_ptr[++id];
-            entry_contribs(i, adj[q], [&](int c) { A_con[w++] = c; });
-        }
-    }
-    // pool position of each entry: lower triangle in the dissection order
-    std::vector<int64_t> A_pos(nentries);
-    for (int i = 0; i < nf; ++i) {
-        auto put = [&](int j) {
-            const int si = iperm_[i], sj = iperm_[j];
-            const int r = std::max(si, sj), c = std::min(si, sj);
-            const Front& F = S.fronts[col2front[c]];
-            int lr;
-            if (r < F.first + F.ncols) lr = r - F.first;
-            else lr = F.ncols + (int)(std::lower_bound(F.rows.begin(), F.rows.end(), r) - F.rows.begin());
-            A_pos[entry_of(i, j)] = F.f_off + lr + (int64_t)(c - F.first) * F.ld();
-        };
-        put(i);
-        for (int q = ptr[i]; q < ptr[i + 1]; ++q)
-            if (adj[q] > i) put(adj[q]);
-    }
+    // lower-triangle entries of A in front storage, with their element
+    // contributions in the order of the reference's triplet list
+    std::vector<int64_t> A_pos;
+    std::vector<int> A_ptr, A_con;
+    assembly_map(S, vinc_ptr, vinc, ptr, adj, A_pos, A_ptr, A_con);
     lap("A pattern (scatter map)");
     // gather incidences, element order per free vertex
     std::vector<int> inc_ptr(nf + 1, 0), inc;

@@ -66,6 +66,18 @@ void free_vertex_graph(int nf, int ne, const int* tets, const int* free_of_vert,
 Symbolic analyse(int n, const std::vector<int>& adj_ptr, const std::vector<int>& adj,
                  const std::vector<double>& coords, int leaf);
 
+// The assembly scatter map of A's lower triangle into the F pool (A is the
+// sum of the reference's triplets, src/TetElements.cpp:483-510).  Entries are
+// the unordered free-vertex pairs {i, j}, i <= j (free numbering), entry ids
+// ebase[i] + the rank of j in {i} + {neighbours of i above i}.  Entry t sums
+// the contributions A_con[A_ptr[t] .. A_ptr[t+1]) = e * 16 + a * 4 + b (slot a
+// of element e holds the lower free index, slot b the other) in element
+// order, and lands at F-pool offset A_pos[t] (lower triangle in the
+// dissection order of S).  vinc/ptr/adj as free_vertex_graph gives them.
+void assembly_map(const Symbolic& S, const std::vector<int>& vinc_ptr, const std::vector<int>& vinc,
+                  const std::vector<int>& ptr, const std::vector<int>& adj, std::vector<int64_t>& A_pos,
+                  std::vector<int>& A_ptr, std::vector<int>& A_con);
+
 // The analysis of a block-diagonal matrix from the analyses of its blocks (one
 // per mesh of a batch), block p taking the columns after blocks 0..p-1: the
 // forest of their trees, level l holding every block's level-l fronts.
