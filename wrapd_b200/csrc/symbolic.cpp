@@ -15,10 +15,15 @@ namespace wrapd {
 namespace {
 
 // Host threads for `n` items of work: one per `grain` items, at most the
-// hardware's threads and 16, at least one.
+// hardware's threads, 16, and WRAPD_HOST_THREADS when that is set to a
+// positive number; at least one.  The results do not depend on the count.
 int host_threads(int64_t n, int64_t grain) {
-    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
-    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({n / grain, (int64_t)hw, 16})));
+    int64_t cap = std::min<int64_t>(16, std::max(1u, std::thread::hardware_concurrency()));
+    if (const char* env = std::getenv("WRAPD_HOST_THREADS")) {
+        const long v = std::strtol(env, nullptr, 10);
+        if (v > 0) cap = std::min<int64_t>(cap, v);
+    }
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(n / grain, cap)));
 }
 
 // fn(t, lo, hi) over `nthreads` contiguous ranges of [0, n), range t on its own
