@@ -208,3 +208,21 @@ def test_plan_rejects_bad_meshes(lib):
         capi.plan(bar.rest, bar.tets, np.array([0, 0], dtype=np.int32))
     with pytest.raises(capi.WrapdError):
         capi.plan(bar.rest, bar.tets, np.arange(bar.n_verts, dtype=np.int32))
+
+
+def test_quasi_plan_flag_needs_no_gpu(lib, tmp_path):
+    """`quasi -plan 1` prints the same analysis from .node/.ele/handles files
+    and exits before any CUDA call."""
+    import os
+    import subprocess
+    bar = bars.bar_8x8x32()
+    files = bars.write_bar(bar, str(tmp_path), "bar")
+    quasi = os.path.join(os.path.dirname(capi.LIB_PATH), "quasi")
+    r = subprocess.run([quasi, "-rest", files["rest"], "-init", files["init"], "-handles", files["handles"],
+                        "-plan", "1"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    got = {k: int(v) for k, v in (line.rsplit(" ", 1) for line in r.stdout.strip().splitlines())}
+    p = capi.plan(bar.rest, bar.tets, bar.pins)
+    assert got == {"free vertices": p["n_free"], "fronts": p["fronts"], "levels": p["levels"],
+                   "factor entries": p["nnz_L"], "factor flops": p["flops"], "F pool bytes": p["f_pool_bytes"],
+                   "Y pool bytes": p["y_pool_bytes"]}

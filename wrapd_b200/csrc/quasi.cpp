@@ -18,7 +18,9 @@
 // Extensions: -youngs E (the reference hard-codes 1e7 Pa, src/Lame.hpp:38),
 // -out DIR, -lbfgs_m M, -rw_every N, -precision fp64|mixed,
 // -prox lbfgs|newton|net (net: the prox network from -net FILE, a raw
-// little-endian float32 blob), -leaf N, -device D, -autotune 0|1.
+// little-endian float32 blob), -leaf N, -device D, -autotune 0|1, -plan 1
+// (print the host analysis and the factor's device pool sizes, then exit
+// without touching the GPU).
 #include <algorithm>
 #include <array>
 #include <cerrno>
@@ -186,7 +188,8 @@ void help() {
         " -global_it N (100)  -global_ls 0|1  -kappa K (1)  -model nh|arap  -poisson P (0.45)\n"
         " -beta_static B (1)  -beta_min B (0.1)  -beta_max B (10)  -p 0|1  -s 0|1 (1)\n"
         "Extensions: -youngs E (1e7)  -out DIR (.)  -lbfgs_m M (6)  -rw_every N  -precision fp64|mixed\n"
-        "            -prox lbfgs|newton|net  -net FILE  -leaf N  -device D  -autotune 0|1\n\n");
+        "            -prox lbfgs|newton|net  -net FILE  -leaf N  -device D  -autotune 0|1\n"
+        "            -plan 1 (print the analysis and device pool sizes, no GPU, then exit)\n\n");
 }
 
 int run(int argc, char** argv) {
@@ -203,7 +206,7 @@ int run(int argc, char** argv) {
     wrapd_settings s;
     wrapd_settings_default(&s);
     std::string rest, init, soln, handles, out = ".", net;
-    int save = 1;
+    int save = 1, plan_only = 0;
     for (size_t i = 0; i < cmds.size(); ++i) {
         const std::string& a = cmds[i];
         std::istringstream v(vals[i]);
@@ -260,6 +263,7 @@ int run(int argc, char** argv) {
         else if (a == "-leaf") s.leaf_size = geti();
         else if (a == "-device") s.device = geti();
         else if (a == "-autotune") s.autotune = geti();
+        else if (a == "-plan") plan_only = geti();
         else fail("Error: Unrecognized command-line argument: " + a);
     }
     const std::vector<int32_t> pins = load_handles(handles);
@@ -270,6 +274,20 @@ int run(int argc, char** argv) {
     if (!soln.empty()) S = load_elenode(soln);
     const int nv = static_cast<int>(R.xyz.size() / 3), nt = static_cast<int>(R.tets.size() / 4);
 
+    if (plan_only) {
+        wrapd_plan* p = nullptr;
+        if (wrapd_plan_create(R.xyz.data(), nv, R.tets.data(), nt, pins.data(), static_cast<int>(pins.size()),
+                              s.leaf_size, &p) != WRAPD_OK)
+            fail(wrapd_last_error(nullptr));
+        int64_t info[8];
+        wrapd_plan_info(p, info);
+        wrapd_plan_destroy(p);
+        std::printf("free vertices %lld\nfronts %lld\nlevels %lld\nfactor entries %lld\n"
+                    "factor flops %lld\nF pool bytes %lld\nY pool bytes %lld\n",
+                    (long long)info[0], (long long)info[1], (long long)info[2], (long long)info[3],
+                    (long long)info[7], (long long)info[4], (long long)info[5]);
+        return 0;
+    }
     wrapd_handle* h = nullptr;
     if (wrapd_create(&s, &h) != WRAPD_OK) fail(wrapd_last_error(nullptr));
     auto check = [&](int rc) {
