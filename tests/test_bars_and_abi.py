@@ -89,6 +89,17 @@ def test_settings_defaults_follow_the_reference(lib_built):
     assert (s.beta_static, s.beta_min, s.beta_max, s.prox_iters, s.youngs, s.lbfgs_m) == (1.0, 0.1, 10.0, 20, 1e7, 6)
 
 
+def test_settings_accept_the_reference_flag_names(lib_built):
+    """The Python mirror maps the reference's flag names (-it, -ra, -rw,
+    -global_it) onto the settings fields and rejects unknown names."""
+    from wrapd_b200.solver import Settings
+    s = Settings(it=500, ra=0, rw=0, global_it=7, tol=1e-9, precision="mixed", youngs=1e5)
+    assert (s.max_iters, s.rot_aware, s.reweighting, s.global_iters, s.tol) == (500, 0, 0, 7, 1e-9)
+    assert (s.precision, s.youngs, s.gamma) == (1, 1e5, 1.5)
+    with pytest.raises(ValueError, match="unknown setting"):
+        Settings(not_a_flag=1)
+
+
 def test_no_device_fails_loudly(lib_built):
     """Without a usable GPU the library refuses to run (there is no CPU path)."""
     try:
