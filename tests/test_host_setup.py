@@ -52,3 +52,24 @@ def test_scatter_map_with_scattered_pins(checker, tmp_path):
 def test_setup_of_the_786k_bar_is_thread_count_independent(checker, tmp_path):
     """138,303 free vertices: every threaded phase runs on several threads."""
     check(checker, bars.bar_32x32x128_bent(), tmp_path, threads=8)
+
+
+def test_cpp_classes_over_the_abi(lib_built, tmp_path):
+    """include/wrapd_gpu.hpp (wrapd::gpu::Solver, Settings, AlgorithmData):
+    defaults, the reference's messages as std::runtime_error, and, with no
+    usable GPU, initialize() failing loudly."""
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no host C++ compiler")
+    libdir = os.path.dirname(lib_built)
+    exe = str(tmp_path / "shim_check")
+    subprocess.run([gxx, "-std=c++17", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "host", "shim_check.cpp"), f"-L{libdir}", "-lwrapd_gpu",
+                    f"-Wl,-rpath,{libdir}", "-o", exe], check=True)
+    try:
+        import torch
+        gpu = torch.cuda.is_available()
+    except ImportError:
+        gpu = False
+    r = subprocess.run([exe] + ([] if gpu else ["nogpu"]), capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
