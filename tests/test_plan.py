@@ -198,6 +198,18 @@ def test_plan_sizes_of_the_786k_bar(lib):
     assert p["nnz_L"] == 61277250
 
 
+def test_plan_sizes_of_the_3m9_bar(lib):
+    """The 3,932,160-tet bar: the host plan gives what the GPU solver reported
+    for it (wrapd_get_info: 16,383 fronts, 14 levels, 567,452,252 factor
+    entries, 2,247,282,490,463 flops) and the two pools that make up 33.7 of
+    the 36.6 GB it holds on the device."""
+    bar = bars.bar_64x64x160()
+    p = capi.plan(bar.rest, bar.tets, bar.pins)
+    assert (p["n_free"], p["fronts"], p["levels"]) == (671775, 16383, 14)
+    assert (p["nnz_L"], p["flops"]) == (567452252, 2247282490463)
+    assert round((p["f_pool_bytes"] + p["y_pool_bytes"]) / 1e9, 1) == 33.7
+
+
 def test_plan_rejects_bad_meshes(lib):
     bar = bars.make_bar(2, 2, 4, twist_deg=0.0, noise=0.0, seed=0)
     bad_tets = bar.tets.copy()
