@@ -511,8 +511,9 @@ void SolverGPU::factor() {
     n_factor++;
 }
 
-// Profile slots: 0 = local step, 1 = gradient + gather, 2 = two-loop vector
-// kernels, 3 = triangular solves, 4 = x update, 5 = host gaps around syncs.
+// Profile slots: 0 = local step, 1 = gradient + gather, 2 = two-loop and
+// x-update vector kernels, 3 = triangular solves, 4 unused, 5 = host gaps
+// around syncs and the reweight/refactor phase.
 void SolverGPU::mark(int slot) {
     if (!profiling) return;
     if (event_next_ == event_pool_.size()) {
