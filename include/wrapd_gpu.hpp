@@ -14,7 +14,11 @@
  *   - solve() runs the whole ADMM loop on the GPU and X() returns the
  *     positions of every added mesh in the order added.
  * Errors throw std::runtime_error with the library's message, as the
- * reference throws std::runtime_error; no error code crosses this layer. */
+ * reference throws std::runtime_error; no error code crosses this layer.
+ * Callers written against the reference's own headers use include/wrapd/
+ * instead: the reference's file and class names (Solver with m_system,
+ * System, TetElements, Settings with parse_args, AlgorithmData) with Eigen
+ * types, over the same C ABI, so that such a caller builds unchanged. */
 #ifndef WRAPD_GPU_HPP
 #define WRAPD_GPU_HPP
 
@@ -102,13 +106,22 @@ public:
         if (m_meshes.empty()) throw std::runtime_error("initialize before add_tetmesh");
         wrapd_handle* h = nullptr;
         if (wrapd_create(&m_settings, &h) != WRAPD_OK) throw std::runtime_error(wrapd_last_error(nullptr));
-        m_h = h;
+        // the handle is kept only once it is initialized: a failed call (bad
+        // mesh, inverted rest tet, out of memory) leaves none behind, so
+        // initialize() can be called again after the input is fixed
+        auto fail = [&](int rc) {
+            if (rc == WRAPD_OK) return;
+            const std::string msg = wrapd_last_error(h);
+            wrapd_destroy(h);
+            throw std::runtime_error(msg);
+        };
         for (const Mesh& m : m_meshes)
-            check(wrapd_add_tetmesh(m_h, m.rest.data(), m.init.data(), m.soln.empty() ? nullptr : m.soln.data(),
-                                    static_cast<int>(m.rest.size() / 3), m.tets.data(),
-                                    static_cast<int>(m.tets.size() / 4), m.pins.data(),
-                                    static_cast<int>(m.pins.size())));
-        check(wrapd_initialize(m_h));
+            fail(wrapd_add_tetmesh(h, m.rest.data(), m.init.data(), m.soln.empty() ? nullptr : m.soln.data(),
+                                   static_cast<int>(m.rest.size() / 3), m.tets.data(),
+                                   static_cast<int>(m.tets.size() / 4), m.pins.data(),
+                                   static_cast<int>(m.pins.size())));
+        fail(wrapd_initialize(h));
+        m_h = h;
         return true;
     }
 

@@ -13,6 +13,8 @@ ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
 LIBORACLE = os.path.join(ORACLE_DIR, "liboracle.so")
 REF_DIR = os.path.join(ORACLE_DIR, "_ref")
 QUASI_REF = os.path.join(REF_DIR, "quasi_ref")
+# The patched build (oracle/Makefile): global L-BFGS history 5, `-rw_every N`.
+QUASI_REF_M5 = os.path.join(REF_DIR, "quasi_ref_m5")
 LIBREF_ELEM = os.path.join(REF_DIR, "libref_elem.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -37,7 +39,7 @@ class OracleProblem(ctypes.Structure):
                 ("beta_static", ctypes.c_double), ("beta_min", ctypes.c_double),
                 ("beta_max", ctypes.c_double), ("rw_every", ctypes.c_int),
                 ("youngs_e", _dp), ("poisson_e", _dp), ("rot_aware", ctypes.c_int), ("model", ctypes.c_int),
-                ("global_ls", ctypes.c_int)]
+                ("global_ls", ctypes.c_int), ("linear_solver", ctypes.c_int)]
 
 
 _lib = None
@@ -99,8 +101,9 @@ class Oracle:
     def __init__(self, rest, init, tets, pins, youngs=1e5, poisson=0.45, max_iters=500, tol=1e-11,
                  lbfgs_m=6, reweighting=1, rw_delay=50, gamma=1.5, rw_every=0, global_iters=100,
                  kappa=1.0, beta_static=1.0, beta_min=0.1, beta_max=10.0, youngs_e=None, poisson_e=None,
-                 rot_aware=1, model=0, global_ls=0):
-        """youngs_e / poisson_e: per-element material (a batch of meshes), or None."""
+                 rot_aware=1, model=0, global_ls=0, linear_solver=0):
+        """youngs_e / poisson_e: per-element material (a batch of meshes), or None.
+        linear_solver = 1: conjugate gradients in place of the envelope LDL^T (large meshes)."""
         self.lib = load_oracle()
         self._keep = [np.ascontiguousarray(rest, dtype=np.float64),
                       np.ascontiguousarray(init, dtype=np.float64),
@@ -116,6 +119,7 @@ class Oracle:
         p.global_iters, p.kappa = global_iters, kappa
         p.beta_static, p.beta_min, p.beta_max = beta_static, beta_min, beta_max
         p.rot_aware, p.model, p.global_ls = rot_aware, model, global_ls
+        p.linear_solver = linear_solver
         if youngs_e is not None:
             self._keep += [np.ascontiguousarray(youngs_e, dtype=np.float64),
                            np.ascontiguousarray(poisson_e, dtype=np.float64)]
@@ -230,11 +234,12 @@ def load_ref_elem():
 
 
 def run_quasi_ref(bar_files: dict, youngs: float, poisson: float, max_iters: int, threads: int = 1,
-                  extra=(), outdir: str | None = None, timeout: float = 3600):
-    """Run the reference solver on .node/.ele/handles files; returns its logs."""
+                  extra=(), outdir: str | None = None, timeout: float = 3600, binary: str = QUASI_REF):
+    """Run the reference solver on .node/.ele/handles files; returns its logs.
+    binary = QUASI_REF_M5 runs the patched build (history 5, -rw_every)."""
     out = outdir or tempfile.mkdtemp(prefix="quasi_ref_")
     os.makedirs(out, exist_ok=True)
-    cmd = [QUASI_REF, "-rest", bar_files["rest"], "-init", bar_files["init"], "-handles", bar_files["handles"],
+    cmd = [binary, "-rest", bar_files["rest"], "-init", bar_files["init"], "-handles", bar_files["handles"],
            "-youngs", repr(float(youngs)), "-poisson", repr(float(poisson)), "-it", str(int(max_iters)),
            "-p", "0", "-out", out, *extra]
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))

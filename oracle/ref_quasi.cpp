@@ -10,7 +10,10 @@
 //     counts, the local/global delta-AL columns, the run times and the final
 //     positions as raw little-endian doubles (final_x.bin, n x 3 row-major);
 //   * the final mesh files (final_mesh.node/.ele/.obj) are written with the
-//     reference's own MeshIO calls, as quasi.cpp:113-130 does.
+//     reference's own MeshIO calls, as quasi.cpp:113-130 does;
+//   * built as quasi_ref_m5 (WRAPD_REF_PATCHED, the patched copy described in
+//     oracle/Makefile: global L-BFGS history 5), it also takes `-rw_every N`,
+//     which sets the reweight-every-N hook of the patched System.cpp.
 // Every other flag is handed to wrapd::Settings::parse_args unchanged.
 //
 // Only tests, the CPU baseline of bench.py and fixture generation run it.
@@ -51,6 +54,11 @@ void write_log(const std::string& path, const std::vector<T>& v) {
 
 }  // namespace
 
+#ifdef WRAPD_REF_PATCHED
+// Read by the patched System::possibly_update_weights (0: the gamma rule).
+int wrapd_ref_rw_every = 0;
+#endif
+
 int main(int argc, char** argv) {
     double youngs = 1.0e7;
     double poisson = 0.45;
@@ -61,6 +69,15 @@ int main(int argc, char** argv) {
         std::string a(argv[i]);
         if (a == "-youngs" && i + 1 < argc) { youngs = std::atof(argv[++i]); continue; }
         if (a == "-out" && i + 1 < argc) { outdir = argv[++i]; continue; }
+        if (a == "-rw_every" && i + 1 < argc) {
+#ifdef WRAPD_REF_PATCHED
+            wrapd_ref_rw_every = std::atoi(argv[++i]);
+            continue;
+#else
+            std::fprintf(stderr, "-rw_every needs the patched build (quasi_ref_m5)\n");
+            return EXIT_FAILURE;
+#endif
+        }
         if (a == "-poisson" && i + 1 < argc) poisson = std::atof(argv[i + 1]);
         pass.push_back(argv[i]);
     }

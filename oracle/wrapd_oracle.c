@@ -365,6 +365,10 @@ typedef struct {
     /* A values in (new) envelope layout, assembled per factorization */
     double* Aenv;
     double* Adiag;
+    /* linear_solver 1: A in CSR (row i: the diagonal, then adj of i in order) */
+    long* cptr;
+    int* ccol;
+    double* cval;
 } env_ldl;
 
 static int cmp_int(const void* a, const void* b) { return (*(const int*)a > *(const int*)b) - (*(const int*)a < *(const int*)b); }
@@ -372,6 +376,7 @@ static int cmp_int(const void* a, const void* b) { return (*(const int*)a > *(co
 static void env_free(env_ldl* f) {
     free(f->adj_ptr); free(f->adj); free(f->perm); free(f->iperm); free(f->first);
     free(f->rowptr); free(f->L); free(f->D); free(f->Aenv); free(f->Adiag);
+    free(f->cptr); free(f->ccol); free(f->cval);
     memset(f, 0, sizeof *f);
 }
 
@@ -726,6 +731,20 @@ static void build_pattern(orc_state* s) {
     np[n] = w;
     memcpy(f->adj_ptr, np, sizeof(int) * (size_t)(n + 1));
     free(np); free(deg); free(fill);
+    if (s->p.linear_solver == 1) {
+        /* CSR with the diagonal first in each row; no ordering, no envelope */
+        f->cptr = (long*)calloc((size_t)n + 1, sizeof(long));
+        for (int i = 0; i < n; ++i) f->cptr[i + 1] = f->cptr[i] + 1 + (f->adj_ptr[i + 1] - f->adj_ptr[i]);
+        f->ccol = NEWI(f->cptr[n]);
+        f->cval = NEWD(f->cptr[n]);
+        for (int i = 0; i < n; ++i) {
+            long o = f->cptr[i];
+            f->ccol[o++] = i;
+            for (int k = f->adj_ptr[i]; k < f->adj_ptr[i + 1]; ++k) f->ccol[o++] = f->adj[k];
+        }
+        f->D = NEWD(n);
+        return;
+    }
     f->perm = NEWI(n); f->iperm = NEWI(n);
     rcm(n, f->adj_ptr, f->adj, f->perm);
     for (int i = 0; i < n; ++i) f->iperm[f->perm[i]] = i;
@@ -767,9 +786,41 @@ static void assemble_A(orc_state* s) {
             }
 }
 
+/* The same values as a full symmetric CSR matrix (both triangles). */
+static int csr_slot(const env_ldl* f, int i, int j) {
+    long lo = f->cptr[i] + 1, hi = f->cptr[i + 1] - 1;   /* neighbours are sorted */
+    if (i == j) return 0;
+    while (lo <= hi) {
+        long m = (lo + hi) / 2;
+        if (f->ccol[m] == j) return (int)(m - f->cptr[i]);
+        if (f->ccol[m] < j) lo = m + 1; else hi = m - 1;
+    }
+    return -1;
+}
+
+static int assemble_A_csr(orc_state* s) {
+    env_ldl* f = &s->A;
+    memset(f->cval, 0, sizeof(double) * (size_t)f->cptr[f->n]);
+    for (int e = 0; e < s->ne; ++e)
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) {
+                int i = s->fidx[4 * e + a], j = s->fidx[4 * e + b];
+                if (i < 0 || j < 0 || i > j) continue;
+                double v = s->w2[e] * s->DtD[16 * e + a + 4 * b];
+                f->cval[f->cptr[i] + csr_slot(f, i, j)] += v;
+                if (i != j) f->cval[f->cptr[j] + csr_slot(f, j, i)] += v;
+            }
+    for (int i = 0; i < f->n; ++i) {
+        f->D[i] = f->cval[f->cptr[i]];
+        if (!(f->D[i] > 0.0)) return E_NOT_SPD;
+    }
+    return E_OK;
+}
+
 /* Up-looking envelope LDL^T. */
 static int factor_A(orc_state* s) {
     env_ldl* f = &s->A;
+    if (s->p.linear_solver == 1) return assemble_A_csr(s);
     assemble_A(s);
     for (int i = 0; i < f->n; ++i) {
         double* Li = f->L + f->rowptr[i];
@@ -791,9 +842,95 @@ static int factor_A(orc_state* s) {
     return E_OK;
 }
 
+/* Column c of y = A x (n x 3 row-major blocks), rows split over host threads. */
+static void csr_mv(const env_ldl* f, const double* x, double* y) {
+    #pragma omp parallel for schedule(static)
+    for (int i = 0; i < f->n; ++i) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (long k = f->cptr[i]; k < f->cptr[i + 1]; ++k) {
+            const double v = f->cval[k];
+            const double* xj = x + 3L * f->ccol[k];
+            a0 += v * xj[0]; a1 += v * xj[1]; a2 += v * xj[2];
+        }
+        y[3L * i] = a0; y[3L * i + 1] = a1; y[3L * i + 2] = a2;
+    }
+}
+
+/* Per-column dot products of two n x 3 blocks: fixed chunks, partials summed in
+ * chunk order (the same result for any thread count). */
+static void dot3n(int n, const double* a, const double* b, double out[3]) {
+    enum { CH = 4096 };
+    const int nch = (n + CH - 1) / CH;
+    double* part = NEWD(3L * nch);
+    #pragma omp parallel for schedule(static)
+    for (int c = 0; c < nch; ++c) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        const int hi = (c + 1) * CH < n ? (c + 1) * CH : n;
+        for (int i = c * CH; i < hi; ++i) {
+            s0 += a[3L * i] * b[3L * i]; s1 += a[3L * i + 1] * b[3L * i + 1]; s2 += a[3L * i + 2] * b[3L * i + 2];
+        }
+        part[3 * c] = s0; part[3 * c + 1] = s1; part[3 * c + 2] = s2;
+    }
+    out[0] = out[1] = out[2] = 0.0;
+    for (int c = 0; c < nch; ++c) { out[0] += part[3 * c]; out[1] += part[3 * c + 1]; out[2] += part[3 * c + 2]; }
+    free(part);
+}
+
+/* x = A^-1 b by Jacobi-preconditioned conjugate gradients, the three columns
+ * side by side, to |b - A x| <= 1e-14 |b| per column (restarted from the true
+ * residual when the recurrence has drifted). */
+static void cg_solve(orc_state* s, const double* b, double* x) {
+    env_ldl* f = &s->A;
+    const int n = f->n;
+    const size_t m = 3 * (size_t)n;
+    double *r = NEWD(m), *z = NEWD(m), *p = NEWD(m), *q = NEWD(m), *xx = NEWD(m);
+    double bb[3], tol2[3];
+    dot3n(n, b, b, bb);
+    for (int c = 0; c < 3; ++c) tol2[c] = 1e-28 * bb[c];
+    for (int restart = 0; restart < 4; ++restart) {
+        csr_mv(f, xx, q);
+        for (size_t i = 0; i < m; ++i) r[i] = b[i] - q[i];
+        double rr[3];
+        dot3n(n, r, r, rr);
+        if (rr[0] <= tol2[0] && rr[1] <= tol2[1] && rr[2] <= tol2[2]) break;
+        for (int i = 0; i < n; ++i) for (int c = 0; c < 3; ++c) z[3L * i + c] = r[3L * i + c] / f->D[i];
+        memcpy(p, z, sizeof(double) * m);
+        double rz[3];
+        dot3n(n, r, z, rz);
+        int done[3] = {rr[0] <= tol2[0], rr[1] <= tol2[1], rr[2] <= tol2[2]};
+        for (int it = 0; it < 50000 && !(done[0] && done[1] && done[2]); ++it) {
+            csr_mv(f, p, q);
+            double pq[3], al[3];
+            dot3n(n, p, q, pq);
+            for (int c = 0; c < 3; ++c) al[c] = done[c] ? 0.0 : rz[c] / pq[c];
+            #pragma omp parallel for schedule(static)
+            for (int i = 0; i < n; ++i)
+                for (int c = 0; c < 3; ++c) {
+                    xx[3L * i + c] += al[c] * p[3L * i + c];
+                    r[3L * i + c] -= al[c] * q[3L * i + c];
+                    z[3L * i + c] = r[3L * i + c] / f->D[i];
+                }
+            double rz2[3], be[3];
+            dot3n(n, r, z, rz2);
+            dot3n(n, r, r, rr);
+            for (int c = 0; c < 3; ++c) {
+                if (rr[c] <= tol2[c]) done[c] = 1;
+                be[c] = done[c] ? 0.0 : rz2[c] / rz[c];
+                rz[c] = rz2[c];
+            }
+            #pragma omp parallel for schedule(static)
+            for (int i = 0; i < n; ++i)
+                for (int c = 0; c < 3; ++c) p[3L * i + c] = z[3L * i + c] + be[c] * p[3L * i + c];
+        }
+    }
+    memcpy(x, xx, sizeof(double) * m);
+    free(r); free(z); free(p); free(q); free(xx);
+}
+
 void orc_solve_A(orc_state* s, const double* b, double* x) {
     env_ldl* f = &s->A;
     int n = f->n;
+    if (s->p.linear_solver == 1) { cg_solve(s, b, x); return; }
     double* z = NEWD(3 * n);
     for (int i = 0; i < n; ++i) for (int c = 0; c < 3; ++c) z[3 * i + c] = b[3 * f->perm[i] + c];
     for (int i = 0; i < n; ++i) {

@@ -47,6 +47,9 @@ typedef struct {
     int rot_aware;        /* -ra      (1); 0 = UnawareGS (src/GlobalStepBehavior.hpp:118-193) */
     int model;            /* -model   (0 = nh, 1 = arap) */
     int global_ls;        /* -global_ls (0); 1 = Backtracking Armijo line search in the global step */
+    int linear_solver;    /* 0: envelope LDL^T (default); 1: Jacobi-preconditioned conjugate gradients to a
+                             relative residual of 1e-14, for systems whose envelope factor does not fit in
+                             memory (the 3.9M-tet bar); same solve up to that residual */
 } orc_problem;
 
 void orc_problem_defaults(orc_problem* p);

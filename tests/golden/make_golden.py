@@ -19,8 +19,23 @@ Outputs (all seeded, reproducible):
                     search shortens steps from iteration 33 on)
   quasi_small.npz   the reference front end's output files for a small bar: the
                     logs, final_mesh.node/.ele/.obj, without and with -soln
+  solve_bar_32x32x128_bent.npz
+                    the benchmarked configuration: the 786,432-tet bar (360 deg
+                    twist + 90 deg bend), 20 ADMM iterations of the patched
+                    reference (quasi_ref_m5: L-BFGS history 5, reweight and
+                    refactor every 10 iterations), and 60 iterations of the
+                    unpatched reference (history 6, gamma rule); one thread
+                    each (the deterministic reference), about 30 min of CPU
+  iters_bar_64x64x160.npz
+                    the 3.9M-tet bar (720 deg twist): the first three ADMM
+                    iterations (L-BFGS history 5, FP64) of the oracle, the C
+                    restatement pinned against the reference by the files above,
+                    with its conjugate-gradient linear solver (the reference's
+                    simplicial factorization of 671,775 unknowns, and the
+                    oracle's envelope one, do not fit in this host's memory);
+                    positions at 16,384 seeded vertices and per-column sums
 
-    python tests/golden/make_golden.py [--only modes|gls|quasi]
+    python tests/golden/make_golden.py [--only modes|gls|quasi|bar_32x32x128_bent|bar_64x64x160]
 """
 from __future__ import annotations
 
@@ -117,10 +132,26 @@ def tiny_step(ref):
                         pins=b.pins, dal=dal[0], grad=g, value=val[0], pe=pe[0], flips=flips[0], grad2=g2)
 
 
-def ref_solve(bar, max_iters, extra=()):
+def ref_solve(bar, max_iters, extra=(), binary=po.QUASI_REF):
     with tempfile.TemporaryDirectory() as d:
         files = bars.write_bar(bar, d, "m")
-        return po.run_quasi_ref(files, E_YOUNG, NU, max_iters, threads=1, extra=list(extra), outdir=d + "/out")
+        return po.run_quasi_ref(files, E_YOUNG, NU, max_iters, threads=1, extra=list(extra), outdir=d + "/out",
+                                timeout=24 * 3600, binary=binary)
+
+
+def bar_32x32x128_bent():
+    """The benchmarked bar against the reference itself, both builds."""
+    b = bars.bar_32x32x128_bent()
+    out = {}
+    for tag, it, extra, binary in [("m5", 20, ("-rw_every", "10"), po.QUASI_REF_M5), ("m6", 60, (), po.QUASI_REF)]:
+        r = ref_solve(b, it, extra, binary)
+        out.update({f"{tag}_objectives": r["objectives"], f"{tag}_inner": r["inner_iters"],
+                    f"{tag}_reweighted": r["reweighted"], f"{tag}_x": r["x"],
+                    f"{tag}_ls_dal": r["ls_delta_al"], f"{tag}_gs_dal": r["gs_delta_al"],
+                    f"{tag}_setup_ms": r["runtime"]["setup_ms"],
+                    f"{tag}_acc_time_s": r["accumulated_time_s"]})
+        print(tag, "done:", r["runtime"], flush=True)
+    np.savez_compressed(os.path.join(HERE, "solve_bar_32x32x128_bent.npz"), **out)
 
 
 def solves():
@@ -176,6 +207,24 @@ def quasi_files():
     np.savez_compressed(os.path.join(HERE, "quasi_small.npz"), **out)
 
 
+X_SAMPLE_64x64x160 = 16384
+
+
+def bar_64x64x160():
+    """Three oracle iterations on the 3.9M-tet bar (the oracle, not the reference:
+    see the module docstring)."""
+    b = bars.bar_64x64x160()
+    o = po.Oracle(b.rest, b.init, b.tets, b.pins, youngs=E_YOUNG, poisson=NU, max_iters=3, lbfgs_m=5, rw_every=20,
+                  linear_solver=1)
+    o.solve()
+    X = o.get("X").reshape(-1, 3)
+    idx = np.sort(np.random.default_rng(64160).choice(b.n_verts, X_SAMPLE_64x64x160, replace=False))
+    np.savez_compressed(os.path.join(HERE, "iters_bar_64x64x160.npz"), objectives=o.get("objectives"),
+                        inner=o.get("inner_iters").astype(np.int32), flips=o.get("flips").astype(np.int32),
+                        ls_dal=o.get("ls_dal"), gs_dal=o.get("gs_dal"), x_idx=idx, x_sample=X[idx],
+                        x_colsum=X.sum(axis=0), x_absmax=np.abs(X).max())
+
+
 def main():
     if not po.ref_available():
         raise SystemExit("oracle/_ref is not built: run `make -C oracle ref` (needs the reference sources)")
@@ -185,6 +234,14 @@ def main():
         return
     if sys.argv[1:] == ["--only", "gls"]:
         global_ls()
+        print("golden vectors written to", HERE)
+        return
+    if sys.argv[1:] == ["--only", "bar_64x64x160"]:
+        bar_64x64x160()
+        print("golden vectors written to", HERE)
+        return
+    if sys.argv[1:] == ["--only", "bar_32x32x128_bent"]:
+        bar_32x32x128_bent()
         print("golden vectors written to", HERE)
         return
     if sys.argv[1:] == ["--only", "quasi"]:
@@ -199,6 +256,8 @@ def main():
     modes()
     global_ls()
     quasi_files()
+    bar_32x32x128_bent()
+    bar_64x64x160()
     print("golden vectors written to", HERE)
 
 

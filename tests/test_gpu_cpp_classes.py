@@ -48,3 +48,29 @@ def test_cpp_solver_matches_the_python_mirror(lib_built, tmp_path):
     assert np.array_equal(obj_cpp, d.objectives)
     assert np.array_equal(x_cpp, x)
     s.close()
+
+
+QUASI_COMPAT = os.path.join(ROOT, "oracle", "_ref", "quasi_compat")
+
+
+def test_reference_front_end_on_the_dropin_headers(lib_built, golden, tmp_path):
+    """The reference's samples/tests/quasi.cpp, unchanged, built against
+    include/wrapd and the GPU library (oracle/_ref/quasi_compat, made where the
+    reference sources are present), run on the small bar: its own log and mesh
+    writers give the reference's files (tests/golden/quasi_small.npz) within
+    the FP64 parity tolerances of test_gpu_quasi.py."""
+    from test_gpu_quasi import _compare
+    if not os.path.exists(QUASI_COMPAT):
+        pytest.skip("oracle/_ref/quasi_compat not built (needs the reference sources)")
+    b = bars.make_bar(3, 3, 8, twist_deg=90.0, noise=0.02, seed=5)
+    files = bars.write_bar(b, str(tmp_path), "q")
+    run = tmp_path / "run"
+    run.mkdir()
+    r = subprocess.run([QUASI_COMPAT, "-rest", files["rest"], "-init", files["init"], "-handles", files["handles"],
+                        "-youngs", "1e5", "-poisson", "0.45", "-it", "40", "-p", "0", "-s", "1"],
+                       capture_output=True, text=True, timeout=300, cwd=str(run))
+    assert r.returncode == 0, r.stdout + r.stderr
+    ours = {name: (run / (name if "." in name else name + ".txt")).read_text()
+            for name in ("objectives", "x_errors", "reweighted", "final_mesh.node", "final_mesh.ele",
+                         "final_mesh.obj")}
+    _compare(golden("quasi_small.npz"), "plain", ours)
