@@ -81,8 +81,9 @@ typedef struct wrapd_settings {
     int device;           /* CUDA device ordinal, 0 */
     int autotune;         /* 0; 1: wrapd_initialize times the candidate tile shapes of the triangular
                              solve (chunk length per level and direction) and of the factorization's
-                             panel steps (fused or split, by the number of tiles) on this system and
-                             keeps the fastest (see wrapd_get_tuning) */
+                             panel steps (fused or split, by the number of tiles), and the first
+                             wrapd_begin_solve the local step's tile (64, 128 or 256 elements per
+                             CTA), on this system, and keeps the fastest (see wrapd_get_tuning) */
 } wrapd_settings;
 
 typedef struct wrapd_handle wrapd_handle;
@@ -112,11 +113,17 @@ WRAPD_API int wrapd_create(const wrapd_settings* s, wrapd_handle** out);
  * src/TetElements.hpp:250-288, src/System.cpp:33-44).  Pins are vertex ids
  * held in place at init_xyz.  soln_xyz may be NULL.  Called again before
  * wrapd_initialize, it appends another mesh (vertex ids of each call are its
- * own, shifted as add_tetmesh's prev_tet_verts does): the meshes form a batch
- * solved as one block-diagonal system -- one local-step launch over all their
- * elements, one factorization holding one tree per mesh.  (The reference's
- * add_tetmesh replaces the element set on a second call; the batch is an
- * extension.)  Positions of the batch are returned in the order added. */
+ * own, shifted as add_tetmesh's prev_tet_verts does): the meshes form a
+ * batch.  Each mesh is solved as the reference solves it alone -- its own
+ * L-BFGS history, early exits, reweighting decisions and convergence test,
+ * bit for bit the same as a handle holding that mesh only -- while the work
+ * of all of them shares the launches: one local-step and one gradient launch
+ * over the unconverged meshes' element tiles, one factorization holding one
+ * tree per mesh.  A converged mesh drops out of the launches.  Batches take
+ * the rotation-aware global step without line search (rot_aware = 1,
+ * global_ls = 0; others give WRAPD_E_UNSUPPORTED at wrapd_initialize).  (The
+ * reference's add_tetmesh replaces the element set on a second call; the
+ * batch is an extension.)  Positions are returned in the order added. */
 WRAPD_API int wrapd_add_tetmesh(wrapd_handle* h, const double* rest_xyz, const double* init_xyz,
                       const double* soln_xyz, int n_verts, const int32_t* tets, int n_tets,
                       const int32_t* pins, int n_pins);
@@ -152,6 +159,16 @@ WRAPD_API int wrapd_get_positions(wrapd_handle* h, double* x_out);
  * to cap entries into out; *len receives the channel's length. */
 WRAPD_API int wrapd_get_log(wrapd_handle* h, int which, double* out, int cap, int* len);
 
+/* The log channel of one mesh of a batch (meshes numbered in the order they
+ * were added): each mesh is an independent ADMM solve -- its own L-BFGS
+ * history and early exits, reweighting decisions and convergence test, as a
+ * reference Solver holding that mesh alone -- and stops logging when it
+ * converges.  wrapd_get_log gives, for a batch, the sums over its meshes of
+ * the energies, flips, inner iterations and |delta AL|, 1 where any mesh
+ * reweighted, and the batch's x error.  (No reference counterpart: the
+ * reference solves one mesh per Solver.) */
+WRAPD_API int wrapd_get_mesh_log(wrapd_handle* h, int mesh, int which, double* out, int cap, int* len);
+
 /* RuntimeData (src/RuntimeData.hpp:30-44): ms[0..5] = setup, local, global,
  * refactor, finish, inner iterations (as a double).  Device times from CUDA
  * events on the handle's stream. */
@@ -169,8 +186,10 @@ WRAPD_API int wrapd_get_counters(wrapd_handle* h, int64_t out[4]);
 /* The tile shapes in use (no reference counterpart): out[0] = the largest
  * panel step (in tiles) whose diagonal block is factored inside the tile
  * launch, out[1] = levels L, then L forward and L backward solve chunk
- * lengths.  *len receives 2 + 2 L.  Chosen by timing when autotune = 1, by
- * fixed rules otherwise. */
+ * lengths (0: each mesh of a batch takes its own), then the local step's
+ * tile (elements per CTA).  *len receives 3 + 2 L.  Chosen by timing when
+ * autotune = 1 (the local tile at the first wrapd_begin_solve), by fixed
+ * rules otherwise. */
 WRAPD_API int wrapd_get_tuning(wrapd_handle* h, int* out, int cap, int* len);
 
 /* Per-phase device timeline (no reference counterpart; the reference's
@@ -254,7 +273,9 @@ WRAPD_API int wrapd_potential_energy_batch(int n, double mu, double lambda, cons
  *   1 MiB inside the library, held by every GPU that loads it until exit.
  *   n may be at most 16,777,216; larger n returns WRAPD_E_INPUT without work.
  *   The first call on each device looks up that array's device address (with
- *   the device current); make that first call before any stream capture.
+ *   the device current); make that first call before any stream capture.  The
+ *   address is kept for the life of the process: do not call this entry point
+ *   after resetting the device (cudaDeviceReset) in the same process.
  *   All calls share the one array: calls that overlap on the GPU (other
  *   streams or threads) race and give wrong sums, so serialise them. */
 WRAPD_API int wrapd_potential_energy_batch_noalloc(int n, double mu, double lambda, const double* d_sigma,

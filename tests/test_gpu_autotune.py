@@ -1,6 +1,7 @@
 """The tile-shape autotuner (settings.autotune = 1): wrapd_initialize times the
 solve's candidate chunk lengths per level and direction and the panel-step
-forms of the factorization on the system at hand, then keeps the fastest.  The
+forms of the factorization on the system at hand, and the first begin_solve
+the local step's tile (elements per CTA), then keeps the fastest.  The
 choice changes only the order of partial sums, so the tuned solver must meet
 the same FP64 bar against the reference as the fixed rules (positions within
 1e-8 of max |x|, identical iteration counts), and report shapes from the
@@ -41,9 +42,11 @@ def test_autotuned_solve_matches_reference(golden):
     assert len(t["solve_chunk_fwd"]) == len(t["solve_chunk_bwd"]) == t["levels"]
     assert set(t["solve_chunk_fwd"]) | set(t["solve_chunk_bwd"]) <= {256, 128, 64}
     assert t["fused_panel_ctas"] in (0, 148, 592, 2368, 1 << 30)
+    assert t["local_tile"] in (64, 128, 256)
 
 
 def test_fixed_rules_reported_without_autotune():
     _, _, t, _ = _solve(0, iters=3)
     assert t["fused_panel_ctas"] == 592
+    assert t["local_tile"] == 128
     assert all(c in (256, 128, 64) for c in t["solve_chunk_fwd"] + t["solve_chunk_bwd"])

@@ -19,6 +19,7 @@ ERRORS = {
     -5: "WRAPD_E_PROX_NEG", -6: "WRAPD_E_TIMEOUT", -7: "WRAPD_E_OOM", -8: "WRAPD_E_CUDA",
     -9: "WRAPD_E_STATE", -10: "WRAPD_E_UNSUPPORTED",
 }
+globals().update({name: code for code, name in ERRORS.items()})   # WRAPD_E_INPUT = -1, ...
 LOGS = {"objectives": 0, "reweighted": 1, "flips": 2, "inner_iters": 3, "ls_delta_al": 4,
         "gs_delta_al": 5, "accumulated_time_s": 6, "x_errors": 7, "prox_iters": 8}
 NET_BLOB = 4755
@@ -65,6 +66,8 @@ SIGNATURES = [
     ("wrapd_get_positions", ctypes.c_int, [ctypes.c_void_p, _dp]),
     ("wrapd_get_log", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_int)]),
+    ("wrapd_get_mesh_log", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_int)]),
     ("wrapd_get_runtime", ctypes.c_int, [ctypes.c_void_p, _dp]),
     ("wrapd_get_info", ctypes.c_int, [ctypes.c_void_p, _dp]),
     ("wrapd_get_counters", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),

@@ -144,9 +144,8 @@ int wrapd_set_prox_net(wrapd_handle* h, const float* blob, int n_blob) {
     return guarded(h, [&](wrapd::SolverGPU& s) { s.set_prox_net(blob); });
 }
 
-int wrapd_get_log(wrapd_handle* h, int which, double* out, int cap, int* len) {
-    return guarded(h, [&](wrapd::SolverGPU& s) {
-        const wrapd::Logs& L = s.logs();
+namespace {
+int copy_log(const wrapd::Logs& L, int which, double* out, int cap, int* len) {
         std::vector<double> v;
         switch (which) {
             case WRAPD_LOG_OBJECTIVES: v = L.objectives; break;
@@ -163,6 +162,18 @@ int wrapd_get_log(wrapd_handle* h, int which, double* out, int cap, int* len) {
         if (len) *len = static_cast<int>(v.size());
         if (out)
             for (int i = 0; i < cap && i < (int)v.size(); ++i) out[i] = v[i];
+        return 0;
+}
+}  // namespace
+
+int wrapd_get_log(wrapd_handle* h, int which, double* out, int cap, int* len) {
+    return guarded(h, [&](wrapd::SolverGPU& s) { copy_log(s.logs(), which, out, cap, len); });
+}
+
+int wrapd_get_mesh_log(wrapd_handle* h, int mesh, int which, double* out, int cap, int* len) {
+    return guarded(h, [&](wrapd::SolverGPU& s) {
+        if (!s.initialized()) throw wrapd::CudaError(WRAPD_E_STATE, "mesh logs before initialize");
+        copy_log(s.mesh_logs(mesh), which, out, cap, len);
     });
 }
 
@@ -194,7 +205,8 @@ int wrapd_set_profiling(wrapd_handle* h, int on) {
 int wrapd_get_tuning(wrapd_handle* h, int* out, int cap, int* len) {
     if (!len || (cap > 0 && !out)) return WRAPD_E_INPUT;
     return guarded(h, [&](wrapd::SolverGPU& s) {
-        const std::vector<int> t = s.chol.tuning();
+        std::vector<int> t = s.chol.tuning();
+        t.push_back(s.local_tile());
         *len = (int)t.size();
         for (int i = 0; i < (int)t.size() && i < cap; ++i) out[i] = t[i];
     });

@@ -302,7 +302,14 @@ __global__ void k_extend_add(double* __restrict__ F, const FrontDesc* __restrict
 // Row s of inv(L) is written to X (pitch xp), columns < nb.  A non-positive
 // (or NaN) pivot sets *bad and continues with a unit pivot.
 constexpr int LSP = NB + 1;
-static_assert(GEMM_THREADS == 128 && NB == 32, "cta_chol_inv maps 128 threads onto 32 rows x 4 column slices");
+static_assert(GEMM_THREADS == 128 && NB == 32, "cta_chol_inv: one warp, one row (then one column) per lane");
+// Warp 0 does both sweeps; the other warps only load the block and wait.
+// Lane i owns row i in the Cholesky sweep (S(i, c) -= t_i S(c, j), with S(c,
+// j) a broadcast read) and column c = i in the inverse sweep (P(r, c) +=
+// L(r, s) f_c, L(r, s) a broadcast read).  Each entry sees the same fma, with
+// the same operands in the same order, as in a 128-thread sweep, so L, D and
+// inv(L) are those of the one-barrier-per-pivot form, with no CTA barrier
+// inside the sweeps (__syncwarp between pivots).
 __device__ __forceinline__ void cta_chol_inv(const double* __restrict__ Fd, int64_t ld, int nb, double* S,
                                              double* Lsm, int lp, double* D, double* X, int xp, bool* bad) {
     const int tid = threadIdx.x;
@@ -311,50 +318,39 @@ __device__ __forceinline__ void cta_chol_inv(const double* __restrict__ Fd, int6
         S[i * LSP + c] = (i < nb && c <= i) ? Fd[i + (int64_t)c * ld] : 0.0;
     }
     __syncthreads();
-    const int i = tid & 31, q = tid >> 5;
     bool b = false;
-    for (int j = 0; j < nb; ++j) {
-        double piv = S[j * LSP + j];
-        const double sij = S[i * LSP + j];
-        double cj[8], ic[8];
-#pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            cj[m] = S[(q + 4 * m) * LSP + j];
-            ic[m] = S[i * LSP + q + 4 * m];
+    if (tid < 32) {
+        const int i = tid;
+        double* Si = S + i * LSP;
+#pragma unroll 1
+        for (int j = 0; j < nb; ++j) {
+            double piv = S[j * LSP + j];
+            const double sij = Si[j];
+            if (!(piv > 0.0)) { b = true; piv = 1.0; }
+            const double rs = rsqrt(piv);
+            if (i >= j && i < nb) Lsm[i * lp + j] = i == j ? piv * rs : sij * rs;
+            if (i == 0) D[j] = rs;
+            const double t = sij * (rs * rs);
+            if (i > j && i < nb) {
+#pragma unroll 4
+                for (int c = j + 1; c <= i; ++c) Si[c] = fma(-t, S[c * LSP + j], Si[c]);
+            }
+            __syncwarp();
         }
-        if (!(piv > 0.0)) { b = true; piv = 1.0; }
-        const double rs = rsqrt(piv);
-        if (q == 0 && i >= j && i < nb) Lsm[i * lp + j] = i == j ? piv * rs : sij * rs;
-        if (tid == 0) D[j] = rs;
-        const double t = sij * (rs * rs);
-#pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            const int c = q + 4 * m;
-            if (c > j && c <= i && i < nb) S[i * LSP + c] = fma(-t, cj[m], ic[m]);
+        for (int idx = i; idx < NB * LSP; idx += 32) S[idx] = 0.0;
+        __syncwarp();
+        const int c = i;
+#pragma unroll 1
+        for (int s = 0; s < nb; ++s) {
+            const double ps = S[s * LSP + c];
+            const double f = (c <= s) ? ((c == s ? 1.0 : 0.0) - ps) * D[s] : 0.0;
+            if (c < nb) X[s * xp + c] = f;
+#pragma unroll 4
+            for (int r = s + 1; r < nb; ++r) S[r * LSP + c] = fma(Lsm[r * lp + s], f, S[r * LSP + c]);
+            __syncwarp();
         }
-        __syncthreads();
     }
-    for (int idx = tid; idx < NB * NB; idx += GEMM_THREADS) S[(idx >> 5) * LSP + (idx & 31)] = 0.0;
     __syncthreads();
-    const int c = tid & 31;
-    for (int s = 0; s < nb; ++s) {
-        const double ps = S[s * LSP + c];
-        const double ds = D[s];
-        double lr[8], pr[8];
-#pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            lr[m] = Lsm[(q + 4 * m) * lp + s];
-            pr[m] = S[(q + 4 * m) * LSP + c];
-        }
-        const double f = (c <= s) ? ((c == s ? 1.0 : 0.0) - ps) * ds : 0.0;
-        if (q == 0 && c < nb) X[s * xp + c] = f;
-#pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            const int r = q + 4 * m;
-            if (r > s && r < nb) S[r * LSP + c] = fma(lr[m], f, pr[m]);
-        }
-        __syncthreads();
-    }
     *bad = b;
 }
 
@@ -1051,11 +1047,12 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
             const FrontDesc& d = h_desc_[fs[q]];
             wg[q] = ceil_div(d.r, TL) * ceil_div(d.k, TL);
         }
-        // Solve items with chunks of `sch` (<= SCH) along the streamed dimension.
-        auto fwd_items = [&](int sch, std::vector<SolveItem>& fwd, int& fbands) {
+        // Solve items with chunks of sch_of(front) (<= SCH) along the streamed dimension.
+        auto fwd_items = [&](auto sch_of, std::vector<SolveItem>& fwd, int& fbands) {
             fwd.clear();
             fbands = 0;
             for (int f : fs) {
+                const int sch = sch_of(f);
                 const FrontDesc& d = h_desc_[f];
                 const int R = d.k + d.r;
                 // forward: row bands; Y bands use columns up to their last row
@@ -1068,10 +1065,11 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
                 }
             }
         };
-        auto bwd_items = [&](int sch, std::vector<SolveItem>& bwd, int& bbands) {
+        auto bwd_items = [&](auto sch_of, std::vector<SolveItem>& bwd, int& bbands) {
             bwd.clear();
             bbands = 0;
             for (int f : fs) {
+                const int sch = sch_of(f);
                 const FrontDesc& d = h_desc_[f];
                 const int R = d.k + d.r;
                 // backward: column bands over rows [b0, R) (Y rows below the band, then the W rows)
@@ -1093,18 +1091,47 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         int fbands = 0, bbands = 0;
         L.cfwd = -1;
         L.cbwd = -1;
+        // per mesh of a batch: its item counts for each candidate (the rule
+        // below applied to the mesh alone)
+        const int nmesh = front_mesh.empty() ? 1 : 1 + *std::max_element(front_mesh.begin(), front_mesh.end());
+        std::vector<std::vector<int>> mfwd(nmesh), mbwd(nmesh);
         for (int sch = SCH, c = 0; sch >= SCH_MIN; sch /= 2, ++c) {
-            fwd_items(sch, fwd, fbands);
-            bwd_items(sch, bwd, bbands);
+            fwd_items([&](int) { return sch; }, fwd, fbands);
+            bwd_items([&](int) { return sch; }, bwd, bbands);
             L.cand.push_back({sch, upload(fwd, st), static_cast<int>(fwd.size()), upload(bwd, st),
                               static_cast<int>(bwd.size())});
             if (L.cfwd < 0 && (int)fwd.size() >= kSolveCtas) L.cfwd = c;
             if (L.cbwd < 0 && (int)bwd.size() >= kSolveCtas) L.cbwd = c;
             solve_parts_ = std::max<int64_t>(solve_parts_, std::max<int64_t>(fwd.size(), bwd.size()));
             solve_bands_ = std::max(solve_bands_, std::max(fbands, bbands));
+            if (nmesh > 1) {
+                for (int m = 0; m < nmesh; ++m) { mfwd[m].push_back(0); mbwd[m].push_back(0); }
+                for (const SolveItem& it : fwd) mfwd[front_mesh[it.front]][c]++;
+                for (const SolveItem& it : bwd) mbwd[front_mesh[it.front]][c]++;
+            }
         }
         if (L.cfwd < 0) L.cfwd = 0;
         if (L.cbwd < 0) L.cbwd = 0;
+        if (nmesh > 1) {
+            // a batch: every front takes its own mesh's choice
+            std::vector<int> sf(nmesh, SCH), sb(nmesh, SCH);
+            for (int m = 0; m < nmesh; ++m) {
+                int cf = -1, cb = -1;
+                for (int c = 0; c < (int)mfwd[m].size(); ++c) {
+                    if (cf < 0 && mfwd[m][c] >= kSolveCtas) cf = c;
+                    if (cb < 0 && mbwd[m][c] >= kSolveCtas) cb = c;
+                }
+                sf[m] = SCH >> std::max(cf, 0);
+                sb[m] = SCH >> std::max(cb, 0);
+            }
+            fwd_items([&](int f) { return sf[front_mesh[f]]; }, fwd, fbands);
+            bwd_items([&](int f) { return sb[front_mesh[f]]; }, bwd, bbands);
+            L.cand.push_back({0, upload(fwd, st), static_cast<int>(fwd.size()), upload(bwd, st),
+                              static_cast<int>(bwd.size())});
+            L.cfwd = L.cbwd = static_cast<int>(L.cand.size()) - 1;
+            solve_parts_ = std::max<int64_t>(solve_parts_, std::max<int64_t>(fwd.size(), bwd.size()));
+            solve_bands_ = std::max(solve_bands_, std::max(fbands, bbands));
+        }
         L.wgemm = make_list(fs, wg, st);
     }
     trsm_nP_.clear();
@@ -1166,7 +1193,9 @@ void CholGPU::autotune(const double* d_w2, const double* d_Di, int ne, cudaStrea
         WRAPD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         return ms / reps;
     };
+    // (a batch keeps its per-mesh chunk lengths: a mesh's solve stays its own)
     for (Level& L : levels_) {
+        if (!front_mesh.empty()) break;
         float best_f = 1e30f, best_b = 1e30f;
         for (int c = 0; c < (int)L.cand.size(); ++c) {
             const Level::SolveCand& C = L.cand[c];

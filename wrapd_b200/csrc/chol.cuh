@@ -93,6 +93,11 @@ public:
     // [fused panel-step limit, levels, forward chunk per level..., backward chunk per level...]
     std::vector<int> tuning() const;
 
+    // Per front, the mesh of a batch it belongs to (empty: one mesh).  Set
+    // before build(): each mesh's solve then takes the chunk lengths it would
+    // take alone, so its partial sums, and results, are those of its own solve.
+    std::vector<int> front_mesh;
+
     int n = 0;
     int* d_status = nullptr;
     int64_t nnz_L = 0;

@@ -103,4 +103,79 @@ __device__ __forceinline__ void grid_reduce(const double (&v)[NV], double* parti
     if (threadIdx.x == 0) *counter = 0u;
 }
 
+// ---- launches over a batch of meshes ----------------------------------------
+// A launch's blocks are tiles: tile b covers items [first, end) of one mesh
+// (elements, free vertices or vector entries; each mesh's items are a
+// contiguous range).  With a table (t != null) tile b is t[b] = {mesh, first,
+// end}; without one (a single mesh) tile b covers [b * per, (b + 1) * per) of
+// [0, n).  Every mesh's tiles start at its own first item, so a mesh's blocks
+// in a batch do exactly the work of the same mesh's blocks when it is solved
+// alone, and the per-mesh sums below add the same partials in the same order:
+// a mesh's results in a batch equal its results alone, bit for bit.
+struct Tiles {
+    const int4* t;       // per tile {mesh, first, end, 0}, or null (one mesh)
+    const int* tile0;    // per mesh its first tile, nm + 1 entries (with t)
+    int n, per;          // one mesh: item count and items per tile
+    int count;           // tiles of the launch
+};
+struct Tile {
+    int mesh, first, end;
+};
+__device__ __forceinline__ Tile tile_at(const Tiles& T, int b) {
+    if (T.t) {
+        const int4 v = T.t[b];
+        return {v.x, v.y, v.z};
+    }
+    return {0, b * T.per, min((b + 1) * T.per, T.n)};
+}
+// `on` (per mesh, null = all) masks whole meshes out of a launch: their tiles
+// return before any work or synchronisation.
+__device__ __forceinline__ bool mesh_on(const int* on, int mesh) { return !on || on[mesh] != 0; }
+
+// Per-mesh grid reduction: per-tile partials; the last tile of each mesh to
+// finish adds that mesh's partials in tile order (thread i takes tiles i,
+// i + blockDim.x, ... of the mesh, then a fixed block sum).  Returns true in
+// the last tile of the mesh, with the totals in tot[] of thread 0.  With one
+// mesh and no table this is grid_reduce's arithmetic.  counters: one per
+// mesh, zero between launches (the last tile resets its mesh's).
+template <int NV, bool MAX = false>
+__device__ __forceinline__ bool seg_reduce(const double (&v)[NV], const Tiles& T, int mesh, double* partials,
+                                           unsigned* counters, double (&tot)[NV]) {
+    __shared__ double sm[32];
+    __shared__ bool last;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        const double r = MAX ? block_max(v[k], sm) : block_sum(v[k], sm);
+        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * NV + k] = r;
+    }
+    const int t0 = T.t ? T.tile0[mesh] : 0, t1 = T.t ? T.tile0[mesh + 1] : (int)gridDim.x;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counters + mesh, 1u) == (unsigned)(t1 - t0 - 1);
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double acc = MAX ? -1.0e308 : 0.0;
+        for (int b = t0 + (int)threadIdx.x; b < t1; b += blockDim.x) {
+            const double p = __ldcg(partials + (size_t)b * NV + k);
+            acc = MAX ? fmax(acc, p) : acc + p;
+        }
+        tot[k] = MAX ? block_max(acc, sm) : block_sum(acc, sm);
+    }
+    if (threadIdx.x == 0) counters[mesh] = 0u;
+    return true;
+}
+
+// seg_reduce writing the totals to out[mesh * stride + k].
+template <int NV, bool MAX = false>
+__device__ __forceinline__ void seg_reduce_out(const double (&v)[NV], const Tiles& T, int mesh, double* partials,
+                                               unsigned* counters, double* out, int stride) {
+    double tot[NV];
+    if (seg_reduce<NV, MAX>(v, T, mesh, partials, counters, tot) && threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) out[(size_t)mesh * stride + k] = tot[k];
+}
+
 }  // namespace wrapd

@@ -31,6 +31,34 @@ struct ElemView {
     const Material* mats;
 };
 
+// ---- per-mesh vectors of the global step ------------------------------------
+// Each mesh of a batch keeps its own L-BFGS state (SplitLBFGS, one per
+// reference Solver): its gradients, its history and its decisions.  The
+// n x 3 vectors are shared buffers in which each mesh owns its range of free
+// vertices; which buffer plays which role is per mesh:
+//   gradients: a ring of three, cur = G[grot % 3], new = G[(grot + 1) % 3],
+//     old = G[(grot + 2) % 3]; "grad_old <- grad, grad <- grad_new" is grot + 1;
+//   history: a ring of M + 1 (s, y) slots, logical entry i (oldest first) at
+//     slot (head + i) % (M + 1), the next pair written to `stage`, the one slot
+//     no live entry uses; "erase the oldest, push" is head + 1.
+constexpr int kMaxHistory = 32;   // longest global L-BFGS history (lbfgs_m)
+constexpr int kHistSlots = kMaxHistory + 1;
+struct MeshCtl {
+    int grot;      // gradient ring position
+    int head;      // history slot of the oldest live entry
+    int k;         // live history entries (SplitLBFGS m_k)
+    int it;        // two-loop length of the current inner iteration, min(M, k)
+    int stage;     // history slot that receives the next s and y
+    int small;     // the two-loop runs in one CTA (3 x free vertices <= kTwoLoopMaxN)
+    int v0, v1;    // the mesh's range in the n x 3 vectors, in doubles
+};
+struct VecPools {
+    double* G[3];
+    double* S[kHistSlots];
+    double* Y[kHistSlots];
+    int M;         // history length (lbfgs_m); slots are taken mod M + 1
+};
+
 // The material of element e: the batch's per-mesh table when there is one,
 // else the handle's single material m0 (also for lanes past the end).
 __device__ __forceinline__ Material elem_material(const ElemView& E, const Material& m0, int e) {

@@ -80,13 +80,15 @@ __device__ __forceinline__ double elastic_energy(const Material& m, const double
 // K + K^T, M = F - U diag(s) (K+K^T) V^T and g_e = w^2 Di^T M^T, plus the AL
 // value 0.5 w^2 |symF - P|^2, the potential energy and the inversion count at
 // x (src/TetElements.cpp:444-468, 598-635).  Outputs out[0..2] = value, pe, flips.
-static __global__ void __launch_bounds__(128) k_grad(ElemView E, const double* __restrict__ x,
+static __global__ void __launch_bounds__(128) k_grad(ElemView E, Tiles T, const int* on, const double* __restrict__ x,
                                               const double* __restrict__ xfix, Material mat0, int write_gel,
-                                              double* partials, unsigned* counter, double* out) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    const Material mat = elem_material(E, mat0, e);
+                                              double* partials, unsigned* counters, double* out, int stride) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
+    const int e = tl.first + threadIdx.x;
+    const Material mat = elem_material(E, mat0, e < tl.end ? e : E.ne);
     double red[3] = {0.0, 0.0, 0.0};
-    if (e < E.ne) {
+    if (e < tl.end) {
         double Fd[9];
         deformation(E, e, x, xfix, true, Fd);
         double F[9], s[3], Us[9], Vs[9];
@@ -161,29 +163,56 @@ static __global__ void __launch_bounds__(128) k_grad(ElemView E, const double* _
                 }
         }
     }
-    grid_reduce<3>(red, partials, counter, out);
+    seg_reduce_out<3>(red, T, tl.mesh, partials, counters, out, stride);
 }
+
+// ---- per-mesh vectors of the global step (MeshCtl, VecPools: elem_types.cuh) --
+__device__ __forceinline__ int hist_slot(const MeshCtl& c, int i, int M) { return (c.head + i) % (M + 1); }
+__device__ __forceinline__ double* g_cur(const VecPools& P, const MeshCtl& c) { return P.G[c.grot % 3]; }
+__device__ __forceinline__ double* g_new(const VecPools& P, const MeshCtl& c) { return P.G[(c.grot + 1) % 3]; }
+__device__ __forceinline__ double* g_old(const VecPools& P, const MeshCtl& c) { return P.G[(c.grot + 2) % 3]; }
+
+// Gather modes: at the start of an ADMM iteration the gradient goes to the
+// mesh's cur buffer and is compared with old (|grad - grad_old|^2, the early
+// return of SplitLBFGS.hpp:138-142); inside the L-BFGS loop it goes to new,
+// y = new - cur is staged with <s, y>; GATHER_PLAIN writes `plain` only.
+enum { GATHER_START = 0, GATHER_LBFGS = 1, GATHER_PLAIN = 2 };
 
 // Free-vertex gather of the element gradients (atomic-free; each vertex's
 // incidences, in element order, are added by eight lanes in a fixed order, so
 // the sum is deterministic):
 //   grad[i] = sum over (e, a) incident to i of gel(a, :)[e].
-// With gold: d = grad - gold; ystage <- d (if given); out[0] = |d|^2 and
-// out[1] = <sstage, d> (if sstage given).  With x: out[2] = |x - xs|^2 (the
-// x error of AlgorithmData, at the point the gradient was taken).
-static __global__ void __launch_bounds__(256) k_gather(int nf, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
-                                                const double* __restrict__ gel, int ne, double* __restrict__ grad,
-                                                const double* __restrict__ gold, double* __restrict__ ystage,
-                                                const double* __restrict__ sstage, const double* __restrict__ x,
-                                                const double* __restrict__ xs, double* partials,
-                                                unsigned* counter, double* out) {
+// Tiles of 32 free vertices (eight lanes each).  Per mesh: out[0] = |d|^2 with
+// d = grad - gold, out[1] = <s_stage, d> (GATHER_LBFGS), out[2] = |x - xs|^2
+// (the x error of AlgorithmData, at the point the gradient was taken; x may be
+// null).
+static __global__ void __launch_bounds__(256) k_gather(Tiles T, const int* on, int mode, const MeshCtl* __restrict__ ctl,
+                                                VecPools P, double* __restrict__ plain, const int* __restrict__ inc_ptr,
+                                                const int* __restrict__ inc, const double* __restrict__ gel, int ne,
+                                                const double* __restrict__ x, const double* __restrict__ xs,
+                                                double* partials, unsigned* counters, double* out, int stride) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
+    double *grad = plain, *ystage = nullptr;
+    const double *gold = nullptr, *sstage = nullptr;
+    if (mode != GATHER_PLAIN) {
+        const MeshCtl c = ctl[tl.mesh];
+        if (mode == GATHER_START) {
+            grad = g_cur(P, c);
+            gold = g_old(P, c);
+        } else {
+            grad = g_new(P, c);
+            gold = g_cur(P, c);
+            ystage = P.Y[c.stage];
+            sstage = P.S[c.stage];
+        }
+    }
     // eight lanes per vertex: lane s of the group adds incidences s, s + 8, ...
     // of the vertex, then the group adds its lanes in a fixed xor tree
-    const int gidx = (blockIdx.x * blockDim.x + threadIdx.x) >> 3, sub = threadIdx.x & 7;
-    const int i = gidx;
+    const int i = tl.first + (threadIdx.x >> 3), sub = threadIdx.x & 7;
     double red[3] = {0.0, 0.0, 0.0};
     double g0 = 0.0, g1 = 0.0, g2 = 0.0;
-    if (i < nf) {
+    if (i < tl.end) {
         for (int t = inc_ptr[i] + sub; t < inc_ptr[i + 1]; t += 8) {
             const int c = inc[t];
             const int e = c >> 2, a = c & 3;
@@ -198,7 +227,7 @@ static __global__ void __launch_bounds__(256) k_gather(int nf, const int* __rest
         g1 += __shfl_xor_sync(0xffffffffu, g1, o);
         g2 += __shfl_xor_sync(0xffffffffu, g2, o);
     }
-    if (i < nf && sub == 0) {
+    if (i < tl.end && sub == 0) {
         grad[3 * (size_t)i] = g0; grad[3 * (size_t)i + 1] = g1; grad[3 * (size_t)i + 2] = g2;
         if (gold) {
             const double d0 = g0 - gold[3 * (size_t)i], d1 = g1 - gold[3 * (size_t)i + 1], d2 = g2 - gold[3 * (size_t)i + 2];
@@ -212,7 +241,7 @@ static __global__ void __launch_bounds__(256) k_gather(int nf, const int* __rest
             red[2] = e0 * e0 + e1 * e1 + e2 * e2;
         }
     }
-    grid_reduce<3>(red, partials, counter, out);
+    seg_reduce_out<3>(red, T, tl.mesh, partials, counters, out, stride);
 }
 
 // ---- local step ---------------------------------------------------------------
@@ -228,18 +257,20 @@ static __global__ void __launch_bounds__(256) k_gather(int nf, const int* __rest
 // prox network's prediction.  The FP32 instantiation always uses Newton.
 // NET needs dynamic shared memory: the network image plus one scratch per warp.
 template <typename C, bool NET>
-__global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat0, int prox_iters, int cand_mode,
-                                               int prox_mode, const unsigned char* __restrict__ net_img,
-                                               double* partials, unsigned* counter, double* out) {
+__global__ void __launch_bounds__(256, 2) k_local(ElemView E, Tiles T, const int* on, Material mat0, int prox_iters,
+                                               int cand_mode, int prox_mode, const unsigned char* __restrict__ net_img,
+                                               double* partials, unsigned* counters, double* out, int stride) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
     double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     extern __shared__ __align__(16) unsigned char local_smem[];
     if constexpr (NET) {
         net::load_image(net_img, local_smem);
         __syncthreads();
     }
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    const Material mat = elem_material(E, mat0, e);
-    const bool valid = e < E.ne;
+    const int e = tl.first + threadIdx.x;
+    const bool valid = e < tl.end;
+    const Material mat = elem_material(E, mat0, valid ? e : E.ne);
     double S[9], Um[9];
     double w2 = 0.0, vol = 1.0;
     C sg[3] = {C(1), C(1), C(1)}, Ue[9], Ve[9];
@@ -352,19 +383,21 @@ __global__ void __launch_bounds__(128, 4) k_local(ElemView E, Material mat0, int
             E.w2c[e] = vol * c;
         }
     }
-    grid_reduce<5>(red, partials, counter, out);
+    seg_reduce_out<5>(red, T, tl.mesh, partials, counters, out, stride);
 }
 
 // initialize_dual_vars (src/TetElements.cpp:145-166): Z = (V diag(s) V^T)^T of
 // F(X) with all four slots read from X, U = 0; then polar_potential_energy
 // (src/TetElements.cpp:638-675) of the new Z.  out[0] = that energy.
-static __global__ void __launch_bounds__(128) k_init_dual(ElemView E, const double* __restrict__ x,
+static __global__ void __launch_bounds__(128) k_init_dual(ElemView E, Tiles T, const int* on, const double* __restrict__ x,
                                                    const double* __restrict__ xfix, Material mat0,
-                                                   double* partials, unsigned* counter, double* out) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    const Material mat = elem_material(E, mat0, e);
+                                                   double* partials, unsigned* counters, double* out, int stride) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
+    const int e = tl.first + threadIdx.x;
+    const Material mat = elem_material(E, mat0, e < tl.end ? e : E.ne);
     double red[1] = {0.0};
-    if (e < E.ne) {
+    if (e < tl.end) {
         double Fd[9];
         deformation(E, e, x, xfix, false, Fd);
         double F[9], s[3], Us[9], Vs[9], Zm[9], Zt[9];
@@ -397,17 +430,19 @@ static __global__ void __launch_bounds__(128) k_init_dual(ElemView E, const doub
             red[0] = E.vol[e] * NH<double>{mat.mu, mat.lambda}.psi_plain(double(s[0]), double(s[1]), double(s[2]));
         }
     }
-    grid_reduce<1>(red, partials, counter, out);
+    seg_reduce_out<1>(red, T, tl.mesh, partials, counters, out, stride);
 }
 
 // Candidate weights of midupdate_weights (src/TetElements.cpp:360-388): from
 // F(X) (from_x = 1) or from the cached singular values.
-static __global__ void __launch_bounds__(128) k_mid_candidates(ElemView E, const double* __restrict__ x,
-                                                        const double* __restrict__ xfix, Material mat0,
-                                                        int from_x, int cand_mode) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+static __global__ void __launch_bounds__(128) k_mid_candidates(ElemView E, Tiles T, const int* on,
+                                                        const double* __restrict__ x, const double* __restrict__ xfix,
+                                                        Material mat0, int from_x, int cand_mode) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
+    const int e = tl.first + threadIdx.x;
+    if (e >= tl.end) return;
     const Material mat = elem_material(E, mat0, e);
-    if (e >= E.ne) return;
     double s[3];
     if (from_x) {
         double Fd[9];
@@ -434,20 +469,26 @@ static __global__ void __launch_bounds__(128) k_mid_candidates(ElemView E, const
 }
 
 // max_wsq_ratio (src/Elements.hpp:56-69): out[0] = max_e max(w2/w2c, w2c/w2).
-static __global__ void __launch_bounds__(256) k_ratio(ElemView E, double* partials, unsigned* counter, double* out) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+// Per mesh (System::possibly_update_weights takes the max over its own elements).
+static __global__ void __launch_bounds__(256) k_ratio(ElemView E, Tiles T, const int* on, double* partials,
+                                               unsigned* counters, double* out, int stride) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
+    const int e = tl.first + threadIdx.x;
     double red[1] = {0.0};
-    if (e < E.ne) {
+    if (e < tl.end) {
         const double a = E.w2[e] / E.w2c[e], b = 1.0 / a;
         red[0] = fmax(a, b);
     }
-    grid_reduce<1, true>(red, partials, counter, out);
+    seg_reduce_out<1, true>(red, T, tl.mesh, partials, counters, out, stride);
 }
 
-// update_actual_weights (src/TetElements.cpp:435-442).
-static __global__ void __launch_bounds__(256) k_apply_weights(ElemView E) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= E.ne) return;
+// update_actual_weights (src/TetElements.cpp:435-442), on the meshes that reweight.
+static __global__ void __launch_bounds__(256) k_apply_weights(ElemView E, Tiles T, const int* on) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
+    const int e = tl.first + threadIdx.x;
+    if (e >= tl.end) return;
     const double r = E.w2[e] / E.w2c[e];
 #pragma unroll
     for (int k = 0; k < 9; ++k) E.U[(size_t)k * E.ne + e] = r * E.U[(size_t)k * E.ne + e];
@@ -455,37 +496,91 @@ static __global__ void __launch_bounds__(256) k_apply_weights(ElemView E) {
 }
 
 // ---- global-step vector kernels (n x 3 FP64, dissection order) ----------------
-// q = src + sign * coef * v; out = base + scale * <w, q>  (w, v optional).
-// The two-loop recursion of SplitLBFGS::minimize (SplitLBFGS.hpp:152-177) is a
-// chain of these: alpha_i = rho_i <s_i, q>, q -= alpha_i y_i, then
-// c_i = alpha_i - rho_i <y_i, q>, q += c_i s_i, and finally <grad, q>.
-static __global__ void __launch_bounds__(256) k_axpy_dot(int n, double* __restrict__ q, const double* __restrict__ src,
-                                                  const double* __restrict__ v, const double* __restrict__ coef,
-                                                  double sign, const double* __restrict__ w,
-                                                  const double* __restrict__ base, double scale, double* partials,
-                                                  unsigned* counter, double* out) {
+// Tiles of kVecTile doubles of one mesh's range (thread t takes entries t,
+// t + 256, ...).  The two-loop recursion of SplitLBFGS::minimize
+// (SplitLBFGS.hpp:152-177) runs as a chain of steps, each an axpy and an inner
+// product per mesh; every mesh walks its own history length `it`:
+//   first loop, step j = it-1 .. 0: q = g (j = it-1) or q -= alpha_{j+1} y_{j+1};
+//     alpha_j = rho_j <s_j, q>;  step -1: q -= alpha_0 y_0 (q = g when it = 0);
+//   second loop, step j = 0 .. it-1: q += c_{j-1} s_{j-1} (j > 0);
+//     c_j = alpha_j - rho_j <y_j, q>;  step it: q += c_{it-1} s_{it-1};
+//     dir = <g, q>.
+// A launch serves one step index j for every mesh; meshes whose walk has no
+// step j return.  alpha_j, c_j and dir are per mesh in the scalar block
+// (scal + mesh * stride + S_ALPHA / S_C / S_DIR).
+constexpr int kVecTile = 2048;
+
+struct TwoLoopSlots {
+    int alpha, c, dir;    // offsets in a mesh's scalar block
+};
+
+static __global__ void __launch_bounds__(256) k_lbfgs_first(Tiles T, const int* on, const MeshCtl* __restrict__ ctl,
+                                                     VecPools P, const double* __restrict__ rho,
+                                                     double* __restrict__ q, int j, TwoLoopSlots sl, double* partials,
+                                                     unsigned* counters, double* scal, int stride) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
+    const MeshCtl c = ctl[tl.mesh];
+    if (j >= c.it || (j == -1 && false)) return;
+    double* sc = scal + (size_t)tl.mesh * stride;
+    const bool first = j == c.it - 1;                  // q = g (also j = -1 with it = 0)
+    const double* g = g_cur(P, c);
+    const double* yv = first ? nullptr : P.Y[hist_slot(c, j + 1, P.M)];
+    const double cf = first ? 0.0 : -__ldcg(sc + sl.alpha + j + 1);
+    const double* sv = j >= 0 ? P.S[hist_slot(c, j, P.M)] : nullptr;
     double red[1] = {0.0};
-    const double cf = v ? sign * (*coef) : 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double qi = src ? src[i] : q[i];
-        if (v) qi = qi + cf * v[i];
+    for (int i = tl.first + (int)threadIdx.x; i < tl.end; i += blockDim.x) {
+        double qi = first ? g[i] : q[i];
+        if (yv) qi = qi + cf * yv[i];
         q[i] = qi;
-        if (w) red[0] += w[i] * qi;
+        if (sv) red[0] += sv[i] * qi;
     }
-    grid_reduce<1>(red, partials, counter, out, base, scale);
+    if (j < 0) return;
+    double tot[1];
+    if (seg_reduce<1>(red, T, tl.mesh, partials, counters, tot) && threadIdx.x == 0)
+        sc[sl.alpha + j] = rho[(size_t)tl.mesh * kHistSlots + hist_slot(c, j, P.M)] * tot[0];
 }
 
-// ---- the two-loop recursion in one CTA, for small systems -------------------------
-// With n <= kTwoLoopMaxN the chain of short reductions above is latency-bound:
-// one 1024-thread CTA runs each half of the recursion, q in registers
-// (kTwoLoopPerThread entries per thread), each inner product a block sum in a
-// fixed order.  Same formulas and the same alpha_i, c_i and decrement slots.
-constexpr int kMaxHistory = 32;   // longest global L-BFGS history (lbfgs_m)
+static __global__ void __launch_bounds__(256) k_lbfgs_second(Tiles T, const int* on, const MeshCtl* __restrict__ ctl,
+                                                      VecPools P, const double* __restrict__ rho,
+                                                      double* __restrict__ q, int j, TwoLoopSlots sl, double* partials,
+                                                      unsigned* counters, double* scal, int stride) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
+    const MeshCtl c = ctl[tl.mesh];
+    if (j > c.it) return;
+    double* sc = scal + (size_t)tl.mesh * stride;
+    const double* sv = j > 0 ? P.S[hist_slot(c, j - 1, P.M)] : nullptr;
+    const double cf = j > 0 ? __ldcg(sc + sl.c + j - 1) : 0.0;
+    const double* w = j < c.it ? P.Y[hist_slot(c, j, P.M)] : g_cur(P, c);
+    double red[1] = {0.0};
+    for (int i = tl.first + (int)threadIdx.x; i < tl.end; i += blockDim.x) {
+        double qi = q[i];
+        if (sv) {
+            qi = qi + cf * sv[i];
+            q[i] = qi;
+        }
+        red[0] += w[i] * qi;
+    }
+    double tot[1];
+    if (seg_reduce<1>(red, T, tl.mesh, partials, counters, tot) && threadIdx.x == 0) {
+        if (j < c.it)
+            sc[sl.c + j] = __ldcg(sc + sl.alpha + j) + (-rho[(size_t)tl.mesh * kHistSlots + hist_slot(c, j, P.M)]) * tot[0];
+        else
+            sc[sl.dir] = tot[0];
+    }
+}
+
+// ---- the two-loop recursion in one CTA per mesh, for small meshes -----------------
+// With 3 x free vertices <= kTwoLoopMaxN the chain of short reductions above is
+// latency-bound: one 1024-thread CTA per mesh runs each half of the
+// recursion, q in registers (kTwoLoopPerThread entries per thread), each inner
+// product a block sum in a fixed order.  Same formulas and the same alpha_i,
+// c_i and decrement slots.  Block b serves mesh b (meshes that are off or not
+// small return).
 constexpr int kTwoLoopThreads = 1024;
 constexpr int kTwoLoopPerThread = 16;
 constexpr int kTwoLoopMaxN = kTwoLoopThreads * kTwoLoopPerThread;
-struct HistPtrs { const double* p[kMaxHistory]; };
-struct HistRho { double r[kMaxHistory]; };
 
 __device__ __forceinline__ double cta_sum_all(double v, double* sm) {
     __shared__ double total;
@@ -497,67 +592,85 @@ __device__ __forceinline__ double cta_sum_all(double v, double* sm) {
 
 // First loop (SplitLBFGS.hpp:152-158): q = g; for i = it-1 .. 0:
 // alpha_i = rho_i <s_i, q>, q -= alpha_i y_i.
-static __global__ void __launch_bounds__(kTwoLoopThreads) k_two_loop_first(int n, double* __restrict__ q,
-                                                                           const double* __restrict__ g,
-                                                                           HistPtrs S, HistPtrs Yh, HistRho rho,
-                                                                           int it, double* __restrict__ alpha) {
+static __global__ void __launch_bounds__(kTwoLoopThreads) k_two_loop_first(const int* on, const MeshCtl* __restrict__ ctl,
+                                                                           VecPools P, const double* __restrict__ rho,
+                                                                           double* __restrict__ q, TwoLoopSlots sl,
+                                                                           double* scal, int stride) {
+    const int m = blockIdx.x;
+    const MeshCtl c = ctl[m];
+    if (!mesh_on(on, m) || !c.small) return;
     __shared__ double sm[32];
+    const int n = c.v1 - c.v0;
+    const double* g = g_cur(P, c) + c.v0;
+    double* qm = q + c.v0;
+    double* alpha = scal + (size_t)m * stride + sl.alpha;
     double qr[kTwoLoopPerThread];
 #pragma unroll
     for (int k = 0; k < kTwoLoopPerThread; ++k) {
         const int i = threadIdx.x + k * kTwoLoopThreads;
         qr[k] = i < n ? g[i] : 0.0;
     }
-    for (int h = it - 1; h >= 0; --h) {
+    for (int h = c.it - 1; h >= 0; --h) {
+        const int hs = hist_slot(c, h, P.M);
+        const double* sp = P.S[hs] + c.v0;
+        const double* yp = P.Y[hs] + c.v0;
         double d = 0.0;
 #pragma unroll
         for (int k = 0; k < kTwoLoopPerThread; ++k) {
             const int i = threadIdx.x + k * kTwoLoopThreads;
-            if (i < n) d += S.p[h][i] * qr[k];
+            if (i < n) d += sp[i] * qr[k];
         }
-        const double a = rho.r[h] * cta_sum_all(d, sm);
+        const double a = rho[(size_t)m * kHistSlots + hs] * cta_sum_all(d, sm);
         if (threadIdx.x == 0) alpha[h] = a;
 #pragma unroll
         for (int k = 0; k < kTwoLoopPerThread; ++k) {
             const int i = threadIdx.x + k * kTwoLoopThreads;
-            if (i < n) qr[k] = qr[k] + (-a) * Yh.p[h][i];
+            if (i < n) qr[k] = qr[k] + (-a) * yp[i];
         }
     }
 #pragma unroll
     for (int k = 0; k < kTwoLoopPerThread; ++k) {
         const int i = threadIdx.x + k * kTwoLoopThreads;
-        if (i < n) q[i] = qr[k];
+        if (i < n) qm[i] = qr[k];
     }
 }
 
 // Second loop (SplitLBFGS.hpp:170-173) after q = A^-1 q: for i = 0 .. it-1:
 // c_i = alpha_i - rho_i <y_i, q>, q += c_i s_i; then dir = <g, q>.
-static __global__ void __launch_bounds__(kTwoLoopThreads) k_two_loop_second(int n, double* __restrict__ q,
-                                                                            const double* __restrict__ g,
-                                                                            HistPtrs S, HistPtrs Yh, HistRho rho,
-                                                                            int it, const double* __restrict__ alpha,
-                                                                            double* __restrict__ C,
-                                                                            double* __restrict__ dir) {
+static __global__ void __launch_bounds__(kTwoLoopThreads) k_two_loop_second(const int* on, const MeshCtl* __restrict__ ctl,
+                                                                            VecPools P, const double* __restrict__ rho,
+                                                                            double* __restrict__ q, TwoLoopSlots sl,
+                                                                            double* scal, int stride) {
+    const int m = blockIdx.x;
+    const MeshCtl c = ctl[m];
+    if (!mesh_on(on, m) || !c.small) return;
     __shared__ double sm[32];
+    const int n = c.v1 - c.v0;
+    const double* g = g_cur(P, c) + c.v0;
+    double* qm = q + c.v0;
+    double* sc = scal + (size_t)m * stride;
     double qr[kTwoLoopPerThread];
 #pragma unroll
     for (int k = 0; k < kTwoLoopPerThread; ++k) {
         const int i = threadIdx.x + k * kTwoLoopThreads;
-        qr[k] = i < n ? q[i] : 0.0;
+        qr[k] = i < n ? qm[i] : 0.0;
     }
-    for (int h = 0; h < it; ++h) {
+    for (int h = 0; h < c.it; ++h) {
+        const int hs = hist_slot(c, h, P.M);
+        const double* sp = P.S[hs] + c.v0;
+        const double* yp = P.Y[hs] + c.v0;
         double d = 0.0;
 #pragma unroll
         for (int k = 0; k < kTwoLoopPerThread; ++k) {
             const int i = threadIdx.x + k * kTwoLoopThreads;
-            if (i < n) d += Yh.p[h][i] * qr[k];
+            if (i < n) d += yp[i] * qr[k];
         }
-        const double c = alpha[h] + (-rho.r[h]) * cta_sum_all(d, sm);
-        if (threadIdx.x == 0) C[h] = c;
+        const double cc = sc[sl.alpha + h] + (-rho[(size_t)m * kHistSlots + hs]) * cta_sum_all(d, sm);
+        if (threadIdx.x == 0) sc[sl.c + h] = cc;
 #pragma unroll
         for (int k = 0; k < kTwoLoopPerThread; ++k) {
             const int i = threadIdx.x + k * kTwoLoopThreads;
-            if (i < n) qr[k] = qr[k] + c * S.p[h][i];
+            if (i < n) qr[k] = qr[k] + cc * sp[i];
         }
     }
     double d = 0.0;
@@ -565,27 +678,57 @@ static __global__ void __launch_bounds__(kTwoLoopThreads) k_two_loop_second(int 
     for (int k = 0; k < kTwoLoopPerThread; ++k) {
         const int i = threadIdx.x + k * kTwoLoopThreads;
         if (i < n) {
-            q[i] = qr[k];
+            qm[i] = qr[k];
             d += g[i] * qr[k];
         }
     }
     const double dd = cta_sum_all(d, sm);
-    if (threadIdx.x == 0) *dir = dd;
+    if (threadIdx.x == 0) sc[sl.dir] = dd;
 }
 
-// x <- x - rate * step with step = q, or grad when the decrement dir <= 0
-// (the steepest-descent restart of SplitLBFGS.hpp:189-194); s = x_new - x_old.
-// rate is 1 unless the global line search chose another (SplitLBFGS.hpp:196-206).
-static __global__ void __launch_bounds__(256) k_xupdate(int n, double* __restrict__ x, const double* __restrict__ q,
-                                                 const double* __restrict__ grad, const double* __restrict__ dir,
-                                                 double rate, double* __restrict__ s) {
-    const bool restart = !(*dir > 0.0);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+// x <- x - rate * step with step = q, or grad when the mesh's decrement
+// dir <= 0 (the steepest-descent restart of SplitLBFGS.hpp:189-194);
+// s = x_new - x_old into the mesh's stage slot.  rate is 1 unless the global
+// line search chose another (SplitLBFGS.hpp:196-206).
+static __global__ void __launch_bounds__(256) k_xupdate(Tiles T, const int* on, const MeshCtl* __restrict__ ctl,
+                                                 VecPools P, double* __restrict__ x, const double* __restrict__ q,
+                                                 const double* scal, int dir_slot, int stride, double rate) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
+    const MeshCtl c = ctl[tl.mesh];
+    const bool restart = !(__ldcg(scal + (size_t)tl.mesh * stride + dir_slot) > 0.0);
+    const double* grad = g_cur(P, c);
+    double* s = P.S[c.stage];
+    for (int i = tl.first + (int)threadIdx.x; i < tl.end; i += blockDim.x) {
         const double xo = x[i];
         const double xn = xo - rate * (restart ? grad[i] : q[i]);
         s[i] = xn - xo;
         x[i] = xn;
     }
+}
+
+// grad_old = 0 (SplitLBFGS keeps grad_old across ADMM iterations and zeroes
+// it with the history, SplitLBFGS.hpp:118-121) on the meshes that are on.
+static __global__ void __launch_bounds__(256) k_zero_old(Tiles T, const int* on, const MeshCtl* __restrict__ ctl,
+                                                  VecPools P) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
+    double* g = g_old(P, ctl[tl.mesh]);
+    for (int i = tl.first + (int)threadIdx.x; i < tl.end; i += blockDim.x) g[i] = 0.0;
+}
+
+// Per mesh |x - xs|^2 (the x error of AlgorithmData::update_per_iter_data).
+static __global__ void __launch_bounds__(256) k_xerr(Tiles T, const int* on, const double* __restrict__ x,
+                                              const double* __restrict__ xs, double* partials, unsigned* counters,
+                                              double* out, int stride) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
+    double red[1] = {0.0};
+    for (int i = tl.first + (int)threadIdx.x; i < tl.end; i += blockDim.x) {
+        const double d = x[i] - xs[i];
+        red[0] += d * d;
+    }
+    seg_reduce_out<1>(red, T, tl.mesh, partials, counters, out, stride);
 }
 
 // Inputs of the global line search (Backtracking::search,
@@ -621,11 +764,13 @@ static __global__ void __launch_bounds__(256) k_ls_trial(int n, double* __restri
 // polar_update, ARAP branch (src/TetElements.cpp:265-282): S = symF + U (both
 // symmetric), Z = (S + I) / 2, U += symF - Z; curr_pe = sum vol |symF - I|^2 / 2.
 // out[0..4] as k_local (no prox: [3] = [4] = 0).
-static __global__ void __launch_bounds__(128) k_local_arap(ElemView E, double* partials, unsigned* counter,
-                                                         double* out) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+static __global__ void __launch_bounds__(128) k_local_arap(ElemView E, Tiles T, const int* on, double* partials,
+                                                         unsigned* counters, double* out, int stride) {
+    const Tile tl = tile_at(T, blockIdx.x);
+    if (!mesh_on(on, tl.mesh)) return;
+    const int e = tl.first + threadIdx.x;
     double red[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (e < E.ne) {
+    if (e < tl.end) {
         double S[9], Um[9], Zm[9];
         load9(E.symF, E.ne, e, S);
         load9(E.U, E.ne, e, Um);
@@ -653,7 +798,7 @@ static __global__ void __launch_bounds__(128) k_local_arap(ElemView E, double* p
         store9(E.Z, E.ne, e, Zm);
         store9(E.U, E.ne, e, Um);
     }
-    grid_reduce<5>(red, partials, counter, out);
+    seg_reduce_out<5>(red, T, tl.mesh, partials, counters, out, stride);
 }
 
 // ---- rotation-unaware ADMM (-ra 0) -----------------------------------------------

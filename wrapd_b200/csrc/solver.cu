@@ -33,9 +33,24 @@ enum : int {
     S_LSV = 88,      // line search: AL value, pe, flips at the trial point
     S_COUNT = 91
 };
+// Launch masks over the meshes of a batch (one int per mesh each).
+enum : int {
+    MK_ALL = 0,      // every mesh
+    MK_ADMM,         // not yet converged
+    MK_LBFGS,        // inside the current SplitLBFGS::minimize iteration
+    MK_RW,           // reweights now
+    MK_L32, MK_L32N, MK_L64, MK_L64N,   // local step: FP32 / FP64 arithmetic, without / with the prox network
+    MK_ZERO,         // grad_old to be zeroed (history empty)
+    MK_SMALL,        // MK_LBFGS meshes whose two-loop runs in one CTA
+    MK_LARGE,        // the other MK_LBFGS meshes
+    MK_COUNT
+};
 // Dynamic shared memory of k_local<double>: the prox L-BFGS history, 48 doubles
-// per thread of a 128-thread block.
+// per thread (kLocalHistBytes for a 128-thread block, the unaware step's).
 constexpr int kLocalHistBytes = 48 * 128 * (int)sizeof(double);
+constexpr int kLocalTileMax = 256;   // largest local-step tile (elements = threads per CTA)
+int local_hist_bytes(int per) { return 48 * per * (int)sizeof(double); }
+int local_net_bytes(int per) { return net::IMAGE_BYTES + (per / 32) * net::WARP_SCRATCH; }
 // Mixed mode switches its local step to FP64 when the normalized energy
 // residual drops below this (the FP32 local step's noise floor is ~1e-7).
 constexpr double kMixedSwitch = 1e-7;
@@ -98,8 +113,8 @@ SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
     WRAPD_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     for (auto& set : evs_)
         for (auto& e : set) WRAPD_CUDA(cudaEventCreate(&e));
-    WRAPD_CUDA(cudaMallocHost(&h_scal_, S_COUNT * sizeof(double)));
-    WRAPD_CUDA(cudaFuncSetAttribute(k_local<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLocalHistBytes));
+    WRAPD_CUDA(cudaFuncSetAttribute(k_local<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    local_hist_bytes(kLocalTileMax)));
     WRAPD_CUDA(cudaFuncSetAttribute(k_local_unaware<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     kLocalHistBytes));
     mat_ = material(cfg.youngs, cfg.poisson);
@@ -126,6 +141,7 @@ SolverGPU::~SolverGPU() {
     for (auto& set : evs_)
         for (auto& e : set) if (e) cudaEventDestroy(e);
     if (h_scal_) cudaFreeHost(h_scal_);
+    if (h_ctl_block_) cudaFreeHost(h_ctl_block_);
     if (st_) cudaStreamDestroy(st_);
 }
 
@@ -214,6 +230,8 @@ void SolverGPU::initialize() {
     // update_all_candidate_weights (src/TetElements.cpp:393-395)
     if (cfg.model != MODEL_NH && cfg.reweighting)
         throw CudaError(WRAPD_E_INPUT, "Adaptive weights are only supported for the NH model (use reweighting = 0)");
+    if (meshes_.size() > 1 && (!cfg.rot_aware || cfg.global_ls))
+        throw CudaError(WRAPD_E_UNSUPPORTED, "a batch of meshes needs the rotation-aware global step without line search");
     auto t0 = std::chrono::steady_clock::now();
     // host phase timings, printed to stderr with verbose >= 2
     std::vector<std::pair<const char*, double>> laps;
@@ -254,11 +272,20 @@ void SolverGPU::initialize() {
     lap("free-vertex graph");
     // one nested dissection per mesh (their graphs are disjoint), then the forest
     std::vector<Symbolic> parts;
-    for (const MeshIn& M : meshes_) {
+    nm = static_cast<int>(meshes_.size());
+    runs_.assign(nm, MeshRun{});
+    for (int mi = 0; mi < nm; ++mi) {
+        const MeshIn& M = meshes_[mi];
         int f0 = -1, f1 = -1;
         for (int i = M.v_off; i < M.v_off + M.nv; ++i)
             if (free_of_vert_[i] >= 0) { if (f0 < 0) f0 = free_of_vert_[i]; f1 = free_of_vert_[i] + 1; }
         if (f0 < 0) throw CudaError(WRAPD_E_INPUT, "a mesh without free vertices");
+        // the merged dissection order keeps each mesh's free vertices together,
+        // at the same offset as the free numbering
+        runs_[mi].e0 = M.e_off;
+        runs_[mi].e1 = M.e_off + M.ne;
+        runs_[mi].f0 = f0;
+        runs_[mi].f1 = f1;
         const int n = f1 - f0;
         std::vector<int> p(n + 1), a(adj.begin() + ptr[f0], adj.begin() + ptr[f1]);
         for (int i = 0; i <= n; ++i) p[i] = ptr[f0 + i] - ptr[f0];
@@ -266,6 +293,8 @@ void SolverGPU::initialize() {
         std::vector<double> c(coords.begin() + 3 * (size_t)f0, coords.begin() + 3 * (size_t)f1);
         parts.push_back(analyse(n, p, a, c, cfg.leaf_size > 0 ? cfg.leaf_size : 64));
     }
+    if (nm > 1)
+        for (int m = 0; m < nm; ++m) chol.front_mesh.insert(chol.front_mesh.end(), parts[m].fronts.size(), m);
     Symbolic S = merge(parts);
     lap("nested dissection + symbolic");
     std::vector<Symbolic>().swap(parts);
@@ -345,30 +374,83 @@ void SolverGPU::initialize() {
     d_xfix_ = dupload(xfix);
     const size_t vb = 3 * (size_t)nf * sizeof(double);
     d_q_ = static_cast<double*>(dalloc(vb));
-    d_gcur_ = static_cast<double*>(dalloc(vb));
-    d_gold_ = static_cast<double*>(dalloc(vb));
-    d_gnew_ = static_cast<double*>(dalloc(vb));
-    d_sstage_ = static_cast<double*>(dalloc(vb));
-    d_ystage_ = static_cast<double*>(dalloc(vb));
-    WRAPD_CUDA(cudaMemsetAsync(d_gold_, 0, vb, st_));
-    WRAPD_CUDA(cudaMemsetAsync(d_gcur_, 0, vb, st_));
-    s_.assign(cfg.lbfgs_m, nullptr);
-    y_.assign(cfg.lbfgs_m, nullptr);
-    for (int i = 0; i < cfg.lbfgs_m; ++i) {
-        s_[i] = static_cast<double*>(dalloc(vb));
-        y_[i] = static_cast<double*>(dalloc(vb));
+    for (double*& g : d_G_) {
+        g = static_cast<double*>(dalloc(vb));
+        WRAPD_CUDA(cudaMemsetAsync(g, 0, vb, st_));
     }
-    rho_.assign(cfg.lbfgs_m, 0.0);
-    const size_t nblk = (size_t)std::max(blocks_for(std::max(ne, nf), 128), blocks_for(8 * (int64_t)nf, 256)) +
-                        2 * kNumSMs + 8;
+    d_S_.assign(cfg.lbfgs_m + 1, nullptr);
+    d_Y_.assign(cfg.lbfgs_m + 1, nullptr);
+    for (int i = 0; i <= cfg.lbfgs_m; ++i) {
+        d_S_[i] = static_cast<double*>(dalloc(vb));
+        d_Y_[i] = static_cast<double*>(dalloc(vb));
+    }
+    // launch tilings: element tiles of 128 and 256, vertex tiles of 32 (the
+    // gather's eight lanes per vertex), vector tiles of kVecTile doubles; each
+    // mesh's tiles start at its first item
+    {
+        std::vector<std::pair<int, int>> er, vr, qr;
+        for (const MeshRun& R : runs_) {
+            er.emplace_back(R.e0, R.e1);
+            vr.emplace_back(R.f0, R.f1);
+            qr.emplace_back(3 * R.f0, 3 * R.f1);
+        }
+        build_tiles(te128_, 128, er);
+        build_tiles(te256_, 256, er);
+        build_tiles(te_local_, local_per_, er);
+        build_tiles(tv32_, 32, vr);
+        build_tiles(tvec_, kVecTile, qr);
+    }
+    // (partials for the largest tile count: 64-element local tiles are the finest)
+    build_tiles(te_local_, 64, [&] {
+        std::vector<std::pair<int, int>> er;
+        for (const MeshRun& R : runs_) er.emplace_back(R.e0, R.e1);
+        return er;
+    }());
+    const int finest_local = te_local_.count;
+    {
+        std::vector<std::pair<int, int>> er;
+        for (const MeshRun& R : runs_) er.emplace_back(R.e0, R.e1);
+        build_tiles(te_local_, local_per_, er);
+    }
+    const size_t nblk = (size_t)std::max({te128_.count, te256_.count, tv32_.count, tvec_.count, finest_local,
+                                          blocks_for(8 * (int64_t)nf, 256), vec_blocks(3 * (int64_t)nf)}) + 8;
     d_partials_ = static_cast<double*>(dalloc(nblk * 5 * sizeof(double)));
-    d_counter_ = static_cast<unsigned*>(dalloc(sizeof(unsigned)));
-    d_scal_ = static_cast<double*>(dalloc(S_COUNT * sizeof(double)));
-    WRAPD_CUDA(cudaMemsetAsync(d_counter_, 0, sizeof(unsigned), st_));
-    WRAPD_CUDA(cudaMemsetAsync(d_scal_, 0, S_COUNT * sizeof(double), st_));
+    d_counters_ = static_cast<unsigned*>(dalloc(nm * sizeof(unsigned)));
+    d_scal_ = static_cast<double*>(dalloc((size_t)nm * kScalStride * sizeof(double)));
+    WRAPD_CUDA(cudaMemsetAsync(d_counters_, 0, nm * sizeof(unsigned), st_));
+    WRAPD_CUDA(cudaMemsetAsync(d_scal_, 0, (size_t)nm * kScalStride * sizeof(double), st_));
+    WRAPD_CUDA(cudaMallocHost(&h_scal_, (size_t)nm * kScalStride * sizeof(double)));
+    std::memset(h_scal_, 0, (size_t)nm * kScalStride * sizeof(double));
     {
         static const double one = 1.0;
         WRAPD_CUDA(cudaMemcpyAsync(d_scal_ + S_ONE, &one, sizeof(double), cudaMemcpyHostToDevice, st_));
+    }
+    // the per-mesh control block: masks, MeshCtl, rho
+    {
+        const size_t mb = (size_t)MK_COUNT * nm * sizeof(int), cb = (size_t)nm * sizeof(MeshCtl),
+                     rb = (size_t)nm * kHistSlots * sizeof(double);
+        const size_t mo = 0, co = (mb + 15) / 16 * 16, ro = (co + cb + 15) / 16 * 16;
+        ctl_bytes_ = ro + rb;
+        d_ctl_block_ = dalloc(ctl_bytes_);
+        WRAPD_CUDA(cudaMallocHost(&h_ctl_block_, ctl_bytes_));
+        std::memset(h_ctl_block_, 0, ctl_bytes_);
+        char* d = static_cast<char*>(d_ctl_block_);
+        char* h = static_cast<char*>(h_ctl_block_);
+        d_ctl_block_masks_ = reinterpret_cast<int*>(d + mo);
+        h_masks_ = reinterpret_cast<int*>(h + mo);
+        d_ctl_ = reinterpret_cast<MeshCtl*>(d + co);
+        h_ctl_ = reinterpret_cast<MeshCtl*>(h + co);
+        d_rho_ = reinterpret_cast<double*>(d + ro);
+        h_rho_ = reinterpret_cast<double*>(h + ro);
+        for (int m = 0; m < nm; ++m) {
+            MeshCtl& c = runs_[m].ctl;
+            c.v0 = 3 * runs_[m].f0;
+            c.v1 = 3 * runs_[m].f1;
+            c.small = (c.v1 - c.v0) <= kTwoLoopMaxN ? 1 : 0;
+            set_mask(MK_ALL, m, true);
+            set_mask(MK_ADMM, m, true);
+        }
+        push_ctl();
     }
     lap("element state upload");
     chol.build(S, A_pos, A_ptr, A_con, st_);
@@ -378,14 +460,14 @@ void SolverGPU::initialize() {
     if (cfg.reweighting) {
         mid_candidates(true, cand_mode_now());
         count_++;
-        apply_weights();
+        apply_weights(MK_ALL);
     }
     if (cfg.autotune) {
         chol.autotune(d_w2_, d_Di_, ne, st_);
         lap("autotune (solve chunks, panel steps)");
     }
     factor();
-    m_k_ = 0;
+    for (MeshRun& R : runs_) R.ctl.k = 0;
     check_status();
     lap("first factorization (graph capture + run)");
     initialized_ = true;
@@ -399,78 +481,161 @@ int SolverGPU::cand_mode_now() const {
     return count_ > cfg.rw_delay ? CAND_HESSIAN : CAND_REST;
 }
 
-#define WRAPD_ELEM_LAUNCH(kernel, grid, block, ...)                    \
-    do {                                                               \
-        kernel<<<grid, block, 0, st_>>>(view(), __VA_ARGS__);          \
-        WRAPD_LAUNCH_CHECK();                                          \
-        kernel_launches++;                                             \
-    } while (0)
-
-void SolverGPU::grad_at_x(bool write_gel) {
-    WRAPD_ELEM_LAUNCH(k_grad, blocks_for(ne, 128), 128, d_x_, d_xfix_, mat_, write_gel ? 1 : 0, d_partials_,
-                      d_counter_, d_scal_ + S_GRAD);
-}
-
-void SolverGPU::gather(double* grad, const double* gold, double* ystage, const double* sstage, bool xerr) {
-    k_gather<<<blocks_for(8 * (int64_t)nf, 256), 256, 0, st_>>>(nf, d_inc_ptr_, d_inc_, d_gel_, ne, grad, gold, ystage, sstage,
-                                                   xerr ? d_x_ : nullptr, d_xsoln_, d_partials_, d_counter_,
-                                                   d_scal_ + S_GATHER);
-    WRAPD_LAUNCH_CHECK();
-    kernel_launches++;
-}
-
-void SolverGPU::local_step(int cand_mode, bool fp32_compute) {
-    if (cfg.model == MODEL_ARAP) {
-        k_local_arap<<<blocks_for(ne, 128), 128, 0, st_>>>(view(), d_partials_, d_counter_, d_scal_ + S_LOCAL);
-        WRAPD_LAUNCH_CHECK();
-        kernel_launches++;
+// ---- batch plumbing ------------------------------------------------------------------
+// Tiles of `per` items over each [first, end) range, meshes in order.
+void SolverGPU::build_tiles(TileSet& t, int per, const std::vector<std::pair<int, int>>& ranges) {
+    t.per = per;
+    t.n = ranges.empty() ? 0 : ranges.back().second;
+    if (ranges.size() == 1) {
+        t.count = blocks_for(ranges[0].second - ranges[0].first, per);
         return;
     }
-    // prox_mode 2 runs the network where the last stretches are a stale warm
-    // start: the first local step and the one after each reweight (the weight
-    // w^2 / vol, an input of the prox, has just changed); elsewhere the last
-    // stretches start the Newton prox at least as well and cost nothing.
-    const bool net = cfg.prox_mode == 2 && (logs_.reweighted.empty() || logs_.reweighted.back() != 0);
-    const int nb = blocks_for(ne, 128);
-    const int net_smem = net::IMAGE_BYTES + 4 * net::WARP_SCRATCH;
-    if (net && !d_net_img_) throw CudaError(WRAPD_E_STATE, "prox_mode 2 needs a network (wrapd_set_prox_net)");
-    if (fp32_compute) {
-        if (net)
-            k_local<float, true><<<nb, 128, net_smem, st_>>>(view(), mat_, cfg.prox_iters, cand_mode, 2, d_net_img_,
-                                                             d_partials_, d_counter_, d_scal_ + S_LOCAL);
-        else
-            k_local<float, false><<<nb, 128, 0, st_>>>(view(), mat_, cfg.prox_iters, cand_mode, 1, nullptr,
-                                                       d_partials_, d_counter_, d_scal_ + S_LOCAL);
-    } else {
-        if (net)
-            k_local<double, true><<<nb, 128, net_smem, st_>>>(view(), mat_, cfg.prox_iters, cand_mode, 2, d_net_img_,
-                                                              d_partials_, d_counter_, d_scal_ + S_LOCAL);
-        else
-            k_local<double, false><<<nb, 128, kLocalHistBytes, st_>>>(view(), mat_, cfg.prox_iters, cand_mode,
-                                                                      (fp32() || cfg.prox_mode == 2) ? 1 : cfg.prox_mode,
-                                                                      nullptr, d_partials_, d_counter_,
-                                                                      d_scal_ + S_LOCAL);
+    std::vector<int4> tab;
+    std::vector<int> t0;
+    for (size_t m = 0; m < ranges.size(); ++m) {
+        t0.push_back(static_cast<int>(tab.size()));
+        const int a = ranges[m].first, b = ranges[m].second;
+        for (int f = a; f < b; f += per) tab.push_back(make_int4((int)m, f, std::min(f + per, b), 0));
+        if (a == b) tab.push_back(make_int4((int)m, a, a, 0));
     }
+    t0.push_back(static_cast<int>(tab.size()));
+    t.count = static_cast<int>(tab.size());
+    t.d_t = dupload(tab);
+    t.d_tile0 = dupload(t0);
+}
+
+bool SolverGPU::any_mask(int which) const {
+    for (int m = 0; m < nm; ++m)
+        if (h_masks_[(size_t)which * nm + m]) return true;
+    return false;
+}
+
+// The pinned mirror of the control block is written only after the stream has
+// read the last upload from it (normally a synchronisation already passed it).
+void SolverGPU::ctl_writable() {
+    if (!ctl_pending_) return;
+    WRAPD_CUDA(cudaStreamSynchronize(st_));
+    ctl_pending_ = false;
+}
+
+// Uploads the masks, MeshCtl and rho of every mesh.
+void SolverGPU::push_ctl() {
+    ctl_writable();
+    for (int m = 0; m < nm; ++m) {
+        h_ctl_[m] = runs_[m].ctl;
+        std::memcpy(h_rho_ + (size_t)m * kHistSlots, runs_[m].rho, sizeof(runs_[m].rho));
+    }
+    WRAPD_CUDA(cudaMemcpyAsync(d_ctl_block_, h_ctl_block_, ctl_bytes_, cudaMemcpyHostToDevice, st_));
+    ctl_pending_ = true;
+}
+
+VecPools SolverGPU::pools() const {
+    VecPools P{};
+    for (int i = 0; i < 3; ++i) P.G[i] = d_G_[i];
+    for (int i = 0; i <= cfg.lbfgs_m; ++i) {
+        P.S[i] = d_S_[i];
+        P.Y[i] = d_Y_[i];
+    }
+    P.M = cfg.lbfgs_m;
+    return P;
+}
+
+const Logs& SolverGPU::mesh_logs(int m) const {
+    if (m < 0 || m >= nm) throw CudaError(WRAPD_E_INPUT, "mesh index out of range");
+    return runs_[m].logs;
+}
+
+#define WRAPD_ELEM_LAUNCH(kernel, tiles, block, ...)                                        \
+    do {                                                                                    \
+        kernel<<<(tiles).count, block, 0, st_>>>(view(), (tiles).view(), __VA_ARGS__);      \
+        WRAPD_LAUNCH_CHECK();                                                               \
+        kernel_launches++;                                                                  \
+    } while (0)
+
+void SolverGPU::grad_at_x(bool write_gel, int mk) {
+    WRAPD_ELEM_LAUNCH(k_grad, te128_, 128, mask(mk), d_x_, d_xfix_, mat_, write_gel ? 1 : 0, d_partials_,
+                      d_counters_, ds(S_GRAD), kScalStride);
+}
+
+void SolverGPU::gather(int mode, int mk, bool xerr, double* plain) {
+    k_gather<<<tv32_.count, 256, 0, st_>>>(tv32_.view(), mask(mk), mode, d_ctl_, pools(), plain, d_inc_ptr_, d_inc_,
+                                           d_gel_, ne, xerr ? d_x_ : nullptr, d_xsoln_, d_partials_, d_counters_,
+                                           ds(S_GATHER), kScalStride);
     WRAPD_LAUNCH_CHECK();
     kernel_launches++;
+}
+
+// The local step over the meshes of MK_ADMM, in the variants the masks
+// MK_L32 / MK_L32N / MK_L64 / MK_L64N assign them (set by the caller).
+void SolverGPU::local_step(int cand_mode) {
+    if (cfg.model == MODEL_ARAP) {
+        WRAPD_ELEM_LAUNCH(k_local_arap, te128_, 128, mask(MK_ADMM), d_partials_, d_counters_, ds(S_LOCAL), kScalStride);
+        return;
+    }
+    const int net_smem = local_net_bytes(te_local_.per);
+    if ((any_mask(MK_L32N) || any_mask(MK_L64N)) && !d_net_img_)
+        throw CudaError(WRAPD_E_STATE, "prox_mode 2 needs a network (wrapd_set_prox_net)");
+    const Tiles T = te_local_.view();
+    const int nb = te_local_.count, bt = te_local_.per;
+    if (any_mask(MK_L32N)) {
+        k_local<float, true><<<nb, bt, net_smem, st_>>>(view(), T, mask(MK_L32N), mat_, cfg.prox_iters, cand_mode, 2,
+                                                         d_net_img_, d_partials_, d_counters_, ds(S_LOCAL), kScalStride);
+        kernel_launches++;
+    }
+    if (any_mask(MK_L32)) {
+        k_local<float, false><<<nb, bt, 0, st_>>>(view(), T, mask(MK_L32), mat_, cfg.prox_iters, cand_mode, 1,
+                                                   nullptr, d_partials_, d_counters_, ds(S_LOCAL), kScalStride);
+        kernel_launches++;
+    }
+    if (any_mask(MK_L64N)) {
+        k_local<double, true><<<nb, bt, net_smem, st_>>>(view(), T, mask(MK_L64N), mat_, cfg.prox_iters, cand_mode, 2,
+                                                          d_net_img_, d_partials_, d_counters_, ds(S_LOCAL), kScalStride);
+        kernel_launches++;
+    }
+    if (any_mask(MK_L64)) {
+        k_local<double, false><<<nb, bt, local_hist_bytes(bt), st_>>>(view(), T, mask(MK_L64), mat_, cfg.prox_iters,
+                                                                  cand_mode,
+                                                                  (fp32() || cfg.prox_mode == 2) ? 1 : cfg.prox_mode,
+                                                                  nullptr, d_partials_, d_counters_, ds(S_LOCAL),
+                                                                  kScalStride);
+        kernel_launches++;
+    }
+    WRAPD_LAUNCH_CHECK();
+}
+
+// Which local-step variant each unconverged mesh runs this iteration:
+// FP32 arithmetic in mixed mode until its refinement phase; prox_mode 2 runs
+// the network where the last stretches are a stale warm start (the mesh's
+// first local step and the one after each of its reweights: the weight
+// w^2 / vol, an input of the prox, has just changed).
+static void set_local_masks(int nm, int* masks, const std::vector<bool>& act, const std::vector<bool>& f32,
+                            const std::vector<bool>& net) {
+    for (int m = 0; m < nm; ++m) {
+        masks[(size_t)MK_L32 * nm + m] = act[m] && f32[m] && !net[m];
+        masks[(size_t)MK_L32N * nm + m] = act[m] && f32[m] && net[m];
+        masks[(size_t)MK_L64 * nm + m] = act[m] && !f32[m] && !net[m];
+        masks[(size_t)MK_L64N * nm + m] = act[m] && !f32[m] && net[m];
+    }
 }
 
 void SolverGPU::local_step_unaware(int cand_mode, bool fp32_compute) {
     const int nb = blocks_for(ne, 128);
     if (fp32_compute && cfg.model == MODEL_NH)
         k_local_unaware<float><<<nb, 128, 0, st_>>>(view(), d_x_, d_xfix_, mat_, cfg.prox_iters, cand_mode, 1,
-                                                    d_partials_, d_counter_, d_scal_ + S_LOCAL);
+                                                    d_partials_, d_counters_, ds(S_LOCAL));
     else
         k_local_unaware<double><<<nb, 128, kLocalHistBytes, st_>>>(view(), d_x_, d_xfix_, mat_, cfg.prox_iters,
                                                                    cand_mode, (fp32() || cfg.prox_mode != 0) ? 1 : 0,
-                                                                   d_partials_, d_counter_, d_scal_ + S_LOCAL);
+                                                                   d_partials_, d_counters_, ds(S_LOCAL));
     WRAPD_LAUNCH_CHECK();
     kernel_launches++;
 }
 
 void SolverGPU::global_step_unaware() {
-    WRAPD_ELEM_LAUNCH(k_rhs_unaware, blocks_for(ne, 128), 128, d_xfix_);
-    gather(d_q_, nullptr, nullptr, nullptr);
+    k_rhs_unaware<<<blocks_for(ne, 128), 128, 0, st_>>>(view(), d_xfix_);
+    WRAPD_LAUNCH_CHECK();
+    kernel_launches++;
+    gather(GATHER_PLAIN, MK_ALL, false, d_q_);
     mark(1);
     chol.solve(d_q_, st_);
     kernel_launches += chol.launches_solve;
@@ -478,7 +643,7 @@ void SolverGPU::global_step_unaware() {
     mark(3);
     WRAPD_CUDA(cudaMemcpyAsync(d_x_, d_q_, 3 * (size_t)nf * sizeof(double), cudaMemcpyDeviceToDevice, st_));
     // update_defo_cache(x, true): singular values for the energy and flips
-    grad_at_x(false);
+    grad_at_x(false, MK_ALL);
     mark(1);
 }
 
@@ -496,13 +661,11 @@ void SolverGPU::set_prox_net(const float* blob) {
 }
 
 void SolverGPU::mid_candidates(bool from_x, int cand_mode) {
-    WRAPD_ELEM_LAUNCH(k_mid_candidates, blocks_for(ne, 128), 128, d_x_, d_xfix_, mat_, from_x ? 1 : 0, cand_mode);
+    WRAPD_ELEM_LAUNCH(k_mid_candidates, te128_, 128, mask(MK_ALL), d_x_, d_xfix_, mat_, from_x ? 1 : 0, cand_mode);
 }
 
-void SolverGPU::apply_weights() {
-    k_apply_weights<<<blocks_for(ne, 256), 256, 0, st_>>>(view());
-    WRAPD_LAUNCH_CHECK();
-    kernel_launches++;
+void SolverGPU::apply_weights(int mk) {
+    WRAPD_ELEM_LAUNCH(k_apply_weights, te256_, 256, mask(mk));
 }
 
 void SolverGPU::factor() {
@@ -540,8 +703,9 @@ void SolverGPU::profile_flush() {
 }
 
 void SolverGPU::sync_read() {
-    WRAPD_CUDA(cudaMemcpyAsync(h_scal_, d_scal_, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st_));
+    WRAPD_CUDA(cudaMemcpyAsync(h_scal_, d_scal_, (size_t)nm * kScalStride * sizeof(double), cudaMemcpyDeviceToHost, st_));
     WRAPD_CUDA(cudaStreamSynchronize(st_));
+    ctl_pending_ = false;
     n_sync++;
     mark(5);
 }
@@ -550,29 +714,74 @@ void SolverGPU::check_status() {
     int status = 0;
     WRAPD_CUDA(cudaMemcpyAsync(&status, chol.d_status, sizeof(int), cudaMemcpyDeviceToHost, st_));
     WRAPD_CUDA(cudaStreamSynchronize(st_));
+    ctl_pending_ = false;
     if (status != 0) {
         WRAPD_CUDA(cudaMemsetAsync(chol.d_status, 0, sizeof(int), st_));
         throw CudaError(status, "factorization of D^T W D hit a non-positive pivot");
     }
 }
 
-// |x - x_soln| (AlgorithmData::update_per_iter_data, src/AlgorithmData.cpp:66-78;
-// x_soln is the rest mesh when no solution mesh is given): q = x - x_soln,
-// <q, q> into the scalar block, read at the next sync.
-void SolverGPU::x_error_launch() {
-    const int n = 3 * nf;
-    k_axpy_dot<<<vec_blocks(n), 256, 0, st_>>>(n, d_q_, d_x_, d_xsoln_, d_scal_ + S_ONE, -1.0, nullptr, nullptr,
-                                               1.0, d_partials_, d_counter_, d_scal_ + S_XERR);
-    k_axpy_dot<<<vec_blocks(n), 256, 0, st_>>>(n, d_q_, nullptr, nullptr, nullptr, 0.0, d_q_, nullptr, 1.0,
-                                               d_partials_, d_counter_, d_scal_ + S_XERR);
+// |x - x_soln|^2 per mesh (AlgorithmData::update_per_iter_data,
+// src/AlgorithmData.cpp:66-78; x_soln is the rest mesh when no solution mesh
+// is given), into the scalar block, read at the next sync.
+void SolverGPU::x_error_launch(int mk) {
+    k_xerr<<<tvec_.count, 256, 0, st_>>>(tvec_.view(), mask(mk), d_x_, d_xsoln_, d_partials_, d_counters_, ds(S_XERR),
+                                         kScalStride);
     WRAPD_LAUNCH_CHECK();
-    kernel_launches += 2;
+    kernel_launches++;
 }
 
-double SolverGPU::x_error() {
-    x_error_launch();
-    sync_read();
-    return std::sqrt(h_scal_[S_XERR]);
+// The local step's tile (elements per CTA, 64, 128 or 256) timed on this
+// system's first local step: every candidate runs the step the solve will run
+// (its precision and prox), from the same saved state, which is restored
+// afterwards; the fastest is kept.  Called once, from the first begin_solve.
+void SolverGPU::autotune_local() {
+    const size_t e9 = 9 * (size_t)ne * sizeof(double), e3 = 3 * (size_t)ne * sizeof(double);
+    double* saved = static_cast<double*>(dalloc(2 * e9 + e3 + (size_t)ne * sizeof(double)));
+    char* sv = reinterpret_cast<char*>(saved);
+    auto copy_state = [&](bool save) {
+        const std::pair<double*, size_t> parts[] = {{d_Z_, e9}, {d_U_, e9}, {d_slast_, e3}, {d_w2c_, (size_t)ne * 8}};
+        size_t off = 0;
+        for (const auto& p : parts) {
+            if (save) WRAPD_CUDA(cudaMemcpyAsync(sv + off, p.first, p.second, cudaMemcpyDeviceToDevice, st_));
+            else WRAPD_CUDA(cudaMemcpyAsync(p.first, sv + off, p.second, cudaMemcpyDeviceToDevice, st_));
+            off += p.second;
+        }
+    };
+    std::vector<bool> act(nm, true), f32(nm), net(nm, false);
+    for (int m = 0; m < nm; ++m) f32[m] = fp32();
+    ctl_writable();
+    set_local_masks(nm, h_masks_, act, f32, net);
+    push_ctl();
+    std::vector<std::pair<int, int>> er;
+    for (const MeshRun& R : runs_) er.emplace_back(R.e0, R.e1);
+    cudaEvent_t e0, e1;
+    WRAPD_CUDA(cudaEventCreate(&e0));
+    WRAPD_CUDA(cudaEventCreate(&e1));
+    copy_state(true);
+    float best = 1e30f;
+    int pick = local_per_;
+    for (int per : {128, 64, 256}) {
+        build_tiles(te_local_, per, er);
+        for (int rep = 0; rep < 2; ++rep) {   // the first run warms up
+            copy_state(false);
+            WRAPD_CUDA(cudaEventRecord(e0, st_));
+            local_step(CAND_NONE);
+            WRAPD_CUDA(cudaEventRecord(e1, st_));
+            WRAPD_CUDA(cudaEventSynchronize(e1));
+        }
+        float ms = 0.f;
+        WRAPD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) { best = ms; pick = per; }
+    }
+    copy_state(false);
+    WRAPD_CUDA(cudaStreamSynchronize(st_));
+    ctl_pending_ = false;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    local_per_ = pick;
+    build_tiles(te_local_, local_per_, er);
+    local_tuned_ = true;
 }
 
 void SolverGPU::begin_solve() {
@@ -582,33 +791,50 @@ void SolverGPU::begin_solve() {
     pend_ = PendingTiming{};
     iter = 0;
     converged_ = false;
-    fp64_phase_ = false;
+    acc_time_s_.assign(1, 0.0);
     for (double& r : runtime_ms) r = 0.0;
+    for (int m = 0; m < nm; ++m) {
+        MeshRun& R = runs_[m];
+        R.logs = Logs();
+        R.converged = false;
+        R.fp64_phase = false;
+        R.m_tol = 1e-15;
+        set_mask(MK_ADMM, m, true);
+    }
+    push_ctl();
     // setup_solve (src/ADMM.cpp:89-107): X = X_init, defo cache, dual variables
     WRAPD_CUDA(cudaMemcpyAsync(d_x_, d_xinit_, 3 * (size_t)nf * sizeof(double), cudaMemcpyDeviceToDevice, st_));
-    grad_at_x(false);
+    grad_at_x(false, MK_ALL);
     if (cfg.rot_aware) {
-        WRAPD_ELEM_LAUNCH(k_init_dual, blocks_for(ne, 128), 128, d_x_, d_xfix_, mat_, d_partials_, d_counter_,
-                          d_scal_ + S_INIT);
+        WRAPD_ELEM_LAUNCH(k_init_dual, te128_, 128, mask(MK_ALL), d_x_, d_xfix_, mat_, d_partials_, d_counters_,
+                          ds(S_INIT), kScalStride);
     } else {
-        WRAPD_ELEM_LAUNCH(k_init_dual_unaware, blocks_for(ne, 128), 128, d_x_, d_xfix_);
+        k_init_dual_unaware<<<blocks_for(ne, 128), 128, 0, st_>>>(view(), d_x_, d_xfix_);
+        WRAPD_LAUNCH_CHECK();
+        kernel_launches++;
     }
+    x_error_launch(MK_ALL);
     sync_read();
-    curr_pe_ = cfg.rot_aware ? h_scal_[S_INIT] : 0.0;
-    // log_initial_data (src/AlgorithmData.cpp:50-64)
-    logs_.objectives.push_back(h_scal_[S_GRAD + 1]);
-    logs_.flips.push_back((int)h_scal_[S_GRAD + 2]);
-    logs_.reweighted.push_back(1);
-    logs_.acc_time_s.push_back(0.0);
-    logs_.x_errors.push_back(1.0);
-    init_xerr_ = x_error();
+    for (int m = 0; m < nm; ++m) {
+        MeshRun& R = runs_[m];
+        R.curr_pe = cfg.rot_aware ? hs(m, S_INIT) : 0.0;
+        // log_initial_data (src/AlgorithmData.cpp:50-64)
+        R.logs.objectives.push_back(hs(m, S_GRAD + 1));
+        R.logs.flips.push_back((int)hs(m, S_GRAD + 2));
+        R.logs.reweighted.push_back(1);
+        R.logs.acc_time_s.push_back(0.0);
+        R.logs.x_errors.push_back(1.0);
+        R.init_xerr = std::sqrt(hs(m, S_XERR));
+    }
+    if (nm > 1) union_logs(0);
+    if (cfg.autotune && !local_tuned_ && cfg.rot_aware && cfg.model == MODEL_NH) autotune_local();
     // initialize_weights (src/GlobalStepBehavior.hpp:223-230)
     if (cfg.reweighting) {
         mid_candidates(false, cand_mode_now());
         count_++;
-        apply_weights();
+        apply_weights(MK_ALL);
         factor();
-        m_k_ = 0;
+        for (MeshRun& R : runs_) R.ctl.k = 0;
         check_status();
     }
     solving_ = true;
@@ -617,84 +843,100 @@ void SolverGPU::begin_solve() {
     runtime_ms[0] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
-// SplitLBFGS::minimize (deps/mcloptlib/include/MCL/SplitLBFGS.hpp:114-256) with
-// LSMethod::None (rate 1).  On entry the gradient at x is in d_gcur_ and the
-// |grad - grad_old|^2 early-return test has passed.
 // Backtracking::search (deps/mcloptlib/include/MCL/Backtracking.hpp:71-98) as
-// SplitLBFGS::minimize calls it for -global_ls 1: p = -q, or -grad with
-// alpha0 = min(1, 1 / max|grad|) after a non-descent restart; Armijo decrease
-// 1e-4, step factor 0.7; a direction of norm <= machine epsilon returns 1e-4.
-// fx0 is the AL value of the last gradient evaluation, which was at x.  Each
-// trial value is one gradient-kernel pass (no gradient rows) at x + alpha p
-// into a staging vector; the element cache it leaves is refreshed by the
-// gradient at the accepted x.  On a non-descent restart the history reset of
-// SplitLBFGS.hpp:189-194 is applied here, before the search.
+// SplitLBFGS::minimize calls it for -global_ls 1 (single meshes): p = -q, or
+// -grad with alpha0 = min(1, 1 / max|grad|) after a non-descent restart;
+// Armijo decrease 1e-4, step factor 0.7; a direction of norm <= machine
+// epsilon returns 1e-4.  fx0 is the AL value of the last gradient evaluation,
+// which was at x.  Each trial value is one gradient-kernel pass (no gradient
+// rows) at x + alpha p into the stage vector; the element cache it leaves is
+// refreshed by the gradient at the accepted x.  On a non-descent restart the
+// history reset of SplitLBFGS.hpp:189-194 is applied here, before the search.
 double SolverGPU::line_search() {
     const int n = 3 * nf, vb = vec_blocks(n);
-    k_ls_norms<<<vb, 256, 0, st_>>>(n, d_q_, d_gcur_, d_partials_, d_counter_, d_scal_ + S_LSN);
-    k_ls_gmax<<<vb, 256, 0, st_>>>(n, d_gcur_, d_partials_, d_counter_, d_scal_ + S_LSM);
+    const MeshCtl& c = runs_[0].ctl;
+    double* gcur = d_G_[c.grot % 3];
+    double* trial = d_S_[c.stage];
+    k_ls_norms<<<vb, 256, 0, st_>>>(n, d_q_, gcur, d_partials_, d_counters_, ds(S_LSN));
+    k_ls_gmax<<<vb, 256, 0, st_>>>(n, gcur, d_partials_, d_counters_, ds(S_LSM));
     WRAPD_LAUNCH_CHECK();
     kernel_launches += 2;
     sync_read();
-    const double dir = h_scal_[S_DIR];
+    const double dir = hs(0, S_DIR);
     if (std::isnan(dir)) throw CudaError(WRAPD_E_NAN, "L-BFGS decrement is NaN");
     const bool restart = !(dir > 0.0);
     ls_restart_ = restart;
-    const double alpha0 = restart ? std::min(1.0, 1.0 / h_scal_[S_LSM]) : 1.0;
-    const double pnorm = std::sqrt(restart ? h_scal_[S_LSN + 1] : h_scal_[S_LSN]);
+    const double alpha0 = restart ? std::min(1.0, 1.0 / hs(0, S_LSM)) : 1.0;
+    const double pnorm = std::sqrt(restart ? hs(0, S_LSN + 1) : hs(0, S_LSN));
     const double decrease = 1.e-4, tau = 0.7;
     if (pnorm <= std::numeric_limits<double>::epsilon()) return decrease;
-    const double fx0 = h_scal_[S_GRAD];
-    const double gtp = restart ? -h_scal_[S_LSN + 1] : -dir;
-    const double* step = restart ? d_gcur_ : d_q_;
+    const double fx0 = hs(0, S_GRAD);
+    const double gtp = restart ? -hs(0, S_LSN + 1) : -dir;
+    const double* step = restart ? gcur : d_q_;
     double alpha = alpha0;
     for (int it = 0; it < 100000; ++it) {
-        k_ls_trial<<<vb, 256, 0, st_>>>(n, d_sstage_, d_x_, step, alpha);
+        k_ls_trial<<<vb, 256, 0, st_>>>(n, trial, d_x_, step, alpha);
         WRAPD_LAUNCH_CHECK();
         kernel_launches++;
-        WRAPD_ELEM_LAUNCH(k_grad, blocks_for(ne, 128), 128, d_sstage_, d_xfix_, mat_, 0, d_partials_, d_counter_,
-                          d_scal_ + S_LSV);
+        WRAPD_ELEM_LAUNCH(k_grad, te128_, 128, mask(MK_ALL), trial, d_xfix_, mat_, 0, d_partials_, d_counters_,
+                          ds(S_LSV), kScalStride);
         sync_read();
-        const double fxa = h_scal_[S_LSV];
+        const double fxa = hs(0, S_LSV);
         if (fxa <= fx0 + alpha * decrease * gtp) return alpha;
         alpha *= tau;
     }
     return -1.0;
 }
 
+// SplitLBFGS::minimize (deps/mcloptlib/include/MCL/SplitLBFGS.hpp:114-256) with
+// LSMethod::None (rate 1), for every mesh R with R.in_loop set: each mesh runs
+// its own minimize (its history, decrement, early exit and iteration budget),
+// all of them in the same launches; a mesh that exits is masked out of the
+// rest.  On entry each such mesh's gradient at x is in its cur buffer and the
+// |grad - grad_old|^2 early-return test has passed.  Sets R.its (the
+// minimize's return value) and R.obj_aft.
 int SolverGPU::lbfgs_minimize() {
-    const int M = cfg.lbfgs_m, n = 3 * nf, vb = vec_blocks(n);
-    int max_iters = cfg.global_iters, global_iter = 1;
-    bool breaking = false;
-    double* A = d_scal_ + S_ALPHA;
-    double* C = d_scal_ + S_C;
-    for (; global_iter <= max_iters; ++global_iter) {
-        const int it = std::min(M, m_k_);
-        const bool small = n <= kTwoLoopMaxN;
-        HistPtrs hs{}, hy{};
-        HistRho hr{};
-        if (small)
-            for (int i = 0; i < it; ++i) { hs.p[i] = s_[i]; hy.p[i] = y_[i]; hr.r[i] = rho_[i]; }
+    const int M = cfg.lbfgs_m;
+    const TwoLoopSlots sl{S_ALPHA, S_C, S_DIR};
+    for (MeshRun& R : runs_)
+        if (R.in_loop) R.max_iters = cfg.global_iters;
+    for (int gi = 1;; ++gi) {
+        // the meshes still in their loop (SplitLBFGS.hpp:145: global_iter <= max_iters)
+        bool any = false;
+        int jmax = 0;
+        for (int m = 0; m < nm; ++m) {
+            MeshRun& R = runs_[m];
+            if (R.in_loop && gi > R.max_iters) {
+                R.its = gi - 1;
+                R.in_loop = false;
+            }
+            set_mask(MK_LBFGS, m, R.in_loop);
+            set_mask(MK_SMALL, m, R.in_loop && R.ctl.small);
+            set_mask(MK_LARGE, m, R.in_loop && !R.ctl.small);
+            if (!R.in_loop) continue;
+            any = true;
+            R.ctl.it = std::min(M, R.ctl.k);
+            R.ctl.stage = (R.ctl.head + std::min(R.ctl.k, M)) % (M + 1);
+            if (!R.ctl.small) jmax = std::max(jmax, R.ctl.it);
+        }
+        if (!any) break;
+        push_ctl();
+        const bool small = any_mask(MK_SMALL), large = any_mask(MK_LARGE);
+        const VecPools P = pools();
         // first loop (newest to oldest): alpha_i = rho_i <s_i, q>, q -= alpha_i y_i
         if (small) {
-            k_two_loop_first<<<1, kTwoLoopThreads, 0, st_>>>(n, d_q_, d_gcur_, hs, hy, hr, it, A);
+            k_two_loop_first<<<nm, kTwoLoopThreads, 0, st_>>>(mask(MK_SMALL), d_ctl_, P, d_rho_, d_q_, sl, d_scal_,
+                                                              kScalStride);
             kernel_launches++;
-        } else if (it == 0) {
-            k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, d_gcur_, nullptr, nullptr, 0.0, nullptr, nullptr, 1.0,
-                                            d_partials_, d_counter_, d_scal_ + S_DUMMY);
-            kernel_launches++;
-        } else {
-            k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, d_gcur_, nullptr, nullptr, 0.0, s_[it - 1], nullptr,
-                                            rho_[it - 1], d_partials_, d_counter_, A + (it - 1));
-            for (int i = it - 2; i >= 0; --i)
-                k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, y_[i + 1], A + (i + 1), -1.0, s_[i], nullptr,
-                                                rho_[i], d_partials_, d_counter_, A + i);
-            k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, y_[0], A, -1.0, nullptr, nullptr, 1.0, d_partials_,
-                                            d_counter_, d_scal_ + S_DUMMY);
-            kernel_launches += it + 1;
         }
+        if (large)
+            for (int j = jmax - 1; j >= -1; --j) {
+                k_lbfgs_first<<<tvec_.count, 256, 0, st_>>>(tvec_.view(), mask(MK_LARGE), d_ctl_, P, d_rho_, d_q_, j, sl,
+                                                            d_partials_, d_counters_, d_scal_, kScalStride);
+                kernel_launches++;
+            }
         WRAPD_LAUNCH_CHECK();
-        // q = A^-1 q, three right-hand sides at once
+        // q = A^-1 q, three right-hand sides at once (the block-diagonal system)
         mark(2);
         chol.solve(d_q_, st_);
         kernel_launches += chol.launches_solve;
@@ -702,184 +944,253 @@ int SolverGPU::lbfgs_minimize() {
         mark(3);
         // second loop (oldest to newest): c_i = alpha_i - rho_i <y_i, q>, q += c_i s_i; then dir = <grad, q>
         if (small) {
-            k_two_loop_second<<<1, kTwoLoopThreads, 0, st_>>>(n, d_q_, d_gcur_, hs, hy, hr, it, A, C,
-                                                              d_scal_ + S_DIR);
+            k_two_loop_second<<<nm, kTwoLoopThreads, 0, st_>>>(mask(MK_SMALL), d_ctl_, P, d_rho_, d_q_, sl, d_scal_,
+                                                               kScalStride);
             kernel_launches++;
-        } else if (it == 0) {
-            k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, nullptr, nullptr, 0.0, d_gcur_, nullptr, 1.0,
-                                            d_partials_, d_counter_, d_scal_ + S_DIR);
-            kernel_launches++;
-        } else {
-            k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, nullptr, nullptr, 0.0, y_[0], A, -rho_[0], d_partials_,
-                                            d_counter_, C);
-            for (int i = 1; i < it; ++i)
-                k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, s_[i - 1], C + (i - 1), 1.0, y_[i], A + i, -rho_[i],
-                                                d_partials_, d_counter_, C + i);
-            k_axpy_dot<<<vb, 256, 0, st_>>>(n, d_q_, nullptr, s_[it - 1], C + (it - 1), 1.0, d_gcur_, nullptr, 1.0,
-                                            d_partials_, d_counter_, d_scal_ + S_DIR);
-            kernel_launches += it + 1;
         }
-        // -global_ls 1: Backtracking::search along p = -q (SplitLBFGS.hpp:196-206)
+        if (large)
+            for (int j = 0; j <= jmax; ++j) {
+                k_lbfgs_second<<<tvec_.count, 256, 0, st_>>>(tvec_.view(), mask(MK_LARGE), d_ctl_, P, d_rho_, d_q_, j,
+                                                             sl, d_partials_, d_counters_, d_scal_, kScalStride);
+                kernel_launches++;
+            }
+        WRAPD_LAUNCH_CHECK();
+        // -global_ls 1 (single meshes): Backtracking::search along p = -q (SplitLBFGS.hpp:196-206)
         double rate = 1.0;
-        if (cfg.global_ls && m_tol_ > 1.e-12) {
+        if (cfg.global_ls && runs_[0].m_tol > 1.e-12) {
             rate = line_search();
             if (rate <= 0.0) {   // SplitMinimizer::FAILURE, after the restart's history reset
-                if (ls_restart_) m_k_ = 0;
+                if (ls_restart_) runs_[0].ctl.k = 0;
+                runs_[0].in_loop = false;
+                runs_[0].its = -1;
                 return -1;
             }
         }
         // x -= rate q (or rate grad on a non-descent direction); s = x_new - x_old
-        k_xupdate<<<vb, 256, 0, st_>>>(n, d_x_, d_q_, d_gcur_, d_scal_ + S_DIR, rate, d_sstage_);
+        k_xupdate<<<tvec_.count, 256, 0, st_>>>(tvec_.view(), mask(MK_LBFGS), d_ctl_, P, d_x_, d_q_, d_scal_, S_DIR,
+                                                kScalStride, rate);
         WRAPD_LAUNCH_CHECK();
         kernel_launches++;
         mark(2);
         // gradient at the new x; y = grad_new - grad
-        grad_at_x(true);
-        gather(d_gnew_, d_gcur_, d_ystage_, d_sstage_, true);
+        grad_at_x(true, MK_LBFGS);
+        gather(GATHER_LBFGS, MK_LBFGS, true);
         mark(1);
         sync_read();
-        const double dir = h_scal_[S_DIR];
-        const double yy = h_scal_[S_GATHER], sy = h_scal_[S_GATHER + 1];
-        if (std::isnan(dir)) throw CudaError(WRAPD_E_NAN, "L-BFGS decrement is NaN");
-        if (dir <= 0.0) {
-            max_iters -= m_k_;
-            m_k_ = 0;
+        for (int m = 0; m < nm; ++m) {
+            MeshRun& R = runs_[m];
+            if (!R.in_loop) continue;
+            MeshCtl& c = R.ctl;
+            const double dir = hs(m, S_DIR);
+            const double yy = hs(m, S_GATHER), sy = hs(m, S_GATHER + 1);
+            if (std::isnan(dir)) throw CudaError(WRAPD_E_NAN, "L-BFGS decrement is NaN");
+            const int stage = c.stage;   // where this iteration's s and y were written
+            if (dir <= 0.0) {
+                R.max_iters -= c.k;
+                c.k = 0;
+                c.head = stage;          // the new entry becomes the oldest
+            } else if (c.k >= M) {
+                c.head = (c.head + 1) % (M + 1);   // erase(begin) + push_back
+            }
+            R.rho[stage] = 1.0 / sy;
+            c.grot += 1;                 // grad_old <- grad, grad <- grad_new
+            if (dir > 0.0 && (dir < cfg.kappa * R.m_tol || dir < cfg.kappa * 1.e-12)) {
+                c.k += 1;
+                R.its = gi;
+                R.in_loop = false;
+            } else if (std::fabs(yy) <= 0.0) {
+                R.its = gi;
+                R.in_loop = false;
+            } else {
+                c.k++;
+            }
         }
-        // history push: s[m_k] / y[m_k], or erase(begin) + push_back
-        if (m_k_ < M) {
-            std::swap(s_[m_k_], d_sstage_);
-            std::swap(y_[m_k_], d_ystage_);
-            rho_[m_k_] = 1.0 / sy;
-        } else {
-            double* so = s_[0];
-            double* yo = y_[0];
-            for (int i = 0; i + 1 < M; ++i) { s_[i] = s_[i + 1]; y_[i] = y_[i + 1]; rho_[i] = rho_[i + 1]; }
-            s_[M - 1] = d_sstage_; y_[M - 1] = d_ystage_; rho_[M - 1] = 1.0 / sy;
-            d_sstage_ = so; d_ystage_ = yo;
-        }
-        // grad_old <- grad, grad <- grad_new
-        double* t = d_gold_;
-        d_gold_ = d_gcur_;
-        d_gcur_ = d_gnew_;
-        d_gnew_ = t;
-        if (dir > 0.0 && (dir < cfg.kappa * m_tol_ || dir < cfg.kappa * 1.e-12)) {
-            m_k_ += 1;
-            breaking = true;
-            break;
-        }
-        if (std::fabs(yy) <= 0.0) { breaking = true; break; }
-        m_k_++;
     }
-    m_k_ = std::min(M, m_k_);
-    return breaking ? global_iter : global_iter - 1;
+    for (MeshRun& R : runs_) R.ctl.k = std::min(M, R.ctl.k);
+    return 0;
+}
+
+// A batch's summary log entry k (after iteration k - 1): sums over the
+// meshes of each one's latest entry (a converged mesh keeps its last values).
+void SolverGPU::union_logs(int k) {
+    double obj = 0.0, ls = 0.0, gs = 0.0, xe2 = 0.0, xi2 = 0.0, prox = 0.0;
+    int flips = 0, rw = 0, inner = 0;
+    for (const MeshRun& R : runs_) {
+        const Logs& L = R.logs;
+        obj += L.objectives.back();
+        flips += L.flips.back();
+        const double xe = L.x_errors.back() * R.init_xerr;
+        xe2 += xe * xe;
+        xi2 += R.init_xerr * R.init_xerr;
+        if (k > 0 && (int)L.objectives.size() == k + 1) {
+            rw |= L.reweighted.back();
+            inner += L.inner.back();
+            ls += L.ls_dal.back();
+            gs += L.gs_dal.back();
+            prox += L.prox_iters.back() * (R.e1 - R.e0);
+        }
+    }
+    logs_.objectives.push_back(obj);
+    logs_.flips.push_back(flips);
+    logs_.x_errors.push_back(xi2 > 0.0 ? std::sqrt(xe2 / xi2) : 0.0);
+    logs_.acc_time_s.push_back(0.0);
+    logs_.reweighted.push_back(k == 0 ? 1 : rw);
+    if (k > 0) {
+        logs_.inner.push_back(inner);
+        logs_.ls_dal.push_back(ls);
+        logs_.gs_dal.push_back(gs);
+        logs_.prox_iters.push_back(prox / double(ne));
+    }
 }
 
 int SolverGPU::iterate(int n, bool* conv) {
     if (!solving_) throw CudaError(WRAPD_E_STATE, "iterate before begin_solve");
     int done = 0;
     *conv = converged_;
+    std::vector<bool> act(nm), f32(nm), net(nm);
+    std::vector<double> dal(nm, 0.0), prox_it(nm, 0.0);
+    std::vector<int> its(nm, 0);
+    std::vector<char> rw(nm, 0);
     while (done < n && iter < cfg.max_iters && !converged_) {
         cudaEvent_t* ev_ = evs_[iter & 1];
+        const int k = iter;
+        // masks of this iteration: the meshes still iterating and their local-step variant
+        for (int m = 0; m < nm; ++m) {
+            const MeshRun& R = runs_[m];
+            act[m] = !R.converged;
+            f32[m] = fp32() && !R.fp64_phase;
+            net[m] = cfg.prox_mode == 2 && R.logs.reweighted.back() != 0;
+            set_mask(MK_ADMM, m, act[m]);
+            set_mask(MK_ZERO, m, act[m] && R.ctl.k == 0);
+            set_mask(MK_RW, m, false);
+        }
+        ctl_writable();
+        set_local_masks(nm, h_masks_, act, f32, net);
+        push_ctl();
         WRAPD_CUDA(cudaEventRecord(ev_[0], st_));
         mark(5);
-        double dal = 0.0, obj_bef = 0.0, obj_aft = 0.0, prox_it = 0.0;
-        int its = 1;
         if (cfg.rot_aware) {
             // ---- local step: polar_update (src/TetElements.cpp:256-356) ----
-            local_step(cand_mode_now(), fp32() && !fp64_phase_);
+            local_step(cand_mode_now());
             if (cfg.reweighting) count_++;
             mark(0);
             WRAPD_CUDA(cudaEventRecord(ev_[1], st_));
             // ---- global step: RotAwareGS::global_step (src/GlobalStepBehavior.hpp:246-258) ----
-            if (m_k_ == 0) WRAPD_CUDA(cudaMemsetAsync(d_gold_, 0, 3 * (size_t)nf * sizeof(double), st_));
-            grad_at_x(true);
-            gather(d_gcur_, d_gold_, nullptr, nullptr, true);
+            if (any_mask(MK_ZERO)) {
+                k_zero_old<<<tvec_.count, 256, 0, st_>>>(tvec_.view(), mask(MK_ZERO), d_ctl_, pools());
+                WRAPD_LAUNCH_CHECK();
+                kernel_launches++;
+            }
+            grad_at_x(true, MK_ADMM);
+            gather(GATHER_START, MK_ADMM, true);
             mark(1);
             sync_read();
             settle_timing(false);   // the previous iteration's events are behind this synchronisation
-            const double bef = h_scal_[S_LOCAL], aft = h_scal_[S_LOCAL + 1], pe = h_scal_[S_LOCAL + 2];
-            prox_it = h_scal_[S_LOCAL + 4];
-            if (h_scal_[S_LOCAL + 3] > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
-            dal = aft - bef + pe - curr_pe_;
-            curr_pe_ = pe;
-            obj_bef = h_scal_[S_GRAD];
-            m_tol_ = std::fabs(dal);
-            its = 0;
-            if (!(h_scal_[S_GATHER] < 1.e-13)) its = lbfgs_minimize();
-            obj_aft = h_scal_[S_GRAD];
+            for (int m = 0; m < nm; ++m) {
+                MeshRun& R = runs_[m];
+                R.in_loop = false;
+                if (!act[m]) continue;
+                const double bef = hs(m, S_LOCAL), aft = hs(m, S_LOCAL + 1), pe = hs(m, S_LOCAL + 2);
+                prox_it[m] = hs(m, S_LOCAL + 4);
+                if (hs(m, S_LOCAL + 3) > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
+                dal[m] = aft - bef + pe - R.curr_pe;
+                R.curr_pe = pe;
+                R.obj_bef = hs(m, S_GRAD);
+                R.m_tol = std::fabs(dal[m]);
+                R.its = 0;
+                R.in_loop = !(hs(m, S_GATHER) < 1.e-13);
+            }
+            if (lbfgs_minimize() < 0) {
+                // a failed global line search ends the minimize with -1 (single mesh)
+            }
+            for (int m = 0; m < nm; ++m) its[m] = act[m] ? runs_[m].its : 0;
         } else {
-            // ---- local_update: TetElements::update (src/TetElements.cpp:193-254) ----
-            local_step_unaware(cand_mode_now(), fp32() && !fp64_phase_);
+            // ---- local_update: TetElements::update (src/TetElements.cpp:193-254), single mesh ----
+            local_step_unaware(cand_mode_now(), fp32() && !runs_[0].fp64_phase);
             if (cfg.reweighting) count_++;
             mark(0);
             WRAPD_CUDA(cudaEventRecord(ev_[1], st_));
             // ---- UnawareGS::global_step (src/GlobalStepBehavior.hpp:162-180): x = A^-1 b ----
             global_step_unaware();
+            x_error_launch(MK_ALL);
             sync_read();
-            prox_it = h_scal_[S_LOCAL + 4];
-            if (h_scal_[S_LOCAL + 3] > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
-            obj_aft = 1.e8;   // UnawareGS::last_step_delta_auglag (src/GlobalStepBehavior.hpp:102)
+            prox_it[0] = hs(0, S_LOCAL + 4);
+            if (hs(0, S_LOCAL + 3) > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
+            dal[0] = 0.0;
+            its[0] = 1;
         }
-        const double pe_x = h_scal_[S_GRAD + 1];
-        const int flips = (int)h_scal_[S_GRAD + 2];
         WRAPD_CUDA(cudaEventRecord(ev_[2], st_));
-        // ---- reweighting: possibly_update_weights (src/System.cpp:50-63) ----
-        bool rw = false;
+        // ---- reweighting: possibly_update_weights (src/System.cpp:50-63), per mesh ----
+        bool any_rw = false;
+        for (int m = 0; m < nm; ++m) rw[m] = 0;
         if (cfg.reweighting) {
             if (cfg.rw_every > 0) {
-                rw = ((iter + 1) % cfg.rw_every) == 0;
+                for (int m = 0; m < nm; ++m) rw[m] = act[m] && ((k + 1) % cfg.rw_every) == 0;
             } else {
-                k_ratio<<<blocks_for(ne, 256), 256, 0, st_>>>(view(), d_partials_, d_counter_, d_scal_ + S_RATIO);
-                WRAPD_LAUNCH_CHECK();
-                kernel_launches++;
+                WRAPD_ELEM_LAUNCH(k_ratio, te256_, 256, mask(MK_ADMM), d_partials_, d_counters_, ds(S_RATIO),
+                                  kScalStride);
                 sync_read();
-                rw = h_scal_[S_RATIO] > cfg.gamma;
+                for (int m = 0; m < nm; ++m) rw[m] = act[m] && hs(m, S_RATIO) > cfg.gamma;
             }
-            if (rw) {
-                apply_weights();
+            for (int m = 0; m < nm; ++m) {
+                set_mask(MK_RW, m, rw[m] != 0);
+                any_rw = any_rw || rw[m];
+            }
+            if (any_rw) {
+                push_ctl();
+                apply_weights(MK_RW);
                 factor();
-                m_k_ = 0;
+                for (int m = 0; m < nm; ++m)
+                    if (rw[m]) runs_[m].ctl.k = 0;
             }
         }
         WRAPD_CUDA(cudaEventRecord(ev_[3], st_));
-        // The x error of the final x: the rotation-aware step's last gradient
-        // gather computed it (outside the timed phases, as the reference logs it);
-        // the rotation-unaware step computes it here.
-        if (!cfg.rot_aware) {
-            x_error_launch();
-            sync_read();
-        }
-        const double xerr2 = cfg.rot_aware ? h_scal_[S_GATHER + 2] : h_scal_[S_XERR];
         if (profiling) {
             sync_read();
             profile_flush();
         }
-        if (rw) check_status();
-        runtime_ms[5] += its;
-        // ---- AlgorithmData::update_per_iter_* (src/AlgorithmData.cpp:66-83) ----
-        const int k = iter;
-        logs_.reweighted.push_back(rw ? 1 : 0);
-        logs_.ls_dal.push_back(std::fabs(dal));
-        logs_.gs_dal.push_back(std::fabs(obj_aft - obj_bef));
-        logs_.inner.push_back(its);
-        logs_.prox_iters.push_back(prox_it / double(ne));
-        logs_.objectives.push_back(pe_x);
-        logs_.flips.push_back(flips);
+        if (any_rw) check_status();
+        // ---- AlgorithmData::update_per_iter_* (src/AlgorithmData.cpp:66-83), per mesh ----
+        acc_time_s_.push_back(0.0);
+        int its_sum = 0;
+        for (int m = 0; m < nm; ++m) {
+            if (!act[m]) continue;
+            MeshRun& R = runs_[m];
+            Logs& L = R.logs;
+            // the energy, flips and x error of the final x: the mesh's last gradient
+            // evaluation and gather (or the rotation-unaware step's) computed them,
+            // outside the timed phases, as the reference logs them
+            const double obj_aft = cfg.rot_aware ? hs(m, S_GRAD) : 1.e8;   // UnawareGS (GlobalStepBehavior.hpp:102)
+            const double pe_x = hs(m, S_GRAD + 1);
+            const int flips = (int)hs(m, S_GRAD + 2);
+            const double xerr2 = cfg.rot_aware ? hs(m, S_GATHER + 2) : hs(m, S_XERR);
+            L.reweighted.push_back(rw[m] ? 1 : 0);
+            L.ls_dal.push_back(std::fabs(dal[m]));
+            L.gs_dal.push_back(cfg.rot_aware ? std::fabs(obj_aft - R.obj_bef) : std::fabs(obj_aft));
+            L.inner.push_back(its[m]);
+            L.prox_iters.push_back(prox_it[m] / double(R.e1 - R.e0));
+            L.objectives.push_back(pe_x);
+            L.flips.push_back(flips);
+            L.acc_time_s.push_back(0.0);
+            L.x_errors.push_back(std::sqrt(xerr2) / R.init_xerr);
+            its_sum += its[m];
+            // ---- ADMM::converged (src/ADMM.cpp:158-169) ----
+            const double res = std::fabs(L.objectives[k + 1] - L.objectives[k]) / (std::fabs(L.objectives[k + 1]) + 1.0);
+            // Mixed mode refinement: once the energy moves less than FP32 can
+            // resolve, finish with FP64 local steps.
+            if (fp32() && !R.fp64_phase && res < kMixedSwitch) R.fp64_phase = true;
+            if ((L.flips[k + 1] == 0 && L.flips[k] == 0 && res < cfg.tol) || (have_soln_ && L.x_errors.back() < 1.e-4))
+                R.converged = true;
+        }
+        runtime_ms[5] += its_sum;
+        if (nm > 1) union_logs(k + 1);
         // phase times: read once a later synchronisation has passed the events
-        logs_.acc_time_s.push_back(0.0);
         pend_ = PendingTiming{true, k, ev_};
-        if (!cfg.rot_aware || profiling || rw) settle_timing(false);
-        const double xe = std::sqrt(xerr2) / init_xerr_;
-        logs_.x_errors.push_back(xe);
+        if (!cfg.rot_aware || profiling || any_rw) settle_timing(false);
         iter = k + 1;
         done++;
-        // ---- ADMM::converged (src/ADMM.cpp:158-169) ----
-        const double res = std::fabs(logs_.objectives[k + 1] - logs_.objectives[k]) / (std::fabs(logs_.objectives[k + 1]) + 1.0);
-        // Mixed mode refinement: once the energy moves less than FP32 can
-        // resolve, finish with FP64 local steps.
-        if (fp32() && !fp64_phase_ && res < kMixedSwitch) fp64_phase_ = true;
-        if ((logs_.flips[k + 1] == 0 && logs_.flips[k] == 0 && res < cfg.tol) || (have_soln_ && xe < 1.e-4))
-            converged_ = true;
+        converged_ = true;
+        for (const MeshRun& R : runs_) converged_ = converged_ && R.converged;
     }
     settle_timing(true);
     *conv = converged_;
@@ -887,7 +1198,7 @@ int SolverGPU::iterate(int n, bool* conv) {
 }
 
 // Adds a finished iteration's phase times (CUDA events) to the runtime and its
-// accumulated-time log entry.  wait = false: a host synchronisation of the
+// accumulated-time log entries.  wait = false: a host synchronisation of the
 // stream has already passed the events.
 void SolverGPU::settle_timing(bool wait) {
     if (!pend_.on) return;
@@ -897,7 +1208,12 @@ void SolverGPU::settle_timing(bool wait) {
     WRAPD_CUDA(cudaEventElapsedTime(&mg, pend_.ev[1], pend_.ev[2]));
     WRAPD_CUDA(cudaEventElapsedTime(&mr, pend_.ev[2], pend_.ev[3]));
     runtime_ms[1] += ml; runtime_ms[2] += mg; runtime_ms[3] += mr;
-    logs_.acc_time_s[pend_.k + 1] = (runtime_ms[1] + runtime_ms[2] + runtime_ms[3]) / 1000.0;
+    const double t = (runtime_ms[1] + runtime_ms[2] + runtime_ms[3]) / 1000.0;
+    const size_t j = (size_t)pend_.k + 1;
+    acc_time_s_[j] = t;
+    for (MeshRun& R : runs_)
+        if (R.logs.acc_time_s.size() > j) R.logs.acc_time_s[j] = t;
+    if (logs_.acc_time_s.size() > j) logs_.acc_time_s[j] = t;
     pend_.on = false;
 }
 
@@ -905,6 +1221,7 @@ void SolverGPU::positions(double* out) {
     std::vector<double> xp(3 * (size_t)nf);
     WRAPD_CUDA(cudaMemcpyAsync(xp.data(), d_x_, xp.size() * sizeof(double), cudaMemcpyDeviceToHost, st_));
     WRAPD_CUDA(cudaStreamSynchronize(st_));
+    ctl_pending_ = false;
     // finish_solve (src/ADMM.cpp:171-182): X = S_free x_free + S_fix x_fix
     for (int i = 0; i < nv; ++i)
         for (int c = 0; c < 3; ++c)
@@ -921,11 +1238,13 @@ void SolverGPU::solve(double* out) {
 }
 
 // ---- components ------------------------------------------------------------------
+// Element-level steps over every mesh; the returned sums are over the batch.
 void SolverGPU::download_elem(const double* d, int comps, std::vector<double>& out) {
     const size_t n = (size_t)comps * ne;
     std::vector<double> soa(n);
     WRAPD_CUDA(cudaMemcpyAsync(soa.data(), d, n * 8, cudaMemcpyDeviceToHost, st_));
     WRAPD_CUDA(cudaStreamSynchronize(st_));
+    ctl_pending_ = false;
     out.resize(n);
     for (int e = 0; e < ne; ++e)
         for (int k = 0; k < comps; ++k) out[(size_t)e * comps + k] = soa[(size_t)k * ne + e];
@@ -938,6 +1257,7 @@ void SolverGPU::upload_elem(double* d, int comps, const double* in) {
         for (int k = 0; k < comps; ++k) soa[(size_t)k * ne + e] = in[(size_t)e * comps + k];
     WRAPD_CUDA(cudaMemcpyAsync(d, soa.data(), n * 8, cudaMemcpyHostToDevice, st_));
     WRAPD_CUDA(cudaStreamSynchronize(st_));
+    ctl_pending_ = false;
 }
 
 void SolverGPU::get_state(const std::string& name, std::vector<double>& out) {
@@ -952,8 +1272,16 @@ void SolverGPU::get_state(const std::string& name, std::vector<double>& out) {
     else if (name == "vol") download_elem(d_vol_, 1, out);
     else if (name == "xfree" || name == "grad") {
         std::vector<double> xp(3 * (size_t)nf);
-        WRAPD_CUDA(cudaMemcpyAsync(xp.data(), name == "xfree" ? d_x_ : d_gcur_, xp.size() * 8, cudaMemcpyDeviceToHost, st_));
+        if (name == "xfree") {
+            WRAPD_CUDA(cudaMemcpyAsync(xp.data(), d_x_, xp.size() * 8, cudaMemcpyDeviceToHost, st_));
+        } else {
+            // each mesh's range from its own cur buffer
+            for (const MeshRun& R : runs_)
+                WRAPD_CUDA(cudaMemcpyAsync(xp.data() + 3 * (size_t)R.f0, d_G_[R.ctl.grot % 3] + 3 * (size_t)R.f0,
+                                           3 * (size_t)(R.f1 - R.f0) * 8, cudaMemcpyDeviceToHost, st_));
+        }
         WRAPD_CUDA(cudaStreamSynchronize(st_));
+        ctl_pending_ = false;
         out.resize(xp.size());
         for (int i = 0; i < nf; ++i)
             for (int c = 0; c < 3; ++c) out[3 * (size_t)i + c] = xp[3 * (size_t)iperm_[i] + c];
@@ -976,44 +1304,64 @@ void SolverGPU::set_state(const std::string& name, const double* in, int64_t n) 
             for (int c = 0; c < 3; ++c) xp[3 * (size_t)iperm_[i] + c] = in[3 * (size_t)i + c];
         WRAPD_CUDA(cudaMemcpyAsync(d_x_, xp.data(), xp.size() * 8, cudaMemcpyHostToDevice, st_));
         WRAPD_CUDA(cudaStreamSynchronize(st_));
+        ctl_pending_ = false;
     } else {
         throw CudaError(WRAPD_E_INPUT, "state " + name + " is read-only");
     }
 }
 
 void SolverGPU::update_defo_cache() {
-    grad_at_x(false);
+    grad_at_x(false, MK_ALL);
     sync_read();
 }
 
 double SolverGPU::polar_update(bool update_candidates) {
-    local_step(update_candidates ? cand_mode_now() : CAND_NONE, fp32() && !fp64_phase_);
+    std::vector<bool> act(nm, true), f32(nm), net(nm, false);
+    for (int m = 0; m < nm; ++m) {
+        f32[m] = fp32() && !runs_[m].fp64_phase;
+        set_mask(MK_ADMM, m, true);
+    }
+    ctl_writable();
+    set_local_masks(nm, h_masks_, act, f32, net);
+    push_ctl();
+    local_step(update_candidates ? cand_mode_now() : CAND_NONE);
     if (update_candidates && cfg.reweighting) count_++;
     sync_read();
-    if (h_scal_[S_LOCAL + 3] > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
-    const double dal = h_scal_[S_LOCAL + 1] - h_scal_[S_LOCAL] + h_scal_[S_LOCAL + 2] - curr_pe_;
-    curr_pe_ = h_scal_[S_LOCAL + 2];
+    double dal = 0.0;
+    for (int m = 0; m < nm; ++m) {
+        if (hs(m, S_LOCAL + 3) > 0.0) throw CudaError(WRAPD_E_PROX_NEG, "negative singular value in a prox solution");
+        dal += hs(m, S_LOCAL + 1) - hs(m, S_LOCAL) + hs(m, S_LOCAL + 2) - runs_[m].curr_pe;
+        runs_[m].curr_pe = hs(m, S_LOCAL + 2);
+    }
     return dal;
 }
 
 double SolverGPU::global_grad(const double* xfree, double* grad) {
     if (xfree) set_state("xfree", xfree, 3LL * nf);
-    grad_at_x(true);
-    gather(d_gcur_, nullptr, nullptr, nullptr);
+    grad_at_x(true, MK_ALL);
+    gather(GATHER_START, MK_ALL, false);
     sync_read();
     if (grad) {
         std::vector<double> g;
         get_state("grad", g);
         std::memcpy(grad, g.data(), g.size() * sizeof(double));
     }
-    return h_scal_[S_GRAD];
+    double v = 0.0;
+    for (int m = 0; m < nm; ++m) v += hs(m, S_GRAD);
+    return v;
 }
 
 void SolverGPU::potential_energy(double* pe, int* flips) {
-    grad_at_x(false);
+    grad_at_x(false, MK_ALL);
     sync_read();
-    if (pe) *pe = h_scal_[S_GRAD + 1];
-    if (flips) *flips = (int)h_scal_[S_GRAD + 2];
+    double p = 0.0;
+    int f = 0;
+    for (int m = 0; m < nm; ++m) {
+        p += hs(m, S_GRAD + 1);
+        f += (int)hs(m, S_GRAD + 2);
+    }
+    if (pe) *pe = p;
+    if (flips) *flips = f;
 }
 
 void SolverGPU::solve_A(const double* b, double* x) {
@@ -1026,6 +1374,7 @@ void SolverGPU::solve_A(const double* b, double* x) {
     kernel_launches += chol.launches_solve;
     WRAPD_CUDA(cudaMemcpyAsync(xp.data(), d_q_, xp.size() * 8, cudaMemcpyDeviceToHost, st_));
     WRAPD_CUDA(cudaStreamSynchronize(st_));
+    ctl_pending_ = false;
     for (int i = 0; i < nf; ++i)
         for (int c = 0; c < 3; ++c) x[3 * (size_t)i + c] = xp[3 * (size_t)iperm_[i] + c];
 }

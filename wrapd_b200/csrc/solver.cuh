@@ -21,14 +21,27 @@ struct Logs {
     std::vector<int> flips, reweighted, inner;
 };
 
+// One tiling of a launch over the batch (see Tiles in common.cuh): device
+// table of {mesh, first, end} per tile and each mesh's first tile.  With one
+// mesh no table is used (tile b covers [b * per, (b + 1) * per)).
+struct TileSet {
+    int4* d_t = nullptr;
+    int* d_tile0 = nullptr;
+    int n = 0, per = 0, count = 0;
+    Tiles view() const { return Tiles{d_t, d_tile0, n, per, count}; }
+};
+
 class SolverGPU {
 public:
     explicit SolverGPU(const wrapd_settings& s);
     ~SolverGPU();
 
     // Appends one mesh (pins: its own vertex ids).  Several meshes make a
-    // batch solved as one block-diagonal system; youngs/poisson > 0 give the
-    // mesh its own material (else the settings').
+    // batch: one launch per kernel over all their elements and one
+    // factorization of the block-diagonal system, while each mesh keeps the
+    // decisions of its own reference Solver (L-BFGS early exit and history,
+    // reweighting, convergence) and stops when it converges; youngs/poisson > 0
+    // give the mesh its own material (else the settings').
     Material material(double youngs, double poisson) const;
     void add_mesh(const double* rest, const double* init, const double* soln, int nv, const int32_t* tets, int ne,
                   const int32_t* pins, int np, double youngs = 0.0, double poisson = 0.0);
@@ -50,7 +63,14 @@ public:
     void potential_energy(double* pe, int* flips);
     void solve_A(const double* b, double* x);
 
-    const Logs& logs() const { return logs_; }
+    // The logs of a single mesh; of a batch, the sums over its meshes
+    // (energies, flips, inner iterations), any reweight, and the x error of
+    // the whole batch.  mesh_logs(m): the logs of mesh m of a batch.
+    const Logs& logs() const { return nm == 1 ? runs_[0].logs : logs_; }
+    const Logs& mesh_logs(int m) const;
+    int meshes() const { return nm; }
+    int local_tile() const { return local_per_; }
+    bool initialized() const { return initialized_; }
     // Optional per-phase device timeline (CUDA events on the handle's stream):
     // slots of kProfileNames, accumulated ms and counts.
     static constexpr int kProfileSlots = 6;
@@ -66,6 +86,7 @@ public:
     int64_t n_factor = 0, n_solve = 0, n_sync = 0;
 
 private:
+    static constexpr int kScalStride = 96;   // scalars per mesh in the device scalar block
     bool fp32() const { return cfg.precision == 1; }
     ElemView view();
     void* dalloc(size_t bytes);
@@ -77,21 +98,34 @@ private:
     std::vector<cudaEvent_t> event_pool_;
     size_t event_next_ = 0;
     void check_status();
-    void grad_at_x(bool write_gel);
-    void gather(double* grad, const double* gold, double* ystage, const double* sstage, bool xerr = false);
+    void grad_at_x(bool write_gel, int mask);
+    void gather(int mode, int mask, bool xerr, double* plain = nullptr);
     void local_step_unaware(int cand_mode, bool fp32_compute);
     void global_step_unaware();
-    void local_step(int cand_mode, bool fp32_compute);
+    void local_step(int cand_mode);
     void mid_candidates(bool from_x, int cand_mode);
-    void apply_weights();
+    void apply_weights(int mask);
     void factor();
     int lbfgs_minimize();
     double line_search();
     int cand_mode_now() const;
     void download_elem(const double* d, int comps, std::vector<double>& out);
     void upload_elem(double* d, int comps, const double* in);
-    double x_error();
-    void x_error_launch();
+    void x_error_launch(int mask);
+    // batch plumbing
+    void build_tiles(TileSet& t, int per, const std::vector<std::pair<int, int>>& ranges);
+    const int* mask(int which) const { return d_ctl_block_masks_ + (size_t)which * nm; }
+    void set_mask(int which, int m, bool on) {
+        ctl_writable();
+        h_masks_[(size_t)which * nm + m] = on ? 1 : 0;
+    }
+    void ctl_writable();          // waits for the last control-block upload to be read
+    bool any_mask(int which) const;
+    void push_ctl();
+    VecPools pools() const;
+    double& hs(int m, int slot) { return h_scal_[(size_t)m * kScalStride + slot]; }
+    double* ds(int slot) const { return d_scal_ + slot; }
+    void union_logs(int k);
 
     // host mesh
     std::vector<double> rest_, init_, soln_;
@@ -119,25 +153,51 @@ private:
     double *d_Z_ = nullptr, *d_U_ = nullptr, *d_symF_ = nullptr, *d_sig_ = nullptr, *d_slast_ = nullptr, *d_gel_ = nullptr;
     int *d_inc_ptr_ = nullptr, *d_inc_ = nullptr;
     double *d_x_ = nullptr, *d_xfix_ = nullptr, *d_xsoln_ = nullptr, *d_xinit_ = nullptr;
-    double *d_q_ = nullptr, *d_gcur_ = nullptr, *d_gold_ = nullptr, *d_gnew_ = nullptr;
-    double *d_sstage_ = nullptr, *d_ystage_ = nullptr;
-    std::vector<double*> s_, y_;
-    std::vector<double> rho_;
+    double* d_q_ = nullptr;
+    double* d_G_[3] = {};                  // gradient ring (see VecPools)
+    std::vector<double*> d_S_, d_Y_;       // history slots, lbfgs_m + 1 each
     double* d_partials_ = nullptr;
     unsigned char* d_net_img_ = nullptr;   // prox network image + FP32 blob staging
-    unsigned* d_counter_ = nullptr;
-    double* d_scal_ = nullptr;
+    unsigned* d_counters_ = nullptr;       // one grid-reduction counter per mesh
+    double* d_scal_ = nullptr;             // kScalStride scalars per mesh
     double* h_scal_ = nullptr;
+    // ---- the meshes of the batch: each its own ADMM and L-BFGS state ----
+    int nm = 0;
+    struct MeshRun {
+        int e0 = 0, e1 = 0, f0 = 0, f1 = 0;    // element range, free-vertex range (dissection order)
+        MeshCtl ctl{};                          // rings and history length, as the kernels see them
+        double rho[kHistSlots] = {};            // 1 / <s, y> per history slot
+        double m_tol = 1e-15, curr_pe = 0.0, init_xerr = 1.0, obj_bef = 0.0;
+        bool converged = false, fp64_phase = false;
+        Logs logs;
+        // one SplitLBFGS::minimize call
+        int max_iters = 0, its = 0;
+        bool in_loop = false;
+    };
+    std::vector<MeshRun> runs_;
+    TileSet te128_, te256_, tv32_, tvec_;
+    TileSet te_local_;                     // the local step's element tiles (local_per_ elements each)
+    int local_per_ = 128;
+    bool local_tuned_ = false;
+    void autotune_local();
+    // control block on the device and its pinned mirror: masks (kMasks x nm
+    // ints), then MeshCtl (nm), then rho (nm x kHistSlots doubles)
+    void* d_ctl_block_ = nullptr;
+    void* h_ctl_block_ = nullptr;
+    size_t ctl_bytes_ = 0;
+    int* d_ctl_block_masks_ = nullptr;
+    int* h_masks_ = nullptr;
+    MeshCtl* d_ctl_ = nullptr;
+    MeshCtl* h_ctl_ = nullptr;
+    double* d_rho_ = nullptr;
+    double* h_rho_ = nullptr;
+    bool ctl_pending_ = false;             // an upload not yet passed by a stream synchronisation
+    std::vector<double> acc_time_s_;       // local + global + refactor seconds after each iteration
     // algorithm state
     int count_ = 0;          // reweight-delay counter (src/TetElements.cpp:404)
-    int m_k_ = 0;
-    double m_tol_ = 1e-15;
     bool ls_restart_ = false;   // the last line search followed a non-descent restart
-    double curr_pe_ = 0.0;
-    double init_xerr_ = 1.0;
     bool initialized_ = false, solving_ = false, converged_ = false;
-    bool fp64_phase_ = false;   // mixed mode: switched to FP64 local steps (refinement)
-    Logs logs_;
+    Logs logs_;              // a batch's summary logs
 };
 
 }  // namespace wrapd

@@ -121,13 +121,20 @@ class Solver:
         return x
 
     # -- data ---------------------------------------------------------------
-    def log(self, name: str) -> np.ndarray:
+    def log(self, name: str, mesh: int | None = None) -> np.ndarray:
+        """AlgorithmData log `name`; of a batch, the batch summary, or with
+        mesh = m the log of the m-th mesh added (its own solve)."""
         n = ctypes.c_int(0)
         h = self._h
-        h.check(h.lib.wrapd_get_log(h.h, capi.LOGS[name], None, 0, ctypes.byref(n)))
+
+        def get(out, cap):
+            if mesh is None:
+                return h.lib.wrapd_get_log(h.h, capi.LOGS[name], out, cap, ctypes.byref(n))
+            return h.lib.wrapd_get_mesh_log(h.h, int(mesh), capi.LOGS[name], out, cap, ctypes.byref(n))
+        h.check(get(None, 0))
         out = np.empty(n.value)
         if n.value:
-            h.check(h.lib.wrapd_get_log(h.h, capi.LOGS[name], capi.dptr(out), n.value, ctypes.byref(n)))
+            h.check(get(capi.dptr(out), n.value))
         return out
 
     def runtime(self) -> dict:
@@ -146,15 +153,16 @@ class Solver:
         return dict(zip(["kernel_launches", "factorizations", "solves", "host_syncs"], list(v)))
 
     def tuning(self) -> dict:
-        """Tile shapes in use (wrapd_get_tuning): the fused panel-step limit and
-        the solve chunk length per level and direction."""
+        """Tile shapes in use (wrapd_get_tuning): the fused panel-step limit, the
+        solve chunk length per level and direction, the local step's tile."""
         n = ctypes.c_int(0)
         self._h.check(self._h.lib.wrapd_get_tuning(self._h.h, None, 0, ctypes.byref(n)))
         out = (ctypes.c_int * n.value)()
         self._h.check(self._h.lib.wrapd_get_tuning(self._h.h, out, n.value, ctypes.byref(n)))
         v = list(out)
         L = v[1]
-        return {"fused_panel_ctas": v[0], "levels": L, "solve_chunk_fwd": v[2:2 + L], "solve_chunk_bwd": v[2 + L:]}
+        return {"fused_panel_ctas": v[0], "levels": L, "solve_chunk_fwd": v[2:2 + L],
+                "solve_chunk_bwd": v[2 + L:2 + 2 * L], "local_tile": v[2 + 2 * L]}
 
     def set_prox_net(self, blob):
         """Install the prox network for prox_mode 2 (an FP32 blob, capi.NET_BLOB floats)."""
@@ -170,8 +178,8 @@ class Solver:
         names = ["local", "grad_gather", "vector", "solve", "unused", "host_gaps"]
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(names)}
 
-    def algorithm_data(self) -> AlgorithmData:
-        return AlgorithmData(**{k: self.log(k) for k in capi.LOGS}, runtime_ms=self.runtime())
+    def algorithm_data(self, mesh: int | None = None) -> AlgorithmData:
+        return AlgorithmData(**{k: self.log(k, mesh) for k in capi.LOGS}, runtime_ms=self.runtime())
 
     # -- TetElements-level components ------------------------------------------
     def get_state(self, name: str) -> np.ndarray:
