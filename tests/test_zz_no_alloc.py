@@ -55,8 +55,42 @@ def test_no_alloc_energy_matches_the_allocating_entry(lib_built):
         assert pe == pytest.approx(pe_ref, rel=1e-12)
         assert int(flips) == flips_ref
     # sizes beyond the fixed scratch are refused, without touching the output
-    d_out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    d_out = torch.full((2,), 7.0, dtype=torch.float64, device="cuda")
     rc = lib.wrapd_potential_energy_batch_noalloc(MAX_N + 1, mu, lam, ctypes.c_void_p(d_out.data_ptr()),
                                                   ctypes.c_void_p(d_out.data_ptr()),
                                                   ctypes.c_void_p(d_out.data_ptr()), None)
-    assert rc == -1
+    assert rc == capi.WRAPD_E_INPUT
+    torch.cuda.synchronize()
+    assert d_out.cpu().tolist() == [7.0, 7.0]
+
+
+def test_no_alloc_energy_empty_batch_and_own_stream(lib_built):
+    """n == 0 writes zeros; a call queued on the caller's own stream is ready
+    once that stream has reached it."""
+    import torch
+    from oracle import pyoracle as po
+    from wrapd_b200 import capi
+
+    lib = capi.load()
+    mu, lam = po.lame(E_YOUNG, NU)
+    d_out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    assert lib.wrapd_potential_energy_batch_noalloc(0, mu, lam, None, None, ctypes.c_void_p(d_out.data_ptr()),
+                                                    None) == capi.WRAPD_OK
+    torch.cuda.synchronize()
+    assert d_out.cpu().tolist() == [0.0, 0.0]
+    sig, vol = _inputs(100_003, 3)
+    pe_ref, flips_ref = capi.potential_energy_batch(mu, lam, sig, vol)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        d_sig = torch.from_numpy(sig).cuda()
+        d_vol = torch.from_numpy(vol).cuda()
+        d_out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
+    rc = lib.wrapd_potential_energy_batch_noalloc(sig.shape[0], mu, lam, ctypes.c_void_p(d_sig.data_ptr()),
+                                                  ctypes.c_void_p(d_vol.data_ptr()), ctypes.c_void_p(d_out.data_ptr()),
+                                                  ctypes.c_void_p(stream.cuda_stream))
+    assert rc == capi.WRAPD_OK
+    stream.synchronize()
+    pe, flips = d_out.cpu().numpy()
+    assert pe == pytest.approx(pe_ref, rel=1e-12)
+    assert int(flips) == flips_ref
