@@ -9,10 +9,18 @@ Metric: ADMM element-iterations per second (elements x iterations / seconds),
 the throughput behind the time-to-energy-gap metric; `local_elems_per_s` adds
 the local step alone.  Inputs are far larger than L2 (the element state is
 ~0.7 GB), so no L2 flush is needed between steps.  The same line carries the
-learned/FP32 form on the same bar, the time to relative energy gap 1e-6 of the
-four solver forms on the 8x8x32 bar and on a 786,432-tet bar with a 180 deg
-twist (the bent bar above keeps inverted elements and does not reach that gap),
-and 64 uneven bars solved as one batch and one by one.
+learned/FP32 form on the same bar; the time to relative energy gap 1e-6 of the
+solver forms on the 8x8x32 bar, on a 786,432-tet bar with a 180 deg twist (the
+bent bar above keeps inverted elements and does not reach that gap) and on the
+3,932,160-tet bar with a 720 deg twist (reweight every 20), plain FP64 against
+learned/FP32; and 64 uneven bars solved as one batch and one by one.
+
+The reference arm (--impl reference) runs the reference's own solver,
+compiled from its sources with two documented one-line patches for the
+settings above (history 5, reweight every 10: oracle/Makefile), on the same
+bar and times the same kind of window (ten iterations hold one reweight and
+refactorization, as any ten of ours do).  Both arms' `e2e` is a whole solve of
+W + K iterations from host data, setup included.
 
 Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
         [--precision fp64|mixed] [--parts main,learned,gap,e2e,batch]
@@ -24,7 +32,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import shutil
 import subprocess
 import sys
@@ -39,6 +46,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "time to rel. energy gap 1e-6: learned/FP32 vs plain FP64 GPU; local elems/s"
 UNIT = "elem-iter/s"
+WORKLOAD = "bar 32x32x128 cubes x6 tets (786,432 tets, 140,481 verts), 360 deg twist + 90 deg bend, E=1e5 nu=0.45"
 E_YOUNG, NU = 1e5, 0.45
 
 
@@ -160,26 +168,37 @@ def grad_step_bytes(ne: int, nf: int, fp: int) -> int:
 
 
 # ---- reference arm -------------------------------------------------------------------
+# The reference refactors with Eigen's single-threaded SimplicialLDLT, about
+# 200 s on the 786,432-tet bar; ten timed iterations hold exactly one of the
+# every-10 refactorizations, the same share as any window of our arm.
+REF_TIMED_ITERS = 10
+
+
 def run_reference(args, rank):
-    """The reference's own CPU solver (oracle/_ref/quasi_ref, compiled from its sources)."""
+    """The reference's own CPU solver on the same workload and settings as our
+    arm: oracle/_ref/quasi_ref_m5, compiled from the reference's sources with
+    the two documented one-line patches of oracle/Makefile (global L-BFGS
+    history 5; reweight + refactorization every 10 iterations).  It times the
+    ADMM iterations W..W+K-1 with K at most REF_TIMED_ITERS (one reweight and
+    refactorization in every ten iterations, as in our arm's window) from its
+    own accumulated_time_s (local + global + refactor, its MicroTimer)."""
     if rank != 0:
         return
     from oracle import pyoracle as po
     from wrapd_b200 import bars
     cores = os.cpu_count() or 1
-    if not os.path.exists(po.QUASI_REF):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/quasi_ref not built (no reference sources)"}))
+    if not os.path.exists(po.QUASI_REF_M5):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/quasi_ref_m5 not built (no reference sources)"}))
         return
     bar = bars.bar_32x32x128_bent()
-    # a bounded sample: the reference's own setup (AMD ordering + first
-    # SimplicialLDLT factorization of 138k unknowns) already takes minutes, and
-    # each of its iterations about 2 s, so at most 10 iterations are timed
-    K, W = min(args.steps, 10), min(args.warmup, 1)
+    W = max(0, args.warmup)
+    K = max(1, min(args.steps, REF_TIMED_ITERS))
     with tempfile.TemporaryDirectory() as d:
         files = bars.write_bar(bar, d, "c1")
         t0 = time.perf_counter()
-        r = po.run_quasi_ref(files, E_YOUNG, NU, W + K, threads=cores, extra=["-rw", "0"], outdir=d + "/out",
-                             timeout=3000)
+        r = po.run_quasi_ref(files, E_YOUNG, NU, W + K, threads=cores, extra=["-rw_every", "10"],
+                             outdir=d + "/out", timeout=3000, binary=po.QUASI_REF_M5)
         wall = time.perf_counter() - t0
     acc = r["accumulated_time_s"]
     timed = float(acc[W + K] - acc[W])
@@ -189,13 +208,18 @@ def run_reference(args, rank):
         "steps_requested": args.steps,
         "warmup": W, "ms_per_step": 1000.0 * timed / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bar generator)",
-        "config": {"workload": "bar 32x32x128 cubes x6 tets (786,432 tets), 360 deg twist + 90 deg bend",
-                   "solver": "reference quasi (Eigen SimplicialLDLT), -rw 0, L-BFGS history 6",
+        "config": {"workload": WORKLOAD, "solver": "reference quasi (Eigen SimplicialLDLT, OpenMP), L-BFGS history 5, "
+                                                   "reweight+refactor every 10 iterations (patched build quasi_ref_m5)",
                    "timed": f"ADMM iterations {W}..{W + K - 1} from the reference's accumulated_time_s"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"the bent 32x32x128 bar, {W + K} ADMM iterations, last {K} timed; setup "
-                                   f"{r['runtime']['setup_ms'] / 1000:.1f} s untimed; wall {wall:.1f} s"},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                         "sample": f"the bent 32x32x128 bar, {W + K} ADMM iterations, iterations {W}..{W + K - 1} "
+                                   f"timed; wall {wall:.1f} s for the whole run"},
+        # e2e: the whole process (mesh files in, setup with AMD ordering and the
+        # first factorizations, W + K iterations, files out), as our e2e leg is a
+        # whole solve of W + K iterations from host buffers
+        "e2e": {"value": bar.n_tets * (W + K) / wall, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0, "wall_s": wall,
+                "includes": "quasi_ref process: load meshes + setup + W+K iterations + output files"},
     }
     print(json.dumps(line))
 
@@ -203,7 +227,8 @@ def run_reference(args, rank):
 # ---- CPU baseline inside our arm -------------------------------------------------------
 def cpu_baseline():
     """The reference on a bounded sample of the workload: a 32x32x16 slice of the bar
-    (98,304 tets, same cross-section), 6 ADMM iterations, all host threads."""
+    (98,304 tets, same cross-section), 6 ADMM iterations, all host threads, the
+    patched build with the benchmark's settings (no reweight falls in 6 iterations)."""
     from oracle import pyoracle as po
     from wrapd_b200 import bars
     cores = os.cpu_count() or 1
@@ -211,13 +236,14 @@ def cpu_baseline():
     W, K = 1, 5
     with tempfile.TemporaryDirectory() as d:
         files = bars.write_bar(bar, d, "s")
-        if os.path.exists(po.QUASI_REF):
-            r = po.run_quasi_ref(files, E_YOUNG, NU, W + K, threads=cores, extra=["-rw", "0"],
-                                 outdir=d + "/out", timeout=600)
+        if os.path.exists(po.QUASI_REF_M5):
+            r = po.run_quasi_ref(files, E_YOUNG, NU, W + K, threads=cores, extra=["-rw_every", "10"],
+                                 outdir=d + "/out", timeout=600, binary=po.QUASI_REF_M5)
             acc = r["accumulated_time_s"]
             v = bar.n_tets * K / float(acc[W + K] - acc[W])
             return {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
-                    "sample": "32x32x16 slice of the bar (98,304 tets), iterations 1-5 of 6, -rw 0"}
+                    "sample": "32x32x16 slice of the bar (98,304 tets), iterations 1-5 of 6, history 5 "
+                              "(quasi_ref_m5)"}
     o = po.Oracle(bar.rest, bar.init, bar.tets, bar.pins, youngs=E_YOUNG, poisson=NU, max_iters=W + K)
     o.setup()
     o.iterate()
@@ -238,6 +264,11 @@ FORMS = [
 ]
 
 
+# Iteration cap of the 3.9M-tet bar's runs to tol 1e-13 (about 20 ms per FP64
+# iteration): E* is the lowest energy the plain FP64 run reaches within it.
+GAP_ITERS_64x64x160 = 3000
+
+
 def gap_time(objectives, acc_time_s, e_star, gap=1e-6):
     """Solver time (local + global + refactor, device events) at the first
     iterate from which (E_k - E*) / |E*| stays <= gap; None if never."""
@@ -249,11 +280,12 @@ def gap_time(objectives, acc_time_s, e_star, gap=1e-6):
     return float(acc_time_s[k]), k
 
 
-def time_to_gap(bar, label, device, base, e_star_iters=20000, gap=1e-6):
+def time_to_gap(bar, label, device, base, e_star_iters=20000, gap=1e-6, forms=None):
     """E* = lowest energy of a long plain-FP64 run (tol 1e-13); then each form
     to convergence at tol 1e-13, reporting its time to the gap, iterations and
     the final positions' error against the plain FP64 run (which matches the
     FP64 oracle to 1e-8 in the parity tests)."""
+    forms = FORMS if forms is None else [f for f in FORMS if f[0] in forms]
     from wrapd_b200 import prox_net
     from wrapd_b200.solver import Solver
 
@@ -273,7 +305,7 @@ def time_to_gap(bar, label, device, base, e_star_iters=20000, gap=1e-6):
     e_star = float(dr.objectives.min())
     out = {"workload": label, "gap": gap, "e_star": e_star, "e_star_run_iters": int(len(dr.objectives) - 1),
            "time_source": "solver accumulated_time_s (CUDA events: local + global + refactor)", "forms": {}}
-    for name, kw in FORMS:
+    for name, kw in forms:
         X, d = (Xr, dr) if name == "plain_fp64" else run(dict(kw, tol=1e-13, max_iters=e_star_iters))
         t, k = gap_time(d.objectives, d.accumulated_time_s, e_star, gap)
         out["forms"][name] = {
@@ -290,9 +322,11 @@ def time_to_gap(bar, label, device, base, e_star_iters=20000, gap=1e-6):
 
 def batch_throughput(device, K):
     """64 uneven bars (n_a, n_b in U{4..16}, n_L in U{8..64}, per-bar E and nu),
-    FP32 local / FP64 global, solved as one batch (one handle, one block-diagonal
-    system) and one bar after another (64 handles); device time of K iterations
-    after 2 warm-up ones, setup excluded and reported apart."""
+    FP32 local / FP64 global, solved as one batch (one handle: shared launches,
+    each bar its own ADMM and L-BFGS decisions, a converged bar drops out) and
+    one bar after another (64 handles); device time of K iterations after 2
+    warm-up ones, setup excluded and reported apart.  Units are the element-
+    iterations the bars actually ran (a bar that converged stops counting)."""
     from wrapd_b200 import bars
     from wrapd_b200.solver import Solver
     triples = bars.batch_bars(64, 0)
@@ -309,43 +343,40 @@ def batch_throughput(device, K):
         s.begin_solve()
         setup = time.perf_counter() - t0
         s.iterate(2)
+        n0 = [len(s.log("objectives", mesh=i)) for i in range(len(group))]
         r0 = s.runtime()
         done, _ = s.iterate(K)
         r1 = s.runtime()
+        n1 = [len(s.log("objectives", mesh=i)) for i in range(len(group))]
         ms = sum(r1[k] - r0[k] for k in ("local_ms", "global_ms", "refactor_ms"))
+        units = sum(g[0].n_tets * (b - a) for g, a, b in zip(group, n0, n1))
+        its = [b - a for a, b in zip(n0, n1)]
         s.close()
-        return ms, done, setup
+        return ms, done, setup, units, its
 
-    ms_b, done_b, setup_b = run(triples)
-    ms_s, setup_s, elem_iter_s = 0.0, 0.0, 0
+    ms_b, done_b, setup_b, units_b, its_b = run(triples)
+    ms_s, setup_s, units_s = 0.0, 0.0, 0
     for tr in triples:
-        ms, done, setup = run([tr])
+        ms, done, setup, units, _ = run([tr])
         ms_s += ms
         setup_s += setup
-        elem_iter_s += tr[0].n_tets * done
+        units_s += units
     return {"workload": "64 uneven bars (seeds 0-63), %d tets in total" % ne_total, "iterations": K,
-            "batch_elem_iter_per_s": ne_total * done_b / (ms_b / 1000.0), "batch_ms_per_iter": ms_b / max(1, done_b),
-            "one_by_one_elem_iter_per_s": elem_iter_s / (ms_s / 1000.0),
-            "batch_speedup": (ne_total * done_b / ms_b) / (elem_iter_s / ms_s),
+            "per_bar_iterations_in_window": its_b,
+            "batch_elem_iter_per_s": units_b / (ms_b / 1000.0), "batch_ms_per_iter": ms_b / max(1, done_b),
+            "one_by_one_elem_iter_per_s": units_s / (ms_s / 1000.0),
+            "batch_speedup": (units_b / ms_b) / (units_s / ms_s),
             "setup_s": {"batch": setup_b, "one_by_one": setup_s}}
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_local_32x32x128.md")
-    if not os.path.exists(path):
-        return None
-    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
-    return float(m.group(1)) if m else None
-
-
-def profile_fp64_pipe():
-    """FP64 pipe utilisation of the local step from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_local_32x32x128.md")
-    if not os.path.exists(path):
-        return None
-    m = re.search(r"FP64 pipe active \(sm__pipe_fp64_cycles_active\) \| ([0-9.]+) %", open(path).read())
-    return float(m.group(1)) / 100.0 if m else None
+# k_local<double>'s DRAM bytes per element and FP64-pipe share, from its
+# one-launch ncu capture on the 32x32x64 bar (393,216 tets; the SoA streams
+# scale with the element count), summarised in profiles/k_local_32x32x128.md.
+# They are copied here, not measured in this run: refresh them with that
+# capture whenever the local step changes.
+K_LOCAL_NCU = {"dram_bytes_per_elem": 2 * 142806784 / 786432, "fp64_pipe_active": 0.362,
+               "source": "ncu --set full, one launch of k_local<double> on the 32x32x64 bar, traffic scaled by "
+                         "the element count (copied constants, not measured in this run)"}
 
 
 def peaks():
@@ -403,7 +434,7 @@ def run_ours(args, rank, world, local, pg):
     # CUDA events on the library's stream around exactly that launch)
     lbytes = local_step_bytes(ne, fp)
     achieved = lbytes / (local_ms / K / 1000.0) / 1e9
-    traffic = profile_traffic()
+    traffic = K_LOCAL_NCU["dram_bytes_per_elem"] * ne if args.precision == "fp64" else None
     # Secondary rooflines, from K more iterations with the per-phase device
     # timeline on (outside the timed region): the factorization against the
     # FP64 tensor-core peak measured here, the 3-RHS solve against HBM.
@@ -441,22 +472,25 @@ def run_ours(args, rank, world, local, pg):
         s2.set_pins(bar.pins)
         s2.initialize()
         s2.begin_solve()
-        done2, _ = s2.iterate(K)
+        done2, _ = s2.iterate(args.warmup + K)
         X = s2.positions()
         e2e_s = time.perf_counter() - t0
         s2.close()
         e2e_s = max_over_ranks(pg, e2e_s)
         e2e_units = sum_over_ranks(pg, float(ne * done2))
-        if done2 != K or not np.isfinite(X).all():
+        if done2 != args.warmup + K or not np.isfinite(X).all():
             raise RuntimeError("the end-to-end solve did not run its iterations to finite positions")
         h2d = bar.rest.nbytes + bar.init.nbytes + bar.tets.nbytes + bar.pins.nbytes
-        e2e = {"value": e2e_units / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d // K),
-               "d2h_bytes_per_step": int(X.nbytes // K), "wall_s": e2e_s,
-               "includes": "create + add_tetmesh + initialize (symbolic + factor) + begin_solve + K iterations "
-                           "+ positions, on every rank at once"}
+        n_e2e = args.warmup + K
+        e2e = {"value": e2e_units / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d // n_e2e),
+               "d2h_bytes_per_step": int(X.nbytes // n_e2e), "wall_s": e2e_s, "iterations": n_e2e,
+               "includes": "a whole solve through the C ABI from host buffers: create + add_tetmesh + initialize "
+                           "(symbolic analysis + first factorization) + begin_solve + W+K iterations + positions "
+                           "out, on every rank at once (the reference arm's e2e is its whole process for the "
+                           "same W+K iterations)"}
     # the learned/FP32 form on the same bar: local step (FP32 SVD + network-started Newton)
     learned = None
-    if rank == 0 and "learned" in parts:
+    if rank == 0 and world == 1 and "learned" in parts:
         from wrapd_b200 import prox_net
         s3 = Solver(**dict(settings, precision="mixed", prox_mode=2))
         s3.add_tetmesh(bar.rest, bar.init, bar.tets)
@@ -479,7 +513,7 @@ def run_ours(args, rank, world, local, pg):
                    "mean_prox_iters": float(np.mean(s3.log("prox_iters")[-K:]))}
         s3.close()
     gap = None
-    if rank == 0 and "gap" in parts:
+    if rank == 0 and world == 1 and "gap" in parts:
         # the 8x8x32 bar, and a 786,432-tet bar with the same 180 deg twist (no
         # bend): the bent bar keeps inverted elements and its energy does
         # not settle to a 1e-6 gap
@@ -488,9 +522,15 @@ def run_ours(args, rank, world, local, pg):
                                          "E=1e5 nu=0.45", local, base),
                "bar_32x32x128": time_to_gap(bars.make_bar(32, 32, 128, twist_deg=180.0, noise=0.02, seed=0),
                                             "bar 32x32x128 cubes x6 tets (786,432 tets), 180 deg twist, E=1e5 "
-                                            "nu=0.45", local, base, e_star_iters=4000)}
+                                            "nu=0.45", local, base, e_star_iters=4000),
+               # the headline configuration: the 3.9M-tet bar, reweight + refactor every 20
+               "bar_64x64x160": time_to_gap(bars.bar_64x64x160(),
+                                            "bar 64x64x160 cubes x6 tets (3,932,160 tets), 720 deg twist, E=1e5 "
+                                            "nu=0.45, reweight+refactor every 20", local,
+                                            dict(base, rw_every=20), e_star_iters=GAP_ITERS_64x64x160,
+                                            forms=("plain_fp64", "fp32_newton", "learned_fp32"))}
     batch = None
-    if rank == 0 and "batch" in parts:
+    if rank == 0 and world == 1 and "batch" in parts:
         batch = batch_throughput(local, min(K, 20))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -514,10 +554,10 @@ def run_ours(args, rank, world, local, pg):
             "roofline": {"kernel": "k_local (fused local step)", "bound": "hbm", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind, "bytes_per_launch": lbytes,
-                         "fp64_pipe_active_ncu": profile_fp64_pipe(),
+                         "fp64_pipe_active_ncu": K_LOCAL_NCU["fp64_pipe_active"],
+                         "traffic_source": K_LOCAL_NCU["source"],
                          "note": "FP64-arithmetic-bound (Jacobi SVD + L-BFGS prox per element); the HBM "
-                                 "fraction is low by design, the FP64 pipe share comes from the ncu capture "
-                                 "in profiles/k_local_32x32x128.md"},
+                                 "fraction is low by design"},
             "roofline_solve": roof_solve,
             "roofline_factorization": roof_fact,
             "gpu_launches": int(c1["kernel_launches"] - c0["kernel_launches"]),

@@ -141,10 +141,13 @@ def ref_solve(bar, max_iters, extra=(), binary=po.QUASI_REF):
 
 def bar_32x32x128_bent():
     """The benchmarked bar against the reference itself, both builds."""
+    import concurrent.futures as cf
     b = bars.bar_32x32x128_bent()
     out = {}
-    for tag, it, extra, binary in [("m5", 20, ("-rw_every", "10"), po.QUASI_REF_M5), ("m6", 60, (), po.QUASI_REF)]:
-        r = ref_solve(b, it, extra, binary)
+    runs = [("m5", 20, ("-rw_every", "10"), po.QUASI_REF_M5), ("m6", 60, (), po.QUASI_REF)]
+    with cf.ThreadPoolExecutor(len(runs)) as ex:   # two single-thread processes side by side
+        results = list(ex.map(lambda a: ref_solve(b, a[1], a[2], a[3]), runs))
+    for (tag, _, _, _), r in zip(runs, results):
         out.update({f"{tag}_objectives": r["objectives"], f"{tag}_inner": r["inner_iters"],
                     f"{tag}_reweighted": r["reweighted"], f"{tag}_x": r["x"],
                     f"{tag}_ls_dal": r["ls_delta_al"], f"{tag}_gs_dal": r["gs_delta_al"],

@@ -1,0 +1,96 @@
+"""GPU parity at the benchmarked sizes.
+
+The 3.9M-tet bar (64x64x160 cubes, 720 deg twist) is compared with the oracle:
+its first three ADMM iterations (tests/golden/iters_bar_64x64x160.npz, the
+oracle with its conjugate-gradient linear solver), the global gradient at
+seeded dual variables, and A (A^-1 b) = b.  Energies within 1e-8 relative,
+positions within 1e-8 of max |x|, identical inner-iteration and flip logs.
+"""
+import numpy as np
+import pytest
+
+from conftest import E_YOUNG, NU
+from oracle import pyoracle as po
+from wrapd_b200 import bars, capi
+from wrapd_b200.solver import Solver
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib(lib_built):
+    capi.load()
+
+
+def make_solver(bar, **kw):
+    kw.setdefault("youngs", E_YOUNG)
+    kw.setdefault("poisson", NU)
+    s = Solver(**kw)
+    s.add_tetmesh(bar.rest, bar.init, bar.tets)
+    s.set_pins(bar.pins)
+    s.initialize()
+    return s
+
+
+def rel_max(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def big4():
+    return bars.bar_64x64x160()
+
+
+def test_bar_64x64x160_first_iterations_match_oracle(golden, big4):
+    g = golden("iters_bar_64x64x160.npz")
+    s = make_solver(big4, lbfgs_m=5, rw_every=20, max_iters=3)
+    X = s.solve()
+    np.testing.assert_array_equal(s.log("inner_iters"), g["inner"])
+    np.testing.assert_array_equal(s.log("flips"), g["flips"])
+    np.testing.assert_allclose(s.log("objectives"), g["objectives"], rtol=1e-8)
+    assert np.abs(X[g["x_idx"]] - g["x_sample"]).max() / float(g["x_absmax"]) < 1e-8
+    np.testing.assert_allclose(X.sum(axis=0), g["x_colsum"], rtol=1e-9, atol=1e-9 * X.shape[0])
+    s.close()
+
+
+def test_bar_64x64x160_gradient_and_solve(big4):
+    """The gradient at seeded dual variables against the oracle (1e-10), and
+    A (A^-1 b) = b for the 671,775-unknown system (1e-9)."""
+    import scipy.sparse as sp
+    bar = big4
+    s = make_solver(bar, lbfgs_m=5, rw_every=20)
+    # A (A^-1 b) = b with A assembled on the host from the solver's weights
+    w2 = s.get_state("w2")
+    free = -np.ones(bar.n_verts, dtype=np.int64)
+    fidx = np.setdiff1d(np.arange(bar.n_verts), bar.pins)
+    free[fidx] = np.arange(fidx.size)
+    P = bar.rest[bar.tets]
+    Dm = np.stack([P[:, 1] - P[:, 0], P[:, 2] - P[:, 0], P[:, 3] - P[:, 0]], axis=2)
+    S = np.array([[-1, -1, -1], [1, 0, 0], [0, 1, 0], [0, 0, 1.0]])
+    Di = np.einsum("ab,nbc->nac", S, np.linalg.inv(Dm))
+    K = w2[:, None, None] * np.einsum("nac,nbc->nab", Di, Di)
+    fi = free[bar.tets]
+    rows = np.repeat(fi, 4, axis=1).ravel()
+    cols = np.tile(fi, (1, 4)).ravel()
+    keep = (rows >= 0) & (cols >= 0)
+    A = sp.csr_matrix((K.ravel()[keep], (rows[keep], cols[keep])), shape=(fidx.size, fidx.size))
+    del K, Di, Dm, P
+    rng = np.random.default_rng(41)
+    b = rng.normal(size=(fidx.size, 3))
+    x = s.solve_A(b)
+    assert np.abs(A @ x - b).max() / np.abs(b).max() < 1e-9
+    # the gradient
+    s.begin_solve()
+    o = po.Oracle(bar.rest, bar.init, bar.tets, bar.pins, youngs=E_YOUNG, poisson=NU, lbfgs_m=5, rw_every=20)
+    o.init_state()
+    Z = o.get("Z") + 0.05 * rng.normal(size=9 * bar.n_tets)
+    U = 0.05 * rng.normal(size=9 * bar.n_tets)
+    o.set("Z", Z)
+    o.set("U", U)
+    s.set_state("Z", Z)
+    s.set_state("U", U)
+    v, gr = s.global_grad()
+    vo, go = o.grad_cached()
+    assert v == pytest.approx(vo, rel=1e-10)
+    assert rel_max(gr, go) < 1e-10
+    s.close()

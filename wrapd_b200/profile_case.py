@@ -1,5 +1,6 @@
-"""A self-contained solve for kernel profiles and size reports: one bar, a
-few ADMM iterations through the C ABI.
+"""Measurement tool (not part of the solver's API): a self-contained solve
+for kernel profiles and size reports, one bar, a few ADMM iterations through
+the C ABI.  The commands recorded in profiles/ run it under ncu.
 
     python -m wrapd_b200.profile_case [--grid 32 32 64] [--iters 2]
         [--precision fp64|mixed] [--prox-mode 0|1|2]
