@@ -292,24 +292,19 @@ __global__ void k_extend_add(double* __restrict__ F, const FrontDesc* __restrict
 
 // ---- panel factorization -------------------------------------------------------
 // Cholesky of the nb x nb (nb <= NB = 32) diagonal block at Fd (column-major,
-// lower part read) and its inverse, by a CTA of 128 threads in shared memory.
-// Right-looking: at pivot j every thread updates a fixed slice of 8 entries
-// of row i = tid % 32 (columns tid / 32 + 4m), with all its operands loaded
-// before the first store, so one barrier per pivot is the only serial step.
-// L(i, j) = A'(i, j) rsqrt(d) goes to Lsm (pitch lp), rsqrt(d) to D.  The
-// inverse is right-looking by rows: row s of inv(L) is (e_s - P(s, :)) / L(s, s)
-// and the rows below add L(r, s) times it to their partial sums P (kept in S).
+// lower part read) and its inverse, in shared memory.  Right-looking: at pivot
+// j, L(i, j) = A'(i, j) rsqrt(d) goes to Lsm (pitch lp), rsqrt(d) to D, and
+// each row i > j updates S(i, c) -= t_i S(c, j) for j < c <= i.  The inverse
+// is right-looking by rows: row s of inv(L) is (e_s - P(s, :)) / L(s, s) and
+// the rows below add L(r, s) times it to their partial sums P (kept in S).
 // Row s of inv(L) is written to X (pitch xp), columns < nb.  A non-positive
 // (or NaN) pivot sets *bad and continues with a unit pivot.
+// Warp 0 does both sweeps (the other warps only load the block and wait):
+// lane i owns row i in the Cholesky sweep (S(c, j) a broadcast read) and
+// column c = i in the inverse sweep (L(r, s) a broadcast read), with
+// __syncwarp between pivots and no CTA barrier inside the sweeps.
 constexpr int LSP = NB + 1;
 static_assert(GEMM_THREADS == 128 && NB == 32, "cta_chol_inv: one warp, one row (then one column) per lane");
-// Warp 0 does both sweeps; the other warps only load the block and wait.
-// Lane i owns row i in the Cholesky sweep (S(i, c) -= t_i S(c, j), with S(c,
-// j) a broadcast read) and column c = i in the inverse sweep (P(r, c) +=
-// L(r, s) f_c, L(r, s) a broadcast read).  Each entry sees the same fma, with
-// the same operands in the same order, as in a 128-thread sweep, so L, D and
-// inv(L) are those of the one-barrier-per-pivot form, with no CTA barrier
-// inside the sweeps (__syncwarp between pivots).
 __device__ __forceinline__ void cta_chol_inv(const double* __restrict__ Fd, int64_t ld, int nb, double* S,
                                              double* Lsm, int lp, double* D, double* X, int xp, bool* bad) {
     const int tid = threadIdx.x;
