@@ -264,9 +264,15 @@ FORMS = [
 ]
 
 
-# Iteration cap of the 3.9M-tet bar's runs to tol 1e-13 (about 20 ms per FP64
-# iteration): E* is the lowest energy the plain FP64 run reaches within it.
-GAP_ITERS_64x64x160 = 3000
+# Iteration caps of the 3.9M-tet bar's runs (about 20 ms per FP64 iteration).
+# With the 180 deg twist the runs converge (tol 1e-13) within the first cap.
+# With the 720 deg twist and reweighting every 20 iterations (the configuration
+# as specified) neither form reaches a 1e-6 gap in thousands of iterations:
+# elements stay inverted while the bar unwinds (120 flips after 2,000 FP64
+# iterations, the energy still falling by percents per hundred iterations), so
+# that configuration is measured per iteration over the second cap.
+GAP_ITERS_64x64x160 = 1500
+PROGRESS_ITERS_64x64x160 = 300
 
 
 def gap_time(objectives, acc_time_s, e_star, gap=1e-6):
@@ -317,6 +323,36 @@ def time_to_gap(bar, label, device, base, e_star_iters=20000, gap=1e-6, forms=No
     p0 = out["forms"]["plain_fp64"]["seconds_to_gap"]
     pl = out["forms"]["learned_fp32"]["seconds_to_gap"]
     out["speedup_learned_fp32_vs_plain_fp64"] = (p0 / pl) if (p0 and pl) else None
+    return out
+
+
+def capped_progress(bar, label, device, base, iters, forms):
+    """Fixed-length runs of a configuration that does not converge within the
+    bench's budget: per form the solver time per iteration (local / global /
+    refactor), the energy and inverted elements after `iters` iterations, and
+    the speed-up per iteration of each form over the plain FP64 one."""
+    from wrapd_b200 import prox_net
+    from wrapd_b200.solver import Solver
+    out = {"workload": label, "iterations": iters, "gap_1e-6_reached": False, "forms": {}}
+    for name, kw in [f for f in FORMS if f[0] in forms]:
+        s = Solver(**dict(base, **kw, device=device, max_iters=iters, tol=0.0))
+        s.add_tetmesh(bar.rest, bar.init, bar.tets)
+        s.set_pins(bar.pins)
+        if kw.get("prox_mode") == 2:
+            s.set_prox_net(prox_net.load_default())
+        s.initialize()
+        s.solve()
+        d, r = s.algorithm_data(), s.runtime()
+        s.close()
+        n = len(d.objectives) - 1
+        out["forms"][name] = {"ms_per_iter": (r["local_ms"] + r["global_ms"] + r["refactor_ms"]) / n,
+                              "local_ms_per_iter": r["local_ms"] / n, "global_ms_per_iter": r["global_ms"] / n,
+                              "refactor_ms_per_iter": r["refactor_ms"] / n, "energy_start": float(d.objectives[0]),
+                              "energy_end": float(d.objectives[-1]), "energy_min": float(d.objectives.min()),
+                              "flips_end": int(d.flips[-1])}
+    p0 = out["forms"]["plain_fp64"]["ms_per_iter"]
+    for name, f in out["forms"].items():
+        f["speedup_per_iter_vs_plain_fp64"] = p0 / f["ms_per_iter"]
     return out
 
 
@@ -523,12 +559,18 @@ def run_ours(args, rank, world, local, pg):
                "bar_32x32x128": time_to_gap(bars.make_bar(32, 32, 128, twist_deg=180.0, noise=0.02, seed=0),
                                             "bar 32x32x128 cubes x6 tets (786,432 tets), 180 deg twist, E=1e5 "
                                             "nu=0.45", local, base, e_star_iters=4000),
-               # the headline configuration: the 3.9M-tet bar, reweight + refactor every 20
-               "bar_64x64x160": time_to_gap(bars.bar_64x64x160(),
-                                            "bar 64x64x160 cubes x6 tets (3,932,160 tets), 720 deg twist, E=1e5 "
-                                            "nu=0.45, reweight+refactor every 20", local,
-                                            dict(base, rw_every=20), e_star_iters=GAP_ITERS_64x64x160,
-                                            forms=("plain_fp64", "fp32_newton", "learned_fp32"))}
+               # the headline size, 3.9M tets: with a 180 deg twist it converges ...
+               "bar_64x64x160_180deg": time_to_gap(bars.make_bar(64, 64, 160, twist_deg=180.0, noise=0.005,
+                                                                 seed=0),
+                                                   "bar 64x64x160 cubes x6 tets (3,932,160 tets), 180 deg twist, "
+                                                   "E=1e5 nu=0.45", local, base, e_star_iters=GAP_ITERS_64x64x160,
+                                                   forms=("plain_fp64", "fp32_newton", "learned_fp32")),
+               # ... with the specified 720 deg twist and reweighting every 20 it does not
+               "bar_64x64x160": capped_progress(bars.bar_64x64x160(),
+                                                "bar 64x64x160 cubes x6 tets (3,932,160 tets), 720 deg twist, E=1e5 "
+                                                "nu=0.45, reweight+refactor every 20", local,
+                                                dict(base, rw_every=20), PROGRESS_ITERS_64x64x160,
+                                                ("plain_fp64", "fp32_newton", "learned_fp32"))}
     batch = None
     if rank == 0 and world == 1 and "batch" in parts:
         batch = batch_throughput(local, min(K, 20))

@@ -341,6 +341,8 @@ void SolverGPU::initialize() {
     if (mats_.size() > 1) {
         d_mid_ = dupload(mid);
         d_mats_ = dupload(mats_);
+    } else {
+        mat_ = mats_[0];   // one material: the mesh's own when it was given one
     }
     d_w2c_ = static_cast<double*>(dalloc(ne * sizeof(double)));
     d_Z_ = static_cast<double*>(dalloc(9 * (size_t)ne * TS));
@@ -1186,7 +1188,8 @@ int SolverGPU::iterate(int n, bool* conv) {
         if (nm > 1) union_logs(k + 1);
         // phase times: read once a later synchronisation has passed the events
         pend_ = PendingTiming{true, k, ev_};
-        if (!cfg.rot_aware || profiling || any_rw) settle_timing(false);
+        if (profiling || any_rw) settle_timing(false);          // a synchronisation passed ev_[3]
+        else if (!cfg.rot_aware) settle_timing(true);          // its last one came before ev_[2]
         iter = k + 1;
         done++;
         converged_ = true;
