@@ -292,19 +292,17 @@ __global__ void k_extend_add(double* __restrict__ F, const FrontDesc* __restrict
 
 // ---- panel factorization -------------------------------------------------------
 // Cholesky of the nb x nb (nb <= NB = 32) diagonal block at Fd (column-major,
-// lower part read) and its inverse, in shared memory.  Right-looking: at pivot
-// j, L(i, j) = A'(i, j) rsqrt(d) goes to Lsm (pitch lp), rsqrt(d) to D, and
-// each row i > j updates S(i, c) -= t_i S(c, j) for j < c <= i.  The inverse
-// is right-looking by rows: row s of inv(L) is (e_s - P(s, :)) / L(s, s) and
-// the rows below add L(r, s) times it to their partial sums P (kept in S).
+// lower part read) and its inverse, by a CTA of 128 threads in shared memory.
+// Right-looking: at pivot j every thread updates a fixed slice of 8 entries
+// of row i = tid % 32 (columns tid / 32 + 4m), with all its operands loaded
+// before the first store, so one barrier per pivot is the only serial step.
+// L(i, j) = A'(i, j) rsqrt(d) goes to Lsm (pitch lp), rsqrt(d) to D.  The
+// inverse is right-looking by rows: row s of inv(L) is (e_s - P(s, :)) / L(s, s)
+// and the rows below add L(r, s) times it to their partial sums P (kept in S).
 // Row s of inv(L) is written to X (pitch xp), columns < nb.  A non-positive
 // (or NaN) pivot sets *bad and continues with a unit pivot.
-// Warp 0 does both sweeps (the other warps only load the block and wait):
-// lane i owns row i in the Cholesky sweep (S(c, j) a broadcast read) and
-// column c = i in the inverse sweep (L(r, s) a broadcast read), with
-// __syncwarp between pivots and no CTA barrier inside the sweeps.
 constexpr int LSP = NB + 1;
-static_assert(GEMM_THREADS == 128 && NB == 32, "cta_chol_inv: one warp, one row (then one column) per lane");
+static_assert(GEMM_THREADS == 128 && NB == 32, "cta_chol_inv maps 128 threads onto 32 rows x 4 column slices");
 __device__ __forceinline__ void cta_chol_inv(const double* __restrict__ Fd, int64_t ld, int nb, double* S,
                                              double* Lsm, int lp, double* D, double* X, int xp, bool* bad) {
     const int tid = threadIdx.x;
@@ -313,39 +311,50 @@ __device__ __forceinline__ void cta_chol_inv(const double* __restrict__ Fd, int6
         S[i * LSP + c] = (i < nb && c <= i) ? Fd[i + (int64_t)c * ld] : 0.0;
     }
     __syncthreads();
+    const int i = tid & 31, q = tid >> 5;
     bool b = false;
-    if (tid < 32) {
-        const int i = tid;
-        double* Si = S + i * LSP;
-#pragma unroll 1
-        for (int j = 0; j < nb; ++j) {
-            double piv = S[j * LSP + j];
-            const double sij = Si[j];
-            if (!(piv > 0.0)) { b = true; piv = 1.0; }
-            const double rs = rsqrt(piv);
-            if (i >= j && i < nb) Lsm[i * lp + j] = i == j ? piv * rs : sij * rs;
-            if (i == 0) D[j] = rs;
-            const double t = sij * (rs * rs);
-            if (i > j && i < nb) {
-#pragma unroll 4
-                for (int c = j + 1; c <= i; ++c) Si[c] = fma(-t, S[c * LSP + j], Si[c]);
-            }
-            __syncwarp();
+    for (int j = 0; j < nb; ++j) {
+        double piv = S[j * LSP + j];
+        const double sij = S[i * LSP + j];
+        double cj[8], ic[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            cj[m] = S[(q + 4 * m) * LSP + j];
+            ic[m] = S[i * LSP + q + 4 * m];
         }
-        for (int idx = i; idx < NB * LSP; idx += 32) S[idx] = 0.0;
-        __syncwarp();
-        const int c = i;
-#pragma unroll 1
-        for (int s = 0; s < nb; ++s) {
-            const double ps = S[s * LSP + c];
-            const double f = (c <= s) ? ((c == s ? 1.0 : 0.0) - ps) * D[s] : 0.0;
-            if (c < nb) X[s * xp + c] = f;
-#pragma unroll 4
-            for (int r = s + 1; r < nb; ++r) S[r * LSP + c] = fma(Lsm[r * lp + s], f, S[r * LSP + c]);
-            __syncwarp();
+        if (!(piv > 0.0)) { b = true; piv = 1.0; }
+        const double rs = rsqrt(piv);
+        if (q == 0 && i >= j && i < nb) Lsm[i * lp + j] = i == j ? piv * rs : sij * rs;
+        if (tid == 0) D[j] = rs;
+        const double t = sij * (rs * rs);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int c = q + 4 * m;
+            if (c > j && c <= i && i < nb) S[i * LSP + c] = fma(-t, cj[m], ic[m]);
         }
+        __syncthreads();
     }
+    for (int idx = tid; idx < NB * NB; idx += GEMM_THREADS) S[(idx >> 5) * LSP + (idx & 31)] = 0.0;
     __syncthreads();
+    const int c = tid & 31;
+    for (int s = 0; s < nb; ++s) {
+        const double ps = S[s * LSP + c];
+        const double ds = D[s];
+        double lr[8], pr[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            lr[m] = Lsm[(q + 4 * m) * lp + s];
+            pr[m] = S[(q + 4 * m) * LSP + c];
+        }
+        const double f = (c <= s) ? ((c == s ? 1.0 : 0.0) - ps) * ds : 0.0;
+        if (q == 0 && c < nb) X[s * xp + c] = f;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int r = q + 4 * m;
+            if (r > s && r < nb) S[r * LSP + c] = fma(lr[m], f, pr[m]);
+        }
+        __syncthreads();
+    }
     *bad = b;
 }
 

@@ -80,7 +80,7 @@ __device__ __forceinline__ double elastic_energy(const Material& m, const double
 // K + K^T, M = F - U diag(s) (K+K^T) V^T and g_e = w^2 Di^T M^T, plus the AL
 // value 0.5 w^2 |symF - P|^2, the potential energy and the inversion count at
 // x (src/TetElements.cpp:444-468, 598-635).  Outputs out[0..2] = value, pe, flips.
-static __global__ void __launch_bounds__(128) k_grad(ElemView E, Tiles T, const int* on, const double* __restrict__ x,
+static __global__ void __launch_bounds__(128, 4) k_grad(ElemView E, Tiles T, const int* on, const double* __restrict__ x,
                                               const double* __restrict__ xfix, Material mat0, int write_gel,
                                               double* partials, unsigned* counters, double* out, int stride) {
     const Tile tl = tile_at(T, blockIdx.x);
