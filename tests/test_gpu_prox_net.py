@@ -1,8 +1,10 @@
 """GPU checks of the prox network: the training kernels' loss and gradient
 against the CPU oracle (same BF16 rounding points; the kernels accumulate in
 FP32, the oracle in float64), the inference kernel against the oracle's
-forward pass, training that lowers the loss, and what the shipped trained
-network gains over starting the Newton prox without it.
+forward pass (the batched inference on the tcgen05 tensor cores, the warm
+start inside the local step on mma.sync), training that lowers the loss, and
+what the shipped trained network gains over starting the Newton prox without
+it.
 
 Tolerances: gradient blocks within 2e-3 relative (L2), loss within 1e-5
 relative: an FP32 sum of 128-sample tiles against float64, where a value near
@@ -64,6 +66,27 @@ def test_prediction_matches_oracle():
     ref = no.predict(blob.astype(np.float64), sig, wov, mu, lam, bf=True)
     scale = blob[10:13].astype(np.float64)
     assert np.all(np.abs(got - ref) <= 1e-3 * scale + 1e-6)
+
+
+def test_tensor_core_prediction_over_many_tiles():
+    """wrapd_net_predict runs on the tcgen05 tensor cores, each CTA looping over
+    tiles of 128 samples: 200,003 samples (a ragged last tile, several tiles per
+    CTA) of the shipped network against the oracle's forward pass, and the
+    result independent of where a sample falls."""
+    mu, lam = prox_net.lame(E_YOUNG, NU)
+    rng = np.random.default_rng(17)
+    n = 200_003
+    sig = np.sort(rng.uniform(0.3, 2.0, (n, 3)), axis=1)[:, ::-1].copy()
+    wov = mu * np.exp(rng.uniform(-2.0, 4.0, n))
+    blob = prox_net.load_default()
+    got = prox_net.predict(blob, sig, wov, mu, lam)
+    ref = no.predict(blob.astype(np.float64), sig, wov, mu, lam, bf=True)
+    scale = blob[10:13].astype(np.float64)
+    assert np.all(np.abs(got - ref) <= 1e-3 * scale + 1e-6)
+    # the same samples in another order (other tiles, other CTAs) give the same values
+    perm = rng.permutation(n)
+    got2 = prox_net.predict(blob, sig[perm], wov[perm], mu, lam)
+    np.testing.assert_array_equal(got2, got[perm])
 
 
 def test_training_lowers_loss_and_is_deterministic():

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "prox_net.cuh"
+#include "prox_net_tc.cuh"
 
 namespace wrapd {
 namespace net {
@@ -361,6 +362,52 @@ __global__ void __launch_bounds__(128) k_predict(const unsigned char* __restrict
     }
 }
 
+__global__ void k_tc_image(const float* __restrict__ blob, unsigned char* __restrict__ img) {
+    tc::build_tc_image(blob, img, threadIdx.x, blockDim.x);
+}
+
+// Batched inference on the tcgen05 tensor cores: each CTA runs tiles of 128
+// samples (tile = blockIdx.x, + gridDim.x, ...) through tc::Cta::forward.
+// A bounded wait that gives up sets *err and ends the CTA's work.
+__global__ void __launch_bounds__(128) k_predict_tc(const unsigned char* __restrict__ gimg, int n,
+                                                    const double* __restrict__ sig, const double* __restrict__ wov,
+                                                    float mu, float lambda, double* __restrict__ out,
+                                                    int* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    tc::Cta cta;
+    cta.img = sm;
+    cta.act = sm + tc::T_BYTES;
+    cta.bar = reinterpret_cast<uint64_t*>(sm + tc::T_BYTES + tc::A_BYTES);
+    cta.tmem_slot = reinterpret_cast<uint32_t*>(sm + tc::T_BYTES + tc::A_BYTES + 8);
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(gimg);
+        uint4* dst = reinterpret_cast<uint4*>(sm);
+        for (int i = threadIdx.x; i < tc::T_BYTES / 16; i += blockDim.x) dst[i] = src[i];
+    }
+    cta.setup();
+    const float* nrm = reinterpret_cast<const float*>(sm + tc::T_NORM);
+    const int ntiles = (n + tc::M - 1) / tc::M;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int e = tile * tc::M + threadIdx.x;
+        const bool valid = e < n;
+        float s[3] = {1.f, 1.f, 1.f}, f[IN], y[OUT] = {0.f, 0.f, 0.f};
+        if (valid) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) s[i] = float(sig[3 * (size_t)e + i]);
+        }
+        features(s, valid ? float(wov[e]) : mu, mu, lambda, f);
+        if (!cta.forward(f, valid, y)) {   // the same verdict in every thread
+            if (threadIdx.x == 0) atomicExch(err, 1);
+            break;
+        }
+        if (valid) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) out[3 * (size_t)e + i] = s[i] + nrm[B_OSCALE + i] * y[i];
+        }
+    }
+    cta.teardown();
+}
+
 }  // namespace
 
 // Device image of a blob, built on `st` into `img` (IMAGE_BYTES).
@@ -597,17 +644,25 @@ WRAPD_API int wrapd_net_predict(const float* blob, int n_blob, int n, const doub
             }
         } bufs;
         float* d_blob = static_cast<float*>(bufs.get(N_BLOB * sizeof(float)));
-        unsigned char* d_img = static_cast<unsigned char*>(bufs.get(IMAGE_BYTES));
+        unsigned char* d_img = static_cast<unsigned char*>(bufs.get(tc::T_BYTES));
         double* d_s = static_cast<double*>(bufs.get(3 * (size_t)n * sizeof(double)));
         double* d_w = static_cast<double*>(bufs.get((size_t)n * sizeof(double)));
         double* d_o = static_cast<double*>(bufs.get(3 * (size_t)n * sizeof(double)));
-        upload_image(blob, d_img, d_blob, 0);
+        int* d_err = static_cast<int*>(bufs.get(sizeof(int)));
+        WRAPD_CUDA(cudaMemcpy(d_blob, blob, N_BLOB * sizeof(float), cudaMemcpyHostToDevice));
+        WRAPD_CUDA(cudaMemset(d_err, 0, sizeof(int)));
+        k_tc_image<<<1, 256>>>(d_blob, d_img);
+        WRAPD_LAUNCH_CHECK();
         WRAPD_CUDA(cudaMemcpy(d_s, sigma_in, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
         WRAPD_CUDA(cudaMemcpy(d_w, wov, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
-        k_predict<<<(n + 127) / 128, 128, IMAGE_BYTES + 4 * WARP_SCRATCH>>>(d_img, n, d_s, d_w, float(mu),
-                                                                           float(lambda), d_o);
+        const int tiles = (n + tc::M - 1) / tc::M;
+        k_predict_tc<<<std::min(tiles, 4 * kNumSMs), 128, tc::SMEM_BYTES>>>(d_img, n, d_s, d_w, float(mu),
+                                                                            float(lambda), d_o, d_err);
         WRAPD_LAUNCH_CHECK();
         WRAPD_CUDA(cudaMemcpy(out, d_o, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+        int err = 0;
+        WRAPD_CUDA(cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) throw CudaError(WRAPD_E_TIMEOUT, "a tensor-core wait of the prox network gave up");
     });
 }
 
