@@ -53,6 +53,7 @@ from oracle import pyoracle as po  # noqa: E402
 from wrapd_b200 import bars  # noqa: E402
 
 E_YOUNG, NU = 1e5, 0.45
+X_SAMPLE = 16384   # vertices whose positions the large-bar fixtures keep
 
 
 def svd_inputs(rng):
@@ -147,14 +148,19 @@ def bar_32x32x128_bent():
     runs = [("m5", 20, ("-rw_every", "10"), po.QUASI_REF_M5), ("m6", 60, (), po.QUASI_REF)]
     with cf.ThreadPoolExecutor(len(runs)) as ex:   # two single-thread processes side by side
         results = list(ex.map(lambda a: ref_solve(b, a[1], a[2], a[3]), runs))
+    # positions: a seeded sample of vertices, the column sums and max |x| (the
+    # whole 140,481 x 3 array would make a 7 MB fixture)
+    idx = np.sort(np.random.default_rng(32128).choice(b.n_verts, X_SAMPLE, replace=False))
     for (tag, _, _, _), r in zip(runs, results):
+        X = np.asarray(r["x"]).reshape(-1, 3)
         out.update({f"{tag}_objectives": r["objectives"], f"{tag}_inner": r["inner_iters"],
-                    f"{tag}_reweighted": r["reweighted"], f"{tag}_x": r["x"],
+                    f"{tag}_reweighted": r["reweighted"], f"{tag}_x_sample": X[idx],
+                    f"{tag}_x_colsum": X.sum(axis=0), f"{tag}_x_absmax": np.abs(X).max(),
                     f"{tag}_ls_dal": r["ls_delta_al"], f"{tag}_gs_dal": r["gs_delta_al"],
                     f"{tag}_setup_ms": r["runtime"]["setup_ms"],
                     f"{tag}_acc_time_s": r["accumulated_time_s"]})
         print(tag, "done:", r["runtime"], flush=True)
-    np.savez_compressed(os.path.join(HERE, "solve_bar_32x32x128_bent.npz"), **out)
+    np.savez_compressed(os.path.join(HERE, "solve_bar_32x32x128_bent.npz"), x_idx=idx, **out)
 
 
 def solves():
@@ -210,7 +216,6 @@ def quasi_files():
     np.savez_compressed(os.path.join(HERE, "quasi_small.npz"), **out)
 
 
-X_SAMPLE_64x64x160 = 16384
 
 
 def bar_64x64x160():
@@ -221,7 +226,7 @@ def bar_64x64x160():
                   linear_solver=1)
     o.solve()
     X = o.get("X").reshape(-1, 3)
-    idx = np.sort(np.random.default_rng(64160).choice(b.n_verts, X_SAMPLE_64x64x160, replace=False))
+    idx = np.sort(np.random.default_rng(64160).choice(b.n_verts, X_SAMPLE, replace=False))
     np.savez_compressed(os.path.join(HERE, "iters_bar_64x64x160.npz"), objectives=o.get("objectives"),
                         inner=o.get("inner_iters").astype(np.int32), flips=o.get("flips").astype(np.int32),
                         ls_dal=o.get("ls_dal"), gs_dal=o.get("gs_dal"), x_idx=idx, x_sample=X[idx],
