@@ -24,8 +24,10 @@ Outputs (all seeded, reproducible):
                     twist + 90 deg bend), 20 ADMM iterations of the patched
                     reference (quasi_ref_m5: L-BFGS history 5, reweight and
                     refactor every 10 iterations), and 60 iterations of the
-                    unpatched reference (history 6, gamma rule); one thread
-                    each (the deterministic reference), about 30 min of CPU
+                    unpatched reference (history 6, gamma rule, which
+                    refactors at every iteration from 50 on); one thread each
+                    (the deterministic reference), about 45 min of CPU for the
+                    two side by side; positions at 16,384 seeded vertices
   iters_bar_64x64x160.npz
                     the 3.9M-tet bar (720 deg twist): the first three ADMM
                     iterations (L-BFGS history 5, FP64) of the oracle, the C
