@@ -234,6 +234,13 @@ WRAPD_API int wrapd_potential_energy(wrapd_handle* h, double* pe, int* flips);
  * x = A^-1 b for an n_free x 3 block (free vertices in ascending id order). */
 WRAPD_API int wrapd_solve_A(wrapd_handle* h, const double* b, double* x);
 
+/* The bounded waits of the solve (no reference counterpart): wrapd_solve_A
+ * with front `front` of the assembly tree never reporting completion, so the
+ * wait of its parent's forward items runs out after about a second.  Returns
+ * WRAPD_E_TIMEOUT when it did (x then holds no solution) and leaves the handle
+ * usable; WRAPD_E_INPUT for a front outside [0, fronts) (wrapd_get_info). */
+WRAPD_API int wrapd_solve_A_holding(wrapd_handle* h, const double* b, double* x, int front);
+
 /* ---- per-element math over a batch, on the current device (handle-free) --
  * The same device functions the ADMM kernels inline.  fp32 = 1 runs them in
  * single precision (the element math of mixed mode). */

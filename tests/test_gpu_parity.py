@@ -143,6 +143,31 @@ def test_solve_A_matches_oracle(dims):
     assert rel_max(s.solve_A(b), o.solve_A(b)) < 1e-11
 
 
+def test_solve_waits_are_bounded():
+    """The solve runs each direction as one launch over a work queue whose
+    items wait for the fronts they read.  Holding back one leaf's completion
+    makes its parent's wait run out: the call returns WRAPD_E_TIMEOUT after
+    about a second instead of hanging, and the handle then solves as before,
+    bit for bit (the queue's results do not depend on the order CTAs take
+    items)."""
+    import time
+    bar = bars.make_bar(8, 8, 32, twist_deg=100.0, noise=0.02, seed=1)
+    s = make_solver(bar)
+    b = np.random.default_rng(5).normal(size=(int(s.info()["n_free"]), 3))
+    x0 = s.solve_A(b)
+    for _ in range(3):
+        np.testing.assert_array_equal(s.solve_A(b), x0)
+    t0 = time.perf_counter()
+    with pytest.raises(capi.WrapdError) as ei:
+        s.solve_A_holding(b, 0)   # front 0 is a leaf: its parent waits on it
+    assert ei.value.name == "WRAPD_E_TIMEOUT"
+    assert time.perf_counter() - t0 < 30.0
+    with pytest.raises(capi.WrapdError) as ei:
+        s.solve_A_holding(b, int(s.info()["fronts"]))
+    assert ei.value.name == "WRAPD_E_INPUT"
+    np.testing.assert_array_equal(s.solve_A(b), x0)
+
+
 # ---- whole solves --------------------------------------------------------------------
 def _compare_solve(s, objectives, inner, reweighted, x, tol_x):
     X = s.solve()

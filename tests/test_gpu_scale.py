@@ -1,5 +1,13 @@
 """GPU parity at the benchmarked sizes.
 
+The 786,432-tet bent bar the bench times (32x32x128 cubes, 360 deg twist and
+90 deg bend) is compared with the reference itself
+(tests/golden/solve_bar_32x32x128_bent.npz, single-threaded reference runs):
+20 iterations at the bench's settings (L-BFGS history 5, reweight and refactor
+every 10 iterations; the patched build quasi_ref_m5) in FP64: identical
+inner-iteration and reweight logs, energies within 1e-8 relative, positions
+within 1e-8 of max |x|.
+
 The 3.9M-tet bar (64x64x160 cubes, 720 deg twist) is compared with the oracle:
 its first three ADMM iterations (tests/golden/iters_bar_64x64x160.npz, the
 oracle with its conjugate-gradient linear solver), the global gradient at
@@ -39,6 +47,28 @@ def rel_max(a, b):
 @pytest.fixture(scope="module")
 def big4():
     return bars.bar_64x64x160()
+
+
+@pytest.fixture(scope="module")
+def bent():
+    return bars.bar_32x32x128_bent()
+
+
+def _positions_err(X, g, tag):
+    return np.abs(X[g["x_idx"]] - g[f"{tag}_x_sample"]).max() / float(g[f"{tag}_x_absmax"])
+
+
+def test_bar_32x32x128_bent_matches_patched_reference(golden, bent):
+    g = golden("solve_bar_32x32x128_bent.npz")
+    s = make_solver(bent, lbfgs_m=5, rw_every=10, max_iters=20)
+    X = s.solve()
+    assert len(s.log("objectives")) == len(g["m5_objectives"])
+    np.testing.assert_array_equal(s.log("inner_iters"), g["m5_inner"])
+    np.testing.assert_array_equal(s.log("reweighted"), g["m5_reweighted"])
+    np.testing.assert_allclose(s.log("objectives"), g["m5_objectives"], rtol=1e-8)
+    assert _positions_err(X, g, "m5") < 1e-8
+    np.testing.assert_allclose(X.sum(axis=0), g["m5_x_colsum"], rtol=1e-8, atol=1e-8 * X.shape[0])
+    s.close()
 
 
 def test_bar_64x64x160_first_iterations_match_oracle(golden, big4):

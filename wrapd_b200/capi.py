@@ -85,6 +85,7 @@ SIGNATURES = [
     ("wrapd_global_grad", ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp]),
     ("wrapd_potential_energy", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_int)]),
     ("wrapd_solve_A", ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    ("wrapd_solve_A_holding", ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.c_int]),
     ("wrapd_svd3_batch", ctypes.c_int, [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp]),
     ("wrapd_prox_batch", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                          _dp, _dp, _dp, _dp, _ip]),

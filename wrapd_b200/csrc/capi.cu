@@ -366,4 +366,9 @@ int wrapd_solve_A(wrapd_handle* h, const double* b, double* x) {
     return guarded(h, [&](wrapd::SolverGPU& s) { s.solve_A(b, x); });
 }
 
+int wrapd_solve_A_holding(wrapd_handle* h, const double* b, double* x, int front) {
+    if (!b || !x) return WRAPD_E_INPUT;
+    return guarded(h, [&](wrapd::SolverGPU& s) { s.solve_A(b, x, front); });
+}
+
 }  // extern "C"

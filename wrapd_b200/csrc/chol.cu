@@ -297,10 +297,12 @@ __global__ void k_extend_add(double* __restrict__ F, const FrontDesc* __restrict
 // of row i = tid % 32 (columns tid / 32 + 4m), with all its operands loaded
 // before the first store, so one barrier per pivot is the only serial step.
 // L(i, j) = A'(i, j) rsqrt(d) goes to Lsm (pitch lp), rsqrt(d) to D.  The
-// inverse is right-looking by rows: row s of inv(L) is (e_s - P(s, :)) / L(s, s)
-// and the rows below add L(r, s) times it to their partial sums P (kept in S).
-// Row s of inv(L) is written to X (pitch xp), columns < nb.  A non-positive
-// (or NaN) pivot sets *bad and continues with a unit pivot.
+// inverse is right-looking by rows with no barrier: lane c of warp 0 owns
+// column c of inv(L), its partial sums P(r, c) in registers; row s of the
+// column is (delta(s, c) - P(s, c)) / L(s, s), and the rows below add L(r, s)
+// times it (the same fma sequence per entry as a row-by-row sweep).  Row s of
+// inv(L) is written to X (pitch xp), columns < nb.  A non-positive (or NaN)
+// pivot sets *bad and continues with a unit pivot.
 constexpr int LSP = NB + 1;
 static_assert(GEMM_THREADS == 128 && NB == 32, "cta_chol_inv maps 128 threads onto 32 rows x 4 column slices");
 __device__ __forceinline__ void cta_chol_inv(const double* __restrict__ Fd, int64_t ld, int nb, double* S,
@@ -334,27 +336,23 @@ __device__ __forceinline__ void cta_chol_inv(const double* __restrict__ Fd, int6
         }
         __syncthreads();
     }
-    for (int idx = tid; idx < NB * NB; idx += GEMM_THREADS) S[(idx >> 5) * LSP + (idx & 31)] = 0.0;
-    __syncthreads();
-    const int c = tid & 31;
-    for (int s = 0; s < nb; ++s) {
-        const double ps = S[s * LSP + c];
-        const double ds = D[s];
-        double lr[8], pr[8];
+    if (tid < 32) {
+        const int c = tid;
+        double P[NB];
 #pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            lr[m] = Lsm[(q + 4 * m) * lp + s];
-            pr[m] = S[(q + 4 * m) * LSP + c];
-        }
-        const double f = (c <= s) ? ((c == s ? 1.0 : 0.0) - ps) * ds : 0.0;
-        if (q == 0 && c < nb) X[s * xp + c] = f;
+        for (int r = 0; r < NB; ++r) P[r] = 0.0;
 #pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            const int r = q + 4 * m;
-            if (r > s && r < nb) S[r * LSP + c] = fma(lr[m], f, pr[m]);
+        for (int s = 0; s < NB; ++s) {
+            if (s < nb) {
+                const double f = (c <= s) ? ((c == s ? 1.0 : 0.0) - P[s]) * D[s] : 0.0;
+                if (c < nb) X[s * xp + c] = f;
+#pragma unroll
+                for (int r = s + 1; r < NB; ++r)
+                    if (r < nb) P[r] = fma(Lsm[r * lp + s], f, P[r]);
+            }
         }
-        __syncthreads();
     }
+    __syncthreads();
     *bad = b;
 }
 
@@ -633,7 +631,7 @@ __device__ __forceinline__ void front_rhs(const double* __restrict__ B, const do
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const int64_t o = iv[q];
-        if (o >= 0) { v0 += U[o]; v1 += U[o + 1]; v2 += U[o + 2]; }
+        if (o >= 0) { v0 += __ldcg(U + o); v1 += __ldcg(U + o + 1); v2 += __ldcg(U + o + 2); }
     }
 }
 
@@ -663,15 +661,15 @@ __device__ __forceinline__ bool band_arrive(unsigned* counter, int nchunk) {
 // 16-byte load per column: the block's leading dimension and the band start are
 // even) and takes columns lo + w, lo + w + 8, ...; the eight warps' sums are
 // added in warp order.
-__global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B, double* __restrict__ Zb,
-                                                   double* __restrict__ U, const int64_t* __restrict__ inv,
-                                                   const double* __restrict__ YW, const FrontDesc* __restrict__ desc,
-                                                   const SolveItem* __restrict__ items, double* __restrict__ P,
-                                                   unsigned* __restrict__ counters) {
+// One forward item (q: its index in the item list, which places its partial
+// sums in P).  Returns true, in every thread, in the CTA that wrote the band's
+// result, after all its writes are visible device-wide.
+__device__ __forceinline__ bool fwd_item(const double* __restrict__ B, double* __restrict__ Zb,
+                                         double* __restrict__ U, const int64_t* __restrict__ inv,
+                                         const double* __restrict__ YW, const FrontDesc& d, const SolveItem& it, int q,
+                                         double* __restrict__ P, unsigned* __restrict__ counters) {
     __shared__ double tv[SCH * 3];
     __shared__ double part[8][TL][3];
-    const SolveItem it = items[blockIdx.x];
-    const FrontDesc d = desc[it.front];
     const int R = d.k + d.r;
     const int nc = it.hi - it.lo;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -724,14 +722,14 @@ __global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B,
     }
     if (it.nchunk > 1) {
         if (row < TL) {
-            double* p = P + 3 * ((int64_t)blockIdx.x * TL + row);
+            double* p = P + 3 * ((int64_t)q * TL + row);
             p[0] = s0; p[1] = s1; p[2] = s2;
         }
-        if (!band_arrive(counters + it.band, it.nchunk)) return;
+        if (!band_arrive(counters + it.band, it.nchunk)) return false;
         if (row < TL) {
             s0 = s1 = s2 = 0.0;
-            for (int q = 0; q < it.nchunk; ++q) {
-                const double* p = P + 3 * ((int64_t)(it.first + q) * TL + row);
+            for (int c = 0; c < it.nchunk; ++c) {
+                const double* p = P + 3 * ((int64_t)(it.first + c) * TL + row);
                 s0 += __ldcg(p); s1 += __ldcg(p + 1); s2 += __ldcg(p + 2);
             }
         }
@@ -747,6 +745,20 @@ __global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B,
             u[0] = v0 - s0; u[1] = v1 - s1; u[2] = v2 - s2;
         }
     }
+    __threadfence();
+    __syncthreads();
+    return true;
+}
+
+__global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B, double* __restrict__ Zb,
+                                                   double* __restrict__ U, const int64_t* __restrict__ inv,
+                                                   const double* __restrict__ YW, const FrontDesc* __restrict__ desc,
+                                                   const SolveItem* __restrict__ items, double* __restrict__ P,
+                                                   unsigned* __restrict__ counters, const int* __restrict__ mesh_on) {
+    const SolveItem it = items[blockIdx.x];
+    const FrontDesc d = desc[it.front];
+    if (mesh_on && !mesh_on[d.mesh]) return;   // the whole band's CTAs: its counter stays 0
+    fwd_item(B, Zb, U, inv, YW, d, it, blockIdx.x, P, counters);
 }
 
 // Backward: a CTA owns a band of 64 columns and a chunk [lo, hi) of the rows
@@ -756,15 +768,12 @@ __global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B,
 // of each as one 16-byte load.  The 8 x 3 lane sums are then added across the
 // warp by a butterfly that halves the values each lane keeps (12, 6, 3) before
 // two plain exchange steps, so the eight columns share 27 shuffles.
-__global__ void __launch_bounds__(256) k_bwd_level(double* __restrict__ x, const double* __restrict__ Zb,
-                                                   const double* __restrict__ YW, const int* __restrict__ rows,
-                                                   const FrontDesc* __restrict__ desc,
-                                                   const SolveItem* __restrict__ items, double* __restrict__ P,
-                                                   unsigned* __restrict__ counters) {
+__device__ __forceinline__ bool bwd_item(double* __restrict__ x, const double* __restrict__ Zb,
+                                         const double* __restrict__ YW, const int* __restrict__ rows,
+                                         const FrontDesc& d, const SolveItem& it, int q, double* __restrict__ P,
+                                         unsigned* __restrict__ counters) {
     __shared__ double in[(SCH + 1) * 3];
     __shared__ double res[TL][3];
-    const SolveItem it = items[blockIdx.x];
-    const FrontDesc d = desc[it.front];
     const int nr = it.hi - it.lo;
     const int nc = min(TL, d.k - it.b0);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -786,7 +795,7 @@ __global__ void __launch_bounds__(256) k_bwd_level(double* __restrict__ x, const
                 v0 = z[0]; v1 = z[1]; v2 = z[2];
             } else {
                 const double* y = x + 3 * (int64_t)rows[d.rows_off + i - d.k];
-                v0 = -y[0]; v1 = -y[1]; v2 = -y[2];
+                v0 = -__ldcg(y); v1 = -__ldcg(y + 1); v2 = -__ldcg(y + 2);
             }
         }
         in[3 * t] = v0; in[3 * t + 1] = v1; in[3 * t + 2] = v2;
@@ -858,14 +867,14 @@ __global__ void __launch_bounds__(256) k_bwd_level(double* __restrict__ x, const
     if (j < TL) { s0 = res[j][0]; s1 = res[j][1]; s2 = res[j][2]; }
     if (it.nchunk > 1) {
         if (j < TL) {
-            double* p = P + 3 * ((int64_t)blockIdx.x * TL + j);
+            double* p = P + 3 * ((int64_t)q * TL + j);
             p[0] = s0; p[1] = s1; p[2] = s2;
         }
-        if (!band_arrive(counters + it.band, it.nchunk)) return;
+        if (!band_arrive(counters + it.band, it.nchunk)) return false;
         if (j < TL) {
             s0 = s1 = s2 = 0.0;
-            for (int q = 0; q < it.nchunk; ++q) {
-                const double* p = P + 3 * ((int64_t)(it.first + q) * TL + j);
+            for (int c = 0; c < it.nchunk; ++c) {
+                const double* p = P + 3 * ((int64_t)(it.first + c) * TL + j);
                 s0 += __ldcg(p); s1 += __ldcg(p + 1); s2 += __ldcg(p + 2);
             }
         }
@@ -873,6 +882,120 @@ __global__ void __launch_bounds__(256) k_bwd_level(double* __restrict__ x, const
     if (j < nc) {
         double* o = x + 3 * ((int64_t)d.first + it.b0 + j);
         o[0] = s0; o[1] = s1; o[2] = s2;
+    }
+    __threadfence();
+    __syncthreads();
+    return true;
+}
+
+__global__ void __launch_bounds__(256) k_bwd_level(double* __restrict__ x, const double* __restrict__ Zb,
+                                                   const double* __restrict__ YW, const int* __restrict__ rows,
+                                                   const FrontDesc* __restrict__ desc,
+                                                   const SolveItem* __restrict__ items, double* __restrict__ P,
+                                                   unsigned* __restrict__ counters, const int* __restrict__ mesh_on) {
+    const SolveItem it = items[blockIdx.x];
+    const FrontDesc d = desc[it.front];
+    if (mesh_on && !mesh_on[d.mesh]) return;
+    bwd_item(x, Zb, YW, rows, d, it, blockIdx.x, P, counters);
+}
+
+// ---- whole-direction solve over a work queue -------------------------------------
+// One launch per direction walks every level: the items of all levels in one
+// list (forward: leaves first; backward: root first), taken in list order by
+// persistent CTAs through an atomic head (each CTA takes its next item while
+// it works on the current one).  An item waits, in thread 0, until the fronts
+// it reads are complete -- forward: both children (their update vectors);
+// backward: the parent (and through it every ancestor, which own the front's
+// rows) -- counted by per-front band counters that each band's writer bumps
+// after its writes are visible.  Every item an item waits on comes earlier in
+// the list and was taken by a running CTA, so the earliest unfinished item
+// never waits and the queue always drains.  A wait polls at most kWaitPolls
+// times (about a second); one that gives up sets *status to WRAPD_E_TIMEOUT and
+// skips its item, and every later wait returns at once, so the launch ends
+// with the error for the host to read.  The results are those of the per-level
+// launches bit for bit: the same items, chunks and chunk order per band.
+constexpr unsigned long long kWaitNs = 1000000000ull;   // one second of the global timer
+constexpr int kWaitPolls = 1 << 24;                      // and at most this many polls
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool wait_bands(const unsigned* done, unsigned target, int* status) {
+    const unsigned long long t0 = global_ns();
+    for (int i = 0; i < kWaitPolls; ++i) {
+        if (ld_acquire(done) >= target) return true;
+        if (*reinterpret_cast<volatile int*>(status) != 0) return false;   // another wait gave up
+        if (global_ns() - t0 > kWaitNs) break;
+        __nanosleep(64);
+    }
+    atomicCAS(status, 0, WRAPD_E_TIMEOUT);
+    return false;
+}
+
+// Takes the CTA's next item (in every thread), prefetching the one after it.
+__device__ __forceinline__ int next_item(const SolveQueue& Q, int* s_cur, int* s_next) {
+    __syncthreads();   // the previous item's shared-memory use is over
+    if (threadIdx.x == 0) {
+        *s_cur = *s_next;
+        if (*s_cur < Q.n) *s_next = static_cast<int>(atomicAdd(Q.head, 1u));
+    }
+    __syncthreads();
+    return *s_cur;
+}
+
+__global__ void __launch_bounds__(256) k_fwd_queue(const double* __restrict__ B, double* __restrict__ Zb,
+                                                   double* __restrict__ U, const int64_t* __restrict__ inv,
+                                                   const double* __restrict__ YW, const FrontDesc* __restrict__ desc,
+                                                   SolveQueue Q, double* __restrict__ P, unsigned* __restrict__ counters,
+                                                   const int* __restrict__ mesh_on) {
+    __shared__ int s_cur, s_next, s_ok;
+    if (threadIdx.x == 0) s_next = static_cast<int>(atomicAdd(Q.head, 1u));
+    for (;;) {
+        const int q = next_item(Q, &s_cur, &s_next);
+        if (q >= Q.n) break;
+        const SolveItem it = Q.items[q];
+        const FrontDesc d = desc[it.front];
+        if (mesh_on && !mesh_on[d.mesh]) continue;
+        if (threadIdx.x == 0) {
+            bool ok = d.child0 < 0 || wait_bands(Q.done + d.child0, Q.nbands[d.child0], Q.status);
+            ok = ok && (d.child1 < 0 || wait_bands(Q.done + d.child1, Q.nbands[d.child1], Q.status));
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) continue;
+        if (fwd_item(B, Zb, U, inv, YW, d, it, q, P, counters) && threadIdx.x == 0 && it.front != Q.hold)
+            atomicAdd(Q.done + it.front, 1u);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_bwd_queue(double* __restrict__ x, const double* __restrict__ Zb,
+                                                   const double* __restrict__ YW, const int* __restrict__ rows,
+                                                   const FrontDesc* __restrict__ desc, SolveQueue Q,
+                                                   double* __restrict__ P, unsigned* __restrict__ counters,
+                                                   const int* __restrict__ mesh_on) {
+    __shared__ int s_cur, s_next, s_ok;
+    if (threadIdx.x == 0) s_next = static_cast<int>(atomicAdd(Q.head, 1u));
+    for (;;) {
+        const int q = next_item(Q, &s_cur, &s_next);
+        if (q >= Q.n) break;
+        const SolveItem it = Q.items[q];
+        const FrontDesc d = desc[it.front];
+        if (mesh_on && !mesh_on[d.mesh]) continue;
+        if (threadIdx.x == 0)
+            s_ok = d.parent < 0 || wait_bands(Q.done + d.parent, Q.nbands[d.parent], Q.status);
+        __syncthreads();
+        if (!s_ok) continue;
+        if (bwd_item(x, Zb, YW, rows, d, it, q, P, counters) && threadIdx.x == 0 && it.front != Q.hold)
+            atomicAdd(Q.done + it.front, 1u);
     }
 }
 
@@ -956,6 +1079,8 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         d.child0 = d.nchild > 0 ? F.children[0] : -1;
         d.child1 = d.nchild > 1 ? F.children[1] : -1;
         d.ldy = static_cast<int>(yw_ld(d.k, d.r));
+        d.mesh = front_mesh.empty() ? 0 : front_mesh[f];
+        d.parent = F.parent;
     }
     std::vector<int64_t> inv(ioff, -1);
     for (int f = 0; f < nfronts; ++f) {
@@ -1103,7 +1228,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
             fwd_items([&](int) { return sch; }, fwd, fbands);
             bwd_items([&](int) { return sch; }, bwd, bbands);
             L.cand.push_back({sch, upload(fwd, st), static_cast<int>(fwd.size()), upload(bwd, st),
-                              static_cast<int>(bwd.size())});
+                              static_cast<int>(bwd.size()), fwd, bwd});
             if (L.cfwd < 0 && (int)fwd.size() >= kSolveCtas) L.cfwd = c;
             if (L.cbwd < 0 && (int)bwd.size() >= kSolveCtas) L.cbwd = c;
             solve_parts_ = std::max<int64_t>(solve_parts_, std::max<int64_t>(fwd.size(), bwd.size()));
@@ -1131,7 +1256,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
             fwd_items([&](int f) { return sf[front_mesh[f]]; }, fwd, fbands);
             bwd_items([&](int f) { return sb[front_mesh[f]]; }, bwd, bbands);
             L.cand.push_back({0, upload(fwd, st), static_cast<int>(fwd.size()), upload(bwd, st),
-                              static_cast<int>(bwd.size())});
+                              static_cast<int>(bwd.size()), fwd, bwd});
             L.cfwd = L.cbwd = static_cast<int>(L.cand.size()) - 1;
             solve_parts_ = std::max<int64_t>(solve_parts_, std::max<int64_t>(fwd.size(), bwd.size()));
             solve_bands_ = std::max(solve_bands_, std::max(fbands, bbands));
@@ -1145,6 +1270,22 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         trsm_nP_.push_back(w);
     }
     count_launches();
+    // work queues: room for every level's longest candidate list; the band
+    // counts do not depend on the chunk length
+    int64_t qcap_f = 0, qcap_b = 0;
+    qbands_f_ = qbands_b_ = 0;
+    for (const Level& L : levels_) {
+        int64_t mf = 0, mb = 0;
+        for (const Level::SolveCand& c : L.cand) { mf = std::max<int64_t>(mf, c.nfwd); mb = std::max<int64_t>(mb, c.nbwd); }
+        qcap_f += mf;
+        qcap_b += mb;
+        if (!L.cand.empty()) {
+            const Level::SolveCand& c = L.cand[0];
+            qbands_f_ += c.hfwd.empty() ? 0 : c.hfwd.back().band + 1;
+            qbands_b_ += c.hbwd.empty() ? 0 : c.hbwd.back().band + 1;
+        }
+    }
+    solve_parts_ = std::max<int64_t>(solve_parts_, std::max(qcap_f, qcap_b));
     d_P_ = dalloc(3 * TL * (size_t)solve_parts_);
     {
         unsigned* c = nullptr;
@@ -1154,12 +1295,79 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         d_cnt_ = c;
         WRAPD_CUDA(cudaMemsetAsync(d_cnt_, 0, std::max(1, solve_bands_) * sizeof(unsigned), st));
     }
+    d_qf_ = upload(std::vector<SolveItem>(std::max<int64_t>(1, qcap_f)), st);
+    d_qb_ = upload(std::vector<SolveItem>(std::max<int64_t>(1, qcap_b)), st);
+    d_qnb_ = upload(std::vector<unsigned>(2 * (size_t)std::max(1, nfronts)), st);
+    qcap_f_ = qcap_f;
+    qcap_b_ = qcap_b;
+    qctl_words_ = 2 + 2 * (size_t)nfronts + qbands_f_ + qbands_b_;
+    d_qctl_ = upload(std::vector<unsigned>(qctl_words_), st);
+    {
+        int dev = 0, sms = 0, bf = 0, bb = 0;
+        WRAPD_CUDA(cudaGetDevice(&dev));
+        WRAPD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        WRAPD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_fwd_queue, 256, 0));
+        WRAPD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, k_bwd_queue, 256, 0));
+        qgrid_f_ = std::max(1, bf) * sms;
+        qgrid_b_ = std::max(1, bb) * sms;
+    }
+    build_queues(st);
     WRAPD_CUDA(cudaStreamSynchronize(st));
+}
+
+// The chosen candidate of every level, concatenated: forward leaves first,
+// backward root first, with item and band indexes made global (each
+// direction's bands numbered from 0 in its own counter range).  Every index
+// the kernels will use is checked against its buffer here.
+void CholGPU::build_queues(cudaStream_t st) {
+    std::vector<SolveItem> qf, qb;
+    std::vector<unsigned> nb(2 * (size_t)std::max(1, nfronts), 0u);
+    auto append = [&](const std::vector<SolveItem>& src, std::vector<SolveItem>& q, int& bands, unsigned* nbands) {
+        const int i0 = static_cast<int>(q.size()), b0 = bands;
+        for (size_t i = 0; i < src.size(); ++i) {
+            SolveItem g = src[i];
+            if ((int)i == g.first) nbands[g.front]++;   // the first chunk of a band
+            g.first += i0;
+            g.band += b0;
+            bands = std::max(bands, g.band + 1);
+            q.push_back(g);
+        }
+    };
+    int bf = 0, bb = 0;
+    for (int l = 0; l < nlevels; ++l) {
+        const Level& L = levels_[l];
+        if (!L.cand.empty()) append(L.cand[L.cfwd].hfwd, qf, bf, nb.data());
+    }
+    for (int l = nlevels - 1; l >= 0; --l) {
+        const Level& L = levels_[l];
+        if (!L.cand.empty()) append(L.cand[L.cbwd].hbwd, qb, bb, nb.data() + nfronts);
+    }
+    auto check = [&](const std::vector<SolveItem>& q, int64_t cap, int nbands, const char* what) {
+        if ((int64_t)q.size() > cap || (int64_t)q.size() > solve_parts_)
+            throw CudaError(WRAPD_E_INPUT, std::string("solve queue longer than its buffers: ") + what);
+        for (size_t i = 0; i < q.size(); ++i) {
+            const SolveItem& g = q[i];
+            const bool ok = g.front >= 0 && g.front < nfronts && g.band >= 0 && g.band < nbands && g.nchunk >= 1 &&
+                            g.first >= 0 && g.first <= (int)i && (int64_t)g.first + g.nchunk <= (int64_t)q.size() &&
+                            (int)i < g.first + g.nchunk;
+            if (!ok) throw CudaError(WRAPD_E_INPUT, std::string("solve queue item out of range: ") + what);
+        }
+    };
+    if (bf != qbands_f_ || bb != qbands_b_) throw CudaError(WRAPD_E_INPUT, "solve queue band count mismatch");
+    check(qf, qcap_f_, qbands_f_, "forward");
+    check(qb, qcap_b_, qbands_b_, "backward");
+    nqf_ = static_cast<int>(qf.size());
+    nqb_ = static_cast<int>(qb.size());
+    if (!qf.empty()) WRAPD_CUDA(cudaMemcpyAsync(d_qf_, qf.data(), qf.size() * sizeof(SolveItem), cudaMemcpyHostToDevice, st));
+    if (!qb.empty()) WRAPD_CUDA(cudaMemcpyAsync(d_qb_, qb.data(), qb.size() * sizeof(SolveItem), cudaMemcpyHostToDevice, st));
+    WRAPD_CUDA(cudaMemcpyAsync(d_qnb_, nb.data(), nb.size() * sizeof(unsigned), cudaMemcpyHostToDevice, st));
+    WRAPD_CUDA(cudaStreamSynchronize(st));   // the host vectors go out of scope
+    if (solve_graph_) { cudaGraphExecDestroy(solve_graph_); solve_graph_ = nullptr; }
 }
 
 void CholGPU::count_launches() {
     launches_factor = 4;   // memsets + assembly + identity
-    launches_solve = 1;    // the right-hand side copy
+    launches_solve = 2;    // the two queue launches (plus a copy and a memset)
     for (const Level& L : levels_) {
         for (const WorkList& e : L.extend) launches_factor += e.total ? 1 : 0;
         for (size_t p = 0; p < L.trsm.size(); ++p) {
@@ -1167,7 +1375,6 @@ void CholGPU::count_launches() {
             launches_factor += (L.trsm[p].total ? 1 : 0) + (L.update[p].total ? 1 : 0);
         }
         launches_factor += L.wgemm.total ? 1 : 0;
-        launches_solve += 2;
     }
 }
 
@@ -1204,16 +1411,19 @@ void CholGPU::autotune(const double* d_w2, const double* d_Di, int ne, cudaStrea
         for (int c = 0; c < (int)L.cand.size(); ++c) {
             const Level::SolveCand& C = L.cand[c];
             const float tf = timed(3, [&] {
-                k_fwd_level<<<C.nfwd, 256, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_desc_, C.fwd, d_P_, d_cnt_);
+                k_fwd_level<<<C.nfwd, 256, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_desc_, C.fwd, d_P_, d_cnt_,
+                                                    nullptr);
             });
             const float tb = timed(3, [&] {
-                k_bwd_level<<<C.nbwd, 256, 0, st>>>(d_T_, d_Z_, d_Y_, d_rows_, d_desc_, C.bwd, d_P_, d_cnt_);
+                k_bwd_level<<<C.nbwd, 256, 0, st>>>(d_T_, d_Z_, d_Y_, d_rows_, d_desc_, C.bwd, d_P_, d_cnt_,
+                                                    nullptr);
             });
             WRAPD_LAUNCH_CHECK();
             if (tf < best_f) { best_f = tf; L.cfwd = c; }
             if (tb < best_b) { best_b = tb; L.cbwd = c; }
         }
     }
+    if (front_mesh.empty()) build_queues(st);
     const int candidates[] = {0, kNumSMs, kFusedPanelCtas, 4 * kFusedPanelCtas, 1 << 30};
     float best = 1e30f;
     int pick = kFusedPanelCtas;
@@ -1296,30 +1506,37 @@ void CholGPU::factor(const double* d_w2, const double* d_Di, int ne, cudaStream_
     WRAPD_CUDA(cudaGraphLaunch(factor_graph_, st));
 }
 
-void CholGPU::solve_launches(double* d_x, cudaStream_t st) {
+void CholGPU::solve_launches(double* d_x, cudaStream_t st, const int* mesh_on, int hold) {
     WRAPD_CUDA(cudaMemcpyAsync(d_T_, d_x, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    for (int l = 0; l < nlevels; ++l) {
-        Level& L = levels_[l];
-        const Level::SolveCand& c = L.cand[L.cfwd];
-        k_fwd_level<<<c.nfwd, 256, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_desc_, c.fwd, d_P_, d_cnt_);
+    WRAPD_CUDA(cudaMemsetAsync(d_qctl_, 0, qctl_words_ * sizeof(unsigned), st));
+    unsigned* bands = d_qctl_ + 2 + 2 * (size_t)nfronts;
+    if (nqf_ > 0) {
+        const SolveQueue Q{d_qf_, nqf_, d_qctl_, d_qctl_ + 2, d_qnb_, d_status, hold};
+        k_fwd_queue<<<std::min(qgrid_f_, nqf_), 256, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_desc_, Q, d_P_, bands,
+                                                           mesh_on);
         WRAPD_LAUNCH_CHECK();
     }
-    for (int l = nlevels - 1; l >= 0; --l) {
-        Level& L = levels_[l];
-        const Level::SolveCand& c = L.cand[L.cbwd];
-        k_bwd_level<<<c.nbwd, 256, 0, st>>>(d_x, d_Z_, d_Y_, d_rows_, d_desc_, c.bwd, d_P_, d_cnt_);
+    if (nqb_ > 0) {
+        const SolveQueue Q{d_qb_, nqb_, d_qctl_ + 1, d_qctl_ + 2 + nfronts, d_qnb_ + nfronts, d_status, hold};
+        k_bwd_queue<<<std::min(qgrid_b_, nqb_), 256, 0, st>>>(d_x, d_Z_, d_Y_, d_rows_, d_desc_, Q, d_P_,
+                                                           bands + qbands_f_, mesh_on);
         WRAPD_LAUNCH_CHECK();
     }
 }
 
-void CholGPU::solve(double* d_x, cudaStream_t st) {
-    if (!use_graphs) { solve_launches(d_x, st); return; }
-    if (!solve_graph_ || solve_graph_x_ != d_x) {
+void CholGPU::solve_holding(double* d_x, int hold, cudaStream_t st) {
+    if (hold < 0 || hold >= nfronts) throw CudaError(WRAPD_E_INPUT, "front index out of range");
+    solve_launches(d_x, st, nullptr, hold);
+}
+
+void CholGPU::solve(double* d_x, cudaStream_t st, const int* mesh_on) {
+    if (!use_graphs) { solve_launches(d_x, st, mesh_on); return; }
+    if (!solve_graph_ || solve_graph_x_ != d_x || solve_graph_mask_ != mesh_on) {
         if (solve_graph_) { cudaGraphExecDestroy(solve_graph_); solve_graph_ = nullptr; }
         cudaGraph_t g;
         WRAPD_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         try {
-            solve_launches(d_x, st);
+            solve_launches(d_x, st, mesh_on);
         } catch (...) {
             cudaStreamEndCapture(st, &g);
             throw;
@@ -1328,6 +1545,7 @@ void CholGPU::solve(double* d_x, cudaStream_t st) {
         WRAPD_CUDA(cudaGraphInstantiate(&solve_graph_, g, 0));
         cudaGraphDestroy(g);
         solve_graph_x_ = d_x;
+        solve_graph_mask_ = mesh_on;
     }
     WRAPD_CUDA(cudaGraphLaunch(solve_graph_, st));
 }

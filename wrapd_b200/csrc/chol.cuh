@@ -29,6 +29,8 @@ struct FrontDesc {
     int first, k, r, ld;
     int64_t f_off, y_off, u_off, rows_off, rel_off, inv_off;
     int nchild, child0, child1, ldy;   // ldy: leading dimension of the front's [Y; W] block
+    int mesh;                          // the mesh of a batch the front belongs to (0: one mesh)
+    int parent;                        // -1 at a root
 };
 
 // A trailing-update job of the blocked factorization: C -= A B'^T over a K range
@@ -41,6 +43,21 @@ struct FrontDesc {
 // arrival counter.
 struct SolveItem {
     int front, b0, lo, hi, nchunk, first, band;
+};
+
+// The items of every level of one direction as one work list (see k_fwd_queue):
+// head is the next item to take; done[f] counts the bands of front f written,
+// complete at nbands[f]; status receives WRAPD_E_TIMEOUT from a wait that gave
+// up; hold is a front whose completion is never counted (-1: none), which
+// makes the waits on it run out (the test of that path).
+struct SolveQueue {
+    const SolveItem* items;
+    int n;
+    unsigned* head;
+    unsigned* done;
+    const unsigned* nbands;
+    int* status;
+    int hold;
 };
 
 struct GemmJob {
@@ -83,8 +100,15 @@ public:
     // (the pointers must stay the same between calls).
     void factor(const double* d_w2, const double* d_Di, int ne, cudaStream_t st);
     // In place: x <- A^-1 x for an n x 3 block in the dissection order
-    // (graph-replayed per vector pointer).
-    void solve(double* d_x, cudaStream_t st);
+    // (graph-replayed per vector and mask pointer): one queue-driven launch per
+    // direction.  With mesh_on (device, one int per mesh) the fronts of a mesh
+    // whose entry is 0 are skipped: that mesh's rows of x keep their input
+    // values.  A dependency wait that gives up leaves WRAPD_E_TIMEOUT in
+    // *d_status.
+    void solve(double* d_x, cudaStream_t st, const int* mesh_on = nullptr);
+    // One solve of x in which front `hold` never reports completion, so that the
+    // waits on it run out (not graph-captured; the test of the bounded waits).
+    void solve_holding(double* d_x, int hold, cudaStream_t st);
     // Times the candidate tile shapes on this system (the solve's chunk length
     // per level and direction; the largest panel step, in tiles, that factors
     // its diagonal block inside the tile launch) and keeps the fastest.  Runs
@@ -118,7 +142,14 @@ private:
         WorkList wgemm;                  // W = L_rs Y tiles
         // solve items for each candidate chunk length: forward (64-row band,
         // column chunk) and backward (64-column band, row chunk)
-        struct SolveCand { int sch; SolveItem* fwd; int nfwd; SolveItem* bwd; int nbwd; };
+        struct SolveCand {
+            int sch;
+            SolveItem* fwd;
+            int nfwd;
+            SolveItem* bwd;
+            int nbwd;
+            std::vector<SolveItem> hfwd, hbwd;   // host copies, for the work queues
+        };
         std::vector<SolveCand> cand;
         int cfwd = 0, cbwd = 0;          // the candidates in use
     };
@@ -144,10 +175,22 @@ private:
     cudaGraphExec_t factor_graph_ = nullptr;
     cudaGraphExec_t solve_graph_ = nullptr;
     double* solve_graph_x_ = nullptr;
+    const int* solve_graph_mask_ = nullptr;
     int fused_ctas_ = 0;                 // panel steps of at most this many tiles run fused (k_panel)
     void count_launches();
     void factor_launches(const double* d_w2, const double* d_Di, int ne, cudaStream_t st);
-    void solve_launches(double* d_x, cudaStream_t st);
+    void solve_launches(double* d_x, cudaStream_t st, const int* mesh_on, int hold = -1);
+    // the work queues of the chosen per-level candidates (after build and autotune)
+    void build_queues(cudaStream_t st);
+    SolveItem* d_qf_ = nullptr;   // forward items, leaves first (capacity: the longest candidates)
+    SolveItem* d_qb_ = nullptr;   // backward items, root first
+    int nqf_ = 0, nqb_ = 0;
+    unsigned* d_qnb_ = nullptr;   // bands per front: forward [0, nfronts), backward [nfronts, 2 nfronts)
+    unsigned* d_qctl_ = nullptr;  // zeroed per solve: 2 heads, done counters (2 nfronts), band counters
+    size_t qctl_words_ = 0;
+    int qbands_f_ = 0, qbands_b_ = 0;   // band counters: forward, then backward
+    int64_t qcap_f_ = 0, qcap_b_ = 0;   // item capacity of d_qf_, d_qb_
+    int qgrid_f_ = 0, qgrid_b_ = 0;   // persistent CTAs per queue launch (resident at once)
     std::vector<void*> allocs_;
     std::vector<FrontDesc> h_desc_;
     std::vector<std::vector<int*>> trsm_nP_;   // per level, per panel step: panel-row tile counts

@@ -141,6 +141,7 @@ SolverGPU::~SolverGPU() {
     for (auto& set : evs_)
         for (auto& e : set) if (e) cudaEventDestroy(e);
     if (h_scal_) cudaFreeHost(h_scal_);
+    if (h_status_) cudaFreeHost(h_status_);
     if (h_ctl_block_) cudaFreeHost(h_ctl_block_);
     if (st_) cudaStreamDestroy(st_);
 }
@@ -423,6 +424,8 @@ void SolverGPU::initialize() {
     WRAPD_CUDA(cudaMemsetAsync(d_scal_, 0, (size_t)nm * kScalStride * sizeof(double), st_));
     WRAPD_CUDA(cudaMallocHost(&h_scal_, (size_t)nm * kScalStride * sizeof(double)));
     std::memset(h_scal_, 0, (size_t)nm * kScalStride * sizeof(double));
+    WRAPD_CUDA(cudaMallocHost(&h_status_, sizeof(int)));
+    *h_status_ = 0;
     {
         static const double one = 1.0;
         WRAPD_CUDA(cudaMemcpyAsync(d_scal_ + S_ONE, &one, sizeof(double), cudaMemcpyHostToDevice, st_));
@@ -704,12 +707,27 @@ void SolverGPU::profile_flush() {
     event_next_ = 0;
 }
 
+// The device status word carries a factorization's non-positive pivot and a
+// solve's dependency wait that gave up; it is read with every scalar block.
+static void throw_status(int status) {
+    if (status == WRAPD_E_TIMEOUT)
+        throw CudaError(status, "a dependency wait of the triangular solve gave up");
+    throw CudaError(status, "factorization of D^T W D hit a non-positive pivot");
+}
+
 void SolverGPU::sync_read() {
     WRAPD_CUDA(cudaMemcpyAsync(h_scal_, d_scal_, (size_t)nm * kScalStride * sizeof(double), cudaMemcpyDeviceToHost, st_));
+    WRAPD_CUDA(cudaMemcpyAsync(h_status_, chol.d_status, sizeof(int), cudaMemcpyDeviceToHost, st_));
     WRAPD_CUDA(cudaStreamSynchronize(st_));
     ctl_pending_ = false;
     n_sync++;
     mark(5);
+    if (*h_status_ != 0) {
+        const int status = *h_status_;
+        *h_status_ = 0;
+        WRAPD_CUDA(cudaMemsetAsync(chol.d_status, 0, sizeof(int), st_));
+        throw_status(status);
+    }
 }
 
 void SolverGPU::check_status() {
@@ -719,7 +737,7 @@ void SolverGPU::check_status() {
     ctl_pending_ = false;
     if (status != 0) {
         WRAPD_CUDA(cudaMemsetAsync(chol.d_status, 0, sizeof(int), st_));
-        throw CudaError(status, "factorization of D^T W D hit a non-positive pivot");
+        throw_status(status);
     }
 }
 
@@ -940,7 +958,7 @@ int SolverGPU::lbfgs_minimize() {
         WRAPD_LAUNCH_CHECK();
         // q = A^-1 q, three right-hand sides at once (the block-diagonal system)
         mark(2);
-        chol.solve(d_q_, st_);
+        chol.solve(d_q_, st_, nm > 1 ? mask(MK_LBFGS) : nullptr);   // the meshes out of their loop skip it
         kernel_launches += chol.launches_solve;
         n_solve++;
         mark(3);
@@ -1367,17 +1385,19 @@ void SolverGPU::potential_energy(double* pe, int* flips) {
     if (flips) *flips = f;
 }
 
-void SolverGPU::solve_A(const double* b, double* x) {
+void SolverGPU::solve_A(const double* b, double* x, int hold) {
     if (!initialized_) throw CudaError(WRAPD_E_STATE, "solve_A before initialize");
     std::vector<double> xp(3 * (size_t)nf);
     for (int i = 0; i < nf; ++i)
         for (int c = 0; c < 3; ++c) xp[3 * (size_t)iperm_[i] + c] = b[3 * (size_t)i + c];
     WRAPD_CUDA(cudaMemcpyAsync(d_q_, xp.data(), xp.size() * 8, cudaMemcpyHostToDevice, st_));
-    chol.solve(d_q_, st_);
+    if (hold < 0)
+        chol.solve(d_q_, st_);
+    else
+        chol.solve_holding(d_q_, hold, st_);
     kernel_launches += chol.launches_solve;
     WRAPD_CUDA(cudaMemcpyAsync(xp.data(), d_q_, xp.size() * 8, cudaMemcpyDeviceToHost, st_));
-    WRAPD_CUDA(cudaStreamSynchronize(st_));
-    ctl_pending_ = false;
+    check_status();
     for (int i = 0; i < nf; ++i)
         for (int c = 0; c < 3; ++c) x[3 * (size_t)i + c] = xp[3 * (size_t)iperm_[i] + c];
 }

@@ -61,7 +61,10 @@ public:
     double polar_update(bool update_candidates);
     double global_grad(const double* xfree, double* grad);
     void potential_energy(double* pe, int* flips);
-    void solve_A(const double* b, double* x);
+    // x = A^-1 b; with hold >= 0, front `hold` never reports completion (the
+    // bounded-wait test: throws WRAPD_E_TIMEOUT)
+    void solve_A(const double* b, double* x, int hold = -1);
+    int n_fronts() const { return chol.nfronts; }
 
     // The logs of a single mesh; of a batch, the sums over its meshes
     // (energies, flips, inner iterations), any reweight, and the x error of
@@ -161,6 +164,7 @@ private:
     unsigned* d_counters_ = nullptr;       // one grid-reduction counter per mesh
     double* d_scal_ = nullptr;             // kScalStride scalars per mesh
     double* h_scal_ = nullptr;
+    int* h_status_ = nullptr;    // pinned: the device status word, read with the scalars
     // ---- the meshes of the batch: each its own ADMM and L-BFGS state ----
     int nm = 0;
     struct MeshRun {

@@ -222,6 +222,14 @@ class Solver:
         self._h.check(self._h.lib.wrapd_solve_A(self._h.h, capi.dptr(bb), capi.dptr(x)))
         return x
 
+    def solve_A_holding(self, b, front):
+        """wrapd_solve_A_holding: the solve with one front never reporting
+        completion; raises WrapdError (WRAPD_E_TIMEOUT) when the waits ran out."""
+        bb = np.ascontiguousarray(b, dtype=np.float64).reshape(-1, 3)
+        x = np.empty_like(bb)
+        self._h.check(self._h.lib.wrapd_solve_A_holding(self._h.h, capi.dptr(bb), capi.dptr(x), int(front)))
+        return x
+
     def close(self):
         self._h.close()
 
