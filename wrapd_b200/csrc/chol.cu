@@ -941,26 +941,30 @@ __device__ __forceinline__ bool wait_bands(const unsigned* done, unsigned target
     return false;
 }
 
-// Takes the CTA's next item (in every thread), prefetching the one after it.
-__device__ __forceinline__ int next_item(const SolveQueue& Q, int* s_cur, int* s_next) {
+// Takes the CTA's next item (in every thread).  Thread 0 keeps the index it
+// fetched for the item after it in a register (`ahead`), so the atomic's
+// round trip runs while the current item is worked on; only its use, one item
+// later, waits for it.
+__device__ __forceinline__ int next_item(const SolveQueue& Q, int* s_cur, int& ahead) {
     __syncthreads();   // the previous item's shared-memory use is over
     if (threadIdx.x == 0) {
-        *s_cur = *s_next;
-        if (*s_cur < Q.n) *s_next = static_cast<int>(atomicAdd(Q.head, 1u));
+        const int cur = ahead;
+        *s_cur = cur;
+        if (cur < Q.n) ahead = static_cast<int>(atomicAdd(Q.head, 1u));
     }
     __syncthreads();
     return *s_cur;
 }
 
-__global__ void __launch_bounds__(256) k_fwd_queue(const double* __restrict__ B, double* __restrict__ Zb,
+__global__ void __launch_bounds__(256, 4) k_fwd_queue(const double* __restrict__ B, double* __restrict__ Zb,
                                                    double* __restrict__ U, const int64_t* __restrict__ inv,
                                                    const double* __restrict__ YW, const FrontDesc* __restrict__ desc,
                                                    SolveQueue Q, double* __restrict__ P, unsigned* __restrict__ counters,
                                                    const int* __restrict__ mesh_on) {
-    __shared__ int s_cur, s_next, s_ok;
-    if (threadIdx.x == 0) s_next = static_cast<int>(atomicAdd(Q.head, 1u));
+    __shared__ int s_cur, s_ok;
+    int ahead = threadIdx.x == 0 ? static_cast<int>(atomicAdd(Q.head, 1u)) : 0;
     for (;;) {
-        const int q = next_item(Q, &s_cur, &s_next);
+        const int q = next_item(Q, &s_cur, ahead);
         if (q >= Q.n) break;
         const SolveItem it = Q.items[q];
         const FrontDesc d = desc[it.front];
@@ -982,10 +986,10 @@ __global__ void __launch_bounds__(256) k_bwd_queue(double* __restrict__ x, const
                                                    const FrontDesc* __restrict__ desc, SolveQueue Q,
                                                    double* __restrict__ P, unsigned* __restrict__ counters,
                                                    const int* __restrict__ mesh_on) {
-    __shared__ int s_cur, s_next, s_ok;
-    if (threadIdx.x == 0) s_next = static_cast<int>(atomicAdd(Q.head, 1u));
+    __shared__ int s_cur, s_ok;
+    int ahead = threadIdx.x == 0 ? static_cast<int>(atomicAdd(Q.head, 1u)) : 0;
     for (;;) {
-        const int q = next_item(Q, &s_cur, &s_next);
+        const int q = next_item(Q, &s_cur, ahead);
         if (q >= Q.n) break;
         const SolveItem it = Q.items[q];
         const FrontDesc d = desc[it.front];
