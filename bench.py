@@ -407,9 +407,8 @@ def batch_throughput(device, K):
 
 # k_local<double>'s DRAM bytes per element and FP64-pipe share, from its
 # one-launch ncu capture on the 32x32x64 bar (393,216 tets; the SoA streams
-# scale with the element count), summarised in profiles/k_local_32x32x128.md.
-# They are copied here, not measured in this run: refresh them with that
-# capture whenever the local step changes.
+# scale with the element count).  They are copied here, not measured in this
+# run: refresh them with that capture whenever the local step changes.
 K_LOCAL_NCU = {"dram_bytes_per_elem": 2 * 142806784 / 786432, "fp64_pipe_active": 0.362,
                "source": "ncu --set full, one launch of k_local<double> on the 32x32x64 bar, traffic scaled by "
                          "the element count (copied constants, not measured in this run)"}

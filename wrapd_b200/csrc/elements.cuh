@@ -80,7 +80,12 @@ __device__ __forceinline__ double elastic_energy(const Material& m, const double
 // K + K^T, M = F - U diag(s) (K+K^T) V^T and g_e = w^2 Di^T M^T, plus the AL
 // value 0.5 w^2 |symF - P|^2, the potential energy and the inversion count at
 // x (src/TetElements.cpp:444-468, 598-635).  Outputs out[0..2] = value, pe, flips.
-static __global__ void __launch_bounds__(128, 4) k_grad(ElemView E, Tiles T, const int* on, const double* __restrict__ x,
+// SEG: a batch (per-mesh sums); a single mesh takes grid_reduce, the same
+// arithmetic.  Register budgets: the single-mesh form compiles to 128 with no
+// occupancy hint; the segmented one is held to 128 (4 CTAs per SM) by the
+// hint, without which it took 166 (3 CTAs per SM).
+template <bool SEG>
+static __global__ void __launch_bounds__(128, SEG ? 4 : 0) k_grad(ElemView E, Tiles T, const int* on, const double* __restrict__ x,
                                               const double* __restrict__ xfix, Material mat0, int write_gel,
                                               double* partials, unsigned* counters, double* out, int stride) {
     const Tile tl = tile_at(T, blockIdx.x);
@@ -163,7 +168,10 @@ static __global__ void __launch_bounds__(128, 4) k_grad(ElemView E, Tiles T, con
                 }
         }
     }
-    seg_reduce_out<3>(red, T, tl.mesh, partials, counters, out, stride);
+    if constexpr (SEG)
+        seg_reduce_out<3>(red, T, tl.mesh, partials, counters, out, stride);
+    else
+        grid_reduce<3>(red, partials, counters, out);
 }
 
 // ---- per-mesh vectors of the global step (MeshCtl, VecPools: elem_types.cuh) --

@@ -558,8 +558,12 @@ const Logs& SolverGPU::mesh_logs(int m) const {
     } while (0)
 
 void SolverGPU::grad_at_x(bool write_gel, int mk) {
-    WRAPD_ELEM_LAUNCH(k_grad, te128_, 128, mask(mk), d_x_, d_xfix_, mat_, write_gel ? 1 : 0, d_partials_,
-                      d_counters_, ds(S_GRAD), kScalStride);
+    if (nm > 1)
+        WRAPD_ELEM_LAUNCH(k_grad<true>, te128_, 128, mask(mk), d_x_, d_xfix_, mat_, write_gel ? 1 : 0, d_partials_,
+                          d_counters_, ds(S_GRAD), kScalStride);
+    else
+        WRAPD_ELEM_LAUNCH(k_grad<false>, te128_, 128, mask(mk), d_x_, d_xfix_, mat_, write_gel ? 1 : 0, d_partials_,
+                          d_counters_, ds(S_GRAD), kScalStride);
 }
 
 void SolverGPU::gather(int mode, int mk, bool xerr, double* plain) {
@@ -898,8 +902,8 @@ double SolverGPU::line_search() {
         k_ls_trial<<<vb, 256, 0, st_>>>(n, trial, d_x_, step, alpha);
         WRAPD_LAUNCH_CHECK();
         kernel_launches++;
-        WRAPD_ELEM_LAUNCH(k_grad, te128_, 128, mask(MK_ALL), trial, d_xfix_, mat_, 0, d_partials_, d_counters_,
-                          ds(S_LSV), kScalStride);
+        WRAPD_ELEM_LAUNCH(k_grad<false>, te128_, 128, mask(MK_ALL), trial, d_xfix_, mat_, 0, d_partials_,
+                          d_counters_, ds(S_LSV), kScalStride);   // one mesh (line search: single meshes only)
         sync_read();
         const double fxa = hs(0, S_LSV);
         if (fxa <= fx0 + alpha * decrease * gtp) return alpha;
