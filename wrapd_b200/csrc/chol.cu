@@ -640,6 +640,7 @@ __device__ __forceinline__ void front_rhs(const double* __restrict__ B, const do
 // partial sums; the last one to arrive adds them in chunk order (deterministic)
 // and writes the band's result, then resets the band counter.
 constexpr int SCH = 256;
+constexpr int FWD_WARPS = 4;          // warps of a forward solve CTA (eight CTAs per SM)
 constexpr int SCH_MIN = 64;
 constexpr int kSolveCtas = 2 * 148;   // two 256-thread CTAs per SM of a B200
 
@@ -659,8 +660,10 @@ __device__ __forceinline__ bool band_arrive(unsigned* counter, int nchunk) {
 
 // Forward: lane l of warp w holds rows b0 + 2l and b0 + 2l + 1 of the band (one
 // 16-byte load per column: the block's leading dimension and the band start are
-// even) and takes columns lo + w, lo + w + 8, ...; the eight warps' sums are
-// added in warp order.
+// even) and takes columns lo + w, lo + w + FWD_WARPS, ...; the warps' sums
+// are added in warp order.  Four-warp CTAs, eight per SM: more items in
+// flight for the latency-bound lower levels (eight-warp CTAs, four per SM,
+// measured 2 % slower per solve; two-warp CTAs 13 % slower).
 // One forward item (q: its index in the item list, which places its partial
 // sums in P).  Returns true, in every thread, in the CTA that wrote the band's
 // result, after all its writes are visible device-wide.
@@ -669,19 +672,19 @@ __device__ __forceinline__ bool fwd_item(const double* __restrict__ B, double* _
                                          const double* __restrict__ YW, const FrontDesc& d, const SolveItem& it, int q,
                                          double* __restrict__ P, unsigned* __restrict__ counters) {
     __shared__ double tv[SCH * 3];
-    __shared__ double part[8][TL][3];
+    __shared__ double part[FWD_WARPS][TL][3];
     const int R = d.k + d.r;
     const int nc = it.hi - it.lo;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i0 = it.b0 + 2 * lane;
     const double* M = YW + d.y_off + i0 + (int64_t)it.lo * d.ldy;
-    // the first eight columns of each warp are in flight while the right-hand
-    // side is gathered
+    // warp w takes columns w, w + FWD_WARPS, ...; its first eight are in flight
+    // while the right-hand side is gathered
     constexpr int PRE = 8;
     double2 pre[PRE];
 #pragma unroll
     for (int u = 0; u < PRE; ++u) {
-        const int j = warp + 8 * u;
+        const int j = warp + FWD_WARPS * u;
         pre[u] = (i0 < R && j < nc) ? __ldg(reinterpret_cast<const double2*>(M + (int64_t)j * d.ldy))
                                     : make_double2(0.0, 0.0);
     }
@@ -694,7 +697,7 @@ __device__ __forceinline__ bool fwd_item(const double* __restrict__ B, double* _
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0;
 #pragma unroll
     for (int u = 0; u < PRE; ++u) {
-        const int j = warp + 8 * u;
+        const int j = warp + FWD_WARPS * u;
         if (j < nc) {
             const double t0 = tv[3 * j], t1 = tv[3 * j + 1], t2 = tv[3 * j + 2];
             a0 = fma(pre[u].x, t0, a0); a1 = fma(pre[u].x, t1, a1); a2 = fma(pre[u].x, t2, a2);
@@ -703,7 +706,7 @@ __device__ __forceinline__ bool fwd_item(const double* __restrict__ B, double* _
     }
     if (i0 < R) {
 #pragma unroll 8
-        for (int j = warp + 8 * PRE; j < nc; j += 8) {
+        for (int j = warp + FWD_WARPS * PRE; j < nc; j += FWD_WARPS) {
             const double2 m = __ldg(reinterpret_cast<const double2*>(M + (int64_t)j * d.ldy));
             const double t0 = tv[3 * j], t1 = tv[3 * j + 1], t2 = tv[3 * j + 2];
             a0 = fma(m.x, t0, a0); a1 = fma(m.x, t1, a1); a2 = fma(m.x, t2, a2);
@@ -718,7 +721,7 @@ __device__ __forceinline__ bool fwd_item(const double* __restrict__ B, double* _
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
     if (row < TL) {
 #pragma unroll
-        for (int w = 0; w < 8; ++w) { s0 += part[w][row][0]; s1 += part[w][row][1]; s2 += part[w][row][2]; }
+        for (int w = 0; w < FWD_WARPS; ++w) { s0 += part[w][row][0]; s1 += part[w][row][1]; s2 += part[w][row][2]; }
     }
     if (it.nchunk > 1) {
         if (row < TL) {
@@ -750,7 +753,7 @@ __device__ __forceinline__ bool fwd_item(const double* __restrict__ B, double* _
     return true;
 }
 
-__global__ void __launch_bounds__(256) k_fwd_level(const double* __restrict__ B, double* __restrict__ Zb,
+__global__ void __launch_bounds__(32 * FWD_WARPS) k_fwd_level(const double* __restrict__ B, double* __restrict__ Zb,
                                                    double* __restrict__ U, const int64_t* __restrict__ inv,
                                                    const double* __restrict__ YW, const FrontDesc* __restrict__ desc,
                                                    const SolveItem* __restrict__ items, double* __restrict__ P,
@@ -909,36 +912,14 @@ __global__ void __launch_bounds__(256) k_bwd_level(double* __restrict__ x, const
 // rows) -- counted by per-front band counters that each band's writer bumps
 // after its writes are visible.  Every item an item waits on comes earlier in
 // the list and was taken by a running CTA, so the earliest unfinished item
-// never waits and the queue always drains.  A wait polls at most kWaitPolls
-// times (about a second); one that gives up sets *status to WRAPD_E_TIMEOUT and
-// skips its item, and every later wait returns at once, so the launch ends
-// with the error for the host to read.  The results are those of the per-level
-// launches bit for bit: the same items, chunks and chunk order per band.
-constexpr unsigned long long kWaitNs = 1000000000ull;   // one second of the global timer
-constexpr int kWaitPolls = 1 << 24;                      // and at most this many polls
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
+// never waits and the queue always drains.  A wait (wait_count_geq) is bounded
+// by one second of the global timer and a poll count; one that gives up sets
+// *status to WRAPD_E_TIMEOUT and skips its item, and every later wait returns at
+// once, so the launch ends with the error for the host to read.  The results
+// are those of the per-level launches bit for bit: the same items, chunks and
+// chunk order per band.
 __device__ __forceinline__ bool wait_bands(const unsigned* done, unsigned target, int* status) {
-    const unsigned long long t0 = global_ns();
-    for (int i = 0; i < kWaitPolls; ++i) {
-        if (ld_acquire(done) >= target) return true;
-        if (*reinterpret_cast<volatile int*>(status) != 0) return false;   // another wait gave up
-        if (global_ns() - t0 > kWaitNs) break;
-        __nanosleep(64);
-    }
-    atomicCAS(status, 0, WRAPD_E_TIMEOUT);
-    return false;
+    return wait_count_geq(done, target, status);
 }
 
 // Takes the CTA's next item (in every thread).  Thread 0 keeps the index it
@@ -956,7 +937,7 @@ __device__ __forceinline__ int next_item(const SolveQueue& Q, int* s_cur, int& a
     return *s_cur;
 }
 
-__global__ void __launch_bounds__(256, 4) k_fwd_queue(const double* __restrict__ B, double* __restrict__ Zb,
+__global__ void __launch_bounds__(32 * FWD_WARPS, 8) k_fwd_queue(const double* __restrict__ B, double* __restrict__ Zb,
                                                    double* __restrict__ U, const int64_t* __restrict__ inv,
                                                    const double* __restrict__ YW, const FrontDesc* __restrict__ desc,
                                                    SolveQueue Q, double* __restrict__ P, unsigned* __restrict__ counters,
@@ -1310,7 +1291,7 @@ void CholGPU::build(const Symbolic& S, const std::vector<int64_t>& A_pos, const 
         int dev = 0, sms = 0, bf = 0, bb = 0;
         WRAPD_CUDA(cudaGetDevice(&dev));
         WRAPD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        WRAPD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_fwd_queue, 256, 0));
+        WRAPD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_fwd_queue, 32 * FWD_WARPS, 0));
         WRAPD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, k_bwd_queue, 256, 0));
         qgrid_f_ = std::max(1, bf) * sms;
         qgrid_b_ = std::max(1, bb) * sms;
@@ -1415,7 +1396,7 @@ void CholGPU::autotune(const double* d_w2, const double* d_Di, int ne, cudaStrea
         for (int c = 0; c < (int)L.cand.size(); ++c) {
             const Level::SolveCand& C = L.cand[c];
             const float tf = timed(3, [&] {
-                k_fwd_level<<<C.nfwd, 256, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_desc_, C.fwd, d_P_, d_cnt_,
+                k_fwd_level<<<C.nfwd, 32 * FWD_WARPS, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_desc_, C.fwd, d_P_, d_cnt_,
                                                     nullptr);
             });
             const float tb = timed(3, [&] {
@@ -1516,7 +1497,7 @@ void CholGPU::solve_launches(double* d_x, cudaStream_t st, const int* mesh_on, i
     unsigned* bands = d_qctl_ + 2 + 2 * (size_t)nfronts;
     if (nqf_ > 0) {
         const SolveQueue Q{d_qf_, nqf_, d_qctl_, d_qctl_ + 2, d_qnb_, d_status, hold};
-        k_fwd_queue<<<std::min(qgrid_f_, nqf_), 256, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_desc_, Q, d_P_, bands,
+        k_fwd_queue<<<std::min(qgrid_f_, nqf_), 32 * FWD_WARPS, 0, st>>>(d_T_, d_Z_, d_U_, d_inv_, d_Y_, d_desc_, Q, d_P_, bands,
                                                            mesh_on);
         WRAPD_LAUNCH_CHECK();
     }

@@ -71,6 +71,39 @@ __device__ __forceinline__ T block_max(T v, T* smem) {
     return r;
 }
 
+// ---- bounded waits between CTAs ----------------------------------------------
+// A wait on a counter that other CTAs raise (release: their writes, a fence,
+// then the atomic) polls it with an acquire load for at most one second of the
+// global timer and kWaitPolls polls.  One that gives up sets *status to
+// WRAPD_E_TIMEOUT (if it was 0) and returns false; a wait that finds *status
+// already set returns false at once, so every waiter of a failed launch ends.
+constexpr unsigned long long kWaitNs = 1000000000ull;
+constexpr int kWaitPolls = 1 << 24;
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool wait_count_geq(const unsigned* count, unsigned target, int* status) {
+    const unsigned long long t0 = global_ns();
+    for (int i = 0; i < kWaitPolls; ++i) {
+        if (ld_acquire(count) >= target) return true;
+        if (*reinterpret_cast<volatile int*>(status) != 0) return false;
+        if (global_ns() - t0 > kWaitNs) break;
+        __nanosleep(64);
+    }
+    atomicCAS(status, 0, WRAPD_E_TIMEOUT);
+    return false;
+}
+
 // ---- deterministic grid reduction: per-block partials, summed in block order
 // by whichever block finishes last. -------------------------------------------
 // out[k] = total_k, or for k = 0 with an affine epilogue: (base ? *base : 0) + scale * total_0.

@@ -52,6 +52,10 @@ struct MeshCtl {
     int small;     // the two-loop runs in one CTA (3 x free vertices <= kTwoLoopMaxN)
     int v0, v1;    // the mesh's range in the n x 3 vectors, in doubles
 };
+// Slots of the two-loop recursion's scalars in a mesh's scalar block.
+struct TwoLoopSlots {
+    int alpha, c, dir;    // offsets in a mesh's scalar block
+};
 struct VecPools {
     double* G[3];
     double* S[kHistSlots];

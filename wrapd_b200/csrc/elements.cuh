@@ -518,9 +518,6 @@ static __global__ void __launch_bounds__(256) k_apply_weights(ElemView E, Tiles 
 // (scal + mesh * stride + S_ALPHA / S_C / S_DIR).
 constexpr int kVecTile = 2048;
 
-struct TwoLoopSlots {
-    int alpha, c, dir;    // offsets in a mesh's scalar block
-};
 
 static __global__ void __launch_bounds__(256) k_lbfgs_first(Tiles T, const int* on, const MeshCtl* __restrict__ ctl,
                                                      VecPools P, const double* __restrict__ rho,
@@ -576,6 +573,114 @@ static __global__ void __launch_bounds__(256) k_lbfgs_second(Tiles T, const int*
             sc[sl.c + j] = __ldcg(sc + sl.alpha + j) + (-rho[(size_t)tl.mesh * kHistSlots + hist_slot(c, j, P.M)]) * tot[0];
         else
             sc[sl.dir] = tot[0];
+    }
+}
+
+// ---- the two-loop recursion in one cooperative launch per loop (one mesh) ---------
+// For a single mesh above the one-CTA size the M + 1 steps of each loop are
+// the k_lbfgs_first / k_lbfgs_second steps above, run by one cooperative launch
+// (all CTAs resident): CTA b takes vector tiles b, b + G, ... and keeps them
+// for the whole loop, each step's inner product is the same per-tile block sum
+// in partials (two buffers, alternating by step), and after a grid barrier
+// every CTA adds the tile partials in the seg_reduce order -- the same alpha_i,
+// c_i and decrement as the per-step launches, bit for bit, in every CTA.  The
+// barrier is a counter the CTAs raise, waited on with wait_count_geq (bounded;
+// a wait that gives up leaves WRAPD_E_TIMEOUT in *status and the CTA returns).
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned target, int* status) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+        ok = wait_count_geq(bar, target, status) ? 1 : 0;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// The total over the mesh's tiles of partials[] in seg_reduce's order (every thread gets it).
+__device__ __forceinline__ double grid_total(const double* partials, int ntiles) {
+    __shared__ double sm[32];
+    __shared__ double total;
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < ntiles; b += blockDim.x) acc += __ldcg(partials + b);
+    const double r = block_sum(acc, sm);
+    if (threadIdx.x == 0) total = r;
+    __syncthreads();
+    return total;
+}
+
+template <bool SECOND>
+static __global__ void __launch_bounds__(256) k_two_loop_grid(Tiles T, const MeshCtl* __restrict__ ctl, VecPools P,
+                                                       const double* __restrict__ rho, double* __restrict__ q,
+                                                       TwoLoopSlots sl, double* partials, unsigned* bar,
+                                                       int* status, double* scal) {
+    __shared__ double sm[32];
+    const MeshCtl c = ctl[0];
+    const int ntiles = T.count, G = gridDim.x;
+    unsigned nbar = 0;
+    if constexpr (!SECOND) {
+        // first loop, j = it - 1 .. -1: q = (first ? g : q) - alpha_{j+1} y_{j+1}; alpha_j = rho_j <s_j, q>
+        double alpha_next = 0.0;
+        for (int j = c.it - 1; j >= -1; --j) {
+            const bool first = j == c.it - 1;
+            const double* g = g_cur(P, c);
+            const double* yv = first ? nullptr : P.Y[hist_slot(c, j + 1, P.M)];
+            const double cf = first ? 0.0 : -alpha_next;
+            const double* sv = j >= 0 ? P.S[hist_slot(c, j, P.M)] : nullptr;
+            double* part = partials + (size_t)(j & 1) * ntiles;
+            for (int t = blockIdx.x; t < ntiles; t += G) {
+                const Tile tl = tile_at(T, t);
+                double red = 0.0;
+                for (int i = tl.first + (int)threadIdx.x; i < tl.end; i += blockDim.x) {
+                    double qi = first ? g[i] : q[i];
+                    if (yv) qi = qi + cf * yv[i];
+                    q[i] = qi;
+                    if (sv) red += sv[i] * qi;
+                }
+                if (j >= 0) {
+                    const double r = block_sum(red, sm);
+                    if (threadIdx.x == 0) part[t] = r;
+                }
+            }
+            if (j < 0) break;
+            nbar += G;
+            if (!grid_barrier(bar, nbar, status)) return;
+            alpha_next = rho[hist_slot(c, j, P.M)] * grid_total(part, ntiles);
+            if (blockIdx.x == 0 && threadIdx.x == 0) scal[sl.alpha + j] = alpha_next;
+        }
+    } else {
+        // second loop, j = 0 .. it: q += c_{j-1} s_{j-1}; c_j = alpha_j - rho_j <y_j, q>, dir = <g, q>
+        double c_prev = 0.0;
+        for (int j = 0; j <= c.it; ++j) {
+            const double* sv = j > 0 ? P.S[hist_slot(c, j - 1, P.M)] : nullptr;
+            const double cf = j > 0 ? c_prev : 0.0;
+            const double* w = j < c.it ? P.Y[hist_slot(c, j, P.M)] : g_cur(P, c);
+            double* part = partials + (size_t)(j & 1) * ntiles;
+            for (int t = blockIdx.x; t < ntiles; t += G) {
+                const Tile tl = tile_at(T, t);
+                double red = 0.0;
+                for (int i = tl.first + (int)threadIdx.x; i < tl.end; i += blockDim.x) {
+                    double qi = q[i];
+                    if (sv) {
+                        qi = qi + cf * sv[i];
+                        q[i] = qi;
+                    }
+                    red += w[i] * qi;
+                }
+                const double r = block_sum(red, sm);
+                if (threadIdx.x == 0) part[t] = r;
+            }
+            nbar += G;
+            if (!grid_barrier(bar, nbar, status)) return;
+            const double tot = grid_total(part, ntiles);
+            if (j < c.it) {
+                c_prev = __ldcg(scal + sl.alpha + j) + (-rho[hist_slot(c, j, P.M)]) * tot;
+                if (blockIdx.x == 0 && threadIdx.x == 0) scal[sl.c + j] = c_prev;
+            } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+                scal[sl.dir] = tot;
+            }
+        }
     }
 }
 

@@ -419,6 +419,20 @@ void SolverGPU::initialize() {
                                           blocks_for(8 * (int64_t)nf, 256), vec_blocks(3 * (int64_t)nf)}) + 8;
     d_partials_ = static_cast<double*>(dalloc(nblk * 5 * sizeof(double)));
     d_counters_ = static_cast<unsigned*>(dalloc(nm * sizeof(unsigned)));
+    // the cooperative two-loop recursion (one mesh above the one-CTA size):
+    // its grid is what fits on the device at once
+    d_bar_ = static_cast<unsigned*>(dalloc(sizeof(unsigned)));
+    coop_grid_ = 0;
+    {
+        int dev = 0, coop = 0, sms = 0, per_sm = 0;
+        WRAPD_CUDA(cudaGetDevice(&dev));
+        WRAPD_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        WRAPD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        WRAPD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_two_loop_grid<false>, 256, 0));
+        int per_sm2 = 0;
+        WRAPD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_two_loop_grid<true>, 256, 0));
+        if (coop && nm == 1) coop_grid_ = std::min(tvec_.count, std::min(per_sm, per_sm2) * sms);
+    }
     d_scal_ = static_cast<double*>(dalloc((size_t)nm * kScalStride * sizeof(double)));
     WRAPD_CUDA(cudaMemsetAsync(d_counters_, 0, nm * sizeof(unsigned), st_));
     WRAPD_CUDA(cudaMemsetAsync(d_scal_, 0, (size_t)nm * kScalStride * sizeof(double), st_));
@@ -912,6 +926,27 @@ double SolverGPU::line_search() {
     return -1.0;
 }
 
+// One loop of the two-loop recursion of a single mesh as one cooperative
+// launch (k_two_loop_grid); its barrier counter starts from 0.
+void SolverGPU::two_loop_grid(bool second, const VecPools& P, const TwoLoopSlots& sl) {
+    WRAPD_CUDA(cudaMemsetAsync(d_bar_, 0, sizeof(unsigned), st_));
+    Tiles T = tvec_.view();
+    VecPools Pc = P;
+    TwoLoopSlots slc = sl;
+    const MeshCtl* ctl = d_ctl_;
+    const double* rho = d_rho_;
+    double* q = d_q_;
+    double* partials = d_partials_;
+    unsigned* bar = d_bar_;
+    int* status = chol.d_status;
+    double* scal = d_scal_;
+    void* args[] = {&T, &ctl, &Pc, &rho, &q, &slc, &partials, &bar, &status, &scal};
+    const void* fn = second ? reinterpret_cast<const void*>(&k_two_loop_grid<true>)
+                            : reinterpret_cast<const void*>(&k_two_loop_grid<false>);
+    WRAPD_CUDA(cudaLaunchCooperativeKernel(fn, dim3(coop_grid_), dim3(256), args, 0, st_));
+    kernel_launches++;
+}
+
 // SplitLBFGS::minimize (deps/mcloptlib/include/MCL/SplitLBFGS.hpp:114-256) with
 // LSMethod::None (rate 1), for every mesh R with R.in_loop set: each mesh runs
 // its own minimize (its history, decrement, early exit and iteration budget),
@@ -953,12 +988,15 @@ int SolverGPU::lbfgs_minimize() {
                                                               kScalStride);
             kernel_launches++;
         }
-        if (large)
+        if (large && coop_grid_ > 0) {
+            two_loop_grid(false, P, sl);
+        } else if (large) {
             for (int j = jmax - 1; j >= -1; --j) {
                 k_lbfgs_first<<<tvec_.count, 256, 0, st_>>>(tvec_.view(), mask(MK_LARGE), d_ctl_, P, d_rho_, d_q_, j, sl,
                                                             d_partials_, d_counters_, d_scal_, kScalStride);
                 kernel_launches++;
             }
+        }
         WRAPD_LAUNCH_CHECK();
         // q = A^-1 q, three right-hand sides at once (the block-diagonal system)
         mark(2);
@@ -972,12 +1010,15 @@ int SolverGPU::lbfgs_minimize() {
                                                                kScalStride);
             kernel_launches++;
         }
-        if (large)
+        if (large && coop_grid_ > 0) {
+            two_loop_grid(true, P, sl);
+        } else if (large) {
             for (int j = 0; j <= jmax; ++j) {
                 k_lbfgs_second<<<tvec_.count, 256, 0, st_>>>(tvec_.view(), mask(MK_LARGE), d_ctl_, P, d_rho_, d_q_, j,
                                                              sl, d_partials_, d_counters_, d_scal_, kScalStride);
                 kernel_launches++;
             }
+        }
         WRAPD_LAUNCH_CHECK();
         // -global_ls 1 (single meshes): Backtracking::search along p = -q (SplitLBFGS.hpp:196-206)
         double rate = 1.0;
