@@ -1134,9 +1134,17 @@ int SolverGPU::iterate(int n, bool* conv) {
         push_ctl();
         WRAPD_CUDA(cudaEventRecord(ev_[0], st_));
         mark(5);
+        // The candidate weights (w2c) are read only by a reweight: the ratio of
+        // the gamma rule every iteration, or with rw_every the reweight every
+        // rw_every-th iteration.  On the other iterations of rw_every the local
+        // step leaves them alone (the reweight's own local step writes them
+        // fresh), which skips the Hessian eigenvalue per element; the results
+        // are the same.
+        int cand = cand_mode_now();
+        if (cfg.rw_every > 0 && ((k + 1) % cfg.rw_every) != 0) cand = CAND_NONE;
         if (cfg.rot_aware) {
             // ---- local step: polar_update (src/TetElements.cpp:256-356) ----
-            local_step(cand_mode_now());
+            local_step(cand);
             if (cfg.reweighting) count_++;
             mark(0);
             WRAPD_CUDA(cudaEventRecord(ev_[1], st_));
@@ -1171,7 +1179,7 @@ int SolverGPU::iterate(int n, bool* conv) {
             for (int m = 0; m < nm; ++m) its[m] = act[m] ? runs_[m].its : 0;
         } else {
             // ---- local_update: TetElements::update (src/TetElements.cpp:193-254), single mesh ----
-            local_step_unaware(cand_mode_now(), fp32() && !runs_[0].fp64_phase);
+            local_step_unaware(cand, fp32() && !runs_[0].fp64_phase);
             if (cfg.reweighting) count_++;
             mark(0);
             WRAPD_CUDA(cudaEventRecord(ev_[1], st_));
