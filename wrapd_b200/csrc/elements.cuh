@@ -82,12 +82,17 @@ __device__ __forceinline__ double elastic_energy(const Material& m, const double
 // x (src/TetElements.cpp:444-468, 598-635).  Outputs out[0..2] = value, pe, flips.
 // SEG: a batch (per-mesh sums); a single mesh takes grid_reduce, the same
 // arithmetic.  Register budgets: the single-mesh form compiles to 128 with no
-// occupancy hint; the segmented one is held to 128 (4 CTAs per SM) by the
-// hint, without which it took 166 (3 CTAs per SM).
-template <bool SEG>
-static __global__ void __launch_bounds__(128, SEG ? 4 : 0) k_grad(ElemView E, Tiles T, const int* on, const double* __restrict__ x,
+// occupancy hint; the segmented one and the UV forms below are held to 128
+// (4 CTAs per SM) by the hint, without which they took 164-168 (3 per SM).
+// UV (single mesh only): 0 = SVD as usual; 1 = also keep U and V of the SVD
+// in uv (U then V, 9 SoA components each); 2 = x is the point of the last
+// UV = 1 launch, so F's SVD is that launch's: sig, U, V and symF are read
+// back instead of recomputed (the same values, so the same results).
+template <bool SEG, int UV = 0>
+static __global__ void __launch_bounds__(128, (SEG || UV != 0) ? 4 : 0) k_grad(ElemView E, Tiles T, const int* on, const double* __restrict__ x,
                                               const double* __restrict__ xfix, Material mat0, int write_gel,
-                                              double* partials, unsigned* counters, double* out, int stride) {
+                                              double* partials, unsigned* counters, double* out, int stride,
+                                              double* __restrict__ uv = nullptr) {
     const Tile tl = tile_at(T, blockIdx.x);
     if (!mesh_on(on, tl.mesh)) return;
     const int e = tl.first + threadIdx.x;
@@ -99,17 +104,29 @@ static __global__ void __launch_bounds__(128, SEG ? 4 : 0) k_grad(ElemView E, Ti
         double F[9], s[3], Us[9], Vs[9];
 #pragma unroll
         for (int i = 0; i < 9; ++i) F[i] = double(Fd[i]);
-        svd3(F, s, Us, Vs);
         double S[9];
+        if constexpr (UV == 2) {
+            load9(uv, E.ne, e, Us);
+            load9(uv + (size_t)9 * E.ne, E.ne, e, Vs);
 #pragma unroll
-        for (int r = 0; r < 3; ++r)
+            for (int i = 0; i < 3; ++i) s[i] = E.sig[(size_t)i * E.ne + e];
+            load9(E.symF, E.ne, e, S);
+        } else {
+            svd3(F, s, Us, Vs);
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
-                M3(S, r, c) = M3(Vs, r, 0) * s[0] * M3(Vs, c, 0) + M3(Vs, r, 1) * s[1] * M3(Vs, c, 1) +
-                              M3(Vs, r, 2) * s[2] * M3(Vs, c, 2);
-        store9(E.symF, E.ne, e, S);
+            for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int i = 0; i < 3; ++i) E.sig[(size_t)i * E.ne + e] = s[i];
+                for (int c = 0; c < 3; ++c)
+                    M3(S, r, c) = M3(Vs, r, 0) * s[0] * M3(Vs, c, 0) + M3(Vs, r, 1) * s[1] * M3(Vs, c, 1) +
+                                  M3(Vs, r, 2) * s[2] * M3(Vs, c, 2);
+            store9(E.symF, E.ne, e, S);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) E.sig[(size_t)i * E.ne + e] = s[i];
+            if constexpr (UV == 1) {
+                store9(uv, E.ne, e, Us);
+                store9(uv + (size_t)9 * E.ne, E.ne, e, Vs);
+            }
+        }
         double Zm[9], Um[9], P[9];
         load9(E.Z, E.ne, e, Zm);
         load9(E.U, E.ne, e, Um);

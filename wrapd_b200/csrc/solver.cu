@@ -346,6 +346,9 @@ void SolverGPU::initialize() {
         mat_ = mats_[0];   // one material: the mesh's own when it was given one
     }
     d_w2c_ = static_cast<double*>(dalloc(ne * sizeof(double)));
+    // U and V of the last gradient's SVD (single mesh): 18 doubles per element
+    d_uv_ = meshes_.size() == 1 ? static_cast<double*>(dalloc((size_t)18 * ne * sizeof(double))) : nullptr;
+    uv_valid_ = false;
     d_Z_ = static_cast<double*>(dalloc(9 * (size_t)ne * TS));
     d_U_ = static_cast<double*>(dalloc(9 * (size_t)ne * TS));
     d_symF_ = static_cast<double*>(dalloc(9 * (size_t)ne * TS));
@@ -571,13 +574,32 @@ const Logs& SolverGPU::mesh_logs(int m) const {
         kernel_launches++;                                                                  \
     } while (0)
 
+// The global gradient at x.  A single mesh in the rotation-aware global step
+// without line search keeps the SVD factors of its last gradient (k_grad
+// UV = 1); the first gradient of the next ADMM iteration is taken at the same
+// x (the local step changes only Z and U), so it reads them back (UV = 2)
+// instead of redoing the per-element SVD.  uv_valid_ is cleared wherever x
+// changes.
 void SolverGPU::grad_at_x(bool write_gel, int mk) {
-    if (nm > 1)
+    if (nm > 1) {
         WRAPD_ELEM_LAUNCH(k_grad<true>, te128_, 128, mask(mk), d_x_, d_xfix_, mat_, write_gel ? 1 : 0, d_partials_,
                           d_counters_, ds(S_GRAD), kScalStride);
-    else
+    } else if (d_uv_ && write_gel && cfg.rot_aware && !cfg.global_ls) {
+        if (uv_valid_)
+            k_grad<false, 2><<<te128_.count, 128, 0, st_>>>(view(), te128_.view(), mask(mk), d_x_, d_xfix_, mat_, 1,
+                                                             d_partials_, d_counters_, ds(S_GRAD), kScalStride, d_uv_);
+        else
+            k_grad<false, 1><<<te128_.count, 128, 0, st_>>>(view(), te128_.view(), mask(mk), d_x_, d_xfix_, mat_, 1,
+                                                             d_partials_, d_counters_, ds(S_GRAD), kScalStride, d_uv_);
+        WRAPD_LAUNCH_CHECK();
+        kernel_launches++;
+        uv_valid_ = true;
+        return;
+    } else {
         WRAPD_ELEM_LAUNCH(k_grad<false>, te128_, 128, mask(mk), d_x_, d_xfix_, mat_, write_gel ? 1 : 0, d_partials_,
                           d_counters_, ds(S_GRAD), kScalStride);
+    }
+    uv_valid_ = false;
 }
 
 void SolverGPU::gather(int mode, int mk, bool xerr, double* plain) {
@@ -664,6 +686,7 @@ void SolverGPU::global_step_unaware() {
     kernel_launches += chol.launches_solve;
     n_solve++;
     mark(3);
+    uv_valid_ = false;
     WRAPD_CUDA(cudaMemcpyAsync(d_x_, d_q_, 3 * (size_t)nf * sizeof(double), cudaMemcpyDeviceToDevice, st_));
     // update_defo_cache(x, true): singular values for the energy and flips
     grad_at_x(false, MK_ALL);
@@ -841,6 +864,7 @@ void SolverGPU::begin_solve() {
     }
     push_ctl();
     // setup_solve (src/ADMM.cpp:89-107): X = X_init, defo cache, dual variables
+    uv_valid_ = false;
     WRAPD_CUDA(cudaMemcpyAsync(d_x_, d_xinit_, 3 * (size_t)nf * sizeof(double), cudaMemcpyDeviceToDevice, st_));
     grad_at_x(false, MK_ALL);
     if (cfg.rot_aware) {
@@ -1032,6 +1056,7 @@ int SolverGPU::lbfgs_minimize() {
             }
         }
         // x -= rate q (or rate grad on a non-descent direction); s = x_new - x_old
+        uv_valid_ = false;   // x moves
         k_xupdate<<<tvec_.count, 256, 0, st_>>>(tvec_.view(), mask(MK_LBFGS), d_ctl_, P, d_x_, d_q_, d_scal_, S_DIR,
                                                 kScalStride, rate);
         WRAPD_LAUNCH_CHECK();
@@ -1376,6 +1401,7 @@ void SolverGPU::set_state(const std::string& name, const double* in, int64_t n) 
         std::vector<double> xp(3 * (size_t)nf);
         for (int i = 0; i < nf; ++i)
             for (int c = 0; c < 3; ++c) xp[3 * (size_t)iperm_[i] + c] = in[3 * (size_t)i + c];
+        uv_valid_ = false;
         WRAPD_CUDA(cudaMemcpyAsync(d_x_, xp.data(), xp.size() * 8, cudaMemcpyHostToDevice, st_));
         WRAPD_CUDA(cudaStreamSynchronize(st_));
         ctl_pending_ = false;

@@ -153,6 +153,8 @@ private:
     std::vector<void*> allocs_;
     int4* d_idx_ = nullptr;
     double *d_Di_ = nullptr, *d_vol_ = nullptr, *d_w2_ = nullptr, *d_w2c_ = nullptr;
+    double* d_uv_ = nullptr;     // U, V of the last gradient's SVD (one mesh), valid at x while uv_valid_
+    bool uv_valid_ = false;
     double *d_Z_ = nullptr, *d_U_ = nullptr, *d_symF_ = nullptr, *d_sig_ = nullptr, *d_slast_ = nullptr, *d_gel_ = nullptr;
     int *d_inc_ptr_ = nullptr, *d_inc_ = nullptr;
     double *d_x_ = nullptr, *d_xfix_ = nullptr, *d_xsoln_ = nullptr, *d_xinit_ = nullptr;
