@@ -211,7 +211,9 @@ WRAPD_API void wrapd_destroy(wrapd_handle* h);
 /* Read or overwrite a state array by name.  Per element, in input order:
  * "Z","U","symF" (9, the reference's column-major Mat3x3), "slast" (3),
  * "w2","w2c","vol" (1).  Per free vertex in ascending vertex id order:
- * "xfree","grad" (3).  Returns the element count written via *len. */
+ * "xfree","grad" (3).  Returns the element count written via *len.  Under
+ * rw_every, wrapd_solve/wrapd_iterate refresh "w2c" only in the local step of
+ * a reweighting iteration (the one that reads it). */
 WRAPD_API int wrapd_get_state(wrapd_handle* h, const char* name, double* out, int64_t cap, int64_t* len);
 WRAPD_API int wrapd_set_state(wrapd_handle* h, const char* name, const double* in, int64_t n);
 
