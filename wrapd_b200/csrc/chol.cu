@@ -670,10 +670,30 @@ __device__ __forceinline__ bool band_arrive(unsigned* counter, int nchunk) {
 // One forward item (q: its index in the item list, which places its partial
 // sums in P).  Returns true, in every thread, in the CTA that wrote the band's
 // result, after all its writes are visible device-wide.
+// The first eight columns of each warp of a forward item (warp w takes columns
+// w, w + FWD_WARPS, ...): [Y; W] does not change during a solve, so they are
+// loaded before the item's dependency wait and its right-hand-side gather.
+constexpr int FWD_PRE = 8;
+__device__ __forceinline__ void fwd_pre(const double* __restrict__ YW, const FrontDesc& d, const SolveItem& it,
+                                        double2 (&pre)[FWD_PRE]) {
+    const int R = d.k + d.r;
+    const int nc = it.hi - it.lo;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i0 = it.b0 + 2 * lane;
+    const double* M = YW + d.y_off + i0 + (int64_t)it.lo * d.ldy;
+#pragma unroll
+    for (int u = 0; u < FWD_PRE; ++u) {
+        const int j = warp + FWD_WARPS * u;
+        pre[u] = (i0 < R && j < nc) ? __ldg(reinterpret_cast<const double2*>(M + (int64_t)j * d.ldy))
+                                    : make_double2(0.0, 0.0);
+    }
+}
+
 __device__ __forceinline__ bool fwd_item(const double* __restrict__ B, double* __restrict__ Zb,
                                          double* __restrict__ U, const int64_t* __restrict__ inv,
                                          const double* __restrict__ YW, const FrontDesc& d, const SolveItem& it, int q,
-                                         double* __restrict__ P, unsigned* __restrict__ counters) {
+                                         double* __restrict__ P, unsigned* __restrict__ counters,
+                                         const double2 (&pre)[FWD_PRE]) {
     __shared__ double tv[SCH * 3];
     __shared__ double part[FWD_WARPS][TL][3];
     const int R = d.k + d.r;
@@ -681,16 +701,7 @@ __device__ __forceinline__ bool fwd_item(const double* __restrict__ B, double* _
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i0 = it.b0 + 2 * lane;
     const double* M = YW + d.y_off + i0 + (int64_t)it.lo * d.ldy;
-    // warp w takes columns w, w + FWD_WARPS, ...; its first eight are in flight
-    // while the right-hand side is gathered
-    constexpr int PRE = 8;
-    double2 pre[PRE];
-#pragma unroll
-    for (int u = 0; u < PRE; ++u) {
-        const int j = warp + FWD_WARPS * u;
-        pre[u] = (i0 < R && j < nc) ? __ldg(reinterpret_cast<const double2*>(M + (int64_t)j * d.ldy))
-                                    : make_double2(0.0, 0.0);
-    }
+    constexpr int PRE = FWD_PRE;
     for (int j = threadIdx.x; j < nc; j += blockDim.x) {
         double v0, v1, v2;
         front_rhs(B, U, inv, d, it.lo + j, v0, v1, v2);
@@ -764,7 +775,9 @@ __global__ void __launch_bounds__(32 * FWD_WARPS) k_fwd_level(const double* __re
     const SolveItem it = items[blockIdx.x];
     const FrontDesc d = desc[it.front];
     if (mesh_on && !mesh_on[d.mesh]) return;   // the whole band's CTAs: its counter stays 0
-    fwd_item(B, Zb, U, inv, YW, d, it, blockIdx.x, P, counters);
+    double2 pre[FWD_PRE];
+    fwd_pre(YW, d, it, pre);
+    fwd_item(B, Zb, U, inv, YW, d, it, blockIdx.x, P, counters, pre);
 }
 
 // Backward: a CTA owns a band of 64 columns and a chunk [lo, hi) of the rows
@@ -774,24 +787,31 @@ __global__ void __launch_bounds__(32 * FWD_WARPS) k_fwd_level(const double* __re
 // of each as one 16-byte load.  The 8 x 3 lane sums are then added across the
 // warp by a butterfly that halves the values each lane keeps (12, 6, 3) before
 // two plain exchange steps, so the eight columns share 27 shuffles.
+// The first row pair of each of the warp's eight columns of a backward item,
+// loaded before the item's dependency wait and its input gather.
+__device__ __forceinline__ void bwd_pre(const double* __restrict__ YW, const FrontDesc& d, const SolveItem& it,
+                                        double2 (&pre)[8]) {
+    const int nr = it.hi - it.lo;
+    const int nc = min(TL, d.k - it.b0);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const double* M0 = YW + d.y_off + it.lo + (int64_t)(it.b0 + warp) * d.ldy;
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+        pre[m] = (2 * lane < nr && warp + 8 * m < nc)
+                     ? __ldg(reinterpret_cast<const double2*>(M0 + (int64_t)(8 * m) * d.ldy + 2 * lane))
+                     : make_double2(0.0, 0.0);
+}
+
 __device__ __forceinline__ bool bwd_item(double* __restrict__ x, const double* __restrict__ Zb,
                                          const double* __restrict__ YW, const int* __restrict__ rows,
                                          const FrontDesc& d, const SolveItem& it, int q, double* __restrict__ P,
-                                         unsigned* __restrict__ counters) {
+                                         unsigned* __restrict__ counters, const double2 (&pre)[8]) {
     __shared__ double in[(SCH + 1) * 3];
     __shared__ double res[TL][3];
     const int nr = it.hi - it.lo;
     const int nc = min(TL, d.k - it.b0);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const double* M0 = YW + d.y_off + it.lo + (int64_t)(it.b0 + warp) * d.ldy;
-    // the first row pair of each of the warp's columns is in flight while the
-    // input rows are gathered
-    double2 pre[8];
-#pragma unroll
-    for (int m = 0; m < 8; ++m)
-        pre[m] = (2 * lane < nr && warp + 8 * m < nc)
-                     ? __ldg(reinterpret_cast<const double2*>(M0 + (int64_t)(8 * m) * d.ldy + 2 * lane))
-                     : make_double2(0.0, 0.0);
     for (int t = threadIdx.x; t < nr + 1; t += blockDim.x) {
         const int i = it.lo + t;
         double v0 = 0.0, v1 = 0.0, v2 = 0.0;
@@ -902,7 +922,9 @@ __global__ void __launch_bounds__(256) k_bwd_level(double* __restrict__ x, const
     const SolveItem it = items[blockIdx.x];
     const FrontDesc d = desc[it.front];
     if (mesh_on && !mesh_on[d.mesh]) return;
-    bwd_item(x, Zb, YW, rows, d, it, blockIdx.x, P, counters);
+    double2 pre[8];
+    bwd_pre(YW, d, it, pre);
+    bwd_item(x, Zb, YW, rows, d, it, blockIdx.x, P, counters, pre);
 }
 
 // ---- whole-direction solve over a work queue -------------------------------------
@@ -953,6 +975,8 @@ __global__ void __launch_bounds__(32 * FWD_WARPS, 8) k_fwd_queue(const double* _
         const SolveItem it = Q.items[q];
         const FrontDesc d = desc[it.front];
         if (mesh_on && !mesh_on[d.mesh]) continue;
+        double2 pre[FWD_PRE];
+        fwd_pre(YW, d, it, pre);   // in flight during the wait
         if (threadIdx.x == 0) {
             bool ok = d.child0 < 0 || wait_bands(Q.done + d.child0, Q.nbands[d.child0], Q.status);
             ok = ok && (d.child1 < 0 || wait_bands(Q.done + d.child1, Q.nbands[d.child1], Q.status));
@@ -960,7 +984,7 @@ __global__ void __launch_bounds__(32 * FWD_WARPS, 8) k_fwd_queue(const double* _
         }
         __syncthreads();
         if (!s_ok) continue;
-        if (fwd_item(B, Zb, U, inv, YW, d, it, q, P, counters) && threadIdx.x == 0 && it.front != Q.hold)
+        if (fwd_item(B, Zb, U, inv, YW, d, it, q, P, counters, pre) && threadIdx.x == 0 && it.front != Q.hold)
             atomicAdd(Q.done + it.front, 1u);
     }
 }
@@ -978,11 +1002,13 @@ __global__ void __launch_bounds__(256) k_bwd_queue(double* __restrict__ x, const
         const SolveItem it = Q.items[q];
         const FrontDesc d = desc[it.front];
         if (mesh_on && !mesh_on[d.mesh]) continue;
+        double2 pre[8];
+        bwd_pre(YW, d, it, pre);   // in flight during the wait
         if (threadIdx.x == 0)
             s_ok = d.parent < 0 || wait_bands(Q.done + d.parent, Q.nbands[d.parent], Q.status);
         __syncthreads();
         if (!s_ok) continue;
-        if (bwd_item(x, Zb, YW, rows, d, it, q, P, counters) && threadIdx.x == 0 && it.front != Q.hold)
+        if (bwd_item(x, Zb, YW, rows, d, it, q, P, counters, pre) && threadIdx.x == 0 && it.front != Q.hold)
             atomicAdd(Q.done + it.front, 1u);
     }
 }
