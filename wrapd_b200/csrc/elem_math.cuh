@@ -301,12 +301,14 @@ __device__ __forceinline__ T cubic_step(T fx0, T gtp, T fxa, T alpha, T fxp, T a
     return (-r1 + d) / (T(3) * r0);
 }
 
+// fx0 and g: the objective and its gradient at x, which the callers already
+// hold (the reference's search evaluates them again at the same x; the values
+// are the same).
 template <typename T>
-__device__ __forceinline__ T linesearch_cubic(const Prox<T>& P, const T* x, const T* p, T alpha0,
+__device__ __forceinline__ T linesearch_cubic(const Prox<T>& P, const T* x, const T* p, T alpha0, T fx0, const T* g,
                                               int max_trials = 4096) {
     if (sqrt(dot3(p, p)) <= Lim<T>::eps()) return T(1e-4);
-    T alpha = alpha0, g[3];
-    const T fx0 = P.value_grad(x, g);
+    T alpha = alpha0;
     const T gtp = dot3(g, p);
     T fxp = fx0, alphap = alpha;
     for (int it = 0; it < max_trials; ++it) {
@@ -342,7 +344,7 @@ __device__ __forceinline__ int prox_lbfgs(const Prox<T>& P, T* x, int max_iters,
     constexpr int M = 8;
     T alpha[M], rho[M];
     T grad[3], q[3], gold[3], xold[3];
-    P.value_grad(x, grad);
+    T fx = P.value_grad(x, grad);
     T gamma_k = T(1), alpha_init = T(1);
     int global_iter = 0;
     int head = 0;   // ring position of the oldest pair once the history is full
@@ -380,7 +382,7 @@ __device__ __forceinline__ int prox_lbfgs(const Prox<T>& P, T* x, int max_iters,
             alpha_init = fmin(T(1), T(1) / ninf);
         }
         const T mq[3] = {-q[0], -q[1], -q[2]};
-        const T rate = linesearch_cubic(P, x, mq, alpha_init);
+        const T rate = linesearch_cubic(P, x, mq, alpha_init, fx, grad);
         if (rate <= T(0)) return -1;
         T xl[3];
 #pragma unroll
@@ -389,7 +391,7 @@ __device__ __forceinline__ int prox_lbfgs(const Prox<T>& P, T* x, int max_iters,
             const T dx[3] = {xl[0] - x[0], xl[1] - x[1], xl[2] - x[2]};
             if (sqrt(dot3(grad, grad)) < T(1e-8) || sqrt(dot3(dx, dx)) < T(1e-8)) break;
         }
-        P.value_grad(x, grad);
+        fx = P.value_grad(x, grad);
         T st[3], yt[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) { st[c] = x[c] - xold[c]; yt[c] = grad[c] - gold[c]; }
@@ -420,7 +422,7 @@ __device__ __forceinline__ int prox_newton(const Prox<T>& P, T* x, int max_iters
     int it = 0;
     for (; it < max_iters; ++it) {
         T g[3], h[6];
-        P.value_grad(x, g);
+        const T fx = P.value_grad(x, g);
         const T xs = fmax(T(1), fmax(fabs(x[0]), fmax(fabs(x[1]), fabs(x[2]))));
         if (sqrt(dot3(g, g)) <= tol * P.wov * xs) break;
         P.nh.hess(x, h);
@@ -458,7 +460,7 @@ __device__ __forceinline__ int prox_newton(const Prox<T>& P, T* x, int max_iters
             ++it;
             break;
         }
-        const T rate = linesearch_cubic(P, x, d, T(1), 40);
+        const T rate = linesearch_cubic(P, x, d, T(1), fx, g, 40);
         if (rate <= T(0)) break;
         const T st[3] = {rate * d[0], rate * d[1], rate * d[2]};
         x[0] += st[0]; x[1] += st[1]; x[2] += st[2];
