@@ -278,11 +278,36 @@ struct Prox {
         const T d0 = x[0] - x0[0], d1 = x[1] - x0[1], d2 = x[2] - x0[2];
         return nh.psi(x[0], x[1], x[2]) + (wov * T(0.5)) * (d0 * d0 + d1 * d1 + d2 * d2);
     }
+    // The gradient and the value together: the same operations as dpsi and
+    // value, with J and log(J) (or the extension fJ below J0) computed once
+    // for both.
     __device__ __forceinline__ T value_grad(const T* x, T* g) const {
-        nh.dpsi(x, g);
+        const T J = x[0] * x[1] * x[2];
+        const T mu = nh.mu, lambda = nh.lambda;
+        T f, lf;
+        if (J > T(NH<T>::J0)) {
+            lf = log(J);
+            f = lambda * lf - mu;
+        } else {
+            lf = nh.fJ_ext(J);
+            const T dfJdJ = T(1) / T(NH<T>::J0) - (J - T(NH<T>::J0)) / (T(NH<T>::J0) * T(NH<T>::J0));
+            f = (lambda * lf - mu) * dfJdJ * J;
+        }
 #pragma unroll
-        for (int i = 0; i < 3; ++i) g[i] = g[i] + wov * (x[i] - x0[i]);
-        return value(x);
+        for (int i = 0; i < 3; ++i) {
+            g[i] = mu * x[i] + f * (T(1) / x[i]);
+            g[i] = g[i] + wov * (x[i] - x0[i]);
+        }
+        T e;
+        if (x[0] < T(0) || x[1] < T(0) || x[2] < T(0)) {
+            e = T(1.e15);
+        } else {
+            const T I1 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+            e = T(0.5) * mu * (I1 - T(3));
+            e += -mu * lf + T(0.5) * lambda * lf * lf;
+        }
+        const T d0 = x[0] - x0[0], d1 = x[1] - x0[1], d2 = x[2] - x0[2];
+        return e + (wov * T(0.5)) * (d0 * d0 + d1 * d1 + d2 * d2);
     }
 };
 
