@@ -278,26 +278,12 @@ struct Prox {
         const T d0 = x[0] - x0[0], d1 = x[1] - x0[1], d2 = x[2] - x0[2];
         return nh.psi(x[0], x[1], x[2]) + (wov * T(0.5)) * (d0 * d0 + d1 * d1 + d2 * d2);
     }
-    // The gradient and the value together: the same operations as dpsi and
-    // value, with J and log(J) (or the extension fJ below J0) computed once
-    // for both.
-    __device__ __forceinline__ T value_grad(const T* x, T* g) const {
-        const T J = x[0] * x[1] * x[2];
+    // The value with its byproducts J = x0 x1 x2 and lf = log(J) (or the
+    // extension fJ below J0): the same operations as value().
+    __device__ __forceinline__ T value_lf(const T* x, T& J, T& lf) const {
         const T mu = nh.mu, lambda = nh.lambda;
-        T f, lf;
-        if (J > T(NH<T>::J0)) {
-            lf = log(J);
-            f = lambda * lf - mu;
-        } else {
-            lf = nh.fJ_ext(J);
-            const T dfJdJ = T(1) / T(NH<T>::J0) - (J - T(NH<T>::J0)) / (T(NH<T>::J0) * T(NH<T>::J0));
-            f = (lambda * lf - mu) * dfJdJ * J;
-        }
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            g[i] = mu * x[i] + f * (T(1) / x[i]);
-            g[i] = g[i] + wov * (x[i] - x0[i]);
-        }
+        J = x[0] * x[1] * x[2];
+        lf = J > T(NH<T>::J0) ? log(J) : nh.fJ_ext(J);
         T e;
         if (x[0] < T(0) || x[1] < T(0) || x[2] < T(0)) {
             e = T(1.e15);
@@ -308,6 +294,30 @@ struct Prox {
         }
         const T d0 = x[0] - x0[0], d1 = x[1] - x0[1], d2 = x[2] - x0[2];
         return e + (wov * T(0.5)) * (d0 * d0 + d1 * d1 + d2 * d2);
+    }
+    // The gradient (dpsi plus the penalty's) from the J and lf of value_lf at
+    // the same x.
+    __device__ __forceinline__ void grad_lf(const T* x, T J, T lf, T* g) const {
+        const T mu = nh.mu, lambda = nh.lambda;
+        T f;
+        if (J > T(NH<T>::J0)) {
+            f = lambda * lf - mu;
+        } else {
+            const T dfJdJ = T(1) / T(NH<T>::J0) - (J - T(NH<T>::J0)) / (T(NH<T>::J0) * T(NH<T>::J0));
+            f = (lambda * lf - mu) * dfJdJ * J;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            g[i] = mu * x[i] + f * (T(1) / x[i]);
+            g[i] = g[i] + wov * (x[i] - x0[i]);
+        }
+    }
+    // The gradient and the value together, log(J) taken once for both.
+    __device__ __forceinline__ T value_grad(const T* x, T* g) const {
+        T J, lf;
+        const T e = value_lf(x, J, lf);
+        grad_lf(x, J, lf, g);
+        return e;
     }
 };
 
@@ -326,20 +336,36 @@ __device__ __forceinline__ T cubic_step(T fx0, T gtp, T fxa, T alpha, T fxp, T a
     return (-r1 + d) / (T(3) * r0);
 }
 
+// The value and the log term at the accepted point of a line search (valid
+// only when the search evaluated a trial and accepted it).
+template <typename T>
+struct LsPoint {
+    T f, J, lf;
+    bool ok;
+};
+
 // fx0 and g: the objective and its gradient at x, which the callers already
 // hold (the reference's search evaluates them again at the same x; the values
-// are the same).
+// are the same).  When acc is given, the value and the log term at the
+// accepted trial point are stored there, so the caller's next gradient needs
+// no second log.
 template <typename T>
 __device__ __forceinline__ T linesearch_cubic(const Prox<T>& P, const T* x, const T* p, T alpha0, T fx0, const T* g,
-                                              int max_trials = 4096) {
+                                              int max_trials = 4096, LsPoint<T>* acc = nullptr) {
     if (sqrt(dot3(p, p)) <= Lim<T>::eps()) return T(1e-4);
     T alpha = alpha0;
     const T gtp = dot3(g, p);
     T fxp = fx0, alphap = alpha;
     for (int it = 0; it < max_trials; ++it) {
         const T xa[3] = {x[0] + alpha * p[0], x[1] + alpha * p[1], x[2] + alpha * p[2]};
-        const T fxa = P.value(xa);
-        if (fxa <= fx0 + alpha * T(1e-4) * gtp) return alpha;
+        T J, lf;
+        const T fxa = P.value_lf(xa, J, lf);
+        if (fxa <= fx0 + alpha * T(1e-4) * gtp) {
+            if (acc) {
+                acc->f = fxa; acc->J = J; acc->lf = lf; acc->ok = true;
+            }
+            return alpha;
+        }
         const T at = it == 0 ? (gtp / (T(2) * (fx0 + gtp - fxa))) : cubic_step(fx0, gtp, fxa, alpha, fxp, alphap);
         fxp = fxa;
         alphap = alpha;
@@ -407,16 +433,25 @@ __device__ __forceinline__ int prox_lbfgs(const Prox<T>& P, T* x, int max_iters,
             alpha_init = fmin(T(1), T(1) / ninf);
         }
         const T mq[3] = {-q[0], -q[1], -q[2]};
-        const T rate = linesearch_cubic(P, x, mq, alpha_init, fx, grad);
+        LsPoint<T> acc;
+        acc.ok = false;
+        const T rate = linesearch_cubic(P, x, mq, alpha_init, fx, grad, 4096, &acc);
         if (rate <= T(0)) return -1;
         T xl[3];
+        // x - rate q is the accepted trial point x + rate (-q), bit for bit
+        // (one rounding each, a fused multiply-add)
 #pragma unroll
         for (int c = 0; c < 3; ++c) { xl[c] = x[c]; x[c] -= rate * q[c]; }
         {
             const T dx[3] = {xl[0] - x[0], xl[1] - x[1], xl[2] - x[2]};
             if (sqrt(dot3(grad, grad)) < T(1e-8) || sqrt(dot3(dx, dx)) < T(1e-8)) break;
         }
-        fx = P.value_grad(x, grad);
+        if (acc.ok) {   // the search's value and log term at this x
+            fx = acc.f;
+            P.grad_lf(x, acc.J, acc.lf, grad);
+        } else {
+            fx = P.value_grad(x, grad);
+        }
         T st[3], yt[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) { st[c] = x[c] - xold[c]; yt[c] = grad[c] - gold[c]; }
