@@ -603,6 +603,15 @@ static __global__ void __launch_bounds__(256) k_lbfgs_second(Tiles T, const int*
 // c_i and decrement as the per-step launches, bit for bit, in every CTA.  The
 // barrier is a counter the CTAs raise, waited on with wait_count_geq (bounded;
 // a wait that gives up leaves WRAPD_E_TIMEOUT in *status and the CTA returns).
+// REG (when the grid has a CTA per tile at the register form's occupancy):
+// a CTA's kTwoLoopPT entries per thread stay in registers for the whole loop,
+// q is stored once at the end, and the two history vectors of the next step
+// (which do not change during the loop) are loaded before the grid barrier, so
+// no step waits on a memory round trip after its barrier.  The per-entry
+// operations and the order of every sum are those of the tile loop.
+constexpr int kTwoLoopGridThreads = 256;
+constexpr int kTwoLoopPT = kVecTile / kTwoLoopGridThreads;
+static_assert(kVecTile % kTwoLoopGridThreads == 0, "whole entries per thread");
 __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned target, int* status) {
     __shared__ int ok;
     __syncthreads();
@@ -627,8 +636,8 @@ __device__ __forceinline__ double grid_total(const double* partials, int ntiles)
     return total;
 }
 
-template <bool SECOND>
-static __global__ void __launch_bounds__(256) k_two_loop_grid(Tiles T, const MeshCtl* __restrict__ ctl, VecPools P,
+template <bool SECOND, bool REG>
+static __global__ void __launch_bounds__(kTwoLoopGridThreads) k_two_loop_grid(Tiles T, const MeshCtl* __restrict__ ctl, VecPools P,
                                                        const double* __restrict__ rho, double* __restrict__ q,
                                                        TwoLoopSlots sl, double* partials, unsigned* bar,
                                                        int* status, double* scal) {
@@ -636,7 +645,96 @@ static __global__ void __launch_bounds__(256) k_two_loop_grid(Tiles T, const Mes
     const MeshCtl c = ctl[0];
     const int ntiles = T.count, G = gridDim.x;
     unsigned nbar = 0;
-    if constexpr (!SECOND) {
+    if constexpr (REG) {
+        // one tile per CTA (the host launches REG only with ntiles <= G), kept in registers
+        const int t = blockIdx.x;
+        const Tile tl = t < ntiles ? tile_at(T, t) : Tile{0, 0, 0};
+        const int i0 = tl.first + (int)threadIdx.x;
+        double qv[kTwoLoopPT], av[kTwoLoopPT], bv[kTwoLoopPT];
+        auto load = [&](double (&v)[kTwoLoopPT], const double* src) {
+#pragma unroll
+            for (int k = 0; k < kTwoLoopPT; ++k) {
+                const int i = i0 + k * kTwoLoopGridThreads;
+                v[k] = (src && i < tl.end) ? src[i] : 0.0;
+            }
+        };
+        auto store_q = [&]() {
+#pragma unroll
+            for (int k = 0; k < kTwoLoopPT; ++k) {
+                const int i = i0 + k * kTwoLoopGridThreads;
+                if (i < tl.end) q[i] = qv[k];
+            }
+        };
+        if constexpr (!SECOND) {
+            // av: y_{j+1} (the update), bv: s_j (the inner product) of step j
+            double alpha_next = 0.0;
+            load(qv, g_cur(P, c));
+            load(bv, c.it - 1 >= 0 ? P.S[hist_slot(c, c.it - 1, P.M)] : nullptr);
+            for (int j = c.it - 1; j >= -1; --j) {
+                const bool first = j == c.it - 1;
+                const double cf = first ? 0.0 : -alpha_next;
+                double red = 0.0;
+#pragma unroll
+                for (int k = 0; k < kTwoLoopPT; ++k) {
+                    if (i0 + k * kTwoLoopGridThreads < tl.end) {
+                        double qi = qv[k];
+                        if (!first) qi = qi + cf * av[k];
+                        qv[k] = qi;
+                        if (j >= 0) red += bv[k] * qi;
+                    }
+                }
+                if (j < 0) break;
+                double* part = partials + (size_t)(j & 1) * ntiles;
+                const double r = block_sum(red, sm);
+                if (threadIdx.x == 0 && t < ntiles) part[t] = r;
+                load(av, P.Y[hist_slot(c, j, P.M)]);
+                load(bv, j - 1 >= 0 ? P.S[hist_slot(c, j - 1, P.M)] : nullptr);
+                nbar += G;
+                if (!grid_barrier(bar, nbar, status)) return;
+                alpha_next = rho[hist_slot(c, j, P.M)] * grid_total(part, ntiles);
+                if (blockIdx.x == 0 && threadIdx.x == 0) scal[sl.alpha + j] = alpha_next;
+            }
+            store_q();
+        } else {
+            // av: s_{j-1} (the update), bv: y_j or g (the inner product) of step j
+            double c_prev = 0.0;
+            load(qv, q);
+            load(bv, 0 < c.it ? P.Y[hist_slot(c, 0, P.M)] : g_cur(P, c));
+            for (int j = 0; j <= c.it; ++j) {
+                const double cf = j > 0 ? c_prev : 0.0;
+                double red = 0.0;
+#pragma unroll
+                for (int k = 0; k < kTwoLoopPT; ++k) {
+                    if (i0 + k * kTwoLoopGridThreads < tl.end) {
+                        double qi = qv[k];
+                        if (j > 0) {
+                            qi = qi + cf * av[k];
+                            qv[k] = qi;
+                        }
+                        red += bv[k] * qi;
+                    }
+                }
+                double* part = partials + (size_t)(j & 1) * ntiles;
+                const double r = block_sum(red, sm);
+                if (threadIdx.x == 0 && t < ntiles) part[t] = r;
+                if (j < c.it) {
+                    load(av, P.S[hist_slot(c, j, P.M)]);
+                    load(bv, j + 1 < c.it ? P.Y[hist_slot(c, j + 1, P.M)] : g_cur(P, c));
+                }
+                nbar += G;
+                if (!grid_barrier(bar, nbar, status)) return;
+                const double tot = grid_total(part, ntiles);
+                if (j < c.it) {
+                    c_prev = __ldcg(scal + sl.alpha + j) + (-rho[hist_slot(c, j, P.M)]) * tot;
+                    if (blockIdx.x == 0 && threadIdx.x == 0) scal[sl.c + j] = c_prev;
+                } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+                    scal[sl.dir] = tot;
+                }
+            }
+            store_q();
+        }
+        return;
+    } else if constexpr (!SECOND) {
         // first loop, j = it - 1 .. -1: q = (first ? g : q) - alpha_{j+1} y_{j+1}; alpha_j = rho_j <s_j, q>
         double alpha_next = 0.0;
         for (int j = c.it - 1; j >= -1; --j) {

@@ -431,10 +431,18 @@ void SolverGPU::initialize() {
         WRAPD_CUDA(cudaGetDevice(&dev));
         WRAPD_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
         WRAPD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        WRAPD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_two_loop_grid<false>, 256, 0));
-        int per_sm2 = 0;
-        WRAPD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_two_loop_grid<true>, 256, 0));
-        if (coop && nm == 1) coop_grid_ = std::min(tvec_.count, std::min(per_sm, per_sm2) * sms);
+        auto fits = [&](const void* f) {
+            int b = 0;
+            WRAPD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, kTwoLoopGridThreads, 0));
+            return b * sms;
+        };
+        const int cap = std::min(fits((const void*)k_two_loop_grid<false, false>),
+                                 fits((const void*)k_two_loop_grid<true, false>));
+        const int cap_reg = std::min(fits((const void*)k_two_loop_grid<false, true>),
+                                     fits((const void*)k_two_loop_grid<true, true>));
+        // the register form when every vector tile gets its own resident CTA
+        coop_reg_ = tvec_.count <= cap_reg;
+        if (coop && nm == 1) coop_grid_ = std::min(tvec_.count, coop_reg_ ? cap_reg : cap);
     }
     d_scal_ = static_cast<double*>(dalloc((size_t)nm * kScalStride * sizeof(double)));
     WRAPD_CUDA(cudaMemsetAsync(d_counters_, 0, nm * sizeof(unsigned), st_));
@@ -965,9 +973,11 @@ void SolverGPU::two_loop_grid(bool second, const VecPools& P, const TwoLoopSlots
     int* status = chol.d_status;
     double* scal = d_scal_;
     void* args[] = {&T, &ctl, &Pc, &rho, &q, &slc, &partials, &bar, &status, &scal};
-    const void* fn = second ? reinterpret_cast<const void*>(&k_two_loop_grid<true>)
-                            : reinterpret_cast<const void*>(&k_two_loop_grid<false>);
-    WRAPD_CUDA(cudaLaunchCooperativeKernel(fn, dim3(coop_grid_), dim3(256), args, 0, st_));
+    const void* fn = coop_reg_ ? (second ? reinterpret_cast<const void*>(&k_two_loop_grid<true, true>)
+                                         : reinterpret_cast<const void*>(&k_two_loop_grid<false, true>))
+                               : (second ? reinterpret_cast<const void*>(&k_two_loop_grid<true, false>)
+                                         : reinterpret_cast<const void*>(&k_two_loop_grid<false, false>));
+    WRAPD_CUDA(cudaLaunchCooperativeKernel(fn, dim3(coop_grid_), dim3(kTwoLoopGridThreads), args, 0, st_));
     kernel_launches++;
 }
 

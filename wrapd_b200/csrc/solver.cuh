@@ -169,6 +169,7 @@ private:
     int* h_status_ = nullptr;    // pinned: the device status word, read with the scalars
     unsigned* d_bar_ = nullptr;  // grid-barrier counter of the cooperative two-loop recursion
     int coop_grid_ = 0;          // its CTAs (0: not used -- a batch, or no cooperative launch)
+    bool coop_reg_ = false;      // its register form (one vector tile per CTA)
     void two_loop_grid(bool second, const VecPools& P, const TwoLoopSlots& sl);
     // ---- the meshes of the batch: each its own ADMM and L-BFGS state ----
     int nm = 0;
