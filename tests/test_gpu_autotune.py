@@ -48,5 +48,5 @@ def test_autotuned_solve_matches_reference(golden):
 def test_fixed_rules_reported_without_autotune():
     _, _, t, _ = _solve(0, iters=3)
     assert t["fused_panel_ctas"] == 592
-    assert t["local_tile"] == 128
+    assert t["local_tile"] == 256
     assert all(c in (256, 128, 64) for c in t["solve_chunk_fwd"] + t["solve_chunk_bwd"])
