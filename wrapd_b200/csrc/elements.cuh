@@ -83,13 +83,14 @@ __device__ __forceinline__ double elastic_energy(const Material& m, const double
 // SEG: a batch (per-mesh sums); a single mesh takes grid_reduce, the same
 // arithmetic.  Register budgets: the single-mesh form compiles to 128 with no
 // occupancy hint; the segmented one and the UV forms below are held to 128
-// (4 CTAs per SM) by the hint, without which they took 164-168 (3 per SM).
+// (16 warps per SM) by the hint, without which they took 164-168.  Launched
+// on 256-element tiles (two CTAs per SM).
 // UV (single mesh only): 0 = SVD as usual; 1 = also keep U and V of the SVD
 // in uv (U then V, 9 SoA components each); 2 = x is the point of the last
 // UV = 1 launch, so F's SVD is that launch's: sig, U, V and symF are read
 // back instead of recomputed (the same values, so the same results).
 template <bool SEG, int UV = 0>
-static __global__ void __launch_bounds__(128, (SEG || UV != 0) ? 4 : 0) k_grad(ElemView E, Tiles T, const int* on, const double* __restrict__ x,
+static __global__ void __launch_bounds__(256, (SEG || UV != 0) ? 2 : 0) k_grad(ElemView E, Tiles T, const int* on, const double* __restrict__ x,
                                               const double* __restrict__ xfix, Material mat0, int write_gel,
                                               double* partials, unsigned* counters, double* out, int stride,
                                               double* __restrict__ uv = nullptr) {

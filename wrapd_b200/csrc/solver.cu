@@ -587,24 +587,26 @@ const Logs& SolverGPU::mesh_logs(int m) const {
 // UV = 1); the first gradient of the next ADMM iteration is taken at the same
 // x (the local step changes only Z and U), so it reads them back (UV = 2)
 // instead of redoing the per-element SVD.  uv_valid_ is cleared wherever x
-// changes.
+// changes.  256-element tiles (786k bar: 1.095 -> 1.077 ms per global step
+// against 128; 3.9M bar: 5.09 -> 4.95 ms), in a batch too, so that a mesh's
+// sums are added in the same order as when it is solved alone.
 void SolverGPU::grad_at_x(bool write_gel, int mk) {
     if (nm > 1) {
-        WRAPD_ELEM_LAUNCH(k_grad<true>, te128_, 128, mask(mk), d_x_, d_xfix_, mat_, write_gel ? 1 : 0, d_partials_,
+        WRAPD_ELEM_LAUNCH(k_grad<true>, te256_, 256, mask(mk), d_x_, d_xfix_, mat_, write_gel ? 1 : 0, d_partials_,
                           d_counters_, ds(S_GRAD), kScalStride);
     } else if (d_uv_ && write_gel && cfg.rot_aware && !cfg.global_ls) {
         if (uv_valid_)
-            k_grad<false, 2><<<te128_.count, 128, 0, st_>>>(view(), te128_.view(), mask(mk), d_x_, d_xfix_, mat_, 1,
+            k_grad<false, 2><<<te256_.count, 256, 0, st_>>>(view(), te256_.view(), mask(mk), d_x_, d_xfix_, mat_, 1,
                                                              d_partials_, d_counters_, ds(S_GRAD), kScalStride, d_uv_);
         else
-            k_grad<false, 1><<<te128_.count, 128, 0, st_>>>(view(), te128_.view(), mask(mk), d_x_, d_xfix_, mat_, 1,
+            k_grad<false, 1><<<te256_.count, 256, 0, st_>>>(view(), te256_.view(), mask(mk), d_x_, d_xfix_, mat_, 1,
                                                              d_partials_, d_counters_, ds(S_GRAD), kScalStride, d_uv_);
         WRAPD_LAUNCH_CHECK();
         kernel_launches++;
         uv_valid_ = true;
         return;
     } else {
-        WRAPD_ELEM_LAUNCH(k_grad<false>, te128_, 128, mask(mk), d_x_, d_xfix_, mat_, write_gel ? 1 : 0, d_partials_,
+        WRAPD_ELEM_LAUNCH(k_grad<false>, te256_, 256, mask(mk), d_x_, d_xfix_, mat_, write_gel ? 1 : 0, d_partials_,
                           d_counters_, ds(S_GRAD), kScalStride);
     }
     uv_valid_ = false;
@@ -948,7 +950,7 @@ double SolverGPU::line_search() {
         k_ls_trial<<<vb, 256, 0, st_>>>(n, trial, d_x_, step, alpha);
         WRAPD_LAUNCH_CHECK();
         kernel_launches++;
-        WRAPD_ELEM_LAUNCH(k_grad<false>, te128_, 128, mask(MK_ALL), trial, d_xfix_, mat_, 0, d_partials_,
+        WRAPD_ELEM_LAUNCH(k_grad<false>, te256_, 256, mask(MK_ALL), trial, d_xfix_, mat_, 0, d_partials_,
                           d_counters_, ds(S_LSV), kScalStride);   // one mesh (line search: single meshes only)
         sync_read();
         const double fxa = hs(0, S_LSV);
