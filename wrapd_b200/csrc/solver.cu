@@ -4,6 +4,7 @@
 #include "elements.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -243,16 +244,26 @@ void SolverGPU::initialize() {
         tl = now;
     };
     // ---- element geometry (TetElements ctor, src/TetElements.cpp:90-142) ----
+    // (on host threads over element ranges; the first inverted element is reported)
     std::vector<double> Di(12 * (size_t)ne), vol(ne), w2(ne);
-    for (int e = 0; e < ne; ++e) {
-        const int* t = &tets_[4 * (size_t)e];
-        double d[12], v;
-        element_geometry(&rest_[3 * (size_t)t[0]], &rest_[3 * (size_t)t[1]], &rest_[3 * (size_t)t[2]],
-                         &rest_[3 * (size_t)t[3]], d, &v);
-        if (v < 0.0) throw CudaError(WRAPD_E_INVERTED_REST, "inverted tet " + std::to_string(e) + " in the rest mesh");
-        for (int k = 0; k < 12; ++k) Di[(size_t)k * ne + e] = d[k];
-        vol[e] = v;
-    }
+    std::atomic<int> first_inverted{ne};
+    host_parallel(ne, 16384, [&](int lo, int hi) {
+        for (int e = lo; e < hi; ++e) {
+            const int* t = &tets_[4 * (size_t)e];
+            double d[12], v;
+            element_geometry(&rest_[3 * (size_t)t[0]], &rest_[3 * (size_t)t[1]], &rest_[3 * (size_t)t[2]],
+                             &rest_[3 * (size_t)t[3]], d, &v);
+            if (v < 0.0) {
+                int cur = first_inverted.load();
+                while (e < cur && !first_inverted.compare_exchange_weak(cur, e)) {}
+                return;
+            }
+            for (int k = 0; k < 12; ++k) Di[(size_t)k * ne + e] = d[k];
+            vol[e] = v;
+        }
+    });
+    if (first_inverted.load() < ne)
+        throw CudaError(WRAPD_E_INVERTED_REST, "inverted tet " + std::to_string(first_inverted.load()) + " in the rest mesh");
     std::vector<int> mid(ne);
     for (const MeshIn& M : meshes_)
         for (int e = M.e_off; e < M.e_off + M.ne; ++e) {

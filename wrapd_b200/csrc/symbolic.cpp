@@ -464,6 +464,10 @@ void assembly_map(const Symbolic& S, const std::vector<int>& vinc_ptr, const std
     });
 }
 
+void host_parallel(int n, int64_t grain, const std::function<void(int, int)>& fn) {
+    parallel_ranges(n, host_threads(n, grain), [&](int, int lo, int hi) { fn(lo, hi); });
+}
+
 Symbolic merge(const std::vector<Symbolic>& parts) {
     if (parts.size() == 1) return parts[0];
     Symbolic S;

@@ -13,6 +13,7 @@
 //     more than its highest child's, so each level can run as one launch).
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <vector>
 
 namespace wrapd {
@@ -82,5 +83,10 @@ void assembly_map(const Symbolic& S, const std::vector<int>& vinc_ptr, const std
 // per mesh of a batch), block p taking the columns after blocks 0..p-1: the
 // forest of their trees, level l holding every block's level-l fronts.
 Symbolic merge(const std::vector<Symbolic>& parts);
+
+// fn(lo, hi) over contiguous ranges of [0, n) on host threads (one per `grain`
+// items, at most 16 or WRAPD_HOST_THREADS); exceptions are rethrown after the
+// join.
+void host_parallel(int n, int64_t grain, const std::function<void(int, int)>& fn);
 
 }  // namespace wrapd
