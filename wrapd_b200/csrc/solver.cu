@@ -61,37 +61,63 @@ int blocks_for(int64_t n, int threads) { return std::max(1, ceil_div(n, threads)
 // Vector kernels use a fixed grid of 2 CTAs per SM (grid-stride loops).
 int vec_blocks(int64_t n) { return std::max(1, std::min(2 * kNumSMs, ceil_div(n, 256))); }
 
-// (S * Dm^-1)^T and the rest volume of one tet, src/TetElements.cpp:93-118.
-void element_geometry(const double* p0, const double* p1, const double* p2, const double* p3, double* Di,
-                      double* vol) {
+__global__ void k_fill(double* __restrict__ p, int64_t n, double v) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// (S * Dm^-1)^T and the rest volume of every tet (src/TetElements.cpp:93-118),
+// and its weight w^2 = beta_static k vol.  Every operation is an explicitly
+// rounded IEEE add, multiply or divide in the order a plain C++ evaluation of
+// the same expressions takes (left to right, no fused multiply-add), so the
+// values are those of that host computation bit for bit.  An inverted tet
+// (negative volume) lowers *first_inverted to its index.
+__global__ void k_element_geometry(int ne, const int* __restrict__ tets, const double* __restrict__ rest,
+                                   const int* __restrict__ mid, const Material* __restrict__ mats, double wr0,
+                                   double beta, double* __restrict__ Di, double* __restrict__ vol,
+                                   double* __restrict__ w2, int* first_inverted) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    const double* p0 = rest + 3 * (size_t)tets[4 * (size_t)e];
+    const double* p1 = rest + 3 * (size_t)tets[4 * (size_t)e + 1];
+    const double* p2 = rest + 3 * (size_t)tets[4 * (size_t)e + 2];
+    const double* p3 = rest + 3 * (size_t)tets[4 * (size_t)e + 3];
     double ed[9];
+#pragma unroll
     for (int r = 0; r < 3; ++r) {
-        ed[r + 0] = p1[r] - p0[r];
-        ed[r + 3] = p2[r] - p0[r];
-        ed[r + 6] = p3[r] - p0[r];
+        ed[r + 0] = __dsub_rn(p1[r], p0[r]);
+        ed[r + 3] = __dsub_rn(p2[r], p0[r]);
+        ed[r + 6] = __dsub_rn(p3[r], p0[r]);
     }
     auto m = [&](int r, int c) { return ed[r + 3 * c]; };
-    const double c00 = m(1, 1) * m(2, 2) - m(1, 2) * m(2, 1);
-    const double c01 = m(1, 2) * m(2, 0) - m(1, 0) * m(2, 2);
-    const double c02 = m(1, 0) * m(2, 1) - m(1, 1) * m(2, 0);
-    const double det = m(0, 0) * c00 + m(0, 1) * c01 + m(0, 2) * c02;
-    const double id = 1.0 / det;
+    auto dd = [](double a, double b, double c, double d) { return __dsub_rn(__dmul_rn(a, b), __dmul_rn(c, d)); };
+    const double c00 = dd(m(1, 1), m(2, 2), m(1, 2), m(2, 1));
+    const double c01 = dd(m(1, 2), m(2, 0), m(1, 0), m(2, 2));
+    const double c02 = dd(m(1, 0), m(2, 1), m(1, 1), m(2, 0));
+    const double det = __dadd_rn(__dadd_rn(__dmul_rn(m(0, 0), c00), __dmul_rn(m(0, 1), c01)), __dmul_rn(m(0, 2), c02));
+    const double id = __ddiv_rn(1.0, det);
     double inv[9];
-    inv[0 + 3 * 0] = c00 * id;
-    inv[1 + 3 * 0] = c01 * id;
-    inv[2 + 3 * 0] = c02 * id;
-    inv[0 + 3 * 1] = (m(0, 2) * m(2, 1) - m(0, 1) * m(2, 2)) * id;
-    inv[1 + 3 * 1] = (m(0, 0) * m(2, 2) - m(0, 2) * m(2, 0)) * id;
-    inv[2 + 3 * 1] = (m(0, 1) * m(2, 0) - m(0, 0) * m(2, 1)) * id;
-    inv[0 + 3 * 2] = (m(0, 1) * m(1, 2) - m(0, 2) * m(1, 1)) * id;
-    inv[1 + 3 * 2] = (m(0, 2) * m(1, 0) - m(0, 0) * m(1, 2)) * id;
-    inv[2 + 3 * 2] = (m(0, 0) * m(1, 1) - m(0, 1) * m(1, 0)) * id;
+    inv[0 + 3 * 0] = __dmul_rn(c00, id);
+    inv[1 + 3 * 0] = __dmul_rn(c01, id);
+    inv[2 + 3 * 0] = __dmul_rn(c02, id);
+    inv[0 + 3 * 1] = __dmul_rn(dd(m(0, 2), m(2, 1), m(0, 1), m(2, 2)), id);
+    inv[1 + 3 * 1] = __dmul_rn(dd(m(0, 0), m(2, 2), m(0, 2), m(2, 0)), id);
+    inv[2 + 3 * 1] = __dmul_rn(dd(m(0, 1), m(2, 0), m(0, 0), m(2, 1)), id);
+    inv[0 + 3 * 2] = __dmul_rn(dd(m(0, 1), m(1, 2), m(0, 2), m(1, 1)), id);
+    inv[1 + 3 * 2] = __dmul_rn(dd(m(0, 2), m(1, 0), m(0, 0), m(1, 2)), id);
+    inv[2 + 3 * 2] = __dmul_rn(dd(m(0, 0), m(1, 1), m(0, 1), m(1, 0)), id);
+    const double v = __ddiv_rn(det, 6.0);
+    if (v < 0.0) atomicMin(first_inverted, e);
     // Di(r, a): a = 0 -> minus the column sums of Dm^-1 rows; a >= 1 -> row a-1 of Dm^-1
+#pragma unroll
     for (int r = 0; r < 3; ++r) {
-        Di[r + 0] = -inv[0 + 3 * r] - inv[1 + 3 * r] - inv[2 + 3 * r];
-        for (int a = 1; a < 4; ++a) Di[r + 3 * a] = inv[(a - 1) + 3 * r];
+        Di[(size_t)r * ne + e] = __dsub_rn(__dsub_rn(-inv[0 + 3 * r], inv[1 + 3 * r]), inv[2 + 3 * r]);
+#pragma unroll
+        for (int a = 1; a < 4; ++a) Di[(size_t)(r + 3 * a) * ne + e] = inv[(a - 1) + 3 * r];
     }
-    *vol = det / 6.0;
+    vol[e] = v;
+    const double wr = mid ? mats[mid[e]].wr : wr0;
+    w2[e] = __dmul_rn(__dmul_rn(beta, wr), v);
 }
 
 }  // namespace
@@ -243,33 +269,53 @@ void SolverGPU::initialize() {
         laps.emplace_back(name, std::chrono::duration<double, std::milli>(now - tl).count());
         tl = now;
     };
-    // ---- element geometry (TetElements ctor, src/TetElements.cpp:90-142) ----
-    // (on host threads over element ranges; the first inverted element is reported)
-    std::vector<double> Di(12 * (size_t)ne), vol(ne), w2(ne);
-    std::atomic<int> first_inverted{ne};
-    host_parallel(ne, 16384, [&](int lo, int hi) {
-        for (int e = lo; e < hi; ++e) {
-            const int* t = &tets_[4 * (size_t)e];
-            double d[12], v;
-            element_geometry(&rest_[3 * (size_t)t[0]], &rest_[3 * (size_t)t[1]], &rest_[3 * (size_t)t[2]],
-                             &rest_[3 * (size_t)t[3]], d, &v);
-            if (v < 0.0) {
-                int cur = first_inverted.load();
-                while (e < cur && !first_inverted.compare_exchange_weak(cur, e)) {}
-                return;
-            }
-            for (int k = 0; k < 12; ++k) Di[(size_t)k * ne + e] = d[k];
-            vol[e] = v;
-        }
-    });
-    if (first_inverted.load() < ne)
-        throw CudaError(WRAPD_E_INVERTED_REST, "inverted tet " + std::to_string(first_inverted.load()) + " in the rest mesh");
+    // ---- element geometry (TetElements ctor, src/TetElements.cpp:90-142): on
+    // the device (k_element_geometry) from the rest positions and the tets,
+    // while the host builds the graph and the dissection below ----
     std::vector<int> mid(ne);
     for (const MeshIn& M : meshes_)
-        for (int e = M.e_off; e < M.e_off + M.ne; ++e) {
-            mid[e] = M.mat;
-            w2[e] = cfg.beta_static * mats_[M.mat].wr * vol[e];
-        }
+        for (int e = M.e_off; e < M.e_off + M.ne; ++e) mid[e] = M.mat;
+    if (mats_.size() > 1) {
+        d_mid_ = dupload(mid);
+        d_mats_ = dupload(mats_);
+    } else {
+        mat_ = mats_[0];   // one material: the mesh's own when it was given one
+    }
+    d_Di_ = static_cast<double*>(dalloc(12 * (size_t)ne * sizeof(double)));
+    d_vol_ = static_cast<double*>(dalloc((size_t)ne * sizeof(double)));
+    d_w2_ = static_cast<double*>(dalloc((size_t)ne * sizeof(double)));
+    const size_t geo_tets = 4 * (size_t)ne * sizeof(int), geo_rest = 3 * (size_t)nv * sizeof(double);
+    const size_t geo_rest_off = (geo_tets + 15) / 16 * 16, geo_flag_off = (geo_rest_off + geo_rest + 15) / 16 * 16;
+    struct GeoBuf {   // freed on every path out of initialize
+        char* p = nullptr;
+        ~GeoBuf() { if (p) cudaFree(p); }
+    } geo;
+    char*& d_geo = geo.p;
+    if (cudaMalloc(&d_geo, geo_flag_off + 16) != cudaSuccess) {
+        cudaGetLastError();
+        throw CudaError(WRAPD_E_OOM, "cudaMalloc of the rest mesh failed");
+    }
+    int* d_first_inverted = reinterpret_cast<int*>(d_geo + geo_flag_off);
+    {
+        const int none = ne;
+        WRAPD_CUDA(cudaMemcpyAsync(d_geo, tets_.data(), geo_tets, cudaMemcpyHostToDevice, st_));
+        WRAPD_CUDA(cudaMemcpyAsync(d_geo + geo_rest_off, rest_.data(), geo_rest, cudaMemcpyHostToDevice, st_));
+        WRAPD_CUDA(cudaMemcpyAsync(d_first_inverted, &none, sizeof(int), cudaMemcpyHostToDevice, st_));
+        k_element_geometry<<<blocks_for(ne, 256), 256, 0, st_>>>(
+            ne, reinterpret_cast<const int*>(d_geo), reinterpret_cast<const double*>(d_geo + geo_rest_off),
+            mats_.size() > 1 ? d_mid_ : nullptr, d_mats_, mats_[0].wr, cfg.beta_static, d_Di_, d_vol_, d_w2_,
+            d_first_inverted);
+        WRAPD_LAUNCH_CHECK();
+    }
+    // the inverted-tet check: read back before the device state is filled in
+    auto check_geometry = [&]() {
+        int first = ne;
+        WRAPD_CUDA(cudaMemcpyAsync(&first, d_first_inverted, sizeof(int), cudaMemcpyDeviceToHost, st_));
+        WRAPD_CUDA(cudaStreamSynchronize(st_));
+        cudaFree(d_geo);
+        d_geo = nullptr;
+        if (first < ne) throw CudaError(WRAPD_E_INVERTED_REST, "inverted tet " + std::to_string(first) + " in the rest mesh");
+    };
     lap("element geometry");
     // ---- free-vertex graph, nested dissection, symbolic factorization ----
     // element incidences per free vertex (free numbering), in element order
@@ -344,18 +390,10 @@ void SolverGPU::initialize() {
         }
     }
     lap("gather incidences");
+    check_geometry();
     // ---- device state ----
     const size_t TS = sizeof(double);
     d_idx_ = dupload(idx);
-    d_Di_ = dupload(Di);
-    d_vol_ = dupload(vol);
-    d_w2_ = dupload(w2);
-    if (mats_.size() > 1) {
-        d_mid_ = dupload(mid);
-        d_mats_ = dupload(mats_);
-    } else {
-        mat_ = mats_[0];   // one material: the mesh's own when it was given one
-    }
     d_w2c_ = static_cast<double*>(dalloc(ne * sizeof(double)));
     // U and V of the last gradient's SVD (single mesh): 18 doubles per element
     d_uv_ = meshes_.size() == 1 ? static_cast<double*>(dalloc((size_t)18 * ne * sizeof(double))) : nullptr;
@@ -368,12 +406,9 @@ void SolverGPU::initialize() {
     d_gel_ = static_cast<double*>(dalloc(12 * (size_t)ne * TS));
     WRAPD_CUDA(cudaMemsetAsync(d_U_, 0, 9 * (size_t)ne * TS, st_));
     WRAPD_CUDA(cudaMemsetAsync(d_Z_, 0, 9 * (size_t)ne * TS, st_));
-    {
-        // m_last_sigma = (1, 1, 1)
-        std::vector<double> ones(3 * (size_t)ne, 1.0);
-        WRAPD_CUDA(cudaMemcpyAsync(d_slast_, ones.data(), ones.size() * 8, cudaMemcpyHostToDevice, st_));
-        WRAPD_CUDA(cudaStreamSynchronize(st_));
-    }
+    // m_last_sigma = (1, 1, 1)
+    k_fill<<<blocks_for(3 * (int64_t)ne, 256), 256, 0, st_>>>(d_slast_, 3 * (int64_t)ne, 1.0);
+    WRAPD_LAUNCH_CHECK();
     d_inc_ptr_ = dupload(inc_ptr);
     d_inc_ = dupload(inc);
     std::vector<double> xp(3 * (size_t)nf), xs(3 * (size_t)nf), xfix(3 * (size_t)std::max(np, 1));
@@ -438,7 +473,7 @@ void SolverGPU::initialize() {
     d_bar_ = static_cast<unsigned*>(dalloc(sizeof(unsigned)));
     coop_grid_ = 0;
     {
-        int dev = 0, coop = 0, sms = 0, per_sm = 0;
+        int dev = 0, coop = 0, sms = 0;
         WRAPD_CUDA(cudaGetDevice(&dev));
         WRAPD_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
         WRAPD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
