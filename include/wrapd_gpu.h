@@ -82,7 +82,7 @@ typedef struct wrapd_settings {
     int autotune;         /* 0; 1: wrapd_initialize times the candidate tile shapes of the triangular
                              solve (chunk length per level and direction) and of the factorization's
                              panel steps (fused or split, by the number of tiles), and the first
-                             wrapd_begin_solve the local step's tile (64, 128 or 256 elements per
+                             wrapd_begin_solve the local step's tile (64, 128, 256 or 512 elements per
                              CTA), on this system, and keeps the fastest (see wrapd_get_tuning) */
 } wrapd_settings;
 

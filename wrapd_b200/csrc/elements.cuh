@@ -283,7 +283,7 @@ static __global__ void __launch_bounds__(256) k_gather(Tiles T, const int* on, i
 // prox network's prediction.  The FP32 instantiation always uses Newton.
 // NET needs dynamic shared memory: the network image plus one scratch per warp.
 template <typename C, bool NET>
-__global__ void __launch_bounds__(256, 2) k_local(ElemView E, Tiles T, const int* on, Material mat0, int prox_iters,
+__global__ void __launch_bounds__(512, 1) k_local(ElemView E, Tiles T, const int* on, Material mat0, int prox_iters,
                                                int cand_mode, int prox_mode, const unsigned char* __restrict__ net_img,
                                                double* partials, unsigned* counters, double* out, int stride) {
     const Tile tl = tile_at(T, blockIdx.x);

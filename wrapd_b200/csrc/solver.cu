@@ -49,7 +49,7 @@ enum : int {
 // Dynamic shared memory of k_local<double>: the prox L-BFGS history, 48 doubles
 // per thread (kLocalHistBytes for a 128-thread block, the unaware step's).
 constexpr int kLocalHistBytes = 48 * 128 * (int)sizeof(double);
-constexpr int kLocalTileMax = 256;   // largest local-step tile (elements = threads per CTA)
+constexpr int kLocalTileMax = 512;   // largest local-step tile (elements = threads per CTA)
 int local_hist_bytes(int per) { return 48 * per * (int)sizeof(double); }
 int local_net_bytes(int per) { return net::IMAGE_BYTES + (per / 32) * net::WARP_SCRATCH; }
 // Mixed mode switches its local step to FP64 when the normalized energy
@@ -142,6 +142,10 @@ SolverGPU::SolverGPU(const wrapd_settings& s) : cfg(s) {
         for (auto& e : set) WRAPD_CUDA(cudaEventCreate(&e));
     WRAPD_CUDA(cudaFuncSetAttribute(k_local<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     local_hist_bytes(kLocalTileMax)));
+    WRAPD_CUDA(cudaFuncSetAttribute(k_local<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    local_net_bytes(kLocalTileMax)));
+    WRAPD_CUDA(cudaFuncSetAttribute(k_local<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    local_net_bytes(kLocalTileMax)));
     WRAPD_CUDA(cudaFuncSetAttribute(k_local_unaware<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     kLocalHistBytes));
     mat_ = material(cfg.youngs, cfg.poisson);
@@ -878,7 +882,7 @@ void SolverGPU::autotune_local() {
     copy_state(true);
     float best = 1e30f;
     int pick = local_per_;
-    for (int per : {128, 64, 256}) {
+    for (int per : {128, 64, 256, 512}) {
         build_tiles(te_local_, per, er);
         for (int rep = 0; rep < 2; ++rep) {   // the first run warms up
             copy_state(false);

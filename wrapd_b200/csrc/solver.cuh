@@ -187,9 +187,10 @@ private:
     std::vector<MeshRun> runs_;
     TileSet te128_, te256_, tv32_, tvec_;
     TileSet te_local_;                     // the local step's element tiles (local_per_ elements each)
-    // 256 elements (eight warps, two CTAs per SM): on the 786k bar the FP64
-    // local step takes 0.58 ms at 256, 0.71 at 128, 0.96 at 64, 1.67 at 32
-    int local_per_ = 256;
+    // 512 elements (16 warps, one CTA per SM): the FP64 local step takes 0.577
+    // ms on the 786k bar (0.587 at 256, 0.71 at 128, 0.96 at 64, 1.67 at 32)
+    // and 2.60 ms on the 3.9M bar (2.79 at 256, 3.65 at 128)
+    int local_per_ = 512;
     bool local_tuned_ = false;
     void autotune_local();
     // control block on the device and its pinned mirror: masks (kMasks x nm
